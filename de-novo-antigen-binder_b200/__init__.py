@@ -1,0 +1,476 @@
+"""binder_b200 — B200 (sm_100a) all-atom scoring + search for de novo antibody design.
+
+Python host-side mirror of the reference engine's GPU interface (Rust crate
+DilaDeniz/de-novo-antigen-binder): ``GpuContext.try_init`` / ``score_batch``
+(gpu.rs:55,166), ``AtomCloud`` (allatom.rs:17), ``ResidueCloud`` (atom.rs:185),
+``SpatialHashGrid`` (spatial.rs:12) and ``compute_forces_with_grid``
+(energy.rs:322).  Every call goes through the C ABI of ``libbinder_b200.so``
+(include/binder_gpu.h); there is no CPU fallback — importing the package
+without the built library, or creating a context without an sm_100 device,
+fails loudly.
+
+The package directory name contains dashes, so it is imported under the name
+``binder_b200`` by :func:`load` in the repository's entry points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libbinder_b200.so"
+SLOTS = 14
+N_AA = 20
+
+AMINO_ACIDS = ["Ala", "Arg", "Asn", "Asp", "Cys", "Gln", "Glu", "Gly", "His", "Ile",
+               "Leu", "Lys", "Met", "Phe", "Pro", "Ser", "Thr", "Trp", "Tyr", "Val"]
+ONE_LETTER = "ARNDCQEGHILKMFPSTWYV"
+
+# GpuAtom (gpu.rs:17-29): 8 x f32
+GPU_ATOM = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("q", "<f4"), ("r_min_half", "<f4"),
+                     ("epsilon", "<f4"), ("hydrophobic", "<f4"), ("_pad", "<f4")])
+
+STATUS = {0: "BINDER_OK", 1: "BINDER_ERR_ARG", 2: "BINDER_ERR_CUDA", 3: "BINDER_ERR_OOM", 4: "BINDER_ERR_TIMEOUT",
+          5: "BINDER_ERR_NAN", 6: "BINDER_ERR_GRID", 7: "BINDER_ERR_STATE", 8: "BINDER_ERR_NODEVICE",
+          9: "BINDER_ERR_CAPACITY"}
+ACC_KAHAN, ACC_F32 = 0, 1
+
+
+class BinderError(RuntimeError):
+    def __init__(self, status, message=""):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{self.name}: {message}" if message else self.name)
+
+
+class _AtomCloudC(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("charge", C.c_void_p),
+                ("r_min_half", C.c_void_p), ("epsilon", C.c_void_p), ("hydrophobic", C.c_void_p),
+                ("atom_type", C.c_void_p), ("residue_idx", C.c_void_p), ("n", C.c_size_t)]
+
+
+class _ResidueCloudC(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("amino_acid", C.c_void_p),
+                ("n", C.c_size_t)]
+
+
+class Params(C.Structure):
+    """binder_params (include/binder_gpu.h); defaults = reference constants."""
+    _fields_ = [("step", C.c_float), ("noise_base", C.c_float), ("t_hot", C.c_float), ("t_cold", C.c_float),
+                ("mutation_p", C.c_float), ("rotamer_move_p", C.c_float), ("backbone_move_p", C.c_float),
+                ("max_torsion_deg", C.c_float), ("iface_cutoff_sq", C.c_float), ("shell_radius", C.c_float),
+                ("max_disp", C.c_float), ("restraint_k", C.c_float), ("ca_cell", C.c_float),
+                ("score_cell", C.c_float), ("accumulate", C.c_int32), ("_reserved", C.c_int32),
+                ("seed", C.c_uint64)]
+
+    @classmethod
+    def defaults(cls, **kw):
+        p = cls()
+        lib().binder_default_params(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+
+_LIB = None
+
+_SIGS = {
+    "binder_abi_version": (C.c_int, []),
+    "binder_status_string": (C.c_char_p, [C.c_int]),
+    "binder_default_params": (None, [C.c_void_p]),
+    "binder_create": (C.c_void_p, [C.c_int, C.c_void_p, C.POINTER(C.c_int)]),
+    "binder_destroy": (None, [C.c_void_p]),
+    "binder_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_last_error": (C.c_char_p, [C.c_void_p]),
+    "binder_synchronize": (C.c_int, [C.c_void_p]),
+    "binder_launch_count": (C.c_uint64, [C.c_void_p]),
+    "binder_table_residue": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_table_atom_type": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_table_rotamers": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "binder_table_residue_level": (C.c_int, [C.c_int, C.c_void_p]),
+    "binder_score_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p,
+                                     C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_score_batch_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p,
+                                         C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_score_batch_ragged": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.c_void_p]),
+    "binder_set_antigen_atoms": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_last_pair_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "binder_grid_cells": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                    C.c_void_p]),
+    "binder_grid_neighbors": (C.c_int, [C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                        C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_compute_forces_with_grid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p]),
+    "binder_forces_allatom": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                        C.c_void_p]),
+    "binder_topk": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]),
+    "binder_topk_segmented": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p]),
+    "binder_build_residues": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "binder_add_antigen": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "binder_clear_antigens": (C.c_int, [C.c_void_p]),
+    "binder_state_upload": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_state_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_diffuse": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_void_p]),
+    "binder_score_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "binder_block": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
+}
+
+
+def lib():
+    """Load libbinder_b200.so and declare every entry point of include/binder_gpu.h."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = Path(os.environ.get("BINDER_B200_LIB", LIB_PATH))
+    if not path.exists():
+        raise ImportError(f"{path} is not built; run `python de-novo-antigen-binder_b200/build.py` "
+                          "(or __graft_entry__.build())")
+    L = C.CDLL(str(path))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _u8(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+# ---- tables ---------------------------------------------------------------------
+class Tables:
+    """The force-field tables compiled into the library (amber.rs / rotamer.rs / atom.rs)."""
+
+    def __init__(self):
+        L = lib()
+        self.n_atoms = np.zeros(N_AA, np.int32)
+        self.charge = np.zeros((N_AA, SLOTS), np.float32)
+        self.atom_type = np.zeros((N_AA, SLOTS), np.uint8)
+        self.hydrophobic = np.zeros((N_AA, SLOTS), np.uint8)
+        for a in range(N_AA):
+            n = C.c_int()
+            L.binder_table_residue(a, C.byref(n), _ptr(self.charge[a]), _ptr(self.atom_type[a]),
+                                   _ptr(self.hydrophobic[a]))
+            self.n_atoms[a] = n.value
+        self.r_min_half = np.zeros(16, np.float32)
+        self.epsilon = np.zeros(16, np.float32)
+        self.hbond = np.zeros(16, np.int32)
+        self.eef1 = np.zeros((16, 3), np.float32)
+        for t in range(16):
+            r, e, h = C.c_float(), C.c_float(), C.c_int()
+            L.binder_table_atom_type(t, C.byref(r), C.byref(e), C.byref(h), _ptr(self.eef1[t]))
+            self.r_min_half[t], self.epsilon[t], self.hbond[t] = r.value, e.value, h.value
+        self.n_rot = np.zeros(N_AA, np.int32)
+        self.rot_chi = np.zeros((N_AA, 5, 4), np.float32)
+        self.residue_level = np.zeros((N_AA, 4), np.float32)
+        for a in range(N_AA):
+            n = C.c_int()
+            L.binder_table_rotamers(a, C.byref(n), _ptr(self.rot_chi[a]))
+            self.n_rot[a] = n.value
+            L.binder_table_residue_level(a, _ptr(self.residue_level[a]))
+
+
+_TABLES = None
+
+
+def tables() -> Tables:
+    global _TABLES
+    if _TABLES is None:
+        _TABLES = Tables()
+    return _TABLES
+
+
+# ---- clouds -----------------------------------------------------------------------
+class AtomCloud:
+    """allatom.rs:17-31 AtomCloud: flat all-atom structure of arrays."""
+
+    def __init__(self, x, y, z, charge, r_min_half, epsilon, hydrophobic, atom_type=None, residue_idx=None):
+        self.x, self.y, self.z = _f32(x), _f32(y), _f32(z)
+        self.charge, self.r_min_half, self.epsilon = _f32(charge), _f32(r_min_half), _f32(epsilon)
+        self.hydrophobic = _u8(hydrophobic)
+        self.atom_type = None if atom_type is None else _u8(atom_type)
+        self.residue_idx = None if residue_idx is None else np.ascontiguousarray(residue_idx, np.uint32)
+
+    def __len__(self):
+        return len(self.x)
+
+    @classmethod
+    def from_slots(cls, aa, pos):
+        """Flatten a slot-layout protein in push_residue order (allatom.rs:201-240)."""
+        T = tables()
+        aa = np.asarray(aa, np.uint8)
+        pos = np.asarray(pos, np.float32).reshape(len(aa), SLOTS, 3)
+        res_idx = np.repeat(np.arange(len(aa), dtype=np.uint32), T.n_atoms[aa])
+        k = np.concatenate([np.arange(T.n_atoms[a]) for a in aa]) if len(aa) else np.zeros(0, int)
+        xyz = pos[res_idx, k]
+        types = T.atom_type[aa[res_idx], k]
+        return cls(xyz[:, 0], xyz[:, 1], xyz[:, 2], T.charge[aa[res_idx], k], T.r_min_half[types],
+                   T.epsilon[types], T.hydrophobic[aa[res_idx], k], types, res_idx)
+
+    def to_gpu_atoms(self):
+        """GpuAtom flattening of run_allatom (diffusion.rs:1029-1040)."""
+        g = np.zeros(len(self), GPU_ATOM)
+        g["x"], g["y"], g["z"] = self.x, self.y, self.z
+        g["q"], g["r_min_half"], g["epsilon"] = self.charge, self.r_min_half, self.epsilon
+        g["hydrophobic"] = self.hydrophobic.astype(np.float32)
+        return g
+
+    def _c(self):
+        s = _AtomCloudC(_ptr(self.x), _ptr(self.y), _ptr(self.z), _ptr(self.charge), _ptr(self.r_min_half),
+                        _ptr(self.epsilon), _ptr(self.hydrophobic), _ptr(self.atom_type), _ptr(self.residue_idx),
+                        len(self.x))
+        return s
+
+
+class ResidueCloud:
+    """atom.rs:185-195 ResidueCloud: Calpha positions + amino acid."""
+
+    def __init__(self, x, y, z, amino_acid):
+        self.x, self.y, self.z = _f32(x), _f32(y), _f32(z)
+        self.amino_acid = _u8(amino_acid)
+
+    def __len__(self):
+        return len(self.x)
+
+    def _c(self):
+        return _ResidueCloudC(_ptr(self.x), _ptr(self.y), _ptr(self.z), _ptr(self.amino_acid), len(self.x))
+
+
+# ---- context ----------------------------------------------------------------------
+class GpuContext:
+    """gpu.rs:46-268 GpuContext on a B200: one device, one stream."""
+
+    def __init__(self, handle, params):
+        self._h = handle
+        self.params = params
+
+    @classmethod
+    def try_init(cls, device=0, params=None):
+        """gpu.rs:55 try_init: None when no sm_100 device is usable."""
+        try:
+            return cls.create(device, params)
+        except BinderError:
+            return None
+
+    @classmethod
+    def create(cls, device=0, params=None):
+        L = lib()
+        params = params or Params.defaults()
+        st = C.c_int(0)
+        h = L.binder_create(device, C.byref(params), C.byref(st))
+        if not h:
+            raise BinderError(st.value, "binder_create failed")
+        return cls(h, params)
+
+    def close(self):
+        if self._h:
+            lib().binder_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, status):
+        if status != 0:
+            msg = lib().binder_last_error(self._h)
+            raise BinderError(status, msg.decode() if msg else "")
+
+    def set_params(self, params):
+        self._check(lib().binder_set_params(self._h, C.byref(params)))
+        self.params = params
+
+    @property
+    def launch_count(self):
+        return int(lib().binder_launch_count(self._h))
+
+    def synchronize(self):
+        self._check(lib().binder_synchronize(self._h))
+
+    # -- score_batch (gpu.rs:166-267) --
+    def score_batch(self, antigen: AtomCloud, candidates, n_ab: int):
+        cand = np.ascontiguousarray(candidates, GPU_ATOM)
+        n_cand = len(cand) // n_ab if n_ab else 0
+        out = np.zeros(n_cand, np.float32)
+        got = C.c_size_t()
+        ag = antigen._c()
+        self._check(lib().binder_score_batch(self._h, C.byref(ag), _ptr(cand), len(cand), n_ab, _ptr(out), n_cand,
+                                             C.byref(got)))
+        return out
+
+    def score_batch_f64(self, antigen: AtomCloud, candidates, n_ab: int, with_abs=False):
+        cand = np.ascontiguousarray(candidates, GPU_ATOM)
+        n_cand = len(cand) // n_ab if n_ab else 0
+        out = np.zeros(n_cand, np.float64)
+        ab = np.zeros(n_cand, np.float64) if with_abs else None
+        got = C.c_size_t()
+        ag = antigen._c()
+        self._check(lib().binder_score_batch_f64(self._h, C.byref(ag), _ptr(cand), len(cand), n_ab, _ptr(out),
+                                                 _ptr(ab), n_cand, C.byref(got)))
+        return (out, ab) if with_abs else out
+
+    def score_batch_ragged(self, antigen: AtomCloud, candidates, offsets, with_abs=False):
+        cand = np.ascontiguousarray(candidates, GPU_ATOM)
+        off = np.ascontiguousarray(offsets, np.int64)
+        n_cand = len(off) - 1
+        out = np.zeros(n_cand, np.float64)
+        ab = np.zeros(n_cand, np.float64) if with_abs else None
+        ag = antigen._c()
+        self._check(lib().binder_score_batch_ragged(self._h, C.byref(ag), _ptr(cand), _ptr(off), n_cand, _ptr(out),
+                                                    _ptr(ab)))
+        return (out, ab) if with_abs else out
+
+    def last_pair_count(self):
+        n = C.c_int64()
+        self._check(lib().binder_last_pair_count(self._h, C.byref(n)))
+        return n.value
+
+    # -- SpatialHashGrid (spatial.rs) --
+    def grid_cells(self, cell, x, y, z):
+        x, y, z = _f32(x), _f32(y), _f32(z)
+        out = np.zeros((len(x), 3), np.int32)
+        self._check(lib().binder_grid_cells(self._h, cell, _ptr(x), _ptr(y), _ptr(z), len(x), _ptr(out)))
+        return out
+
+    def grid_neighbors(self, cell, ax, ay, az, px, py, pz):
+        """build + query_neighbors for each probe: (offsets int64[n_q+1], indices uint32)."""
+        ax, ay, az, px, py, pz = (_f32(v) for v in (ax, ay, az, px, py, pz))
+        off = np.zeros(len(px) + 1, np.int64)
+        total = C.c_size_t(0)
+        cap = max(1, len(px) * 32)
+        idx = np.zeros(cap, np.uint32)
+        st = lib().binder_grid_neighbors(self._h, cell, _ptr(ax), _ptr(ay), _ptr(az), len(ax), _ptr(px), _ptr(py),
+                                         _ptr(pz), len(px), _ptr(off), _ptr(idx), cap, C.byref(total))
+        if st == 9:
+            cap = max(1, total.value)
+            idx = np.zeros(cap, np.uint32)
+            st = lib().binder_grid_neighbors(self._h, cell, _ptr(ax), _ptr(ay), _ptr(az), len(ax), _ptr(px),
+                                             _ptr(py), _ptr(pz), len(px), _ptr(off), _ptr(idx), cap, C.byref(total))
+        self._check(st)
+        return off, idx[:total.value]
+
+    # -- forces --
+    def compute_forces_with_grid(self, antigen: ResidueCloud, cell: float, antibody: ResidueCloud):
+        """energy.rs:322-398 on the GPU; returns (fx, fy, fz)."""
+        n = len(antibody)
+        fx, fy, fz = np.zeros(n, np.float32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+        ag, ab = antigen._c(), antibody._c()
+        self._check(lib().binder_compute_forces_with_grid(self._h, C.byref(ag), cell, C.byref(ab), _ptr(fx),
+                                                          _ptr(fy), _ptr(fz)))
+        return fx, fy, fz
+
+    def forces_allatom(self, antigen: AtomCloud, candidates, offsets):
+        cand = np.ascontiguousarray(candidates, GPU_ATOM)
+        off = np.ascontiguousarray(offsets, np.int64)
+        n_cand = len(off) - 1
+        f = np.zeros((len(cand), 3), np.float32)
+        e = np.zeros(n_cand, np.float64)
+        ag = antigen._c()
+        self._check(lib().binder_forces_allatom(self._h, C.byref(ag), _ptr(cand), _ptr(off), n_cand, _ptr(f),
+                                                _ptr(e)))
+        return f, e
+
+    # -- survivor selection --
+    def topk(self, energies, k):
+        e = np.ascontiguousarray(energies, np.float64)
+        out = np.zeros(k, np.int32)
+        self._check(lib().binder_topk(self._h, _ptr(e), len(e), k, _ptr(out)))
+        return out
+
+    def topk_segmented(self, energies, seg_offsets, k):
+        e = np.ascontiguousarray(energies, np.float64)
+        so = np.ascontiguousarray(seg_offsets, np.int64)
+        out = np.zeros((len(so) - 1) * k, np.int32)
+        self._check(lib().binder_topk_segmented(self._h, _ptr(e), _ptr(so), len(so) - 1, k, _ptr(out)))
+        return out.reshape(len(so) - 1, k)
+
+    # -- residue construction --
+    def build_residues(self, ca_xyz, aa, chi=None):
+        """protein_from_ca_trace (allatom.rs:523-541): (pos [n,14,3], chi [n,4])."""
+        ca = _f32(ca_xyz).reshape(-1, 3)
+        aa = _u8(aa)
+        n = len(aa)
+        pos = np.zeros((n, SLOTS, 3), np.float32)
+        chi_out = np.zeros((n, 4), np.float32)
+        chi_in = None if chi is None else _f32(chi).reshape(n, 4)
+        self._check(lib().binder_build_residues(self._h, n, _ptr(ca), _ptr(aa), _ptr(chi_in), _ptr(pos),
+                                                _ptr(chi_out)))
+        return pos, chi_out
+
+    # -- resident search state --
+    def add_antigen(self, aa, pos):
+        aa = _u8(aa)
+        pos = _f32(pos)
+        out = C.c_int32()
+        self._check(lib().binder_add_antigen(self._h, len(aa), _ptr(aa), _ptr(pos), C.byref(out)))
+        return out.value
+
+    def clear_antigens(self):
+        self._check(lib().binder_clear_antigens(self._h))
+
+    def state_upload(self, aa, chi, pos, n_res=None, uniform_n_res=0, antigen_id=None, cand_id=None):
+        aa, chi, pos = _u8(aa), _f32(chi), _f32(pos)
+        nr = None if n_res is None else np.ascontiguousarray(n_res, np.int32)
+        n_cand = len(nr) if nr is not None else len(aa) // max(1, uniform_n_res)
+        agi = None if antigen_id is None else np.ascontiguousarray(antigen_id, np.int32)
+        cid = None if cand_id is None else np.ascontiguousarray(cand_id, np.uint32)
+        self._check(lib().binder_state_upload(self._h, n_cand, _ptr(nr), uniform_n_res, _ptr(agi), _ptr(cid),
+                                              _ptr(aa), _ptr(chi), _ptr(pos)))
+        self._state_res = len(aa)
+        self._state_cand = n_cand
+
+    def state_download(self):
+        n = self._state_res
+        aa = np.zeros(n, np.uint8)
+        chi = np.zeros((n, 4), np.float32)
+        pos = np.zeros((n, SLOTS, 3), np.float32)
+        self._check(lib().binder_state_download(self._h, _ptr(aa), _ptr(chi), _ptr(pos)))
+        return aa, chi, pos
+
+    def diffuse(self, n_steps, step0=0, with_noise=False, with_mc=False, temps=None):
+        t = None if temps is None else _f32(temps)
+        self._check(lib().binder_diffuse(self._h, n_steps, step0, int(with_noise), int(with_mc), _ptr(t)))
+
+    def score_state(self, full=False):
+        out = np.zeros(self._state_cand, np.float64)
+        self._check(lib().binder_score_state(self._h, int(full), _ptr(out)))
+        return out
+
+    def block(self, n_steps, step0=0, k=64, n_segments=1):
+        e = np.zeros(self._state_cand, np.float64)
+        top = np.zeros(n_segments * k, np.int32) if k else None
+        self._check(lib().binder_block(self._h, n_steps, step0, k, _ptr(e), _ptr(top)))
+        return e, (top.reshape(n_segments, k) if k else None)
+
+
+def temperature(iteration, total, t_hot=3.0, t_cold=0.02):
+    """diffusion.rs:102-104 in f32: T_HOT * (T_COLD/T_HOT)^(iter/total)."""
+    t_hot, t_cold = np.float32(t_hot), np.float32(t_cold)
+    return np.float32(t_hot * np.power(np.float32(t_cold / t_hot), np.float32(iteration) / np.float32(total)))
+
+
+from . import workloads  # noqa: E402,F401  (seeded synthetic inputs)

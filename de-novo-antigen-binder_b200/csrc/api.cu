@@ -1,0 +1,1077 @@
+// api.cu — the extern "C" boundary (include/binder_gpu.h): context, device
+// buffers, antigen residency, resident search state and every entry point.
+//
+// Host code here only validates, lays data out, moves it and launches kernels;
+// every computation of the hot path runs in the k_*.cu kernels.  Nothing throws
+// across the ABI: each entry point returns a binder_status and records a message
+// for binder_last_error().
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "binder_gpu.h"
+#include "kernels.h"
+
+using namespace binder;
+
+namespace {
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(size_t m) {
+        if (m <= n && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
+        if (e == cudaSuccess) n = std::max<size_t>(m, 1);
+        else p = nullptr;
+        return e;
+    }
+};
+
+template <class T>
+struct HBuf {  // pinned host staging
+    T* p = nullptr;
+    size_t n = 0;
+    HBuf() = default;
+    HBuf(const HBuf&) = delete;
+    ~HBuf() { if (p) cudaFreeHost(p); }
+    cudaError_t ensure(size_t m) {
+        if (m <= n && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMallocHost(&p, std::max<size_t>(m, 1) * sizeof(T));
+        if (e == cudaSuccess) n = std::max<size_t>(m, 1);
+        return e;
+    }
+};
+
+struct GridBuf {
+    DBuf<int4> cells;
+    DBuf<int> counts, cell_start, cursor, sorted_idx;
+    DBuf<int> minmax;
+    GridView view{};
+};
+
+// One resident antigen: all-atom records + score grid, Calpha cloud + CG grid.
+struct Antigen {
+    int n_atoms = 0, n_res = 0;
+    DBuf<float> x, y, z, q, rmh, eps;
+    DBuf<uint8_t> hyd, type;
+    GridBuf grid;
+    DBuf<float4> pq, prm;
+    DBuf<float> cax, cay, caz;
+    DBuf<uint8_t> caa;
+    GridBuf ca_grid;
+    DBuf<float4> ca_pq, ca_prm, ca_atom, ca_atom_prm;
+    AgView view{};
+};
+
+struct State {
+    int n_cand = 0, total_res = 0, n_ag_groups = 0;
+    DBuf<int> cand_res_off, cand_ag, res_cand, ag_cand_idx;
+    DBuf<long long> ag_cand_off;
+    DBuf<uint32_t> cand_id;
+    DBuf<uint8_t> res_aa;
+    DBuf<float4> res_chi, res_pos;
+    DBuf<float> stage;  // packed slot staging for upload/download
+    std::vector<int> h_res_off;
+    int n_segments = 0;
+    StateView view() {
+        StateView v;
+        v.n_cand = n_cand;
+        v.total_res = total_res;
+        v.cand_res_off = cand_res_off.p;
+        v.cand_ag = cand_ag.p;
+        v.cand_id = cand_id.p;
+        v.res_aa = res_aa.p;
+        v.res_chi = res_chi.p;
+        v.res_pos = res_pos.p;
+        v.res_cand = res_cand.p;
+        return v;
+    }
+};
+
+const float RADS_PER_DEG = 3.14159265358979323846f / 180.0f;
+const size_t MAX_GRID_CELLS = (size_t)1 << 24;
+
+}  // namespace
+
+struct binder_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    binder_params params{};
+    std::string err;
+    uint64_t launches = 0;
+    int num_sms = 148;
+    // drop-in antigen (score_batch path) and its host copy for change detection
+    Antigen dropin;
+    DBuf<AgView> d_dropin_view;
+    bool dropin_valid = false;
+    std::vector<float> dropin_key;
+    // resident search antigens
+    std::vector<std::unique_ptr<Antigen>> ags;
+    DBuf<AgView> d_views;
+    DBuf<float4> d_res_tab;
+    // scratch
+    DBuf<float> cand;
+    DBuf<long long> off;
+    DBuf<double> energy, energy_abs;
+    DBuf<float> force;
+    DBuf<long long> pairs;
+    DBuf<uint32_t> errf;
+    DBuf<int> topk;
+    DBuf<float> temps;
+    DBuf<float> tmp_f;
+    DBuf<uint8_t> tmp_u8;
+    DBuf<float4> tmp_f4a, tmp_f4b;
+    DBuf<long long> tmp_ll;
+    DBuf<uint32_t> tmp_u32;
+    HBuf<double> h_energy;
+    HBuf<uint32_t> h_err;
+    size_t last_n_cand = 0;
+    bool last_batch_valid = false;
+    State st;
+};
+
+namespace {
+
+int fail(binder_ctx* ctx, int status, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return status;
+}
+
+int cuda_fail(binder_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return fail(ctx, BINDER_ERR_OOM, "%s: out of device memory", what);
+    }
+    return fail(ctx, BINDER_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                      \
+    do {                                                    \
+        cudaError_t e__ = (call);                           \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, what); \
+    } while (0)
+
+#define LAUNCHED(what)                                      \
+    do {                                                    \
+        ctx->launches++;                                    \
+        cudaError_t e__ = cudaGetLastError();               \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, what); \
+    } while (0)
+
+int enter(binder_ctx* ctx) {
+    if (!ctx) return BINDER_ERR_ARG;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    ctx->err.clear();
+    return BINDER_OK;
+}
+
+// Reset the device error word before a group of launches.
+int clear_err(binder_ctx* ctx) {
+    CK(ctx->errf.ensure(1), "alloc err");
+    CK(cudaMemsetAsync(ctx->errf.p, 0, sizeof(uint32_t), ctx->stream), "memset err");
+    return BINDER_OK;
+}
+
+// Copy the device error word back (synchronises the stream) and map it to a status.
+int check_err(binder_ctx* ctx) {
+    CK(ctx->h_err.ensure(1), "alloc host err");
+    CK(cudaMemcpyAsync(ctx->h_err.p, ctx->errf.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "err D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    uint32_t f = ctx->h_err.p[0];
+    if (f & ERRF_NAN) return fail(ctx, BINDER_ERR_NAN, "non-finite coordinate in input");
+    if (f & ERRF_TIMEOUT) return fail(ctx, BINDER_ERR_TIMEOUT, "device wait timed out");
+    if (f & ERRF_RANGE) return fail(ctx, BINDER_ERR_ARG, "device index out of range");
+    return BINDER_OK;
+}
+
+template <class T>
+int upload(binder_ctx* ctx, DBuf<T>& d, const T* h, size_t n, const char* what) {
+    CK(d.ensure(n), what);
+    if (n) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream), what);
+    return BINDER_OK;
+}
+
+// Counting-sort grid over n points (device x/y/z).  spatial.rs:23-39 semantics.
+int build_grid(binder_ctx* ctx, const float* x, const float* y, const float* z, int n, float cell, GridBuf& G) {
+    if (!(cell > 0.0f) || !std::isfinite(cell)) return fail(ctx, BINDER_ERR_ARG, "grid cell must be positive");
+    const float inv = 1.0f / cell;
+    G.view.inv = inv;
+    G.view.cell = cell;
+    int h_mm[6] = {INT32_MAX, INT32_MAX, INT32_MAX, INT32_MIN, INT32_MIN, INT32_MIN};
+    CK(G.minmax.ensure(6), "grid alloc");
+    CK(G.cells.ensure(n), "grid alloc");
+    CK(cudaMemcpyAsync(G.minmax.p, h_mm, sizeof(h_mm), cudaMemcpyHostToDevice, ctx->stream), "grid H2D");
+    int st = clear_err(ctx);
+    if (st) return st;
+    launch_cell_coords(ctx->stream, x, y, z, n, inv, G.cells.p, G.minmax.p, ctx->errf.p);
+    if (n > 0) LAUNCHED("cell_coords");
+    CK(cudaMemcpyAsync(h_mm, G.minmax.p, sizeof(h_mm), cudaMemcpyDeviceToHost, ctx->stream), "grid D2H");
+    st = check_err(ctx);
+    if (st) return st;
+    if (n == 0) {
+        for (int k = 0; k < 3; ++k) h_mm[k] = 0, h_mm[k + 3] = 0;
+    }
+    const long long nx = (long long)h_mm[3] - h_mm[0] + 1, ny = (long long)h_mm[4] - h_mm[1] + 1,
+                    nz = (long long)h_mm[5] - h_mm[2] + 1;
+    if (nx <= 0 || ny <= 0 || nz <= 0 || (double)nx * ny * nz > (double)MAX_GRID_CELLS)
+        return fail(ctx, BINDER_ERR_GRID, "grid box %lldx%lldx%lld exceeds %zu cells (cell %.3g)", nx, ny, nz,
+                    MAX_GRID_CELLS, (double)cell);
+    const int ncell = (int)(nx * ny * nz);
+    G.view.ox = h_mm[0]; G.view.oy = h_mm[1]; G.view.oz = h_mm[2];
+    G.view.nx = (int)nx; G.view.ny = (int)ny; G.view.nz = (int)nz;
+    CK(G.counts.ensure(ncell), "grid alloc");
+    CK(G.cell_start.ensure(ncell + 1), "grid alloc");
+    CK(G.cursor.ensure(ncell + 1), "grid alloc");
+    CK(G.sorted_idx.ensure(n), "grid alloc");
+    CK(cudaMemsetAsync(G.counts.p, 0, ncell * sizeof(int), ctx->stream), "grid memset");
+    launch_cell_hist(ctx->stream, G.cells.p, n, G.view.ox, G.view.oy, G.view.oz, G.view.ny, G.view.nz, G.counts.p);
+    if (n > 0) LAUNCHED("cell_hist");
+    launch_exclusive_scan(ctx->stream, G.counts.p, ncell, G.cell_start.p);
+    LAUNCHED("exclusive_scan");
+    CK(cudaMemcpyAsync(G.cursor.p, G.cell_start.p, (ncell + 1) * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream),
+       "grid D2D");
+    launch_stable_scatter(ctx->stream, G.cells.p, n, G.cursor.p, G.sorted_idx.p);
+    LAUNCHED("stable_scatter");
+    G.view.cell_start = G.cell_start.p;
+    return BINDER_OK;
+}
+
+// All-atom records + score grid of an antigen given as a host AtomCloud.
+int build_antigen_atoms(binder_ctx* ctx, Antigen& A, const float* x, const float* y, const float* z, const float* q,
+                        const float* rmh, const float* eps, const uint8_t* hyd, const uint8_t* type, size_t n) {
+    if (n > (size_t)INT32_MAX / 2) return fail(ctx, BINDER_ERR_ARG, "antigen too large");
+    int s;
+    if ((s = upload(ctx, A.x, x, n, "antigen x")) || (s = upload(ctx, A.y, y, n, "antigen y")) ||
+        (s = upload(ctx, A.z, z, n, "antigen z")) || (s = upload(ctx, A.q, q, n, "antigen q")) ||
+        (s = upload(ctx, A.rmh, rmh, n, "antigen rmh")) || (s = upload(ctx, A.eps, eps, n, "antigen eps")) ||
+        (s = upload(ctx, A.hyd, hyd, n, "antigen hyd")))
+        return s;
+    if (type) {
+        if ((s = upload(ctx, A.type, type, n, "antigen type"))) return s;
+    }
+    A.n_atoms = (int)n;
+    if ((s = build_grid(ctx, A.x.p, A.y.p, A.z.p, (int)n, ctx->params.score_cell, A.grid))) return s;
+    CK(A.pq.ensure(n), "antigen alloc");
+    CK(A.prm.ensure(n), "antigen alloc");
+    launch_gather_atoms(ctx->stream, A.grid.sorted_idx.p, (int)n, A.x.p, A.y.p, A.z.p, A.q.p, A.rmh.p, A.eps.p,
+                        A.hyd.p, type ? A.type.p : nullptr, A.pq.p, A.prm.p);
+    if (n > 0) LAUNCHED("gather_atoms");
+    A.view.pq = A.pq.p;
+    A.view.prm = A.prm.p;
+    A.view.grid = A.grid.view;
+    A.view.n_atoms = (int)n;
+    return BINDER_OK;
+}
+
+// Residue-level Calpha cloud + CG grid (run_allatom ag_ca, diffusion.rs:994-1004).
+int build_antigen_ca(binder_ctx* ctx, Antigen& A, const float* x, const float* y, const float* z, const uint8_t* aa,
+                     size_t n, float cell) {
+    int s;
+    if ((s = upload(ctx, A.cax, x, n, "ca x")) || (s = upload(ctx, A.cay, y, n, "ca y")) ||
+        (s = upload(ctx, A.caz, z, n, "ca z")) || (s = upload(ctx, A.caa, aa, n, "ca aa")))
+        return s;
+    A.n_res = (int)n;
+    if ((s = build_grid(ctx, A.cax.p, A.cay.p, A.caz.p, (int)n, cell, A.ca_grid))) return s;
+    CK(A.ca_pq.ensure(n), "ca alloc");
+    CK(A.ca_prm.ensure(n), "ca alloc");
+    launch_gather_ca(ctx->stream, A.ca_grid.sorted_idx.p, (int)n, A.cax.p, A.cay.p, A.caz.p, A.caa.p,
+                     ctx->d_res_tab.p, A.ca_pq.p, A.ca_prm.p);
+    if (n > 0) LAUNCHED("gather_ca");
+    A.view.ca_pq = A.ca_pq.p;
+    A.view.ca_prm = A.ca_prm.p;
+    A.view.ca_grid = A.ca_grid.view;
+    A.view.n_res = (int)n;
+    return BINDER_OK;
+}
+
+int validate_cloud(binder_ctx* ctx, const binder_atom_cloud* c, const char* what) {
+    if (!c) return fail(ctx, BINDER_ERR_ARG, "%s: NULL cloud", what);
+    if (c->n && (!c->x || !c->y || !c->z || !c->charge || !c->r_min_half || !c->epsilon || !c->hydrophobic))
+        return fail(ctx, BINDER_ERR_ARG, "%s: NULL array", what);
+    return BINDER_OK;
+}
+
+// Upload the drop-in antigen when its contents differ from the resident copy.
+int ensure_dropin(binder_ctx* ctx, const binder_atom_cloud* ag) {
+    int s = validate_cloud(ctx, ag, "antigen");
+    if (s) return s;
+    const size_t n = ag->n;
+    std::vector<float> key;
+    key.reserve(n * 7 + 2);
+    key.push_back((float)n);
+    key.push_back(ag->atom_type ? 1.0f : 0.0f);
+    for (size_t i = 0; i < n; ++i) {
+        key.push_back(ag->x[i]); key.push_back(ag->y[i]); key.push_back(ag->z[i]);
+        key.push_back(ag->charge[i]); key.push_back(ag->r_min_half[i]); key.push_back(ag->epsilon[i]);
+        key.push_back((float)ag->hydrophobic[i] + (ag->atom_type ? 256.0f * ag->atom_type[i] : 0.0f));
+    }
+    if (ctx->dropin_valid && key.size() == ctx->dropin_key.size() &&
+        std::memcmp(key.data(), ctx->dropin_key.data(), key.size() * sizeof(float)) == 0)
+        return BINDER_OK;
+    ctx->dropin_valid = false;
+    if ((s = build_antigen_atoms(ctx, ctx->dropin, ag->x, ag->y, ag->z, ag->charge, ag->r_min_half, ag->epsilon,
+                                 ag->hydrophobic, ag->atom_type, n)))
+        return s;
+    CK(ctx->d_dropin_view.ensure(1), "view alloc");
+    CK(cudaMemcpyAsync(ctx->d_dropin_view.p, &ctx->dropin.view, sizeof(AgView), cudaMemcpyHostToDevice, ctx->stream),
+       "view H2D");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    ctx->dropin_key.swap(key);
+    ctx->dropin_valid = true;
+    return BINDER_OK;
+}
+
+int grid_ctas(binder_ctx* ctx, int n_cand) { return std::min(n_cand, ctx->num_sms * 8); }
+
+// Score n_cand ragged candidates already in ctx->cand / ctx->off against the drop-in antigen.
+int score_resident_batch(binder_ctx* ctx, int n_cand, bool want_abs) {
+    int s;
+    CK(ctx->energy.ensure(n_cand), "alloc energy");
+    if (want_abs) CK(ctx->energy_abs.ensure(n_cand), "alloc energy");
+    if ((s = clear_err(ctx))) return s;
+    ScoreOut o{ctx->energy.p, want_abs ? ctx->energy_abs.p : nullptr, nullptr, nullptr, ctx->errf.p};
+    launch_score_flat(ctx->stream, ctx->cand.p, ctx->off.p, n_cand, ctx->d_dropin_view.p, nullptr,
+                      ctx->params.accumulate, o, grid_ctas(ctx, n_cand), 256);
+    LAUNCHED("score_flat");
+    ctx->last_n_cand = (size_t)n_cand;
+    ctx->last_batch_valid = true;
+    return BINDER_OK;
+}
+
+int fetch_energies(binder_ctx* ctx, int n, double* out, double* out_abs, float* out32) {
+    CK(ctx->h_energy.ensure(2 * (size_t)n), "alloc host");
+    CK(cudaMemcpyAsync(ctx->h_energy.p, ctx->energy.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+       "energy D2H");
+    if (out_abs)
+        CK(cudaMemcpyAsync(ctx->h_energy.p + n, ctx->energy_abs.p, n * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "energy D2H");
+    int s = check_err(ctx);
+    if (s) return s;
+    if (out) std::memcpy(out, ctx->h_energy.p, n * sizeof(double));
+    if (out_abs) std::memcpy(out_abs, ctx->h_energy.p + n, n * sizeof(double));
+    if (out32)
+        for (int i = 0; i < n; ++i) out32[i] = (float)ctx->h_energy.p[i];
+    return BINDER_OK;
+}
+
+int score_batch_common(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                       size_t n_atoms, size_t n_ab, double* out64, double* out_abs, float* out32, size_t out_cap,
+                       size_t* out_n_cand) {
+    int s = enter(ctx);
+    if (s) return s;
+    const size_t n_cand = n_ab == 0 ? 0 : n_atoms / n_ab;
+    if (out_n_cand) *out_n_cand = n_cand;
+    if (n_cand == 0) return BINDER_OK;
+    if (!candidates) return fail(ctx, BINDER_ERR_ARG, "candidates is NULL");
+    if (out_cap < n_cand) return fail(ctx, BINDER_ERR_CAPACITY, "out_cap %zu < n_cand %zu", out_cap, n_cand);
+    if (n_cand > (size_t)INT32_MAX) return fail(ctx, BINDER_ERR_ARG, "too many candidates");
+    if ((s = ensure_dropin(ctx, antigen))) return s;
+    const size_t used = n_cand * n_ab;
+    CK(ctx->cand.ensure(used * 8), "alloc candidates");
+    CK(cudaMemcpyAsync(ctx->cand.p, candidates, used * sizeof(binder_gpu_atom), cudaMemcpyHostToDevice, ctx->stream),
+       "candidates H2D");
+    CK(ctx->off.ensure(n_cand + 1), "alloc offsets");
+    launch_uniform_offsets(ctx->stream, ctx->off.p, (int)n_cand, (long long)n_ab);
+    LAUNCHED("uniform_offsets");
+    if ((s = score_resident_batch(ctx, (int)n_cand, out_abs != nullptr))) return s;
+    return fetch_energies(ctx, (int)n_cand, out64, out_abs, out32);
+}
+
+void refresh_views(binder_ctx* ctx, std::vector<AgView>& v) {
+    v.clear();
+    for (auto& a : ctx->ags) v.push_back(a->view);
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int binder_abi_version(void) { return BINDER_ABI_VERSION; }
+
+int binder_table_residue(int aa, int* n_atoms, float* charge, uint8_t* atom_type, uint8_t* hydrophobic) {
+    if (aa < 0 || aa >= N_AA) return BINDER_ERR_ARG;
+    if (n_atoms) *n_atoms = BT_TOPO_N[aa];
+    for (int k = 0; k < SLOTS; ++k) {
+        if (charge) charge[k] = BT_SLOT_Q[aa][k];
+        if (atom_type) atom_type[k] = BT_SLOT_TYPE[aa][k];
+        if (hydrophobic) hydrophobic[k] = BT_SLOT_HYD[aa][k];
+    }
+    return BINDER_OK;
+}
+
+int binder_table_atom_type(int t, float* rmh, float* eps, int* hb, float* eef1) {
+    if (t < 0 || t >= 16) return BINDER_ERR_ARG;
+    if (rmh) *rmh = BT_NB[t][0];
+    if (eps) *eps = BT_NB[t][1];
+    if (hb) *hb = BT_HB[t];
+    if (eef1)
+        for (int k = 0; k < 3; ++k) eef1[k] = BT_EEF1[t][k];
+    return BINDER_OK;
+}
+
+int binder_table_rotamers(int aa, int* n, float* chi) {
+    if (aa < 0 || aa >= N_AA) return BINDER_ERR_ARG;
+    if (n) *n = BT_ROT_N[aa];
+    if (chi)
+        for (int r = 0; r < 5; ++r)
+            for (int c = 0; c < 4; ++c) chi[r * 4 + c] = BT_ROT_CHI[aa][r][c];
+    return BINDER_OK;
+}
+
+int binder_table_residue_level(int aa, float* out4) {
+    if (aa < 0 || aa >= N_AA || !out4) return BINDER_ERR_ARG;
+    for (int k = 0; k < 4; ++k) out4[k] = BT_RES[aa][k];
+    return BINDER_OK;
+}
+
+const char* binder_status_string(int s) {
+    switch (s) {
+        case BINDER_OK: return "ok";
+        case BINDER_ERR_ARG: return "invalid argument";
+        case BINDER_ERR_CUDA: return "CUDA error";
+        case BINDER_ERR_OOM: return "out of memory";
+        case BINDER_ERR_TIMEOUT: return "device wait timed out";
+        case BINDER_ERR_NAN: return "non-finite input";
+        case BINDER_ERR_GRID: return "grid too large";
+        case BINDER_ERR_STATE: return "call out of order";
+        case BINDER_ERR_NODEVICE: return "no usable sm_100 device";
+        case BINDER_ERR_CAPACITY: return "output buffer too small";
+        default: return "unknown status";
+    }
+}
+
+void binder_default_params(binder_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->step = 0.08f;
+    p->noise_base = 0.25f;
+    p->t_hot = 3.0f;
+    p->t_cold = 0.02f;
+    p->mutation_p = 0.08f;
+    p->rotamer_move_p = 0.12f;
+    p->backbone_move_p = 0.04f;
+    p->max_torsion_deg = 15.0f;
+    p->iface_cutoff_sq = 64.0f;
+    p->shell_radius = 20.0f;
+    p->max_disp = 2.0f;
+    p->restraint_k = 0.02f;
+    p->ca_cell = 10.0f;
+    p->score_cell = 8.0f;
+    p->accumulate = BINDER_ACC_KAHAN;
+    p->seed = 0;
+}
+
+binder_ctx* binder_create(int device, const binder_params* params, int* status) {
+    int dummy;
+    if (!status) status = &dummy;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        *status = BINDER_ERR_NODEVICE;
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        *status = BINDER_ERR_NODEVICE;
+        return nullptr;
+    }
+    binder_ctx* ctx = new (std::nothrow) binder_ctx();
+    if (!ctx) {
+        *status = BINDER_ERR_OOM;
+        return nullptr;
+    }
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    if (params) ctx->params = *params;
+    else binder_default_params(&ctx->params);
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        score_init_tables() != cudaSuccess || search_init_tables() != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        *status = BINDER_ERR_CUDA;
+        return nullptr;
+    }
+    float4 tab[N_AA];
+    for (int a = 0; a < N_AA; ++a) tab[a] = make_float4(BT_RES[a][0], BT_RES[a][1], BT_RES[a][2], BT_RES[a][3]);
+    if (ctx->d_res_tab.ensure(N_AA) != cudaSuccess ||
+        cudaMemcpy(ctx->d_res_tab.p, tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        *status = BINDER_ERR_CUDA;
+        return nullptr;
+    }
+    *status = BINDER_OK;
+    return ctx;
+}
+
+void binder_destroy(binder_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    delete ctx;
+    if (s) cudaStreamDestroy(s);
+}
+
+int binder_set_params(binder_ctx* ctx, const binder_params* p) {
+    if (!ctx || !p) return BINDER_ERR_ARG;
+    if (!(p->score_cell > 0.f) || !(p->ca_cell > 0.f)) return fail(ctx, BINDER_ERR_ARG, "cell sizes must be positive");
+    if (p->score_cell != ctx->params.score_cell) ctx->dropin_valid = false;
+    ctx->params = *p;
+    return BINDER_OK;
+}
+
+const char* binder_last_error(const binder_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int binder_synchronize(binder_ctx* ctx) {
+    int s = enter(ctx);
+    if (s) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+uint64_t binder_launch_count(const binder_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int binder_score_batch(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                       size_t n_atoms, size_t n_ab, float* out, size_t out_cap, size_t* out_n_cand) {
+    if (!out && n_ab && n_atoms / n_ab) return fail(ctx, BINDER_ERR_ARG, "out_energies is NULL");
+    return score_batch_common(ctx, antigen, candidates, n_atoms, n_ab, nullptr, nullptr, out, out_cap, out_n_cand);
+}
+
+int binder_score_batch_f64(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                           size_t n_atoms, size_t n_ab, double* out, double* out_abs, size_t out_cap,
+                           size_t* out_n_cand) {
+    if (!out && n_ab && n_atoms / n_ab) return fail(ctx, BINDER_ERR_ARG, "out_energies is NULL");
+    return score_batch_common(ctx, antigen, candidates, n_atoms, n_ab, out, out_abs, nullptr, out_cap, out_n_cand);
+}
+
+int binder_score_batch_ragged(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                              const int64_t* offsets, size_t n_cand, double* out, double* out_abs) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_cand == 0) return BINDER_OK;
+    if (!offsets || !out) return fail(ctx, BINDER_ERR_ARG, "NULL offsets/out");
+    if (n_cand > (size_t)INT32_MAX) return fail(ctx, BINDER_ERR_ARG, "too many candidates");
+    if (offsets[0] != 0) return fail(ctx, BINDER_ERR_ARG, "offsets[0] must be 0");
+    for (size_t c = 0; c < n_cand; ++c)
+        if (offsets[c + 1] < offsets[c]) return fail(ctx, BINDER_ERR_ARG, "offsets must be non-decreasing");
+    const size_t n_atoms = (size_t)offsets[n_cand];
+    if (n_atoms && !candidates) return fail(ctx, BINDER_ERR_ARG, "candidates is NULL");
+    if ((s = ensure_dropin(ctx, antigen))) return s;
+    CK(ctx->cand.ensure(n_atoms * 8), "alloc candidates");
+    if (n_atoms)
+        CK(cudaMemcpyAsync(ctx->cand.p, candidates, n_atoms * sizeof(binder_gpu_atom), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "candidates H2D");
+    if ((s = upload(ctx, ctx->off, (const long long*)offsets, n_cand + 1, "offsets H2D"))) return s;
+    if ((s = score_resident_batch(ctx, (int)n_cand, out_abs != nullptr))) return s;
+    return fetch_energies(ctx, (int)n_cand, out, out_abs, nullptr);
+}
+
+int binder_set_antigen_atoms(binder_ctx* ctx, const binder_atom_cloud* antigen) {
+    int s = enter(ctx);
+    if (s) return s;
+    return ensure_dropin(ctx, antigen);
+}
+
+int binder_last_pair_count(binder_ctx* ctx, int64_t* out_pairs) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!out_pairs) return fail(ctx, BINDER_ERR_ARG, "NULL out");
+    if (!ctx->last_batch_valid || !ctx->dropin_valid) return fail(ctx, BINDER_ERR_STATE, "no scored batch");
+    const int n_cand = (int)ctx->last_n_cand;
+    CK(ctx->pairs.ensure(1), "alloc");
+    CK(cudaMemsetAsync(ctx->pairs.p, 0, sizeof(long long), ctx->stream), "memset");
+    if ((s = clear_err(ctx))) return s;
+    ScoreOut o{ctx->energy.p, nullptr, nullptr, ctx->pairs.p, ctx->errf.p};
+    launch_score_flat(ctx->stream, ctx->cand.p, ctx->off.p, n_cand, ctx->d_dropin_view.p, nullptr, 0, o,
+                      grid_ctas(ctx, n_cand), 256);
+    LAUNCHED("score_flat_count");
+    long long h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->pairs.p, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if ((s = check_err(ctx))) return s;
+    *out_pairs = h;
+    return BINDER_OK;
+}
+
+int binder_grid_cells(binder_ctx* ctx, float cell, const float* x, const float* y, const float* z, size_t n,
+                      int32_t* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n == 0) return BINDER_OK;
+    if (!x || !y || !z || !out) return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    if (!(cell > 0.0f)) return fail(ctx, BINDER_ERR_ARG, "cell must be positive");
+    CK(ctx->tmp_f.ensure(3 * n), "alloc");
+    CK(cudaMemcpyAsync(ctx->tmp_f.p, x, n * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    CK(cudaMemcpyAsync(ctx->tmp_f.p + n, y, n * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    CK(cudaMemcpyAsync(ctx->tmp_f.p + 2 * n, z, n * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    DBuf<int> d_out;
+    CK(d_out.ensure(3 * n), "alloc");
+    launch_cells_out(ctx->stream, ctx->tmp_f.p, ctx->tmp_f.p + n, ctx->tmp_f.p + 2 * n, (int)n, 1.0f / cell, d_out.p);
+    LAUNCHED("cells_out");
+    CK(cudaMemcpyAsync(out, d_out.p, 3 * n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_grid_neighbors(binder_ctx* ctx, float cell, const float* ax, const float* ay, const float* az, size_t n_ag,
+                          const float* px, const float* py, const float* pz, size_t n_q, int64_t* out_offsets,
+                          uint32_t* out_idx, size_t cap, size_t* out_total) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!out_offsets || (n_q && (!px || !py || !pz)) || (n_ag && (!ax || !ay || !az)))
+        return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    if (n_ag > (size_t)INT32_MAX / 2 || n_q > (size_t)INT32_MAX / 2) return fail(ctx, BINDER_ERR_ARG, "too many points");
+    DBuf<float> pts;
+    CK(pts.ensure(3 * (n_ag + n_q) + 1), "alloc");
+    float* dax = pts.p;
+    float* day = dax + n_ag;
+    float* daz = day + n_ag;
+    float* dpx = daz + n_ag;
+    float* dpy = dpx + n_q;
+    float* dpz = dpy + n_q;
+    if (n_ag) {
+        CK(cudaMemcpyAsync(dax, ax, n_ag * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(day, ay, n_ag * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(daz, az, n_ag * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    }
+    if (n_q) {
+        CK(cudaMemcpyAsync(dpx, px, n_q * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(dpy, py, n_q * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(dpz, pz, n_q * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    }
+    GridBuf G;
+    if ((s = build_grid(ctx, dax, day, daz, (int)n_ag, cell, G))) return s;
+    DBuf<long long> counts;
+    CK(counts.ensure(n_q + 1), "alloc");
+    launch_nb_count(ctx->stream, G.view, dpx, dpy, dpz, (int)n_q, counts.p);
+    if (n_q) LAUNCHED("nb_count");
+    std::vector<long long> h(n_q + 1, 0);
+    if (n_q) CK(cudaMemcpyAsync(h.data(), counts.p, n_q * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    long long total = 0;
+    for (size_t q = 0; q < n_q; ++q) {
+        long long c = h[q];
+        out_offsets[q] = total;
+        h[q] = total;
+        total += c;
+    }
+    out_offsets[n_q] = total;
+    h[n_q] = total;
+    if (out_total) *out_total = (size_t)total;
+    if ((size_t)total > cap) return fail(ctx, BINDER_ERR_CAPACITY, "neighbour list needs %lld entries", total);
+    if (total == 0) return BINDER_OK;
+    if (!out_idx) return fail(ctx, BINDER_ERR_ARG, "NULL out_idx");
+    CK(cudaMemcpyAsync(counts.p, h.data(), (n_q + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    DBuf<uint32_t> idx;
+    CK(idx.ensure(total), "alloc");
+    launch_nb_fill(ctx->stream, G.view, G.sorted_idx.p, dpx, dpy, dpz, (int)n_q, counts.p, idx.p);
+    LAUNCHED("nb_fill");
+    CK(cudaMemcpyAsync(out_idx, idx.p, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_compute_forces_with_grid(binder_ctx* ctx, const binder_residue_cloud* antigen, float cell,
+                                    const binder_residue_cloud* antibody, float* fx, float* fy, float* fz) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!antigen || !antibody) return fail(ctx, BINDER_ERR_ARG, "NULL cloud");
+    const size_t na = antigen->n, nb = antibody->n;
+    if (nb == 0) return BINDER_OK;
+    if (!fx || !fy || !fz || !antibody->x || !antibody->y || !antibody->z || !antibody->amino_acid ||
+        (na && (!antigen->x || !antigen->y || !antigen->z || !antigen->amino_acid)))
+        return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    for (size_t i = 0; i < na; ++i)
+        if (antigen->amino_acid[i] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "antigen amino acid out of range");
+    for (size_t i = 0; i < nb; ++i)
+        if (antibody->amino_acid[i] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "antibody amino acid out of range");
+    Antigen A;
+    if ((s = build_antigen_ca(ctx, A, antigen->x, antigen->y, antigen->z, antigen->amino_acid, na, cell))) return s;
+    DBuf<AgView> dv;
+    CK(dv.ensure(1), "alloc");
+    CK(cudaMemcpyAsync(dv.p, &A.view, sizeof(AgView), cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    DBuf<float> b;
+    DBuf<uint8_t> baa;
+    CK(b.ensure(6 * nb), "alloc");
+    CK(cudaMemcpyAsync(b.p, antibody->x, nb * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    CK(cudaMemcpyAsync(b.p + nb, antibody->y, nb * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    CK(cudaMemcpyAsync(b.p + 2 * nb, antibody->z, nb * 4, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    if ((s = upload(ctx, baa, antibody->amino_acid, nb, "aa H2D"))) return s;
+    launch_cg_forces(ctx->stream, dv.p, b.p, b.p + nb, b.p + 2 * nb, baa.p, (int)nb, b.p + 3 * nb, b.p + 4 * nb,
+                     b.p + 5 * nb);
+    LAUNCHED("cg_forces");
+    CK(cudaMemcpyAsync(fx, b.p + 3 * nb, nb * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaMemcpyAsync(fy, b.p + 4 * nb, nb * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaMemcpyAsync(fz, b.p + 5 * nb, nb * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_forces_allatom(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                          const int64_t* offsets, size_t n_cand, float* out_force, double* out_e) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_cand == 0) return BINDER_OK;
+    if (!offsets || !out_force) return fail(ctx, BINDER_ERR_ARG, "NULL offsets/out");
+    if (offsets[0] != 0) return fail(ctx, BINDER_ERR_ARG, "offsets[0] must be 0");
+    for (size_t c = 0; c < n_cand; ++c)
+        if (offsets[c + 1] < offsets[c]) return fail(ctx, BINDER_ERR_ARG, "offsets must be non-decreasing");
+    const size_t n_atoms = (size_t)offsets[n_cand];
+    if ((s = ensure_dropin(ctx, antigen))) return s;
+    CK(ctx->cand.ensure(n_atoms * 8), "alloc");
+    if (n_atoms)
+        CK(cudaMemcpyAsync(ctx->cand.p, candidates, n_atoms * 32, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    if ((s = upload(ctx, ctx->off, (const long long*)offsets, n_cand + 1, "offsets H2D"))) return s;
+    CK(ctx->energy.ensure(n_cand), "alloc");
+    CK(ctx->force.ensure(3 * n_atoms), "alloc");
+    if ((s = clear_err(ctx))) return s;
+    ScoreOut o{ctx->energy.p, nullptr, ctx->force.p, nullptr, ctx->errf.p};
+    launch_score_flat(ctx->stream, ctx->cand.p, ctx->off.p, (int)n_cand, ctx->d_dropin_view.p, nullptr,
+                      ctx->params.accumulate, o, grid_ctas(ctx, (int)n_cand), 256);
+    LAUNCHED("score_flat_force");
+    ctx->last_batch_valid = false;
+    if (n_atoms)
+        CK(cudaMemcpyAsync(out_force, ctx->force.p, 3 * n_atoms * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    return fetch_energies(ctx, (int)n_cand, out_e, nullptr, nullptr);
+}
+
+int binder_topk_segmented(binder_ctx* ctx, const double* e, const int64_t* seg_off, size_t n_seg, size_t k,
+                          int32_t* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_seg == 0 || k == 0) return BINDER_OK;
+    if (!seg_off || !out) return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    if (k > 1024) return fail(ctx, BINDER_ERR_ARG, "k must be <= 1024");
+    if (seg_off[0] < 0) return fail(ctx, BINDER_ERR_ARG, "negative offset");
+    for (size_t i = 0; i < n_seg; ++i)
+        if (seg_off[i + 1] < seg_off[i]) return fail(ctx, BINDER_ERR_ARG, "offsets must be non-decreasing");
+    const size_t n = (size_t)seg_off[n_seg];
+    if (n > (size_t)INT32_MAX) return fail(ctx, BINDER_ERR_ARG, "too many energies");
+    if (n && !e) return fail(ctx, BINDER_ERR_ARG, "NULL energies");
+    if ((s = upload(ctx, ctx->energy, e, n, "energies H2D"))) return s;
+    if ((s = upload(ctx, ctx->tmp_ll, (const long long*)seg_off, n_seg + 1, "offsets H2D"))) return s;
+    CK(ctx->topk.ensure(n_seg * k), "alloc");
+    launch_topk_segments(ctx->stream, ctx->energy.p, nullptr, ctx->tmp_ll.p, (int)n_seg, (int)k, ctx->topk.p);
+    LAUNCHED("topk");
+    CK(cudaMemcpyAsync(out, ctx->topk.p, n_seg * k * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_topk(binder_ctx* ctx, const double* e, size_t n, size_t k, int32_t* out) {
+    if (!ctx) return BINDER_ERR_ARG;
+    if (k > n) return fail(ctx, BINDER_ERR_ARG, "k > n");
+    const int64_t off[2] = {0, (int64_t)n};
+    return binder_topk_segmented(ctx, e, off, 1, k, out);
+}
+
+int binder_build_residues(binder_ctx* ctx, size_t n, const float* ca_xyz, const uint8_t* aa, const float* chi,
+                          float* out_pos, float* out_chi) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n == 0) return BINDER_OK;
+    if (!ca_xyz || !aa || !out_pos) return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    for (size_t i = 0; i < n; ++i)
+        if (aa[i] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid %d out of range", (int)aa[i]);
+    if ((s = upload(ctx, ctx->tmp_f, ca_xyz, 3 * n, "ca H2D"))) return s;
+    if ((s = upload(ctx, ctx->tmp_u8, aa, n, "aa H2D"))) return s;
+    DBuf<float4> trig;
+    DBuf<float> chi_d;
+    if (chi) {
+        // sin/cos of chi*PI/180 with the host C library, as for the rotamer table
+        std::vector<float4> h(2 * n);
+        for (size_t r = 0; r < n; ++r) {
+            float t[8];
+            for (int c = 0; c < 4; ++c) {
+                const float x = chi[4 * r + c] * RADS_PER_DEG;
+                t[2 * c] = std::sin(x);
+                t[2 * c + 1] = std::cos(x);
+            }
+            h[2 * r] = make_float4(t[0], t[1], t[2], t[3]);
+            h[2 * r + 1] = make_float4(t[4], t[5], t[6], t[7]);
+        }
+        if ((s = upload(ctx, trig, h.data(), 2 * n, "trig H2D"))) return s;
+        if ((s = upload(ctx, chi_d, chi, 4 * n, "chi H2D"))) return s;
+        CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    }
+    CK(ctx->tmp_f4a.ensure(n * SLOT_STRIDE), "alloc");
+    CK(ctx->tmp_f4b.ensure(n), "alloc");
+    launch_build_residues(ctx->stream, (int)n, ctx->tmp_f.p, ctx->tmp_u8.p, chi ? trig.p : nullptr,
+                          chi ? chi_d.p : nullptr, ctx->tmp_f4a.p, ctx->tmp_f4b.p);
+    LAUNCHED("build_residues");
+    DBuf<float> outd;
+    CK(outd.ensure(n * SLOTS * 3), "alloc");
+    launch_unpack_slots(ctx->stream, (int)n, ctx->tmp_f4a.p, outd.p);
+    LAUNCHED("unpack_slots");
+    CK(cudaMemcpyAsync(out_pos, outd.p, n * SLOTS * 3 * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if (out_chi) CK(cudaMemcpyAsync(out_chi, ctx->tmp_f4b.p, n * 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_add_antigen(binder_ctx* ctx, size_t n_res, const uint8_t* aa, const float* pos, int32_t* out_id) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_res == 0 || !aa || !pos) return fail(ctx, BINDER_ERR_ARG, "empty antigen");
+    for (size_t r = 0; r < n_res; ++r)
+        if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
+    // flatten the slot layout into the AtomCloud of push_residue (allatom.rs:201-240)
+    std::vector<float> x, y, z, q, rmh, eps;
+    std::vector<uint8_t> hyd, type;
+    std::vector<float> cx(n_res), cy(n_res), cz(n_res);
+    std::vector<float4> ca_atom(n_res), ca_prm(n_res);
+    for (size_t r = 0; r < n_res; ++r) {
+        const int a = aa[r];
+        for (int k = 0; k < BT_TOPO_N[a]; ++k) {
+            const float* p = pos + (r * SLOTS + k) * 3;
+            const int t = BT_SLOT_TYPE[a][k];
+            x.push_back(p[0]); y.push_back(p[1]); z.push_back(p[2]);
+            q.push_back(BT_SLOT_Q[a][k]);
+            rmh.push_back(BT_NB[t][0]);
+            eps.push_back(BT_NB[t][1]);
+            hyd.push_back(BT_SLOT_HYD[a][k]);
+            type.push_back((uint8_t)t);
+        }
+        const float* ca = pos + (r * SLOTS + 1) * 3;
+        cx[r] = ca[0]; cy[r] = ca[1]; cz[r] = ca[2];
+        const int t = BT_SLOT_TYPE[a][1];
+        ca_atom[r] = make_float4(ca[0], ca[1], ca[2], BT_SLOT_Q[a][1]);
+        ca_prm[r] = make_float4(BT_NB[t][0], BT_NB[t][1], (float)BT_SLOT_HYD[a][1], (float)t);
+    }
+    std::unique_ptr<Antigen> A(new (std::nothrow) Antigen());
+    if (!A) return fail(ctx, BINDER_ERR_OOM, "host allocation");
+    if ((s = build_antigen_atoms(ctx, *A, x.data(), y.data(), z.data(), q.data(), rmh.data(), eps.data(), hyd.data(),
+                                 type.data(), x.size())))
+        return s;
+    if ((s = build_antigen_ca(ctx, *A, cx.data(), cy.data(), cz.data(), aa, n_res, ctx->params.ca_cell))) return s;
+    if ((s = upload(ctx, A->ca_atom, ca_atom.data(), n_res, "ca atoms"))) return s;
+    if ((s = upload(ctx, A->ca_atom_prm, ca_prm.data(), n_res, "ca atoms"))) return s;
+    A->view.ca_atom = A->ca_atom.p;
+    A->view.ca_atom_prm = A->ca_atom_prm.p;
+    // ca_center_of_mass (allatom.rs:183-195): sequential f32 sums
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    for (size_t r = 0; r < n_res; ++r) { sx += cx[r]; sy += cy[r]; sz += cz[r]; }
+    const float nf = (float)n_res;
+    A->view.cx = sx / nf;
+    A->view.cy = sy / nf;
+    A->view.cz = sz / nf;
+    ctx->ags.push_back(std::move(A));
+    std::vector<AgView> views;
+    refresh_views(ctx, views);
+    CK(ctx->d_views.ensure(views.size()), "alloc");
+    CK(cudaMemcpyAsync(ctx->d_views.p, views.data(), views.size() * sizeof(AgView), cudaMemcpyHostToDevice, ctx->stream),
+       "views H2D");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    if (out_id) *out_id = (int32_t)(ctx->ags.size() - 1);
+    return BINDER_OK;
+}
+
+int binder_clear_antigens(binder_ctx* ctx) {
+    int s = enter(ctx);
+    if (s) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    ctx->ags.clear();
+    ctx->st.n_cand = 0;
+    ctx->st.total_res = 0;
+    return BINDER_OK;
+}
+
+int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
+                        const float* pos) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (ctx->ags.empty()) return fail(ctx, BINDER_ERR_STATE, "no antigen added");
+    if (n_cand == 0 || n_cand > (size_t)INT32_MAX / 64) return fail(ctx, BINDER_ERR_ARG, "bad candidate count");
+    State& S = ctx->st;
+    std::vector<int> off(n_cand + 1, 0), ag(n_cand, 0);
+    std::vector<uint32_t> ids(n_cand);
+    for (size_t c = 0; c < n_cand; ++c) {
+        const int nr = n_res ? n_res[c] : uniform_n_res;
+        if (nr < 0 || nr > 4096) return fail(ctx, BINDER_ERR_ARG, "bad residue count %d", nr);
+        off[c + 1] = off[c] + nr;
+        ag[c] = antigen_id ? antigen_id[c] : 0;
+        if (ag[c] < 0 || ag[c] >= (int)ctx->ags.size()) return fail(ctx, BINDER_ERR_ARG, "bad antigen id");
+        ids[c] = cand_id ? cand_id[c] : (uint32_t)c;
+    }
+    const int total = off[n_cand];
+    if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
+    for (int r = 0; r < total; ++r)
+        if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
+    std::vector<int> res_cand(total);
+    for (size_t c = 0; c < n_cand; ++c)
+        for (int r = off[c]; r < off[c + 1]; ++r) res_cand[r] = (int)c;
+    // candidates grouped by antigen (stable) for per-antigen survivor selection
+    const int n_ag = (int)ctx->ags.size();
+    std::vector<long long> g_off(n_ag + 1, 0);
+    for (size_t c = 0; c < n_cand; ++c) g_off[ag[c] + 1]++;
+    for (int a = 0; a < n_ag; ++a) g_off[a + 1] += g_off[a];
+    std::vector<int> g_idx(n_cand);
+    std::vector<long long> cur(g_off.begin(), g_off.end() - 1);
+    for (size_t c = 0; c < n_cand; ++c) g_idx[cur[ag[c]]++] = (int)c;
+    S.n_cand = (int)n_cand;
+    S.total_res = total;
+    S.h_res_off = off;
+    S.n_segments = n_ag;
+    if ((s = upload(ctx, S.cand_res_off, off.data(), off.size(), "state")) ||
+        (s = upload(ctx, S.cand_ag, ag.data(), ag.size(), "state")) ||
+        (s = upload(ctx, S.cand_id, ids.data(), ids.size(), "state")) ||
+        (s = upload(ctx, S.res_cand, res_cand.data(), res_cand.size(), "state")) ||
+        (s = upload(ctx, S.ag_cand_idx, g_idx.data(), g_idx.size(), "state")) ||
+        (s = upload(ctx, S.ag_cand_off, g_off.data(), g_off.size(), "state")) ||
+        (s = upload(ctx, S.res_aa, aa, (size_t)total, "state")))
+        return s;
+    CK(S.res_chi.ensure(total), "alloc");
+    if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
+    CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
+    launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
+    if (total) LAUNCHED("pack_slots");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_state_download(binder_ctx* ctx, uint8_t* aa, float* chi, float* pos) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no state");
+    const int total = S.total_res;
+    if (total == 0) return BINDER_OK;
+    if (aa) CK(cudaMemcpyAsync(aa, S.res_aa.p, total, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if (chi) CK(cudaMemcpyAsync(chi, S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if (pos) {
+        CK(S.stage.ensure((size_t)total * SLOTS * 3), "alloc");
+        launch_unpack_slots(ctx->stream, total, S.res_pos.p, S.stage.p);
+        LAUNCHED("unpack_slots");
+        CK(cudaMemcpyAsync(pos, S.stage.p, (size_t)total * SLOTS * 3 * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+}  // extern "C"
+
+namespace {
+StepParams step_params(const binder_params& p) {
+    StepParams s;
+    s.step = p.step;
+    s.noise_base = p.noise_base;
+    s.t_hot = p.t_hot;
+    s.t_cold = p.t_cold;
+    s.mutation_p = p.mutation_p;
+    s.rotamer_move_p = p.rotamer_move_p;
+    s.backbone_move_p = p.backbone_move_p;
+    s.max_torsion_deg = p.max_torsion_deg;
+    s.iface_cutoff_sq = p.iface_cutoff_sq;
+    s.shell_radius = p.shell_radius;
+    s.max_disp = p.max_disp;
+    s.restraint_k = p.restraint_k;
+    s.seed = p.seed;
+    return s;
+}
+
+int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise, int with_mc, const float* temps) {
+    State& S = ctx->st;
+    if (temps) {
+        int s = upload(ctx, ctx->temps, temps, (size_t)n_steps, "temps H2D");
+        if (s) return s;
+    }
+    launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise, with_mc,
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p);
+    LAUNCHED("diffuse");
+    return BINDER_OK;
+}
+
+int enqueue_score_state(binder_ctx* ctx, int full) {
+    State& S = ctx->st;
+    CK(ctx->energy.ensure(S.n_cand), "alloc");
+    ScoreOut o{ctx->energy.p, nullptr, nullptr, nullptr, ctx->errf.p};
+    launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
+                       grid_ctas(ctx, S.n_cand), 256);
+    LAUNCHED("score_state");
+    return BINDER_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int binder_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise, int with_mc, const float* temps) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (ctx->st.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (n_steps < 0) return fail(ctx, BINDER_ERR_ARG, "negative step count");
+    if (with_mc) return fail(ctx, BINDER_ERR_ARG, "Metropolis moves are not enabled in this build");
+    if (n_steps == 0) return BINDER_OK;
+    if ((s = clear_err(ctx))) return s;
+    if ((s = enqueue_diffuse(ctx, n_steps, step0, with_noise, with_mc, temps))) return s;
+    return check_err(ctx);
+}
+
+int binder_score_state(binder_ctx* ctx, int full, double* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (ctx->st.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (!out) return fail(ctx, BINDER_ERR_ARG, "NULL out");
+    if ((s = clear_err(ctx))) return s;
+    if ((s = enqueue_score_state(ctx, full))) return s;
+    return fetch_energies(ctx, ctx->st.n_cand, out, nullptr, nullptr);
+}
+
+int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_e, int32_t* out_topk) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
+    if ((s = clear_err(ctx))) return s;
+    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, step0, 0, 0, nullptr))) return s;
+    if ((s = enqueue_score_state(ctx, 0))) return s;
+    if (k > 0) {
+        CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
+        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
+                             ctx->topk.p);
+        LAUNCHED("topk");
+        if (out_topk)
+            CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * k * sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream),
+               "D2H");
+    }
+    return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// common.cuh — shared definitions of the sm_100a kernels: constants, packed
+// force-field tables, exact-rounding helpers, the Philox generator, the device
+// views of antigens and of the resident candidate state.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace binder {
+
+#include "binder_tables.inc"  // host copies of the reference tables (BT_*)
+
+constexpr int SLOTS = 14;        // max heavy atoms per residue (TRP, amber.rs:311-326)
+constexpr int SLOT_STRIDE = 16;  // float4 slots per residue in device state (256 B, two 128 B lines)
+constexpr int N_AA = 20;
+constexpr int GLY = 7;
+constexpr int CYS = 4;
+
+// energy.rs:13-27
+constexpr float COULOMB_K = 332.0f;
+constexpr float CUTOFF_SQ = 100.0f;
+constexpr float MIN_R_SQ = 0.25f;
+constexpr float HYDRO_CUTOFF_SQ = 36.0f;
+constexpr float HYDRO_BONUS = -0.5f;
+constexpr float HB_R0 = 2.9f;
+constexpr float HB_SIGMA = 0.35f;
+constexpr float HB_DEPTH = 1.5f;
+constexpr float HB_CUTOFF_SQ = 25.0f;
+// solvation.rs:23-27
+constexpr float PI32 = 5.568328f;
+constexpr float SOLV_CUTOFF_SQ = 81.0f;
+// allatom.rs:494-497
+constexpr float N_CA_BOND = 1.46f;
+constexpr float CA_C_BOND = 1.52f;
+constexpr float C_O_BOND = 1.23f;
+constexpr float CA_CB_BOND = 1.52f;
+
+// error flags a kernel may raise (read back by the host after the launch)
+enum : uint32_t { ERRF_NAN = 1u, ERRF_TIMEOUT = 2u, ERRF_RANGE = 4u };
+
+// ---- exact-rounding helpers: one IEEE rounding per operation, never fused --------
+// The reference is Rust, which never contracts a*b+c; where bit-exact parity with
+// its f32 results is required these helpers stop nvcc from forming FMAs.
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float xsqrt(float a) { return __fsqrt_rn(a); }
+// squared distance with the reference's rounding: (dx*dx + dy*dy) + dz*dz
+__device__ __forceinline__ float xdist2(float dx, float dy, float dz) {
+    return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
+}
+
+// Rust `f32 as i32`: saturating, NaN -> 0
+__host__ __device__ __forceinline__ int32_t sat_i32(float v) {
+    if (v != v) return 0;
+    if (v >= 2147483648.0f) return INT32_MAX;
+    if (v < -2147483648.0f) return INT32_MIN;
+    return (int32_t)v;
+}
+
+// ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) --------------------------
+struct U4 { uint32_t x, y, z, w; };
+__host__ __device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                               uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return U4{c0, c1, c2, c3};
+}
+// Draw conventions (identical in the oracle): counter = (candidate, step,
+// stream << 16 | residue, 0), key = seed.  Uniform float from the top 24 bits,
+// integer range by multiply-shift, float range lo + u*(hi-lo) rounded per op.
+enum : uint32_t { STREAM_NOISE = 0, STREAM_MC = 1, STREAM_BACKBONE = 2 };
+__host__ __device__ __forceinline__ U4 rng_draw(uint64_t seed, uint32_t cand, uint32_t step, uint32_t stream,
+                                                 uint32_t r) {
+    return philox(cand, step, (stream << 16) | (r & 0xFFFFu), 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+__device__ __forceinline__ float u01(uint32_t x) { return xmul((float)(x >> 8), 1.0f / 16777216.0f); }
+__device__ __forceinline__ uint32_t urange(uint32_t x, uint32_t n) { return (uint32_t)(((uint64_t)x * n) >> 32); }
+__device__ __forceinline__ float frange(uint32_t x, float lo, float hi) { return xadd(lo, xmul(u01(x), xsub(hi, lo))); }
+
+// ---- device views ----------------------------------------------------------------
+// A uniform cell box over the cells that contain atoms (the reference's HashMap
+// holds exactly those cells; a probe outside the box finds nothing, as a missing
+// HashMap key does).
+struct GridView {
+    const int* cell_start;  // ncell + 1
+    int ox, oy, oz;         // cell index of box corner
+    int nx, ny, nz;
+    float inv;              // f32 reciprocal of the cell edge (spatial.rs:26)
+    float cell;
+};
+
+// One resident antigen.
+struct AgView {
+    // all atoms, sorted by score-grid cell (ascending original index within a cell)
+    const float4* pq;   // x, y, z, q*sqrt(332)
+    const float4* prm;  // r_min_half, sqrt(epsilon), hydrophobic (0/1), atom type
+    GridView grid;
+    int n_atoms;
+    // Calpha cloud (run_allatom ag_ca, diffusion.rs:994-1002) sorted by CA-grid cell
+    const float4* ca_pq;   // x, y, z, residue-level charge (atom.rs:55-63)
+    const float4* ca_prm;  // residue-level epsilon, sigma, hydrophobic, 0
+    GridView ca_grid;
+    // Calpha atoms in residue order with their AMBER parameters (diffusion.rs:440-446)
+    const float4* ca_atom;      // x, y, z, partial charge
+    const float4* ca_atom_prm;  // r_min_half, epsilon, hydrophobic, atom type
+    int n_res;
+    float cx, cy, cz;  // ca_center_of_mass (allatom.rs:183-195)
+};
+
+// Resident candidate state (slot layout).
+struct StateView {
+    int n_cand;
+    int total_res;
+    const int* cand_res_off;  // n_cand + 1
+    const int* cand_ag;       // n_cand
+    const uint32_t* cand_id;  // n_cand
+    uint8_t* res_aa;          // total_res
+    float4* res_chi;          // total_res (degrees)
+    float4* res_pos;          // total_res * SLOT_STRIDE
+    const int* res_cand;      // total_res
+};
+
+// spatial.rs:61-67: (x * inv).floor() as i32 — one f32 multiply, floor, saturating cast
+__device__ __forceinline__ int cell_coord(float v, float inv) { return sat_i32(floorf(xmul(v, inv))); }
+
+// Range of atoms of cell (cx+dx, cy+dy, cz+dz); false when the cell holds none.
+// i32 addition wraps, as in the reference's release build (spatial.rs:52).
+__device__ __forceinline__ bool probe_cell(const GridView& g, int cx, int cy, int cz, int dx, int dy, int dz, int& a0,
+                                           int& a1) {
+    int nx_ = (int)((unsigned)cx + (unsigned)dx), ny_ = (int)((unsigned)cy + (unsigned)dy),
+        nz_ = (int)((unsigned)cz + (unsigned)dz);
+    long long ix = (long long)nx_ - g.ox, iy = (long long)ny_ - g.oy, iz = (long long)nz_ - g.oz;
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= g.nx || iy >= g.ny || iz >= g.nz) return false;
+    int lin = ((int)ix * g.ny + (int)iy) * g.nz + (int)iz;
+    a0 = g.cell_start[lin];
+    a1 = g.cell_start[lin + 1];
+    return a1 > a0;
+}
+
+// Search parameters as the kernels see them.
+struct StepParams {
+    float step, noise_base, t_hot, t_cold, mutation_p, rotamer_move_p, backbone_move_p, max_torsion_deg,
+        iface_cutoff_sq, shell_radius, max_disp, restraint_k;
+    uint64_t seed;
+};
+
+}  // namespace binder

@@ -1,0 +1,87 @@
+// k_topk.cu — survivor selection: the k lowest energies of each segment in
+// stable ascending order (diffusion.rs:1042-1057 sorts with a stable sort and
+// truncates to the population).
+//
+// One CTA per segment.  Energies are mapped to order-preserving 64-bit keys
+// (-0.0 folded onto +0.0, NaN after every number) and paired with their index,
+// so a plain lexicographic (key, index) order is exactly the stable sort.  The
+// CTA keeps a running best-k list in shared memory and merges the segment in
+// chunks with a bitonic sort of (chunk + best-k) elements.
+#include "kernels.h"
+
+namespace binder {
+
+constexpr int TOPK_SORT = 4096;   // elements per bitonic pass (pow2)
+constexpr int TOPK_MAX_K = 1024;  // best-k kept between passes
+constexpr int TOPK_THREADS = 1024;
+
+__device__ __forceinline__ unsigned long long order_key(double e) {
+    if (e != e) return 0xFFFFFFFFFFFFFFFFull;  // NaN last
+    e = e + 0.0;                               // -0.0 -> +0.0
+    unsigned long long b = (unsigned long long)__double_as_longlong(e);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict__ e,
+                                                        const int* __restrict__ idx_list,
+                                                        const long long* __restrict__ seg_off, int k,
+                                                        int* __restrict__ out_idx) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(smem_raw);
+    int* idx = reinterpret_cast<int*>(key + TOPK_SORT);
+    const int seg = blockIdx.x;
+    const long long b0 = seg_off[seg], b1 = seg_off[seg + 1];
+    const long long n = b1 - b0;
+    const int chunk = TOPK_SORT - k;  // new elements per pass
+    int kept = 0;                     // valid entries at the front of key/idx
+    for (long long base = 0; base < n || base == 0; base += chunk) {
+        const long long take = min((long long)chunk, n - base);
+        // slots [kept, TOPK_SORT): new chunk, padded with +inf keys
+        for (int t = threadIdx.x; t < TOPK_SORT; t += blockDim.x) {
+            if (t < kept) continue;
+            const long long j = base + (t - kept);
+            if (t - kept < take) {
+                const int g = idx_list ? idx_list[b0 + j] : (int)(b0 + j);
+                key[t] = order_key(e[g]);
+                idx[t] = g;
+            } else {
+                key[t] = 0xFFFFFFFFFFFFFFFFull;
+                idx[t] = INT32_MAX;
+            }
+        }
+        __syncthreads();
+        for (int size = 2; size <= TOPK_SORT; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int t = threadIdx.x; t < TOPK_SORT / 2; t += blockDim.x) {
+                    const int lo = 2 * t - (t & (stride - 1));
+                    const int hi = lo + stride;
+                    const bool up = ((lo & size) == 0);
+                    const unsigned long long kl = key[lo], kh = key[hi];
+                    const int il = idx[lo], ih = idx[hi];
+                    const bool gt = (kl > kh) || (kl == kh && il > ih);
+                    if (gt == up) {
+                        key[lo] = kh; key[hi] = kl;
+                        idx[lo] = ih; idx[hi] = il;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        kept = (int)min((long long)k, (long long)kept + take);
+        if (take <= 0) break;
+    }
+    for (int t = threadIdx.x; t < k; t += blockDim.x)
+        out_idx[(long long)seg * k + t] = (t < kept && idx[t] != INT32_MAX) ? idx[t] : -1;
+}
+
+int launch_topk_segments(cudaStream_t s, const double* energies, const int* idx_list, const long long* seg_off,
+                         int n_seg, int k, int* out_idx) {
+    if (n_seg <= 0 || k <= 0) return 0;
+    if (k > TOPK_MAX_K) return -1;
+    const size_t smem = (size_t)TOPK_SORT * (sizeof(unsigned long long) + sizeof(int));
+    cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_topk<<<n_seg, TOPK_THREADS, smem, s>>>(energies, idx_list, seg_off, k, out_idx);
+    return 1;
+}
+
+}  // namespace binder

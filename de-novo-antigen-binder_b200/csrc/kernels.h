@@ -1,0 +1,60 @@
+// kernels.h — host-side launchers of the sm_100a kernels (one declaration per
+// kernel family; definitions live in the k_*.cu translation units).
+#pragma once
+
+#include "common.cuh"
+
+namespace binder {
+
+// ---- k_grid.cu: SpatialHashGrid ----
+void launch_cell_coords(cudaStream_t s, const float* x, const float* y, const float* z, int n, float inv, int4* cells,
+                        int* minmax, uint32_t* err);
+void launch_cell_hist(cudaStream_t s, int4* cells, int n, int ox, int oy, int oz, int ny, int nz, int* counts);
+void launch_exclusive_scan(cudaStream_t s, const int* counts, int n, int* out);
+void launch_stable_scatter(cudaStream_t s, const int4* cells, int n, int* cursor, int* sorted_idx);
+void launch_gather_atoms(cudaStream_t s, const int* sorted_idx, int n, const float* x, const float* y,
+                         const float* z, const float* q, const float* rmh, const float* eps, const uint8_t* hyd,
+                         const uint8_t* type, float4* pq, float4* prm);
+void launch_gather_ca(cudaStream_t s, const int* sorted_idx, int n, const float* x, const float* y, const float* z,
+                      const uint8_t* aa, const float4* res_tab, float4* pq, float4* prm);
+void launch_nb_count(cudaStream_t s, const GridView& g, const float* px, const float* py, const float* pz, int n_q,
+                     long long* counts);
+void launch_nb_fill(cudaStream_t s, const GridView& g, const int* sorted_idx, const float* px, const float* py,
+                    const float* pz, int n_q, const long long* offsets, uint32_t* out);
+void launch_cells_out(cudaStream_t s, const float* x, const float* y, const float* z, int n, float inv, int* out);
+
+// ---- k_score.cu: all-atom pair energy / force ----
+cudaError_t score_init_tables();
+struct ScoreOut {
+    double* energy;       // per candidate
+    double* abs_sum;      // per candidate sum of |pair term| (may be null)
+    float* force;         // per candidate atom, 3 floats (may be null)
+    long long* pairs;     // pair counter (may be null)
+    uint32_t* err;        // error flags
+};
+// flat GpuAtom candidates (8 floats per atom), ragged offsets (n_cand + 1)
+int launch_score_flat(cudaStream_t s, const float* atoms, const long long* offsets, int n_cand, const AgView* ags,
+                      const int* cand_ag, int accumulate, const ScoreOut& out, int grid_ctas, int block);
+// resident state (slot layout); full = add H-bond + EEF1 + disulfide
+int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
+                       const ScoreOut& out, int grid_ctas, int block);
+
+void launch_uniform_offsets(cudaStream_t s, long long* off, int n_cand, long long n_ab);
+
+// ---- k_topk.cu ----
+// idx_list (may be null): segment entries are energies[idx_list[j]] and report idx_list[j]
+int launch_topk_segments(cudaStream_t s, const double* energies, const int* idx_list, const long long* seg_off,
+                         int n_seg, int k, int* out_idx);
+
+// ---- k_search.cu: residues, CG forces, Langevin, Metropolis ----
+cudaError_t search_init_tables();
+void launch_build_residues(cudaStream_t s, int n, const float* ca_xyz, const uint8_t* aa, const float4* chi_trig,
+                           const float* chi_deg, float4* out_pos, float4* out_chi);
+void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const float* by, const float* bz,
+                      const uint8_t* baa, int n, float* fx, float* fy, float* fz);
+void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                    uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err);
+void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);
+void launch_unpack_slots(cudaStream_t s, int n_res, const float4* in, float* out);
+
+}  // namespace binder

@@ -1,0 +1,239 @@
+/*
+ * binder_gpu.h — C ABI of the B200 (sm_100a) all-atom scoring + search library
+ * (libbinder_b200.so).
+ *
+ * This is the drop-in boundary for the hot path of the reference antibody
+ * design engine (Rust crate DilaDeniz/de-novo-antigen-binder).  The reference has
+ * no FFI; each entry point below names the Rust item it replaces (file:line in
+ * the reference project) so that a Rust caller can bind it with `extern "C"`
+ * declarations and keep its call sites unchanged.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Host buffers are caller-owned and only
+ *     borrowed for the duration of a call; device memory is owned by the context.
+ *   - Every entry point returns a binder_status (0 = BINDER_OK).  Nothing throws
+ *     or aborts across the ABI; binder_last_error() describes the last failure.
+ *   - One context = one device + one CUDA stream.  Calls on one context are
+ *     serialised on that stream and the context is not thread-safe; separate
+ *     contexts are independent.
+ *   - There is no CPU fallback: a context whose device or kernels are missing
+ *     fails binder_create() with BINDER_ERR_NODEVICE / BINDER_ERR_CUDA.
+ *   - Candidate proteins use the "slot layout": residue r of a protein owns 14
+ *     atom slots; slot k holds topology atom k of the residue's amino acid in the
+ *     order of the reference's residue tables (amber.rs:126-351), i.e. the order
+ *     AtomProtein::push_residue appends them (allatom.rs:201-240).  Unused slots
+ *     are zero.  Positions are float[n_res][14][3]; chi angles float[n_res][4] in
+ *     degrees; amino acids uint8 in AminoAcid order (atom.rs:4-25).
+ */
+#ifndef BINDER_GPU_H
+#define BINDER_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BINDER_ABI_VERSION 1
+#define BINDER_MAX_SLOTS 14
+
+enum binder_status {
+    BINDER_OK = 0,
+    BINDER_ERR_ARG = 1,       /* invalid argument (NULL, size, amino acid out of range) */
+    BINDER_ERR_CUDA = 2,      /* CUDA runtime error (launch, copy) */
+    BINDER_ERR_OOM = 3,       /* device or host allocation failed */
+    BINDER_ERR_TIMEOUT = 4,   /* a bounded device wait gave up */
+    BINDER_ERR_NAN = 5,       /* non-finite coordinate in an input */
+    BINDER_ERR_GRID = 6,      /* spatial grid box too large for the cell size */
+    BINDER_ERR_STATE = 7,     /* call out of order (e.g. no antigen / no candidates) */
+    BINDER_ERR_NODEVICE = 8,  /* no usable sm_100 device */
+    BINDER_ERR_CAPACITY = 9   /* output buffer too small; required size reported */
+};
+
+typedef struct binder_ctx binder_ctx;
+
+/* GpuAtom (gpu.rs:17-29): 8 x f32 = 32 bytes, layout identical to the Rust
+   #[repr(C)] struct and to the reference shader's storage buffer. */
+typedef struct binder_gpu_atom {
+    float x, y, z, q, r_min_half, epsilon, hydrophobic, _pad;
+} binder_gpu_atom;
+
+/* AtomCloud (allatom.rs:17-31), borrowed structure-of-arrays. */
+typedef struct binder_atom_cloud {
+    const float* x;
+    const float* y;
+    const float* z;
+    const float* charge;
+    const float* r_min_half;
+    const float* epsilon;
+    const uint8_t* hydrophobic;  /* 1 = hydrophobic */
+    const uint8_t* atom_type;    /* AtomType (amber.rs:13-30); may be NULL for scoring */
+    const uint32_t* residue_idx; /* may be NULL */
+    size_t n;
+} binder_atom_cloud;
+
+/* ResidueCloud (atom.rs:185-195): positions + amino acid.  charge, epsilon,
+   sigma and hydrophobic are derived from amino_acid as ResidueCloud::push does
+   (atom.rs:221-231). */
+typedef struct binder_residue_cloud {
+    const float* x;
+    const float* y;
+    const float* z;
+    const uint8_t* amino_acid;
+    size_t n;
+} binder_residue_cloud;
+
+/* Search hyper-parameters.  Defaults = the reference constants
+   (diffusion.rs:65-83, energy.rs:13-27, spatial grid cell diffusion.rs:1003). */
+typedef struct binder_params {
+    float step;             /* STEP 0.08 */
+    float noise_base;       /* NOISE_BASE 0.25 */
+    float t_hot;            /* T_HOT 3.0 */
+    float t_cold;           /* T_COLD 0.02 */
+    float mutation_p;       /* MUTATION_P 0.08 */
+    float rotamer_move_p;   /* ROTAMER_MOVE_P 0.12 */
+    float backbone_move_p;  /* BACKBONE_MOVE_P 0.04 */
+    float max_torsion_deg;  /* MAX_TORSION_DEG 15 */
+    float iface_cutoff_sq;  /* IFACE_CUTOFF_SQ 64 */
+    float shell_radius;     /* restraint radius, INIT_RADIUS 20 */
+    float max_disp;         /* MAX_DISP 2.0 */
+    float restraint_k;      /* RESTRAINT_K 0.02 */
+    float ca_cell;          /* Calpha grid cell for the CG force, 10 A */
+    float score_cell;       /* all-atom grid cell for scoring, 8 A */
+    int32_t accumulate;     /* BINDER_ACC_KAHAN (default) or BINDER_ACC_F32 */
+    int32_t _reserved;
+    uint64_t seed;          /* Philox key for every stochastic move */
+} binder_params;
+
+#define BINDER_ACC_KAHAN 0  /* f32 pair terms, compensated per-lane sums, FP64 cross-lane/block reduction */
+#define BINDER_ACC_F32 1    /* f32 pair terms, plain f32 per-lane sums, FP64 cross-lane/block reduction */
+
+/* ---- force-field tables compiled into the library (amber.rs, rotamer.rs) ----
+   Residue aa: its atom count and per-slot partial charge, AMBER type and
+   hydrophobic flag (amber.rs:126-378).  Arrays have 14 entries. */
+int binder_table_residue(int aa, int* n_atoms, float* charge, uint8_t* atom_type, uint8_t* hydrophobic);
+/* AMBER type: r_min_half, epsilon (amber.rs:46-63), H-bond flags bit0 donor /
+   bit1 acceptor (amber.rs:72-84), EEF1 dg_ref, vol, lambda (amber.rs:414-431). */
+int binder_table_atom_type(int type, float* r_min_half, float* epsilon, int* hbond_flags, float* eef1);
+/* rotamers(aa) (rotamer.rs:468): count and chi tuples float[5][4]. */
+int binder_table_rotamers(int aa, int* n, float* chi);
+/* residue-level charge, epsilon, sigma, hydrophobic (atom.rs:55-104). */
+int binder_table_residue_level(int aa, float* out4);
+
+/* ---- context --------------------------------------------------------------- */
+int binder_abi_version(void);
+const char* binder_status_string(int status);
+void binder_default_params(binder_params* out);
+/* GpuContext::try_init (gpu.rs:55-155).  params NULL = defaults.  Returns NULL
+   and sets *status when no sm_100 device is usable (the reference returns None). */
+binder_ctx* binder_create(int device, const binder_params* params, int* status);
+void binder_destroy(binder_ctx* ctx);
+int binder_set_params(binder_ctx* ctx, const binder_params* params);
+const char* binder_last_error(const binder_ctx* ctx);
+int binder_synchronize(binder_ctx* ctx);
+/* number of kernels this context has launched (instrumentation for benchmarks) */
+uint64_t binder_launch_count(const binder_ctx* ctx);
+
+/* ---- score_batch: GpuContext::score_batch (gpu.rs:166-267) --------------------
+   energies[c] = AMBER LJ + Coulomb + hydrophobic energy of candidate c against
+   the antigen (energy.wgsl:67-94; the LJ/Coulomb/hydrophobic part of
+   interaction_energy_atoms_breakdown, energy.rs:261-314).  candidates is the
+   flat n_cand*n_ab GpuAtom array; n_cand = n_atoms / n_ab, 0 when n_ab == 0
+   (gpu.rs:172-174).  *out_n_cand receives n_cand; out_cap must be >= n_cand.
+   The antigen is uploaded and its spatial grid rebuilt only when its contents
+   change between calls. */
+int binder_score_batch(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                       size_t n_atoms, size_t n_ab, float* out_energies, size_t out_cap, size_t* out_n_cand);
+/* same, FP64 energies; out_abs (may be NULL) = sum of |pair term| per candidate */
+int binder_score_batch_f64(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                           size_t n_atoms, size_t n_ab, double* out_energies, double* out_abs, size_t out_cap,
+                           size_t* out_n_cand);
+/* ragged candidates: candidate c is atoms [offsets[c], offsets[c+1]).  Lifts the
+   reference's uniform-n_ab restriction (gpu.rs:163). */
+int binder_score_batch_ragged(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                              const int64_t* offsets, size_t n_cand, double* out_energies, double* out_abs);
+/* make `antigen` the context's resident antigen 0 (upload + grid build) */
+int binder_set_antigen_atoms(binder_ctx* ctx, const binder_atom_cloud* antigen);
+/* count of (candidate atom, antigen atom) pairs with 0.25 <= r^2 <= 100 among the
+   last ragged/uniform batch scored (pair-evals of one scoring) */
+int binder_last_pair_count(binder_ctx* ctx, int64_t* out_pairs);
+
+/* ---- SpatialHashGrid (spatial.rs:12-67) --------------------------------------
+   Cell of each point: floor(coord * (1/cell)) with the f32 reciprocal
+   (spatial.rs:26,61-67).  out_cells = int32[3n]. */
+int binder_grid_cells(binder_ctx* ctx, float cell, const float* x, const float* y, const float* z, size_t n,
+                      int32_t* out_cells);
+/* build(x,y,z) (spatial.rs:31-39) over the n_ag points, then query_neighbors
+   (spatial.rs:44-58) for each of the n_q probe points: the candidate indices of
+   probe q are out_idx[out_offsets[q] .. out_offsets[q+1]), in the reference's
+   callback order (cells dx, dy, dz in -1..1, atoms ascending within a cell).
+   Returns BINDER_ERR_CAPACITY with *out_total set when cap is too small. */
+int binder_grid_neighbors(binder_ctx* ctx, float cell, const float* ax, const float* ay, const float* az,
+                          size_t n_ag, const float* px, const float* py, const float* pz, size_t n_q,
+                          int64_t* out_offsets, uint32_t* out_idx, size_t cap, size_t* out_total);
+
+/* ---- forces ------------------------------------------------------------------
+   compute_forces_with_grid (energy.rs:322-398): coarse-grained (Calpha) force on
+   every antibody residue from the antigen residues found by the 27-cell probe of
+   a grid with the given cell (the reference uses 10 A).  Bit-exact with the
+   reference's f32 operation order. */
+int binder_compute_forces_with_grid(binder_ctx* ctx, const binder_residue_cloud* antigen, float cell,
+                                    const binder_residue_cloud* antibody, float* fx, float* fy, float* fz);
+/* All-atom AMBER force (no reference counterpart): -grad of the score's LJ +
+   Coulomb terms on every candidate atom, plus each candidate's energy.
+   out_force = float[3 * n_atoms]. */
+int binder_forces_allatom(binder_ctx* ctx, const binder_atom_cloud* antigen, const binder_gpu_atom* candidates,
+                          const int64_t* offsets, size_t n_cand, float* out_force, double* out_energies);
+
+/* ---- survivor selection (diffusion.rs:1042-1057) ------------------------------
+   Indices of the k lowest energies in stable ascending order (ties keep index
+   order; NaN sorts after every number). */
+int binder_topk(binder_ctx* ctx, const double* energies, size_t n, size_t k, int32_t* out_idx);
+/* independent top-k per segment [seg_offsets[s], seg_offsets[s+1]); out_idx is
+   int32[n_seg * k] of global indices, -1 where a segment has fewer than k. */
+int binder_topk_segmented(binder_ctx* ctx, const double* energies, const int64_t* seg_offsets, size_t n_seg,
+                          size_t k, int32_t* out_idx);
+
+/* ---- residue construction (rotamer.rs:198-232, 439-462; allatom.rs:502-541) ---
+   protein_from_ca_trace: ideal backbone around each Calpha and side chain placed
+   by NERF at the given chi (NULL = the top rotamer of each amino acid).
+   out_pos = float[n][14][3], out_chi = float[n][4] (may be NULL). */
+int binder_build_residues(binder_ctx* ctx, size_t n, const float* ca_xyz, const uint8_t* aa, const float* chi,
+                          float* out_pos, float* out_chi);
+
+/* ---- resident search state ---------------------------------------------------
+   The antigen protein (slot layout) for the search.  Uploads its atoms, builds
+   the all-atom grid (params.score_cell), its Calpha cloud + grid (params.ca_cell)
+   and ca_center_of_mass (allatom.rs:183-195).  Returns the antigen id (>= 0) in
+   *out_id; several antigens may be resident (batched workloads). */
+int binder_add_antigen(binder_ctx* ctx, size_t n_res, const uint8_t* aa, const float* pos, int32_t* out_id);
+int binder_clear_antigens(binder_ctx* ctx);
+/* Upload n_cand candidates into device state.  n_res[c] residues each (NULL +
+   uniform_n_res for a uniform population), concatenated in candidate order;
+   antigen_id[c] (NULL = all 0).  cand_id[c] is the Philox counter word of the
+   candidate (NULL = c). */
+int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
+                        const float* pos);
+/* Copy the device state back (same layout as the upload). */
+int binder_state_download(binder_ctx* ctx, uint8_t* aa, float* chi, float* pos);
+/* n_steps allatom_diffusion_step's (diffusion.rs:290-419) on every resident
+   candidate: CG force + restraint + clamp (+ noise when with_noise) (+ rotamer /
+   mutation / backbone Metropolis moves when with_mc).  step0 = Philox counter of
+   the first step; temps = per-step temperatures (NULL = t_hot). */
+int binder_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise, int with_mc, const float* temps);
+/* Score every resident candidate against its antigen: LJ + Coulomb + hydrophobic
+   (full = 0) or allatom_energy (diffusion.rs:281-283: + H-bond + EEF1 +
+   disulfide, full = 1).  out = double[n_cand] (host). */
+int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
+/* The phase-1 block: n_steps gradient-only steps, one score of every candidate,
+   then the k lowest per antigen (diffusion.rs:1018-1057 with scoring every
+   n_steps).  out_energies double[n_cand], out_topk int32[n_antigen * k]
+   (either may be NULL). */
+int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_energies, int32_t* out_topk);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
