@@ -1,0 +1,387 @@
+"""bench.py — throughput of the all-atom search hot path on B200.
+
+One "step" = one phase-1 block of the search (diffusion.rs:1018-1057 with
+scoring every 10 steps): 10 gradient-only allatom_diffusion_steps of every
+candidate (coarse-grained grid force, restraint, 2 A clamp, rigid residue
+translation), one all-atom LJ + Coulomb + hydrophobic score of every candidate,
+and the top-64 survivor selection.  Workload: 1024 antibodies x 20 residues
+against a 300-residue (2505-atom) compact globule, seeded synthetic inputs.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line.  value = candidate-steps/s over all ranks (device time
+with CUDA events on the library's stream, max over ranks); e2e = the same
+metric through the C ABI with host buffers (state upload, block, state +
+energies + survivors download every step).  The reference arm times the CPU
+restatement of the reference's algorithm (the Rust crate cannot be built on
+this image) with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_STEPS_PER_BLOCK = 10
+TOP_K = 64
+# Algorithmic flops per in-cutoff pair (FADD/FMUL = 1, FFMA = 2, rsqrt/sqrt/div
+# MUFU sequences not counted):
+#  all-atom score pair: dx,dy,dz 3 + r^2 5 + 1/r^2 1 + R 1 + R^2 1 + s2 1 + s6 2 +
+#    eps 1 + LJ 3 + Coulomb 2 + hydrophobic 1 + accumulate 2 = 23 -> 24 with the cutoff select
+SCORE_FLOPS_PER_PAIR = 24
+#  coarse-grained force pair (energy.rs:362-391): dx,dy,dz 3 + r^2 5 + eps 1 + sigma 2 +
+#    sigma^2 1 + s2 1 + s6 2 + s12 1 + f_lj 5 + f_total 2 + 3 x (mul + add) 6 = 29
+CG_FLOPS_PER_PAIR = 29
+FALLBACK_HBM_GBS = 6650.0
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": FALLBACK_HBM_GBS, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        self.t_start = time.time()
+
+    def mark(self, which):
+        setattr(self, which, time.time())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = []
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9], float(parts[3])))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        # samples with the GPU busy (the timed loop keeps it busy; idle samples read ~120 MHz)
+        busy = [r for r in rows if r[0] > 0.5 * r[1]] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in busy for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows), "samples_busy": len(busy),
+                "power_w_max": max(r[3] for r in rows)}
+
+
+def dist_init(world):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        dist.init_process_group(backend="cpu:gloo,cuda:nccl", timeout=timedelta(seconds=120))
+    return torch, dist
+
+
+def max_over_ranks(torch, dist, world, value, device):
+    if world == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(torch, dist, world, value, device):
+    if world == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def merge_survivors(torch, dist, world, energies, idx, rank, n_cand, k=TOP_K):
+    """Global top-k of every rank's local survivors: one all-gather of k (E, index) pairs."""
+    local = np.stack([energies[idx], (idx + rank * n_cand).astype(np.float64)], axis=1)
+    if world == 1:
+        allv = local
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(local))
+        out = [torch.zeros_like(t) for _ in range(world)]
+        dist.all_gather(out, t)
+        allv = torch.cat(out).numpy()
+    order = np.lexsort((allv[:, 1], np.where(np.isnan(allv[:, 0]), np.inf, allv[:, 0])))
+    return allv[order[:k], 1].astype(np.int64), allv[order[:k], 0]
+
+
+def build_workload(pkg, ctx, rank):
+    wl = pkg.workloads
+    cfg = wl.config1(salt=rank)
+    ag_aa, ag_ca = cfg["antigens"][0]
+    ag_pos, _ = ctx.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    p = ctx.params
+    p.shell_radius = float(cfg["shell"][0])
+    ctx.set_params(p)
+    ctx.add_antigen(ag_aa, ag_pos)
+    pop = cfg["pop"]
+    pos, chi = ctx.build_residues(pop.ca, pop.aa)
+    return cfg, ag_aa, ag_pos, pop, pos, chi
+
+
+def cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, step0):
+    """The reference algorithm on the host: 10 gradient steps (grid CG force),
+    brute-force f32 all-atom score (energy.rs:261-301 order), stable top-64."""
+    n_cand = len(aa) // n_res
+    ids = np.arange(n_cand, dtype=np.uint32)
+    for s in range(N_STEPS_PER_BLOCK):
+        A.step(prm, aa, chi, pos, n_res, ids, step0 + s, 3.0, False, False, threads=threads)
+    cands, off = [], [0]
+    for c in range(n_cand):
+        g = orc.gpu_atoms(orc.flatten(aa[c * n_res:(c + 1) * n_res], pos[c * n_res:(c + 1) * n_res]))
+        cands.append(g)
+        off.append(off[-1] + len(g))
+    e = orc.score_batch32(ag_atoms, np.concatenate(cands), np.asarray(off, np.int64), threads=threads)
+    return orc.topk(e.astype(np.float64), min(TOP_K, n_cand))
+
+
+def cpu_sample(orc, cfg, ag_aa, ag_pos, pop, target_s, threads, n_max=None):
+    """Time the reference algorithm on a bounded sample of the candidates."""
+    n_res = int(pop.n_res[0])
+    A = orc.Antigen(ag_aa, ag_pos)
+    prm = orc.OrcParams.defaults(shell_radius=float(cfg["shell"][0]))
+    ag_atoms = orc.gpu_atoms(orc.flatten(ag_aa, ag_pos))
+    n_total = pop.n_cand if n_max is None else min(n_max, pop.n_cand)
+    n = min(threads * 2, n_total)
+    while True:
+        aa = pop.aa[: n * n_res].copy()
+        pos, chi = orc.build_residues(pop.ca[: n * n_res], aa)
+        t0 = time.perf_counter()
+        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, 0)
+        dt = time.perf_counter() - t0
+        if dt > 0.25 * target_s or n >= n_total:
+            break
+        n = min(n_total, max(n * 2, int(n * 0.5 * target_s / max(dt, 1e-6))))
+    return n, dt, A, prm, ag_atoms, n_res
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_ctypes as orc
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    cfg = pkg.workloads.config1()
+    ag_aa, ag_ca = cfg["antigens"][0]
+    ag_pos, _ = orc.build_residues(ag_ca, ag_aa)
+    pop = cfg["pop"]
+    threads = os.cpu_count() or 1
+    # each step: one block over a sample sized so the whole K+W run stays within minutes
+    budget = max(0.5, min(4.0, 150.0 / max(1, args.steps + args.warmup)))
+    n, _, A, prm, ag_atoms, n_res = cpu_sample(orc, cfg, ag_aa, ag_pos, pop, budget, threads)
+    aa = pop.aa[: n * n_res].copy()
+    pos, chi = orc.build_residues(pop.ca[: n * n_res], aa)
+    for w in range(args.warmup):
+        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, w * N_STEPS_PER_BLOCK)
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads,
+                            (args.warmup + k) * N_STEPS_PER_BLOCK)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = n * N_STEPS_PER_BLOCK / (ms / 1e3)
+    sample = (f"{n} of 1024 candidates per step (10 gradient steps + brute-force f32 score + top-64), "
+              f"CPU restatement of the reference")
+    line = {"impl": "reference", "metric": "candidate-steps/s", "value": value, "unit": "candidate-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": workload_config(),
+            "cpu_baseline": {"value": value, "unit": "candidate-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "candidate-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config():
+    return {"workload": "search block: 1024 antibodies x 20 residues vs 300-residue globule (2505 atoms); "
+                        "10 gradient steps + all-atom score + top-64 per step",
+            "n_candidates": 1024, "residues_per_candidate": 20, "antigen_residues": 300,
+            "gradient_steps_per_block": N_STEPS_PER_BLOCK, "top_k": TOP_K, "score_cell_A": 8.0,
+            "cutoff_A": 10.0, "ca_cell_A": 10.0,
+            "l2": "256 MiB buffer written between timed steps (flush); working set 5 MiB",
+            "precision": "f32 pair terms, Kahan lane sums, FP64 reductions"}
+
+
+def run_ours(args, rank, world, local_rank):
+    torch, dist = dist_init(world)
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(local_rank)
+    cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, rank)
+    n_cand, n_res = pop.n_cand, int(pop.n_res[0])
+    ctx.state_upload(pop.aa, chi, pos, uniform_n_res=n_res)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    # warm-up (untimed)
+    for w in range(args.warmup):
+        ctx.block_async(N_STEPS_PER_BLOCK, w * N_STEPS_PER_BLOCK, TOP_K)
+    ctx.block_fetch(TOP_K)
+
+    # algorithmic work of the timed blocks: in-cutoff pairs (counted, untimed, state unchanged)
+    cg_pairs, score_pairs = ctx.state_pair_counts(N_STEPS_PER_BLOCK)
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    ctx.set_timing(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    step0 = args.warmup * N_STEPS_PER_BLOCK
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()  # L2 flush between timed steps, outside the timed events
+            starts[k].record(ext)
+        ctx.block_async(N_STEPS_PER_BLOCK, step0 + k * N_STEPS_PER_BLOCK, TOP_K)
+        with torch.cuda.stream(ext):
+            stops[k].record(ext)
+    e_last, top_last = ctx.block_fetch(TOP_K)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = ctx.launch_count - launches0
+    phase_ms, n_blocks = ctx.timing_summary()
+    ctx.set_timing(False)
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    ms_local = statistics.mean(step_ms)
+    ms = max_over_ranks(torch, dist, world, ms_local, device)
+    total_cand = sum_over_ranks(torch, dist, world, float(n_cand), device)
+    value = total_cand * N_STEPS_PER_BLOCK / (ms / 1e3)
+    ph = phase_ms / max(1, n_blocks)  # mean ms per launch: [gradient, score, top-k]
+    survivors, surv_e = merge_survivors(torch, dist, world, e_last, top_last[0].astype(np.int64), rank, n_cand)
+
+    # e2e through the C ABI with pinned host buffers, copies in the timed region
+    h_aa = torch.empty(n_cand * n_res, dtype=torch.uint8, pin_memory=True).numpy()
+    h_chi = torch.empty((n_cand * n_res, 4), dtype=torch.float32, pin_memory=True).numpy()
+    h_pos = torch.empty((n_cand * n_res, 14, 3), dtype=torch.float32, pin_memory=True).numpy()
+    h_e = torch.empty(n_cand, dtype=torch.float64, pin_memory=True).numpy()
+    h_top = torch.empty(TOP_K, dtype=torch.int32, pin_memory=True).numpy()
+    a0, c0, p0 = ctx.state_download()
+    h_aa[:], h_chi[:], h_pos[:] = a0, c0, p0
+    e2e_steps = max(1, min(args.steps, 200))
+    t_e2e = []
+    for k in range(e2e_steps + 1):
+        t0 = time.perf_counter()
+        ctx.state_upload(h_aa, h_chi, h_pos, uniform_n_res=n_res)
+        ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K, out_e=h_e, out_top=h_top)
+        ctx.state_download(h_aa, h_chi, h_pos)
+        if k:  # first iteration warms the pinned paths
+            t_e2e.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks(torch, dist, world, 1e3 * statistics.mean(t_e2e), device)
+    h2d = h_aa.nbytes + h_chi.nbytes + h_pos.nbytes
+    d2h = h_e.nbytes + h_top.nbytes + h_aa.nbytes + h_chi.nbytes + h_pos.nbytes
+
+    peaks, peaks_kind = load_peaks()
+    fp32_scalar, fp32_packed = ctx.fp32_peak()
+    fp32_peak = max(fp32_scalar, fp32_packed)
+    kern = {
+        "langevin_cg": {"ms": float(ph[0]), "pairs": int(cg_pairs),
+                        "tflops": CG_FLOPS_PER_PAIR * cg_pairs / (ph[0] * 1e-3) / 1e12},
+        "score_allatom": {"ms": float(ph[1]), "pairs": int(score_pairs),
+                          "tflops": SCORE_FLOPS_PER_PAIR * score_pairs / (ph[1] * 1e-3) / 1e12},
+        "topk": {"ms": float(ph[2])},
+    }
+    dom = max(("langevin_cg", "score_allatom"), key=lambda k: kern[k]["ms"])
+    achieved = kern[dom]["tflops"]
+    line = {
+        "metric": "candidate-steps/s", "value": value, "unit": "candidate-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": workload_config(),
+        "pair_evals_per_s": total_cand / n_cand * score_pairs / (ph[1] * 1e-3),
+        "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_source": "FP32 FMA microbenchmark on this GPU (max of scalar/f32x2), "
+                                    f"scalar {fp32_scalar:.1f}, packed {fp32_packed:.1f}; "
+                                    f"nominal {148 * 128 * 2 * 1.965e-3:.1f} at 1965 MHz",
+                     "flops_per_pair": SCORE_FLOPS_PER_PAIR if dom == "score_allatom" else CG_FLOPS_PER_PAIR},
+        "kernels": kern,
+        "e2e": {"value": total_cand * N_STEPS_PER_BLOCK / (e2e_ms / 1e3), "unit": "candidate-steps/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "api": "binder_state_upload + binder_block + binder_state_download, pinned host buffers"},
+        "clocks": clocks, "gpu_launches": int(launches),
+        "survivors": {"best_energy": float(surv_e[0]), "best_index": int(survivors[0])},
+        "hbm_peak_gbs": peaks.get("hbm_gbs"), "peaks_file": peaks_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_ctypes as orc
+        threads = os.cpu_count() or 1
+        n, dt, *_ = cpu_sample(orc, cfg, ag_aa, np.ascontiguousarray(ag_pos), pop, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": n * N_STEPS_PER_BLOCK / dt, "unit": "candidate-steps/s", "cores": threads,
+                                "kind": "port",
+                                "sample": f"one block (10 gradient steps + brute-force f32 score + top-64) over "
+                                          f"{n} of 1024 candidates, {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

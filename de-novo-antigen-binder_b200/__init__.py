@@ -120,6 +120,12 @@ _SIGS = {
     "binder_diffuse": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_int, C.c_void_p]),
     "binder_score_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "binder_block": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
+    "binder_stream": (C.c_void_p, [C.c_void_p]),
+    "binder_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "binder_timing_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
+    "binder_block_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_state_pair_counts": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "binder_fp32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 
@@ -443,11 +449,12 @@ class GpuContext:
         self._state_res = len(aa)
         self._state_cand = n_cand
 
-    def state_download(self):
+    def state_download(self, aa=None, chi=None, pos=None):
+        """Device state -> host (optionally into caller-provided, e.g. pinned, arrays)."""
         n = self._state_res
-        aa = np.zeros(n, np.uint8)
-        chi = np.zeros((n, 4), np.float32)
-        pos = np.zeros((n, SLOTS, 3), np.float32)
+        aa = np.zeros(n, np.uint8) if aa is None else aa
+        chi = np.zeros((n, 4), np.float32) if chi is None else chi
+        pos = np.zeros((n, SLOTS, 3), np.float32) if pos is None else pos
         self._check(lib().binder_state_download(self._h, _ptr(aa), _ptr(chi), _ptr(pos)))
         return aa, chi, pos
 
@@ -460,11 +467,47 @@ class GpuContext:
         self._check(lib().binder_score_state(self._h, int(full), _ptr(out)))
         return out
 
-    def block(self, n_steps, step0=0, k=64, n_segments=1):
-        e = np.zeros(self._state_cand, np.float64)
-        top = np.zeros(n_segments * k, np.int32) if k else None
+    def block(self, n_steps, step0=0, k=64, n_segments=1, out_e=None, out_top=None):
+        e = np.zeros(self._state_cand, np.float64) if out_e is None else out_e
+        top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
         self._check(lib().binder_block(self._h, n_steps, step0, k, _ptr(e), _ptr(top)))
         return e, (top.reshape(n_segments, k) if k else None)
+
+    def block_async(self, n_steps, step0=0, k=64):
+        """Enqueue one block on the context stream; results stay on the device."""
+        self._check(lib().binder_block(self._h, n_steps, step0, k, None, None))
+
+    def block_fetch(self, k=64, n_segments=1, out_e=None, out_top=None):
+        e = np.zeros(self._state_cand, np.float64) if out_e is None else out_e
+        top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
+        self._check(lib().binder_block_fetch(self._h, _ptr(e), _ptr(top)))
+        return e, (top.reshape(n_segments, k) if k else None)
+
+    # -- instrumentation --
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        return int(lib().binder_stream(self._h) or 0)
+
+    def set_timing(self, on=True):
+        self._check(lib().binder_set_timing(self._h, int(on)))
+
+    def timing_summary(self):
+        """(summed [gradient, scoring, top-k] ms, number of blocks) since set_timing."""
+        out = np.zeros(3, np.float64)
+        n = C.c_int32()
+        self._check(lib().binder_timing_summary(self._h, _ptr(out), C.byref(n)))
+        return out, n.value
+
+    def state_pair_counts(self, n_steps):
+        a, b = C.c_int64(), C.c_int64()
+        self._check(lib().binder_state_pair_counts(self._h, n_steps, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def fp32_peak(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(lib().binder_fp32_peak(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
 
 def temperature(iteration, total, t_hot=3.0, t_cold=0.02):

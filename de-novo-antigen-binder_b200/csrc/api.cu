@@ -149,7 +149,18 @@ struct binder_ctx {
     size_t last_n_cand = 0;
     bool last_batch_valid = false;
     State st;
+    // per-phase event timing of binder_block: a ring of 4 events per block
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    int ev_blocks = 0;
+    int last_k = 0;
+    bool async_pending = false;
+    ~binder_ctx() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
 };
+static const int TIMING_RING = 4096;
 
 namespace {
 
@@ -1058,20 +1069,129 @@ int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* ou
     State& S = ctx->st;
     if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
     if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
-    if ((s = clear_err(ctx))) return s;
+    const bool async = out_e == nullptr && out_topk == nullptr;
+    // the device error word accumulates over a run of enqueued blocks until fetched
+    if (!ctx->async_pending && (s = clear_err(ctx))) return s;
+    ctx->async_pending = async;
+    const bool tm = ctx->timing && ctx->ev_blocks < TIMING_RING;
+    cudaEvent_t* ev = tm ? &ctx->ev[4 * ctx->ev_blocks] : nullptr;
+    if (tm) CK(cudaEventRecord(ev[0], ctx->stream), "event");
     if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, step0, 0, 0, nullptr))) return s;
+    if (tm) CK(cudaEventRecord(ev[1], ctx->stream), "event");
     if ((s = enqueue_score_state(ctx, 0))) return s;
+    if (tm) CK(cudaEventRecord(ev[2], ctx->stream), "event");
     if (k > 0) {
         CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
         launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
                              ctx->topk.p);
         LAUNCHED("topk");
-        if (out_topk)
-            CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * k * sizeof(int), cudaMemcpyDeviceToHost,
-                               ctx->stream),
-               "D2H");
     }
+    if (tm) {
+        CK(cudaEventRecord(ev[3], ctx->stream), "event");
+        ctx->ev_blocks++;
+    }
+    ctx->last_k = k;
+    if (async) return BINDER_OK;
+    return binder_block_fetch(ctx, out_e, out_topk);
+}
+
+int binder_block_fetch(binder_ctx* ctx, double* out_e, int32_t* out_topk) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    ctx->async_pending = false;
+    if (ctx->last_k > 0 && out_topk)
+        CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * ctx->last_k * sizeof(int),
+                           cudaMemcpyDeviceToHost, ctx->stream),
+           "D2H");
     return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);
+}
+
+void* binder_stream(binder_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int binder_set_timing(binder_ctx* ctx, int on) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (ctx->ev.empty()) {
+        ctx->ev.assign(4 * TIMING_RING, nullptr);
+        for (auto& e : ctx->ev) CK(cudaEventCreate(&e), "event");
+    }
+    ctx->timing = on != 0;
+    ctx->ev_blocks = 0;
+    return BINDER_OK;
+}
+
+int binder_timing_summary(binder_ctx* ctx, double* sums, int32_t* n_blocks) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!sums) return fail(ctx, BINDER_ERR_ARG, "NULL out");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    sums[0] = sums[1] = sums[2] = 0.0;
+    for (int b = 0; b < ctx->ev_blocks; ++b)
+        for (int i = 0; i < 3; ++i) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->ev[4 * b + i], ctx->ev[4 * b + i + 1]), "event");
+            sums[i] += ms;
+        }
+    if (n_blocks) *n_blocks = ctx->ev_blocks;
+    ctx->ev_blocks = 0;
+    return BINDER_OK;
+}
+
+int binder_state_pair_counts(binder_ctx* ctx, int n_steps, int64_t* out_cg, int64_t* out_score) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    CK(ctx->pairs.ensure(2), "alloc");
+    CK(cudaMemsetAsync(ctx->pairs.p, 0, 2 * sizeof(long long), ctx->stream), "memset");
+    if ((s = clear_err(ctx))) return s;
+    launch_diffuse_count(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, ctx->pairs.p);
+    if (n_steps > 0) LAUNCHED("diffuse_count");
+    launch_score_state_count(ctx->stream, S.view(), ctx->d_views.p, ctx->pairs.p + 1, ctx->errf.p,
+                             grid_ctas(ctx, S.n_cand));
+    LAUNCHED("score_state_count");
+    long long h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, ctx->pairs.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if ((s = check_err(ctx))) return s;
+    if (out_cg) *out_cg = h[0];
+    if (out_score) *out_score = h[1];
+    return BINDER_OK;
+}
+
+int binder_fp32_peak(binder_ctx* ctx, double* scalar, double* packed) {
+    int s = enter(ctx);
+    if (s) return s;
+    DBuf<float> scratch;
+    const int ctas = ctx->num_sms * 8;
+    CK(scratch.ensure(ctas), "alloc");
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a), "event");
+    CK(cudaEventCreate(&b), "event");
+    for (int v = 0; v < 2; ++v) {
+        double best = 0.0;
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(a, ctx->stream);
+            const double flops = launch_ffma(ctx->stream, scratch.p, ctas, 2048, v == 1);
+            ctx->launches++;
+            cudaEventRecord(b, ctx->stream);
+            cudaError_t e = cudaEventSynchronize(b);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                return cuda_fail(ctx, e, "ffma");
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+        }
+        if (v == 0 && scalar) *scalar = best;
+        if (v == 1 && packed) *packed = best;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return BINDER_OK;
 }
 
 }  // extern "C"

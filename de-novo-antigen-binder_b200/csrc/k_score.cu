@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(NW * 32) k_score_flat(const float4* __restrict
         double ea = 0.0;
         if (ABS) ea = cta_sum<NW>((double)acc.abs_s, sm2, lane, warp);
         if (threadIdx.x == 0) {
-            out[c] = e;
+            if (out) out[c] = e;
             if (ABS) out_abs[c] = ea;
         }
         if (COUNT) my_pairs += acc.pairs;
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(NW * 32) k_score_state(StateView st, const AgV
             }
         }
         if (threadIdx.x == 0) {
-            out[c] = e;
+            if (out) out[c] = e;
             if (ABS) out_abs[c] = ea;
         }
         if (COUNT) my_pairs += acc.pairs;
@@ -353,6 +353,14 @@ int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, i
     }
 #undef BINDER_STATE
     return 1;
+}
+
+void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,
+                              uint32_t* err, int grid_ctas) {
+    if (st.n_cand <= 0) return;
+    const int g = grid_ctas > 0 ? min(grid_ctas, st.n_cand) : st.n_cand;
+    k_score_state<NW_SCORE, true, false, false, true>
+        <<<g, NW_SCORE * 32, 0, s>>>(st, ags, nullptr, nullptr, pairs, err);
 }
 
 }  // namespace binder

@@ -167,7 +167,9 @@ __global__ void k_build_residues(int n, const float* __restrict__ ca_xyz, const 
 // ---- coarse-grained force (energy.rs:322-398), reference f32 order ---------------
 struct CgB { float x, y, z, q, eps, sig; float hyd; };
 
-__device__ __forceinline__ void cg_force(const AgView& A, const CgB& b, float& fx, float& fy, float& fz) {
+template <bool COUNT = false>
+__device__ __forceinline__ void cg_force(const AgView& A, const CgB& b, float& fx, float& fy, float& fz,
+                                         int* n_pairs = nullptr) {
     const GridView& g = A.ca_grid;
     const int cx = cell_coord(b.x, g.inv), cy = cell_coord(b.y, g.inv), cz = cell_coord(b.z, g.inv);
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
@@ -182,6 +184,7 @@ __device__ __forceinline__ void cg_force(const AgView& A, const CgB& b, float& f
                     const float ddx = xsub(b.x, apq.x), ddy = xsub(b.y, apq.y), ddz = xsub(b.z, apq.z);
                     const float r_sq = xdist2(ddx, ddy, ddz);
                     if (r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ) continue;
+                    if (COUNT) ++*n_pairs;
                     const float eps_ij = xsqrt(xmul(b.eps, aprm.x));
                     const float sig_ij = xmul(0.5f, xadd(b.sig, aprm.y));
                     const float sigma_sq = xmul(sig_ij, sig_ij);
@@ -221,9 +224,12 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 
 // ---- Langevin steps without Metropolis moves (diffusion.rs:306-339) ----------------
 // One thread per residue; the residue's atoms stay in registers for n_steps.
+// COUNT: count the in-cutoff CG pairs of the same trajectory, leave the state as is.
+template <bool COUNT>
 __global__ void __launch_bounds__(128) k_langevin(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                    int n_steps, uint32_t step0, int with_noise,
-                                                   const float* __restrict__ temps, uint32_t* __restrict__ err) {
+                                                   const float* __restrict__ temps, uint32_t* __restrict__ err,
+                                                   long long* __restrict__ pair_count) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= st.total_res) return;
     const int c = st.res_cand[r];
@@ -239,12 +245,13 @@ __global__ void __launch_bounds__(128) k_langevin(StateView st, const AgView* __
         const float4 v = k < n_at ? slot[k] : make_float4(0.f, 0.f, 0.f, 0.f);
         at[k] = {v.x, v.y, v.z};
     }
-    if (!isfinite(at[1].x) || !isfinite(at[1].y) || !isfinite(at[1].z)) atomicOr(err, ERRF_NAN);
+    if (err && (!isfinite(at[1].x) || !isfinite(at[1].y) || !isfinite(at[1].z))) atomicOr(err, ERRF_NAN);
     const float4 res = s_res[aa];
+    int n_pairs = 0;
     for (int s = 0; s < n_steps; ++s) {
         const F3 ca = at[1];  // Calpha is topology atom 1 of every residue (amber.rs:358-377)
         float fx, fy, fz;
-        cg_force(A, CgB{ca.x, ca.y, ca.z, res.x, res.y, res.z, res.w}, fx, fy, fz);
+        cg_force<COUNT>(A, CgB{ca.x, ca.y, ca.z, res.x, res.y, res.z, res.w}, fx, fy, fz, &n_pairs);
         // harmonic restraint toward the shell (diffusion.rs:317-327)
         const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
         const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
@@ -273,6 +280,10 @@ __global__ void __launch_bounds__(128) k_langevin(StateView st, const AgView* __
             if (k < n_at) at[k] = {xadd(at[k].x, delta.x), xadd(at[k].y, delta.y), xadd(at[k].z, delta.z)};
         }
     }
+    if (COUNT) {
+        atomicAdd((unsigned long long*)pair_count, (unsigned long long)n_pairs);
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < SLOTS; ++k)
         if (k < n_at) slot[k] = make_float4(at[k].x, at[k].y, at[k].z, 0.f);
@@ -293,7 +304,14 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
                     uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err) {
     if (st.total_res <= 0 || n_steps <= 0) return;
     (void)with_mc;
-    k_langevin<<<(st.total_res + 127) / 128, 128, 0, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err);
+    k_langevin<false>
+        <<<(st.total_res + 127) / 128, 128, 0, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, nullptr);
+}
+
+void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                          long long* pairs) {
+    if (st.total_res <= 0 || n_steps <= 0) return;
+    k_langevin<true><<<(st.total_res + 127) / 128, 128, 0, s>>>(st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs);
 }
 
 }  // namespace binder

@@ -55,6 +55,15 @@ void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const f
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err);
 void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);
+// pair counting (same trajectory as launch_diffuse with noise off, state not written)
+void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                          long long* pairs);
+// state scoring pair count
+void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,
+                              uint32_t* err, int grid_ctas);
+
+// ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
+double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);
 void launch_unpack_slots(cudaStream_t s, int n_res, const float4* in, float* out);
 
 }  // namespace binder

@@ -124,11 +124,14 @@ def _globule_antigen(n_res, rng):
     return random_sequence(n_res, rng), ca, radius
 
 
-def config1(n_cand=1024, n_res=20):
+def config1(n_cand=1024, n_res=20, salt=0):
+    """salt != 0 draws an independent antibody population against the same antigen."""
     rng = rng_for(1)
     ag_aa, ag_ca, radius = _globule_antigen(300, rng)
     shell = radius + 4.0
     c = ca_center(ag_ca)
+    if salt:
+        rng = rng_for(1, salt)
     ca = sphere_points(n_cand * n_res, shell, c, rng)
     aa = random_sequence(n_cand * n_res, rng)
     pop = Population(ca, aa, np.full(n_cand, n_res, np.int32), np.zeros(n_cand, np.int32))

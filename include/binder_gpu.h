@@ -229,9 +229,28 @@ int binder_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise,
 int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
 /* The phase-1 block: n_steps gradient-only steps, one score of every candidate,
    then the k lowest per antigen (diffusion.rs:1018-1057 with scoring every
-   n_steps).  out_energies double[n_cand], out_topk int32[n_antigen * k]
-   (either may be NULL). */
+   n_steps).  out_energies double[n_cand], out_topk int32[n_antigen * k].  When
+   both are NULL the block is only enqueued on the context stream (no host
+   synchronisation); binder_block_fetch then returns the results of the last
+   block and reports any device error. */
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_energies, int32_t* out_topk);
+int binder_block_fetch(binder_ctx* ctx, double* out_energies, int32_t* out_topk);
+
+/* ---- instrumentation (no reference counterpart) --------------------------------
+   The context's CUDA stream (cudaStream_t), for callers that time or order work
+   around the library's launches. */
+void* binder_stream(binder_ctx* ctx);
+/* With timing on, binder_block records CUDA events on the context stream around
+   each of its phases (up to 4096 blocks).  binder_timing_summary synchronises,
+   returns the summed [gradient steps, scoring, top-k] milliseconds and the
+   number of blocks recorded since binder_set_timing, and restarts the record. */
+int binder_set_timing(binder_ctx* ctx, int on);
+int binder_timing_summary(binder_ctx* ctx, double* out_ms_sums, int32_t* out_blocks);
+/* In-cutoff pair counts of the resident state: Calpha pairs of n_steps gradient
+   steps (state left unchanged) and all-atom pairs of one scoring. */
+int binder_state_pair_counts(binder_ctx* ctx, int n_steps, int64_t* out_cg_pairs, int64_t* out_score_pairs);
+/* FP32 FMA throughput of the device (TFLOP/s), scalar and packed f32x2. */
+int binder_fp32_peak(binder_ctx* ctx, double* out_tflops_scalar, double* out_tflops_packed);
 
 #ifdef __cplusplus
 }

@@ -74,7 +74,7 @@ def test_grid_neighbors_bit_exact(ctx, oracle, cell, n_ag, n_q):
 
 
 def test_grid_far_probe_and_huge_box(ctx, oracle, pkg):
-    ag = np.float32([[0, 0, 0], [1e4, 0, 0]])
+    ag = np.float32([[0, 0, 0], [1e5, 0, 0]])  # 1e8 cells of 1 mA > 2^24 cap
     with pytest.raises(pkg.BinderError) as e:
         ctx.grid_neighbors(0.001, ag[:, 0], ag[:, 1], ag[:, 2], [0.0], [0.0], [0.0])
     assert e.value.status == 6  # BINDER_ERR_GRID
