@@ -173,6 +173,29 @@ int binder_grid_neighbors(binder_ctx* ctx, float cell, const float* ax, const fl
                           size_t n_ag, const float* px, const float* py, const float* pz, size_t n_q,
                           int64_t* out_offsets, uint32_t* out_idx, size_t cap, size_t* out_total);
 
+/* No counterpart in the reference.  binder_grid_neighbors for callers that
+   cannot allocate device memory: hosts that own all device memory through their
+   own pool or arena and cannot let a library call cudaMalloc/cudaFree, or loops
+   where an allocation would stall the device.  Inputs (antigen points, probe
+   points) and outputs (offsets int64[n_q+1], indices uint32[cap]) are device
+   buffers owned by the caller; the kernels' scratch lives in one fixed-size
+   device array inside the library (about 4.3 MB, held on every GPU that loads
+   the library until the process exits).  No context is needed; work is enqueued
+   on `stream` (a cudaStream_t, 0 = legacy default stream) and the call returns
+   once the neighbour-list fill is enqueued.  Results equal binder_grid_neighbors.
+   Limits: n_ag <= BINDER_NOALLOC_MAX_ATOMS (else BINDER_ERR_ARG) and the box of
+   occupied cells <= BINDER_NOALLOC_MAX_CELLS (else BINDER_ERR_GRID);
+   BINDER_ERR_CAPACITY with *out_total set when cap is too small.  Every call
+   shares the scratch array: calls whose GPU work overlaps (different streams or
+   threads) race.  The first call on a device looks the array up on that device
+   (make it before any stream capture).  */
+#define BINDER_NOALLOC_MAX_ATOMS 65536
+#define BINDER_NOALLOC_MAX_CELLS 262144
+int binder_grid_neighbors_noalloc(float cell, const float* d_ax, const float* d_ay, const float* d_az,
+                                  size_t n_ag, const float* d_px, const float* d_py, const float* d_pz,
+                                  size_t n_q, int64_t* d_out_offsets, uint32_t* d_out_idx, size_t cap,
+                                  size_t* out_total, void* stream);
+
 /* ---- forces ------------------------------------------------------------------
    compute_forces_with_grid (energy.rs:322-398): coarse-grained (Calpha) force on
    every antibody residue from the antigen residues found by the 27-cell probe of
