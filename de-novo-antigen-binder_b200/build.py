@@ -73,7 +73,8 @@ def build(force=False, verbose=False, extra_flags=()):
         raise RuntimeError("nvcc build failed")
     objs = [BUILD / (s.stem + ".o") for s in sources]
     if force or jobs or _stale(LIB, objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIB)] + [str(o) for o in objs]
+        cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-Xlinker", "--no-undefined", "-o", str(LIB)] + \
+            [str(o) for o in objs]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

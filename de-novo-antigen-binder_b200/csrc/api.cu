@@ -81,6 +81,7 @@ struct Antigen {
     DBuf<uint8_t> caa;
     GridBuf ca_grid;
     DBuf<float4> ca_pq, ca_prm, ca_atom, ca_atom_prm;
+    DBuf<int4> ca_cell;
     AgView view{};
 };
 
@@ -94,6 +95,13 @@ struct State {
     DBuf<float> stage;  // packed slot staging for upload/download
     std::vector<int> h_res_off;
     int n_segments = 0;
+    // residue order by Calpha cell for the Langevin kernel
+    DBuf<int> key_base, keys, key_counts, key_cursor, order;
+    int n_keys = 0;
+    bool order_valid = false;
+    // scoring work queue and per-residue energies
+    DBuf<int> queue;
+    DBuf<double> res_e, res_abs;
     StateView view() {
         StateView v;
         v.n_cand = n_cand;
@@ -314,11 +322,13 @@ int build_antigen_ca(binder_ctx* ctx, Antigen& A, const float* x, const float* y
     if ((s = build_grid(ctx, A.cax.p, A.cay.p, A.caz.p, (int)n, cell, A.ca_grid))) return s;
     CK(A.ca_pq.ensure(n), "ca alloc");
     CK(A.ca_prm.ensure(n), "ca alloc");
+    CK(A.ca_cell.ensure(n), "ca alloc");
     launch_gather_ca(ctx->stream, A.ca_grid.sorted_idx.p, (int)n, A.cax.p, A.cay.p, A.caz.p, A.caa.p,
-                     ctx->d_res_tab.p, A.ca_pq.p, A.ca_prm.p);
+                     ctx->d_res_tab.p, A.ca_grid.view.inv, A.ca_pq.p, A.ca_prm.p, A.ca_cell.p);
     if (n > 0) LAUNCHED("gather_ca");
     A.view.ca_pq = A.ca_pq.p;
     A.view.ca_prm = A.ca_prm.p;
+    A.view.ca_cell = A.ca_cell.p;
     A.view.ca_grid = A.ca_grid.view;
     A.view.n_res = (int)n;
     return BINDER_OK;
@@ -972,6 +982,24 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
     launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
     if (total) LAUNCHED("pack_slots");
+    // sort keys: one range of Calpha-grid cells per antigen
+    std::vector<int> kb(n_ag);
+    int nk = 0;
+    for (int a = 0; a < n_ag; ++a) {
+        kb[a] = nk;
+        const GridView& g = ctx->ags[a]->view.ca_grid;
+        nk += (g.nx + 2 * RES_KEY_MARGIN) * (g.ny + 2 * RES_KEY_MARGIN) * (g.nz + 2 * RES_KEY_MARGIN);
+    }
+    S.n_keys = nk;
+    if ((s = upload(ctx, S.key_base, kb.data(), kb.size(), "state"))) return s;
+    CK(S.keys.ensure(std::max(total, 1)), "alloc");
+    CK(S.order.ensure(std::max(total, 1)), "alloc");
+    CK(S.key_counts.ensure(nk + 1), "alloc");
+    CK(S.key_cursor.ensure(nk + 1), "alloc");
+    CK(S.queue.ensure(1), "alloc");
+    CK(S.res_e.ensure(std::max(total, 1)), "alloc");
+    CK(S.res_abs.ensure(std::max(total, 1)), "alloc");
+    S.order_valid = false;
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
     return BINDER_OK;
 }
@@ -1016,24 +1044,49 @@ StepParams step_params(const binder_params& p) {
     return s;
 }
 
+// residues sorted by (antigen, Calpha cell): thread order of the Langevin kernel and
+// visiting order of the scoring work queue
+int enqueue_order(binder_ctx* ctx) {
+    State& S = ctx->st;
+    launch_residue_order(ctx->stream, S.view(), ctx->d_views.p, S.key_base.p, S.n_keys, S.keys.p, S.key_counts.p,
+                         S.key_cursor.p, S.order.p);
+    ctx->launches += 3;
+    LAUNCHED("residue_order");
+    S.order_valid = true;
+    return BINDER_OK;
+}
+
 int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise, int with_mc, const float* temps) {
     State& S = ctx->st;
     if (temps) {
         int s = upload(ctx, ctx->temps, temps, (size_t)n_steps, "temps H2D");
         if (s) return s;
     }
+    int s = enqueue_order(ctx);
+    if (s) return s;
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise, with_mc,
-                   temps ? ctx->temps.p : nullptr, ctx->errf.p);
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
 
+StateScoreScratch score_scratch(binder_ctx* ctx) {
+    State& S = ctx->st;
+    return StateScoreScratch{S.order_valid ? S.order.p : nullptr, S.queue.p, S.res_e.p, S.res_abs.p};
+}
+
+int persistent_ctas(binder_ctx* ctx) { return ctx->num_sms * 4; }
+
 int enqueue_score_state(binder_ctx* ctx, int full) {
     State& S = ctx->st;
     CK(ctx->energy.ensure(S.n_cand), "alloc");
+    if (!S.order_valid) {
+        int s = enqueue_order(ctx);
+        if (s) return s;
+    }
     ScoreOut o{ctx->energy.p, nullptr, nullptr, nullptr, ctx->errf.p};
-    launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
-                       grid_ctas(ctx, S.n_cand), 256);
+    ctx->launches += launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
+                                        score_scratch(ctx), persistent_ctas(ctx)) - 1;
     LAUNCHED("score_state");
     return BINDER_OK;
 }
@@ -1150,7 +1203,7 @@ int binder_state_pair_counts(binder_ctx* ctx, int n_steps, int64_t* out_cg, int6
     launch_diffuse_count(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, ctx->pairs.p);
     if (n_steps > 0) LAUNCHED("diffuse_count");
     launch_score_state_count(ctx->stream, S.view(), ctx->d_views.p, ctx->pairs.p + 1, ctx->errf.p,
-                             grid_ctas(ctx, S.n_cand));
+                             score_scratch(ctx), persistent_ctas(ctx));
     LAUNCHED("score_state_count");
     long long h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, ctx->pairs.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "D2H");

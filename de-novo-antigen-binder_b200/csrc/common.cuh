@@ -35,6 +35,9 @@ constexpr float CA_C_BOND = 1.52f;
 constexpr float C_O_BOND = 1.23f;
 constexpr float CA_CB_BOND = 1.52f;
 
+// residue sort keys cover the antigen's Calpha-grid box widened by this many cells
+constexpr int RES_KEY_MARGIN = 3;
+
 // error flags a kernel may raise (read back by the host after the launch)
 enum : uint32_t { ERRF_NAN = 1u, ERRF_TIMEOUT = 2u, ERRF_RANGE = 4u };
 
@@ -110,6 +113,7 @@ struct AgView {
     // Calpha cloud (run_allatom ag_ca, diffusion.rs:994-1002) sorted by CA-grid cell
     const float4* ca_pq;   // x, y, z, residue-level charge (atom.rs:55-63)
     const float4* ca_prm;  // residue-level epsilon, sigma, hydrophobic, 0
+    const int4* ca_cell;   // CA-grid cell of each sorted Calpha
     GridView ca_grid;
     // Calpha atoms in residue order with their AMBER parameters (diffusion.rs:440-446)
     const float4* ca_atom;      // x, y, z, partial charge

@@ -111,13 +111,15 @@ __global__ void k_gather_atoms(const int* __restrict__ sorted_idx, int n, const 
 // Residue-level Calpha records (ResidueCloud::push, atom.rs:221-231) in grid order.
 __global__ void k_gather_ca(const int* __restrict__ sorted_idx, int n, const float* __restrict__ x,
                             const float* __restrict__ y, const float* __restrict__ z, const uint8_t* __restrict__ aa,
-                            const float4* __restrict__ res_tab, float4* __restrict__ pq, float4* __restrict__ prm) {
+                            const float4* __restrict__ res_tab, float inv, float4* __restrict__ pq,
+                            float4* __restrict__ prm, int4* __restrict__ cells) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     int i = sorted_idx[j];
     float4 t = res_tab[aa[i]];  // charge, epsilon, sigma, hydrophobic
     pq[j] = make_float4(x[i], y[i], z[i], t.x);
     prm[j] = make_float4(t.y, t.z, t.w, __int_as_float(i));
+    cells[j] = make_int4(cell_coord(x[i], inv), cell_coord(y[i], inv), cell_coord(z[i], inv), 0);
 }
 
 // ---- 27-cell probe in the reference's callback order (probe_cell, common.cuh) ----
@@ -183,8 +185,8 @@ void launch_gather_atoms(cudaStream_t s, const int* sorted_idx, int n, const flo
     if (n > 0) k_gather_atoms<<<nblk(n, 256), 256, 0, s>>>(sorted_idx, n, x, y, z, q, rmh, eps, hyd, type, pq, prm);
 }
 void launch_gather_ca(cudaStream_t s, const int* sorted_idx, int n, const float* x, const float* y, const float* z,
-                      const uint8_t* aa, const float4* res_tab, float4* pq, float4* prm) {
-    if (n > 0) k_gather_ca<<<nblk(n, 256), 256, 0, s>>>(sorted_idx, n, x, y, z, aa, res_tab, pq, prm);
+                      const uint8_t* aa, const float4* res_tab, float inv, float4* pq, float4* prm, int4* cells) {
+    if (n > 0) k_gather_ca<<<nblk(n, 256), 256, 0, s>>>(sorted_idx, n, x, y, z, aa, res_tab, inv, pq, prm, cells);
 }
 void launch_nb_count(cudaStream_t s, const GridView& g, const float* px, const float* py, const float* pz, int n_q,
                      long long* counts) {

@@ -184,6 +184,281 @@ __device__ __forceinline__ double cta_sum(double v, double* sm, int lane, int wa
     return t;
 }
 
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// ---- grouped scoring: one warp per group of <= 16 nearby candidate atoms ----------
+// A group (a residue of the resident state, or 8 consecutive GpuAtoms) sits in
+// shared memory.  The warp walks the grid columns within 10 A + group radius of
+// the group centre (warp-uniform loop, lanes stride a column's contiguous atom
+// range), keeps the antigen atoms that pass a sphere test in a per-warp queue, and
+// evaluates full batches of 32 queued atoms against every group atom — so the
+// pair math never runs on idle lanes.  Every lane visits its antigen atoms in
+// increasing grid order, which keeps the sums deterministic.
+constexpr int GMAX = 16;
+constexpr int FLAT_GROUP = 8;
+
+struct GroupSmem {
+    float4 pos[GMAX];  // x, y, z, q*sqrt(332)
+    float4 prm[GMAX];  // r_min_half, sqrt(epsilon), hydrophobic, AMBER type
+    int q[64];         // queued antigen atom indices
+};
+
+struct SrcStateG {
+    StateView st;
+    __device__ int ag(int c) const { return st.cand_ag[c]; }
+    __device__ int n_groups(int c) const { return st.cand_res_off[c + 1] - st.cand_res_off[c]; }
+    __device__ int load(int c, int g, int lane, GroupSmem& s, bool& bad) const {
+        const int r = st.cand_res_off[c] + g;
+        const int aa = st.res_aa[r];
+        const int n = c_topo_n[aa];
+        if (lane < n) {
+            const float4 p = st.res_pos[(size_t)r * SLOT_STRIDE + lane];
+            const float4 m = c_slot_prm[aa][lane];
+            bad = !finite3(p.x, p.y, p.z);
+            s.pos[lane] = make_float4(p.x, p.y, p.z, m.x);
+            s.prm[lane] = make_float4(m.y, m.z, m.w, (float)c_slot_type[aa][lane]);
+        }
+        return n;
+    }
+};
+
+struct SrcFlatG {
+    const float4* atoms;  // binder_gpu_atom = 2 x float4
+    const long long* off;
+    const int* cand_ag;
+    __device__ int ag(int c) const { return cand_ag ? cand_ag[c] : 0; }
+    __device__ int n_groups(int c) const {
+        return (int)((off[c + 1] - off[c] + FLAT_GROUP - 1) / FLAT_GROUP);
+    }
+    __device__ int load(int c, int g, int lane, GroupSmem& s, bool& bad) const {
+        const long long j0 = off[c] + (long long)g * FLAT_GROUP;
+        const int n = (int)min((long long)FLAT_GROUP, off[c + 1] - j0);
+        if (lane < n) {
+            const float4 p0 = __ldg(&atoms[2 * (j0 + lane)]);
+            const float4 p1 = __ldg(&atoms[2 * (j0 + lane) + 1]);
+            bad = !finite3(p0.x, p0.y, p0.z);
+            s.pos[lane] = make_float4(p0.x, p0.y, p0.z, p0.w * SQRT_COULOMB_K);
+            s.prm[lane] = make_float4(p1.x, sqrtf(p1.y), p1.z > 0.5f ? 1.0f : 0.0f, 0.0f);
+        }
+        return n;
+    }
+};
+
+// One antigen atom (this lane's) against the n group atoms in shared memory.
+template <bool KAHAN, bool FULL, bool ABS, bool COUNT>
+__device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const float4* __restrict__ prm,
+                                            const GroupSmem& s, int n, int idx, Acc& acc) {
+    const float4 a = __ldg(&pq[idx]);
+    const float4 ap = __ldg(&prm[idx]);
+    float part = 0.0f, pabs = 0.0f;
+    int np = 0;
+    for (int j = 0; j < n; ++j) {
+        const float4 b = s.pos[j];
+        const float4 bp = s.prm[j];
+        const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+        const float r2 = xdist2(dx, dy, dz);  // reference rounding: same pair set
+        if (r2 <= CUTOFF_SQ && r2 >= MIN_R_SQ) {
+            const float ir = rsqrtf(r2);
+            const float ir2 = ir * ir;
+            const float R = bp.x + ap.x;
+            const float s2 = R * R * ir2;
+            const float s6 = s2 * s2 * s2;
+            const float lj = (bp.y * ap.y) * (s6 * (s6 - 2.0f));
+            const float coul = (b.w * a.w) * ir;
+            const float hyd = (r2 < HYDRO_CUTOFF_SQ) ? HYDRO_BONUS * (bp.z * ap.z) : 0.0f;
+            float e = lj + coul + hyd;
+            if (FULL) {
+                const int bt = (int)bp.w, at = (int)ap.w;
+                if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) &&
+                    r2 <= HB_CUTOFF_SQ) {
+                    const float z = (r2 * ir - HB_R0) / HB_SIGMA;
+                    e += -HB_DEPTH * __expf(-0.5f * z * z);
+                }
+                const float4 ej = c_eef1[bt];
+                if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
+                    const float4 ei = c_eef1[at];
+                    const float r = r2 * ir;
+                    const float xi = r / ei.z, xj = r / ej.z;
+                    e += -(ei.x * ej.y * __expf(-(xi * xi)) * ei.w + ej.x * ei.y * __expf(-(xj * xj)) * ej.w);
+                }
+            }
+            part += e;
+            if (ABS) pabs += fabsf(lj) + fabsf(coul) + fabsf(hyd);
+            if (COUNT) ++np;
+        }
+    }
+    acc_add<KAHAN>(acc, part);
+    if (ABS) acc.abs_s += pabs;
+    if (COUNT) acc.pairs += np;
+}
+
+// Everything one warp does for one group already in shared memory (n atoms): centre
+// and radius, warp-uniform walk over the culled grid columns, sphere prefilter into
+// the queue, batched pair evaluation.  Accumulates into the lane's acc.
+template <bool KAHAN, bool FULL, bool ABS, bool COUNT>
+__device__ __forceinline__ void score_group(const AgView* __restrict__ Ap, GroupSmem& s, int n, int lane,
+                                            unsigned lt, Acc& acc) {
+    const float4* __restrict__ pq = Ap->pq;
+    const float4* __restrict__ prm = Ap->prm;
+    const int* __restrict__ cell_start = Ap->grid.cell_start;
+    const float inv = Ap->grid.inv;
+    const int ox = Ap->grid.ox, oy = Ap->grid.oy, oz = Ap->grid.oz;
+    const int gnx = Ap->grid.nx, gny = Ap->grid.ny, gnz = Ap->grid.nz;
+    // group centre and radius
+    float px = 0.f, py = 0.f, pz = 0.f;
+    if (lane < n) {
+        const float4 p = s.pos[lane];
+        px = p.x; py = p.y; pz = p.z;
+    }
+    const float inv_n = 1.0f / (float)n;
+    const float cx = warp_sum_f(px) * inv_n, cy = warp_sum_f(py) * inv_n, cz = warp_sum_f(pz) * inv_n;
+    const float dgx = px - cx, dgy = py - cy, dgz = pz - cz;
+    const float rad2 = warp_max_f(lane < n ? dgx * dgx + dgy * dgy + dgz * dgz : 0.0f);
+    const float reach = 10.01f + sqrtf(rad2) * 1.0001f + 1e-3f;
+    const float reach2 = reach * reach;
+    // grid columns within reach of the centre (cell units)
+    const float ux = cx * inv - (float)ox, uy = cy * inv - (float)oy, uz = cz * inv - (float)oz;
+    const float rc = reach * inv, rc2 = rc * rc;
+    const int i0 = max(0, (int)floorf(ux - rc)), i1 = min(gnx - 1, (int)floorf(ux + rc));
+    const int j0 = max(0, (int)floorf(uy - rc)), j1 = min(gny - 1, (int)floorf(uy + rc));
+    int qn = 0;
+    for (int i = i0; i <= i1; ++i) {
+        const float ddx = fmaxf(fmaxf((float)i - ux, ux - (float)(i + 1)), 0.0f);
+        for (int j = j0; j <= j1; ++j) {
+            const float ddy = fmaxf(fmaxf((float)j - uy, uy - (float)(j + 1)), 0.0f);
+            const float rem2 = rc2 - ddx * ddx - ddy * ddy;
+            if (rem2 < 0.0f) continue;
+            const float rem = sqrtf(rem2);
+            const int k0 = max(0, (int)floorf(uz - rem)), k1 = min(gnz - 1, (int)floorf(uz + rem));
+            if (k0 > k1) continue;
+            const int base = (i * gny + j) * gnz;
+            const int a0 = __ldg(&cell_start[base + k0]);
+            const int a1 = __ldg(&cell_start[base + k1 + 1]);
+            for (int t0 = a0; t0 < a1; t0 += 32) {
+                const int t = t0 + lane;
+                bool pass = false;
+                if (t < a1) {
+                    const float4 a = __ldg(&pq[t]);
+                    const float ex = a.x - cx, ey = a.y - cy, ez = a.z - cz;
+                    pass = ex * ex + ey * ey + ez * ez <= reach2;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, pass);
+                if (pass) s.q[qn + __popc(m & lt)] = t;
+                qn += __popc(m);
+                __syncwarp();
+                if (qn >= 32) {
+                    group_pairs<KAHAN, FULL, ABS, COUNT>(pq, prm, s, n, s.q[lane], acc);
+                    __syncwarp();
+                    if (lane < qn - 32) s.q[lane] = s.q[32 + lane];
+                    qn -= 32;
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    if (lane < qn) group_pairs<KAHAN, FULL, ABS, COUNT>(pq, prm, s, n, s.q[lane], acc);
+    __syncwarp();
+}
+
+// Resident state: persistent warps take residues from a work queue (an atomic
+// counter, residues in Calpha-cell order so neighbouring warps share antigen atoms
+// in L1) and write one FP64 energy per residue; k_sum_residues adds a candidate's
+// residues in index order.  No CTA barrier: warps never wait for each other.
+template <int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
+__global__ void __launch_bounds__(NW * 32) k_score_residues(StateView st, const AgView* __restrict__ ags,
+                                                             const int* __restrict__ order, int* __restrict__ queue,
+                                                             double* __restrict__ res_e, double* __restrict__ res_abs,
+                                                             long long* __restrict__ pair_count,
+                                                             uint32_t* __restrict__ err) {
+    __shared__ GroupSmem gs[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    GroupSmem& s = gs[warp];
+    SrcStateG src{st};
+    int my_pairs = 0;
+    for (;;) {
+        int gi = 0;
+        if (lane == 0) gi = atomicAdd(queue, 1);
+        gi = __shfl_sync(0xffffffffu, gi, 0);
+        if (gi >= st.total_res) break;
+        const int r = order ? order[gi] : gi;
+        const int c = st.res_cand[r];
+        bool bad = false;
+        const int n = src.load(c, r - st.cand_res_off[c], lane, s, bad);
+        Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0};
+        if (__any_sync(0xffffffffu, bad)) {
+            if (lane == 0) atomicOr(err, ERRF_NAN);
+        } else if (n > 0) {
+            __syncwarp();
+            score_group<KAHAN, FULL, ABS, COUNT>(&ags[st.cand_ag[c]], s, n, lane, lt, acc);
+        }
+        __syncwarp();
+        const double e = warp_sum_d(KAHAN ? ((double)acc.s - (double)acc.c) : (double)acc.s);
+        const double ea = ABS ? warp_sum_d((double)acc.abs_s) : 0.0;
+        if (lane == 0) {
+            if (res_e) res_e[r] = e;
+            if (ABS) res_abs[r] = ea;
+        }
+        if (COUNT) my_pairs += acc.pairs;
+    }
+    if (COUNT) {
+        int p = my_pairs;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        if (lane == 0 && p) atomicAdd((unsigned long long*)pair_count, (unsigned long long)p);
+    }
+}
+
+template <class Src, int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
+__global__ void __launch_bounds__(NW * 32) k_score_grouped(Src src, int n_cand, const AgView* __restrict__ ags,
+                                                            double* __restrict__ out, double* __restrict__ out_abs,
+                                                            long long* __restrict__ pair_count,
+                                                            uint32_t* __restrict__ err) {
+    __shared__ GroupSmem gs[NW];
+    __shared__ double sm[NW];
+    __shared__ double sm2[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    GroupSmem& s = gs[warp];
+    int my_pairs = 0;
+    for (int c = blockIdx.x; c < n_cand; c += gridDim.x) {
+        const AgView* Ap = &ags[src.ag(c)];
+        Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0};
+        const int ng = src.n_groups(c);
+        for (int gi = warp; gi < ng; gi += NW) {
+            bool bad = false;
+            const int n = src.load(c, gi, lane, s, bad);
+            if (__any_sync(0xffffffffu, bad)) {
+                if (lane == 0) atomicOr(err, ERRF_NAN);
+                __syncwarp();
+                continue;
+            }
+            if (n == 0) continue;
+            __syncwarp();
+            score_group<KAHAN, FULL, ABS, COUNT>(Ap, s, n, lane, lt, acc);
+        }
+        const double lane_e = KAHAN ? ((double)acc.s - (double)acc.c) : (double)acc.s;
+        const double e = cta_sum<NW>(lane_e, sm, lane, warp);
+        double ea = 0.0;
+        if (ABS) ea = cta_sum<NW>((double)acc.abs_s, sm2, lane, warp);
+        if (COUNT) my_pairs += acc.pairs;
+        if (threadIdx.x == 0) {
+            if (out) out[c] = e;
+            if (ABS) out_abs[c] = ea;
+        }
+    }
+    if (COUNT) {
+        int p = my_pairs;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        if (lane == 0 && p) atomicAdd((unsigned long long*)pair_count, (unsigned long long)p);
+    }
+}
+
 // ---- flat GpuAtom candidates (binder_gpu_atom = 2 x float4) -------------------------
 template <int NW, bool KAHAN, bool ABS, bool FORCE, bool COUNT>
 __global__ void __launch_bounds__(NW * 32) k_score_flat(const float4* __restrict__ atoms,
@@ -240,76 +515,46 @@ __global__ void __launch_bounds__(NW * 32) k_score_flat(const float4* __restrict
     }
 }
 
-// ---- resident state (slot layout) -------------------------------------------------
-template <int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
-__global__ void __launch_bounds__(NW * 32) k_score_state(StateView st, const AgView* __restrict__ ags,
-                                                          double* __restrict__ out, double* __restrict__ out_abs,
-                                                          long long* __restrict__ pair_count,
-                                                          uint32_t* __restrict__ err) {
-    __shared__ double sm[NW];
-    __shared__ double sm2[NW];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int my_pairs = 0;
-    for (int c = blockIdx.x; c < st.n_cand; c += gridDim.x) {
-        const AgView A = ags[st.cand_ag[c]];
-        const int r0 = st.cand_res_off[c], r1 = st.cand_res_off[c + 1];
-        const int n_work = (r1 - r0) * SLOT_STRIDE;
-        Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0};
-        for (int w = warp; w < n_work; w += NW) {
-            const int r = r0 + (w >> 4), k = w & (SLOT_STRIDE - 1);
-            const int aa = st.res_aa[r];
-            if (k >= c_topo_n[aa]) continue;
-            const float4 p = st.res_pos[(size_t)r * SLOT_STRIDE + k];
-            if (!finite3(p.x, p.y, p.z)) {
-                if (lane == 0) atomicOr(err, ERRF_NAN);
-                continue;
-            }
-            const float4 prm = c_slot_prm[aa][k];
-            AtomIn b;
-            b.x = p.x; b.y = p.y; b.z = p.z;
-            b.qs = prm.x; b.rmh = prm.y; b.se = prm.z; b.h = prm.w;
-            b.type = c_slot_type[aa][k];
-            atom_vs_antigen<KAHAN, FULL, ABS, false, COUNT>(A, b, acc, lane);
-        }
-        const double lane_e = KAHAN ? ((double)acc.s - (double)acc.c) : (double)acc.s;
-        double e = cta_sum<NW>(lane_e, sm, lane, warp);
-        double ea = 0.0;
-        if (ABS) ea = cta_sum<NW>((double)acc.abs_s, sm2, lane, warp);
-        if (FULL) {
-            // disulfide_energy (allatom.rs:155-180): Gaussian well between Cys SG atoms
-            if (threadIdx.x == 0) {
-                float ds = 0.0f;
-                for (int ri = r0; ri < r1; ++ri) {
-                    if (st.res_aa[ri] != CYS) continue;
-                    const float4 pi = st.res_pos[(size_t)ri * SLOT_STRIDE + 5];
-                    for (int rj = ri + 1; rj < r1; ++rj) {
-                        if (st.res_aa[rj] != CYS) continue;
-                        const float4 pj = st.res_pos[(size_t)rj * SLOT_STRIDE + 5];
-                        const float d = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
-                        if (d > 4.0f) continue;
-                        const float z = xdiv(xsub(d, 2.05f), 0.4f);
-                        ds = xsub(ds, xmul(4.0f, expf(xmul(xmul(-0.5f, z), z))));
-                    }
-                }
-                e += (double)ds;
-            }
-        }
-        if (threadIdx.x == 0) {
-            if (out) out[c] = e;
-            if (ABS) out_abs[c] = ea;
-        }
-        if (COUNT) my_pairs += acc.pairs;
-    }
-    if (COUNT) {
-        int p = my_pairs;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
-        if (lane == 0 && p) atomicAdd((unsigned long long*)pair_count, (unsigned long long)p);
-    }
-}
-
 // ---- launchers ----------------------------------------------------------------------
 constexpr int NW_SCORE = 8;
+
+// disulfide_energy (allatom.rs:155-180) of candidate c of the resident state: Gaussian
+// well between every pair of Cys SG atoms (topology atom 5), reference f32 order.
+__device__ float disulfide_energy(const StateView& st, int c) {
+    const int r0 = st.cand_res_off[c], r1 = st.cand_res_off[c + 1];
+    float ds = 0.0f;
+    for (int ri = r0; ri < r1; ++ri) {
+        if (st.res_aa[ri] != CYS) continue;
+        const float4 pi = st.res_pos[(size_t)ri * SLOT_STRIDE + 5];
+        for (int rj = ri + 1; rj < r1; ++rj) {
+            if (st.res_aa[rj] != CYS) continue;
+            const float4 pj = st.res_pos[(size_t)rj * SLOT_STRIDE + 5];
+            const float d = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
+            if (d > 4.0f) continue;
+            const float z = xdiv(xsub(d, 2.05f), 0.4f);
+            ds = xsub(ds, xmul(4.0f, expf(xmul(xmul(-0.5f, z), z))));
+        }
+    }
+    return ds;
+}
+
+__global__ void k_add_disulfide(StateView st, double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < st.n_cand) out[c] += (double)disulfide_energy(st, c);
+}
+
+template <class Src>
+static void grouped(cudaStream_t s, const Src& src, int n_cand, const AgView* ags, bool kahan, bool full, bool abs_,
+                    bool count, const ScoreOut& o, int g) {
+#define BINDER_G(K, FU, A, C) \
+    k_score_grouped<Src, NW_SCORE, K, FU, A, C><<<g, NW_SCORE * 32, 0, s>>>(src, n_cand, ags, o.energy, o.abs_sum, \
+                                                                          o.pairs, o.err)
+    if (count) BINDER_G(true, false, false, true);
+    else if (full) BINDER_G(true, true, false, false);
+    else if (abs_) { if (kahan) BINDER_G(true, false, true, false); else BINDER_G(false, false, true, false); }
+    else { if (kahan) BINDER_G(true, false, false, false); else BINDER_G(false, false, false, false); }
+#undef BINDER_G
+}
 
 int launch_score_flat(cudaStream_t s, const float* atoms, const long long* offsets, int n_cand, const AgView* ags,
                       const int* cand_ag, int accumulate, const ScoreOut& o, int grid_ctas, int block) {
@@ -318,49 +563,61 @@ int launch_score_flat(cudaStream_t s, const float* atoms, const long long* offse
     const float4* a4 = reinterpret_cast<const float4*>(atoms);
     const int g = grid_ctas > 0 ? min(grid_ctas, n_cand) : n_cand;
     const bool kahan = accumulate == 0;
-#define BINDER_FLAT(K, A, F, C)                                                                                 \
-    k_score_flat<NW_SCORE, K, A, F, C><<<g, NW_SCORE * 32, 0, s>>>(a4, offsets, n_cand, ags, cand_ag, o.energy, \
-                                                                   o.abs_sum, o.force, o.pairs, o.err)
-    if (o.force) {
-        if (kahan) BINDER_FLAT(true, false, true, false); else BINDER_FLAT(false, false, true, false);
-    } else if (o.pairs) {
-        BINDER_FLAT(true, false, false, true);
-    } else if (o.abs_sum) {
-        if (kahan) BINDER_FLAT(true, true, false, false); else BINDER_FLAT(false, true, false, false);
-    } else {
-        if (kahan) BINDER_FLAT(true, false, false, false); else BINDER_FLAT(false, false, false, false);
+    if (o.force) {  // per-atom warps: each warp owns one candidate atom's force
+        if (kahan)
+            k_score_flat<NW_SCORE, true, false, true, false><<<g, NW_SCORE * 32, 0, s>>>(
+                a4, offsets, n_cand, ags, cand_ag, o.energy, o.abs_sum, o.force, o.pairs, o.err);
+        else
+            k_score_flat<NW_SCORE, false, false, true, false><<<g, NW_SCORE * 32, 0, s>>>(
+                a4, offsets, n_cand, ags, cand_ag, o.energy, o.abs_sum, o.force, o.pairs, o.err);
+        return 1;
     }
-#undef BINDER_FLAT
+    SrcFlatG src{a4, offsets, cand_ag};
+    grouped(s, src, n_cand, ags, kahan, false, o.abs_sum != nullptr, o.pairs != nullptr, o, g);
     return 1;
+}
+
+// candidate energy = its residues' energies added in index order (+ disulfide when full)
+__global__ void k_sum_residues(StateView st, const double* __restrict__ res_e, const double* __restrict__ res_abs,
+                               int full, double* __restrict__ out, double* __restrict__ out_abs) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= st.n_cand) return;
+    double e = 0.0, ea = 0.0;
+    for (int r = st.cand_res_off[c]; r < st.cand_res_off[c + 1]; ++r) {
+        e += res_e[r];
+        if (res_abs) ea += res_abs[r];
+    }
+    if (full) e += (double)disulfide_energy(st, c);
+    out[c] = e;
+    if (out_abs) out_abs[c] = ea;
 }
 
 int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& o, int grid_ctas, int block) {
-    (void)block;
+                       const ScoreOut& o, const StateScoreScratch& scr, int grid_ctas) {
     if (st.n_cand <= 0) return 0;
-    const int g = grid_ctas > 0 ? min(grid_ctas, st.n_cand) : st.n_cand;
-    const bool kahan = accumulate == 0;
-#define BINDER_STATE(K, FU, A, C) \
-    k_score_state<NW_SCORE, K, FU, A, C><<<g, NW_SCORE * 32, 0, s>>>(st, ags, o.energy, o.abs_sum, o.pairs, o.err)
-    if (o.pairs) {
-        BINDER_STATE(true, false, false, true);
-    } else if (full) {
-        BINDER_STATE(true, true, false, false);
-    } else if (o.abs_sum) {
-        if (kahan) BINDER_STATE(true, false, true, false); else BINDER_STATE(false, false, true, false);
-    } else {
-        if (kahan) BINDER_STATE(true, false, false, false); else BINDER_STATE(false, false, false, false);
-    }
-#undef BINDER_STATE
-    return 1;
+    const bool kahan = accumulate == 0, abs_ = o.abs_sum != nullptr, count = o.pairs != nullptr;
+    const int g = grid_ctas > 0 ? grid_ctas : 148 * 4;
+    cudaMemsetAsync(scr.queue, 0, sizeof(int), s);
+#define BINDER_R(K, FU, A, C)                                                                                    \
+    k_score_residues<NW_SCORE, K, FU, A, C><<<g, NW_SCORE * 32, 0, s>>>(st, ags, scr.order, scr.queue,          \
+                                                                      count ? nullptr : scr.res_e,            \
+                                                                      scr.res_abs, o.pairs, o.err)
+    if (count) BINDER_R(true, false, false, true);
+    else if (full) BINDER_R(true, true, false, false);
+    else if (abs_) { if (kahan) BINDER_R(true, false, true, false); else BINDER_R(false, false, true, false); }
+    else { if (kahan) BINDER_R(true, false, false, false); else BINDER_R(false, false, false, false); }
+#undef BINDER_R
+    if (!count)
+        k_sum_residues<<<(st.n_cand + 127) / 128, 128, 0, s>>>(st, scr.res_e, abs_ ? scr.res_abs : nullptr, full,
+                                                               o.energy, o.abs_sum);
+    return count ? 2 : 3;  // launches issued (memset counted)
 }
 
 void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,
-                              uint32_t* err, int grid_ctas) {
+                              uint32_t* err, const StateScoreScratch& scr, int grid_ctas) {
     if (st.n_cand <= 0) return;
-    const int g = grid_ctas > 0 ? min(grid_ctas, st.n_cand) : st.n_cand;
-    k_score_state<NW_SCORE, true, false, false, true>
-        <<<g, NW_SCORE * 32, 0, s>>>(st, ags, nullptr, nullptr, pairs, err);
+    ScoreOut o{nullptr, nullptr, nullptr, pairs, err};
+    launch_score_state(s, st, ags, 0, 0, o, scr, grid_ctas);
 }
 
 }  // namespace binder

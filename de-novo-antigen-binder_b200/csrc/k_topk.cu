@@ -36,8 +36,11 @@ __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict_
     int kept = 0;                     // valid entries at the front of key/idx
     for (long long base = 0; base < n || base == 0; base += chunk) {
         const long long take = min((long long)chunk, n - base);
-        // slots [kept, TOPK_SORT): new chunk, padded with +inf keys
-        for (int t = threadIdx.x; t < TOPK_SORT; t += blockDim.x) {
+        // bitonic size: the next power of two holding the kept list and the chunk
+        int N = 64;
+        while (N < kept + take) N <<= 1;
+        // slots [kept, N): new chunk, padded with +inf keys
+        for (int t = threadIdx.x; t < N; t += blockDim.x) {
             if (t < kept) continue;
             const long long j = base + (t - kept);
             if (t - kept < take) {
@@ -50,9 +53,9 @@ __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict_
             }
         }
         __syncthreads();
-        for (int size = 2; size <= TOPK_SORT; size <<= 1) {
+        for (int size = 2; size <= N; size <<= 1) {
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                for (int t = threadIdx.x; t < TOPK_SORT / 2; t += blockDim.x) {
+                for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
                     const int lo = 2 * t - (t & (stride - 1));
                     const int hi = lo + stride;
                     const bool up = ((lo & size) == 0);

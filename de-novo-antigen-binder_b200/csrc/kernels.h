@@ -16,7 +16,7 @@ void launch_gather_atoms(cudaStream_t s, const int* sorted_idx, int n, const flo
                          const float* z, const float* q, const float* rmh, const float* eps, const uint8_t* hyd,
                          const uint8_t* type, float4* pq, float4* prm);
 void launch_gather_ca(cudaStream_t s, const int* sorted_idx, int n, const float* x, const float* y, const float* z,
-                      const uint8_t* aa, const float4* res_tab, float4* pq, float4* prm);
+                      const uint8_t* aa, const float4* res_tab, float inv, float4* pq, float4* prm, int4* cells);
 void launch_nb_count(cudaStream_t s, const GridView& g, const float* px, const float* py, const float* pz, int n_q,
                      long long* counts);
 void launch_nb_fill(cudaStream_t s, const GridView& g, const int* sorted_idx, const float* px, const float* py,
@@ -35,9 +35,16 @@ struct ScoreOut {
 // flat GpuAtom candidates (8 floats per atom), ragged offsets (n_cand + 1)
 int launch_score_flat(cudaStream_t s, const float* atoms, const long long* offsets, int n_cand, const AgView* ags,
                       const int* cand_ag, int accumulate, const ScoreOut& out, int grid_ctas, int block);
-// resident state (slot layout); full = add H-bond + EEF1 + disulfide
+// resident state (slot layout); full = add H-bond + EEF1 + disulfide.  Persistent
+// warps over a residue work queue; per-residue FP64 energies summed per candidate.
+struct StateScoreScratch {
+    const int* order;  // residue visiting order (may be null)
+    int* queue;        // work counter (reset by the launcher)
+    double* res_e;     // total_res
+    double* res_abs;   // total_res (abs sums)
+};
 int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& out, int grid_ctas, int block);
+                       const ScoreOut& out, const StateScoreScratch& scr, int grid_ctas);
 
 void launch_uniform_offsets(cudaStream_t s, long long* off, int n_cand, long long n_ab);
 
@@ -53,14 +60,18 @@ void launch_build_residues(cudaStream_t s, int n, const float* ca_xyz, const uin
 void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const float* by, const float* bz,
                       const uint8_t* baa, int n, float* fx, float* fy, float* fz);
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
-                    uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err);
+                    uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err,
+                    const int* order);
+// residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
+void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
+                          int* keys, int* counts, int* cursor, int* order);
 void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);
 // pair counting (same trajectory as launch_diffuse with noise off, state not written)
 void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           long long* pairs);
 // state scoring pair count
 void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,
-                              uint32_t* err, int grid_ctas);
+                              uint32_t* err, const StateScoreScratch& scr, int grid_ctas);
 
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
 double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);
