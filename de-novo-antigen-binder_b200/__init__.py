@@ -75,6 +75,20 @@ class Params(C.Structure):
         return p
 
 
+class RunCfg(C.Structure):
+    """binder_run_cfg (include/binder_gpu.h): the run_allatom schedule."""
+    _fields_ = [("phase1_steps", C.c_int32), ("score_every", C.c_int32), ("survivors", C.c_int32),
+                ("phase2_steps", C.c_int32), ("top_n", C.c_int32), ("phase1_mc", C.c_int32)]
+
+    @classmethod
+    def defaults(cls, **kw):
+        c = cls()
+        lib().binder_default_run_cfg(C.byref(c))
+        for k, v in kw.items():
+            setattr(c, k, v)
+        return c
+
+
 _LIB = None
 
 _SIGS = {
@@ -126,6 +140,11 @@ _SIGS = {
     "binder_block_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "binder_state_pair_counts": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "binder_fp32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "binder_mc_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "binder_state_select": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "binder_state_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "binder_default_run_cfg": (None, [C.c_void_p]),
+    "binder_run_allatom": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 
@@ -461,6 +480,42 @@ class GpuContext:
     def diffuse(self, n_steps, step0=0, with_noise=False, with_mc=False, temps=None):
         t = None if temps is None else _f32(temps)
         self._check(lib().binder_diffuse(self._h, n_steps, step0, int(with_noise), int(with_mc), _ptr(t)))
+
+    def mc_stats(self, reset=False):
+        """int64[n_cand, 4]: mutation/rotamer tried, accepted, backbone tried, accepted."""
+        out = np.zeros((self._state_cand, 4), np.int64)
+        self._check(lib().binder_mc_stats(self._h, _ptr(out), int(reset)))
+        return out
+
+    def state_select(self, idx):
+        """Keep candidates idx (in that order) of the resident state."""
+        idx = np.ascontiguousarray(idx, np.int32)
+        self._check(lib().binder_state_select(self._h, _ptr(idx), len(idx)))
+        self._sync_state_info()
+
+    def _sync_state_info(self):
+        n, t = C.c_int32(), C.c_int32()
+        self._check(lib().binder_state_info(self._h, C.byref(n), C.byref(t), None))
+        self._state_cand, self._state_res = n.value, t.value
+
+    def state_info(self):
+        """(n_cand, total_res, original upload index of each candidate)."""
+        n, t = C.c_int32(), C.c_int32()
+        self._check(lib().binder_state_info(self._h, C.byref(n), C.byref(t), None))
+        orig = np.zeros(n.value, np.int32)
+        self._check(lib().binder_state_info(self._h, C.byref(n), C.byref(t), _ptr(orig)))
+        return n.value, t.value, orig
+
+    def run_allatom(self, cfg=None, n_segments=1):
+        """run_allatom (diffusion.rs:983-1107) on the resident state.  Returns
+        (cand[n_segments, top_n], energy[n_segments, top_n]); the resident state then
+        holds the ranked results."""
+        cfg = RunCfg.defaults() if cfg is None else cfg
+        cand = np.zeros(n_segments * cfg.top_n, np.int32)
+        e = np.zeros(n_segments * cfg.top_n, np.float64)
+        self._check(lib().binder_run_allatom(self._h, C.byref(cfg), _ptr(cand), _ptr(e)))
+        self._sync_state_info()
+        return cand.reshape(n_segments, -1), e.reshape(n_segments, -1)
 
     def score_state(self, full=False):
         out = np.zeros(self._state_cand, np.float64)

@@ -30,6 +30,10 @@ struct DBuf {
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
     ~DBuf() { release(); }
+    void swap(DBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
     void release() {
         if (p) cudaFree(p);
         p = nullptr;
@@ -91,9 +95,14 @@ struct State {
     DBuf<long long> ag_cand_off;
     DBuf<uint32_t> cand_id;
     DBuf<uint8_t> res_aa;
-    DBuf<float4> res_chi, res_pos;
+    DBuf<float4> res_chi, res_pos, res_trig;
     DBuf<float> stage;  // packed slot staging for upload/download
-    std::vector<int> h_res_off;
+    std::vector<int> h_res_off, h_cand_ag;
+    std::vector<uint32_t> h_cand_id;
+    std::vector<int> h_orig;  // index of each candidate in the last full upload
+    int max_res = 0;
+    // Metropolis statistics, 4 per candidate (tried / accepted: mutation+rotamer, backbone)
+    DBuf<long long> mc_stats;
     int n_segments = 0;
     // residue order by Calpha cell for the Langevin kernel
     DBuf<int> key_base, keys, key_counts, key_cursor, order;
@@ -112,6 +121,7 @@ struct State {
         v.res_aa = res_aa.p;
         v.res_chi = res_chi.p;
         v.res_pos = res_pos.p;
+        v.res_trig = res_trig.p;
         v.res_cand = res_cand.p;
         return v;
     }
@@ -538,7 +548,8 @@ binder_ctx* binder_create(int device, const binder_params* params, int* status) 
     if (params) ctx->params = *params;
     else binder_default_params(&ctx->params);
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        score_init_tables() != cudaSuccess || search_init_tables() != cudaSuccess) {
+        score_init_tables() != cudaSuccess || search_init_tables() != cudaSuccess ||
+        anneal_init_tables() != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
         *status = BINDER_ERR_CUDA;
@@ -931,31 +942,22 @@ int binder_clear_antigens(binder_ctx* ctx) {
     return BINDER_OK;
 }
 
-int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
-                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
-                        const float* pos) {
-    int s = enter(ctx);
-    if (s) return s;
-    if (ctx->ags.empty()) return fail(ctx, BINDER_ERR_STATE, "no antigen added");
-    if (n_cand == 0 || n_cand > (size_t)INT32_MAX / 64) return fail(ctx, BINDER_ERR_ARG, "bad candidate count");
+}  // extern "C"
+
+namespace {
+// Candidate metadata of the resident state: residue offsets, antigen, Philox id,
+// per-antigen candidate groups, sort keys and scratch sizes.
+int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vector<int>& ag,
+                   const std::vector<uint32_t>& ids, const std::vector<int>& orig) {
     State& S = ctx->st;
-    std::vector<int> off(n_cand + 1, 0), ag(n_cand, 0);
-    std::vector<uint32_t> ids(n_cand);
-    for (size_t c = 0; c < n_cand; ++c) {
-        const int nr = n_res ? n_res[c] : uniform_n_res;
-        if (nr < 0 || nr > 4096) return fail(ctx, BINDER_ERR_ARG, "bad residue count %d", nr);
-        off[c + 1] = off[c] + nr;
-        ag[c] = antigen_id ? antigen_id[c] : 0;
-        if (ag[c] < 0 || ag[c] >= (int)ctx->ags.size()) return fail(ctx, BINDER_ERR_ARG, "bad antigen id");
-        ids[c] = cand_id ? cand_id[c] : (uint32_t)c;
-    }
+    const size_t n_cand = ag.size();
     const int total = off[n_cand];
-    if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
-    for (int r = 0; r < total; ++r)
-        if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
     std::vector<int> res_cand(total);
-    for (size_t c = 0; c < n_cand; ++c)
+    int max_res = 0;
+    for (size_t c = 0; c < n_cand; ++c) {
+        max_res = std::max(max_res, off[c + 1] - off[c]);
         for (int r = off[c]; r < off[c + 1]; ++r) res_cand[r] = (int)c;
+    }
     // candidates grouped by antigen (stable) for per-antigen survivor selection
     const int n_ag = (int)ctx->ags.size();
     std::vector<long long> g_off(n_ag + 1, 0);
@@ -966,22 +968,20 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     for (size_t c = 0; c < n_cand; ++c) g_idx[cur[ag[c]]++] = (int)c;
     S.n_cand = (int)n_cand;
     S.total_res = total;
+    S.max_res = max_res;
     S.h_res_off = off;
+    S.h_cand_ag = ag;
+    S.h_cand_id = ids;
+    S.h_orig = orig;
     S.n_segments = n_ag;
+    int s;
     if ((s = upload(ctx, S.cand_res_off, off.data(), off.size(), "state")) ||
         (s = upload(ctx, S.cand_ag, ag.data(), ag.size(), "state")) ||
         (s = upload(ctx, S.cand_id, ids.data(), ids.size(), "state")) ||
         (s = upload(ctx, S.res_cand, res_cand.data(), res_cand.size(), "state")) ||
         (s = upload(ctx, S.ag_cand_idx, g_idx.data(), g_idx.size(), "state")) ||
-        (s = upload(ctx, S.ag_cand_off, g_off.data(), g_off.size(), "state")) ||
-        (s = upload(ctx, S.res_aa, aa, (size_t)total, "state")))
+        (s = upload(ctx, S.ag_cand_off, g_off.data(), g_off.size(), "state")))
         return s;
-    CK(S.res_chi.ensure(total), "alloc");
-    if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
-    if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
-    CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
-    launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
-    if (total) LAUNCHED("pack_slots");
     // sort keys: one range of Calpha-grid cells per antigen
     std::vector<int> kb(n_ag);
     int nk = 0;
@@ -1000,6 +1000,129 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     CK(S.res_e.ensure(std::max(total, 1)), "alloc");
     CK(S.res_abs.ensure(std::max(total, 1)), "alloc");
     S.order_valid = false;
+    return BINDER_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
+                        const float* pos) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (ctx->ags.empty()) return fail(ctx, BINDER_ERR_STATE, "no antigen added");
+    if (n_cand == 0 || n_cand > (size_t)INT32_MAX / 64) return fail(ctx, BINDER_ERR_ARG, "bad candidate count");
+    State& S = ctx->st;
+    std::vector<int> off(n_cand + 1, 0), ag(n_cand, 0), orig(n_cand);
+    std::vector<uint32_t> ids(n_cand);
+    for (size_t c = 0; c < n_cand; ++c) {
+        const int nr = n_res ? n_res[c] : uniform_n_res;
+        if (nr < 0 || nr > 4096) return fail(ctx, BINDER_ERR_ARG, "bad residue count %d", nr);
+        off[c + 1] = off[c] + nr;
+        ag[c] = antigen_id ? antigen_id[c] : 0;
+        if (ag[c] < 0 || ag[c] >= (int)ctx->ags.size()) return fail(ctx, BINDER_ERR_ARG, "bad antigen id");
+        ids[c] = cand_id ? cand_id[c] : (uint32_t)c;
+        orig[c] = (int)c;
+    }
+    const int total = off[n_cand];
+    if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
+    for (int r = 0; r < total; ++r)
+        if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
+    // sin/cos of every chi (the NERF dihedrals of a rejected move's rebuild), with
+    // the C library's sinf/cosf of chi * PI/180 as place_atom computes them
+    std::vector<float4> trig((size_t)2 * total);
+    for (int r = 0; r < total; ++r) {
+        float sc[8];
+        for (int k = 0; k < 4; ++k) {
+            const float x = chi[4 * r + k] * RADS_PER_DEG;
+            sc[2 * k] = std::sin(x);
+            sc[2 * k + 1] = std::cos(x);
+        }
+        trig[2 * r] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+        trig[2 * r + 1] = make_float4(sc[4], sc[5], sc[6], sc[7]);
+    }
+    if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
+    if ((s = upload(ctx, S.res_aa, aa, (size_t)total, "state"))) return s;
+    if ((s = upload(ctx, S.res_trig, trig.data(), trig.size(), "state"))) return s;
+    CK(S.res_chi.ensure(total), "alloc");
+    if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+    if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
+    CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
+    launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
+    if (total) LAUNCHED("pack_slots");
+    CK(S.mc_stats.ensure(4 * n_cand), "alloc");
+    CK(cudaMemsetAsync(S.mc_stats.p, 0, 4 * n_cand * sizeof(long long), ctx->stream), "memset");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no state");
+    if (n == 0 || !idx) return fail(ctx, BINDER_ERR_ARG, "empty selection");
+    std::vector<int> off(n + 1, 0), ag(n), orig(n), map;
+    std::vector<uint32_t> ids(n);
+    for (size_t j = 0; j < n; ++j) {
+        const int c = idx[j];
+        if (c < 0 || c >= S.n_cand) return fail(ctx, BINDER_ERR_ARG, "candidate index %d out of range", c);
+        off[j + 1] = off[j] + (S.h_res_off[c + 1] - S.h_res_off[c]);
+        ag[j] = S.h_cand_ag[c];
+        ids[j] = S.h_cand_id[c];
+        orig[j] = S.h_orig[c];
+        for (int r = S.h_res_off[c]; r < S.h_res_off[c + 1]; ++r) map.push_back(r);
+    }
+    const int total = off[n];
+    // gather residues (and statistics) into fresh buffers, then swap them in
+    DBuf<int> d_map, d_cidx;
+    DBuf<uint8_t> aa;
+    DBuf<float4> chi, trig, pos;
+    DBuf<long long> stats;
+    if ((s = upload(ctx, d_map, map.data(), map.size(), "select")) ||
+        (s = upload(ctx, d_cidx, idx, n, "select")))
+        return s;
+    CK(aa.ensure(std::max(total, 1)), "alloc");
+    CK(chi.ensure(std::max(total, 1)), "alloc");
+    CK(trig.ensure(2 * std::max(total, 1)), "alloc");
+    CK(pos.ensure((size_t)std::max(total, 1) * SLOT_STRIDE), "alloc");
+    CK(stats.ensure(4 * n), "alloc");
+    launch_gather_state(ctx->stream, total, d_map.p, S.res_aa.p, S.res_chi.p, S.res_trig.p, S.res_pos.p, aa.p, chi.p,
+                        trig.p, pos.p, (int)n, d_cidx.p, S.mc_stats.p, stats.p);
+    LAUNCHED("gather_state");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    S.res_aa.swap(aa);
+    S.res_chi.swap(chi);
+    S.res_trig.swap(trig);
+    S.res_pos.swap(pos);
+    S.mc_stats.swap(stats);
+    if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_state_info(binder_ctx* ctx, int32_t* n_cand, int32_t* total_res, int32_t* orig_idx) {
+    int s = enter(ctx);
+    if (s) return s;
+    const State& S = ctx->st;
+    if (n_cand) *n_cand = S.n_cand;
+    if (total_res) *total_res = S.total_res;
+    if (orig_idx)
+        for (int c = 0; c < S.n_cand; ++c) orig_idx[c] = S.h_orig[c];
+    return BINDER_OK;
+}
+
+int binder_mc_stats(binder_ctx* ctx, int64_t* out, int reset) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no state");
+    if (out)
+        CK(cudaMemcpyAsync(out, S.mc_stats.p, (size_t)S.n_cand * 4 * sizeof(long long), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "D2H");
+    if (reset) CK(cudaMemsetAsync(S.mc_stats.p, 0, (size_t)S.n_cand * 4 * sizeof(long long), ctx->stream), "memset");
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
     return BINDER_OK;
 }
@@ -1062,6 +1185,17 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
         int s = upload(ctx, ctx->temps, temps, (size_t)n_steps, "temps H2D");
         if (s) return s;
     }
+    if (with_mc) {
+        if (S.max_res > ANNEAL_MAX_RES)
+            return fail(ctx, BINDER_ERR_ARG, "Metropolis steps hold at most %d residues per candidate", ANNEAL_MAX_RES);
+        CK(launch_anneal(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
+                         temps ? ctx->temps.p : nullptr, ctx->params.accumulate, S.max_res, ctx->errf.p,
+                         S.mc_stats.p),
+           "anneal");
+        LAUNCHED("anneal");
+        S.order_valid = false;  // residues moved: the cell order is stale
+        return BINDER_OK;
+    }
     int s = enqueue_order(ctx);
     if (s) return s;
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise, with_mc,
@@ -1099,7 +1233,6 @@ int binder_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise,
     if (s) return s;
     if (ctx->st.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
     if (n_steps < 0) return fail(ctx, BINDER_ERR_ARG, "negative step count");
-    if (with_mc) return fail(ctx, BINDER_ERR_ARG, "Metropolis moves are not enabled in this build");
     if (n_steps == 0) return BINDER_OK;
     if ((s = clear_err(ctx))) return s;
     if ((s = enqueue_diffuse(ctx, n_steps, step0, with_noise, with_mc, temps))) return s;
@@ -1159,6 +1292,87 @@ int binder_block_fetch(binder_ctx* ctx, double* out_e, int32_t* out_topk) {
                            cudaMemcpyDeviceToHost, ctx->stream),
            "D2H");
     return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);
+}
+
+void binder_default_run_cfg(binder_run_cfg* c) {
+    if (!c) return;
+    c->phase1_steps = 200;
+    c->score_every = 10;
+    c->survivors = 64;
+    c->phase2_steps = 600;
+    c->top_n = 64;
+    c->phase1_mc = 0;
+}
+
+int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* out_cand, double* out_energy) {
+    int s = enter(ctx);
+    if (s) return s;
+    binder_run_cfg cfg;
+    if (cfg_in) cfg = *cfg_in;
+    else binder_default_run_cfg(&cfg);
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (cfg.phase1_steps < 0 || cfg.phase2_steps < 0 || cfg.survivors < 1 || cfg.survivors > 1024 || cfg.top_n < 1 ||
+        cfg.top_n > 1024)
+        return fail(ctx, BINDER_ERR_ARG, "bad run configuration");
+    const binder_params& P = ctx->params;
+    // temperature (diffusion.rs:102-104): phase 1 on the schedule of both phases
+    // (diffusion.rs:1019), phase 2 on its own (:1089)
+    auto temp = [&](int iter, int total) {
+        return P.t_hot * std::pow(P.t_cold / P.t_hot, (float)iter / (float)total);
+    };
+    const int n1 = cfg.phase1_steps, n2 = cfg.phase2_steps;
+    std::vector<float> t1(std::max(n1, 1)), t2(std::max(n2, 1));
+    for (int i = 0; i < n1; ++i) t1[i] = temp(i, n1 + n2);
+    for (int i = 0; i < n2; ++i) t2[i] = temp(i, n2);
+    const int k1 = cfg.survivors;
+    CK(ctx->topk.ensure((size_t)S.n_segments * std::max(k1, cfg.top_n)), "alloc");
+    if ((s = clear_err(ctx))) return s;
+    // ---- phase 1: blocks of score_every steps, each scored with its survivors ----
+    const int per = cfg.score_every > 0 ? cfg.score_every : std::max(n1, 1);
+    int s0 = 0;
+    do {
+        const int ns = std::min(per, n1 - s0);
+        if (ns > 0 && (s = enqueue_diffuse(ctx, ns, (uint32_t)s0, 0, cfg.phase1_mc, &t1[s0]))) return s;
+        if ((s = enqueue_score_state(ctx, 0))) return s;
+        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k1,
+                             ctx->topk.p);
+        LAUNCHED("topk");
+        s0 += std::max(ns, 1);
+    } while (s0 < n1);
+    if ((s = check_err(ctx))) return s;
+    std::vector<int32_t> top((size_t)S.n_segments * k1);
+    CK(cudaMemcpyAsync(top.data(), ctx->topk.p, top.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream),
+       "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    std::vector<int32_t> surv;
+    for (int32_t i : top)
+        if (i >= 0) surv.push_back(i);
+    if ((s = binder_state_select(ctx, surv.data(), surv.size()))) return s;
+    // ---- phase 2: Langevin + Metropolis on the survivors (diffusion.rs:1083-1095) ----
+    if ((s = clear_err(ctx))) return s;
+    if (n2 > 0 && (s = enqueue_diffuse(ctx, n2, (uint32_t)n1, 1, 1, t2.data()))) return s;
+    // final allatom_energy and ranking (diffusion.rs:1092-1098)
+    if ((s = enqueue_score_state(ctx, 1))) return s;
+    const int k2 = cfg.top_n;
+    launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k2,
+                         ctx->topk.p);
+    LAUNCHED("topk");
+    std::vector<double> e(S.n_cand);
+    std::vector<int32_t> rank((size_t)S.n_segments * k2);
+    if ((s = fetch_energies(ctx, S.n_cand, e.data(), nullptr, nullptr))) return s;
+    CK(cudaMemcpyAsync(rank.data(), ctx->topk.p, rank.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream),
+       "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    std::vector<int32_t> keep;
+    for (size_t j = 0; j < rank.size(); ++j) {
+        const int32_t i = rank[j];
+        if (out_cand) out_cand[j] = i >= 0 ? S.h_orig[i] : -1;
+        if (out_energy) out_energy[j] = i >= 0 ? e[i] : std::nan("");
+        if (i >= 0) keep.push_back(i);
+    }
+    // the resident state becomes the results in rank order
+    return binder_state_select(ctx, keep.data(), keep.size());
 }
 
 void* binder_stream(binder_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

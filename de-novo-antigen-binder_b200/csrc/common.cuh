@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 namespace binder {
@@ -53,6 +54,15 @@ __device__ __forceinline__ float xsqrt(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ float xdist2(float dx, float dy, float dz) {
     return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
 }
+
+// Transcendentals of the Metropolis path (acceptance exp, H-bond and disulfide
+// Gaussians, rotation by a random torsion): evaluated in double and rounded once
+// to f32, on the device and in the CPU restatement alike.  Both double functions
+// are within 1 ulp of the exact value, so the two f32 results agree unless the
+// exact value lies within about 2^-29 (relative) of an f32 rounding boundary.
+__host__ __device__ __forceinline__ float mc_exp(float x) { return (float)exp((double)x); }
+__host__ __device__ __forceinline__ float mc_sin(float x) { return (float)sin((double)x); }
+__host__ __device__ __forceinline__ float mc_cos(float x) { return (float)cos((double)x); }
 
 // Rust `f32 as i32`: saturating, NaN -> 0
 __host__ __device__ __forceinline__ int32_t sat_i32(float v) {
@@ -131,6 +141,7 @@ struct StateView {
     const uint32_t* cand_id;  // n_cand
     uint8_t* res_aa;          // total_res
     float4* res_chi;          // total_res (degrees)
+    float4* res_trig;         // 2 * total_res: sin/cos of chi1, chi2 | chi3, chi4
     float4* res_pos;          // total_res * SLOT_STRIDE
     const int* res_cand;      // total_res
 };

@@ -532,7 +532,7 @@ __device__ float disulfide_energy(const StateView& st, int c) {
             const float d = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
             if (d > 4.0f) continue;
             const float z = xdiv(xsub(d, 2.05f), 0.4f);
-            ds = xsub(ds, xmul(4.0f, expf(xmul(xmul(-0.5f, z), z))));
+            ds = xsub(ds, xmul(4.0f, mc_exp(xmul(xmul(-0.5f, z), z))));
         }
     }
     return ds;

@@ -66,12 +66,28 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);
 void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);
+// gather residues map[0..total) (slot layout + aa, chi, trig) and the Metropolis
+// statistics of candidates cidx[0..n_cand) into fresh buffers
+void launch_gather_state(cudaStream_t s, int total, const int* map, const uint8_t* aa, const float4* chi,
+                         const float4* trig, const float4* pos, uint8_t* o_aa, float4* o_chi, float4* o_trig,
+                         float4* o_pos, int n_cand, const int* cidx, const long long* stats, long long* o_stats);
 // pair counting (same trajectory as launch_diffuse with noise off, state not written)
 void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           long long* pairs);
 // state scoring pair count
 void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,
                               uint32_t* err, const StateScoreScratch& scr, int grid_ctas);
+
+// ---- k_anneal.cu: Langevin + Metropolis steps, one CTA per candidate ----
+constexpr int ANNEAL_MAX_RES = 128;  // residues per candidate held in shared memory
+cudaError_t anneal_init_tables();
+size_t anneal_smem(int max_res);
+// accumulate: 1 = the reference's f32 sums, else f32 terms summed in double.
+// stats (may be null): 4 per candidate, += mutation/rotamer tried, accepted,
+// backbone tried, accepted.
+cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                          uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
+                          uint32_t* err, long long* stats);
 
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
 double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);

@@ -244,8 +244,21 @@ int binder_state_download(binder_ctx* ctx, uint8_t* aa, float* chi, float* pos);
 /* n_steps allatom_diffusion_step's (diffusion.rs:290-419) on every resident
    candidate: CG force + restraint + clamp (+ noise when with_noise) (+ rotamer /
    mutation / backbone Metropolis moves when with_mc).  step0 = Philox counter of
-   the first step; temps = per-step temperatures (NULL = t_hot). */
+   the first step; temps = per-step temperatures (NULL = t_hot).  With with_mc the
+   Metropolis energies follow params.accumulate: BINDER_ACC_F32 = the reference's
+   f32 sums, otherwise the same f32 pair terms summed in double and an FP64
+   acceptance test.  with_mc holds at most 128 residues per candidate. */
 int binder_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise, int with_mc, const float* temps);
+/* Metropolis move counts since the upload, int64[n_cand][4]: mutation/rotamer
+   tried, accepted, backbone tried, accepted (no reference counterpart).
+   reset != 0 zeroes them after the copy. */
+int binder_mc_stats(binder_ctx* ctx, int64_t* out, int reset);
+/* Keep candidates idx[0..n) of the resident state, in that order (survivor
+   selection, diffusion.rs:1044-1057: the kept AtomProteins move into a new Vec). */
+int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n);
+/* Resident candidate count, residue count and, per candidate, its index in the
+   last binder_state_upload (orig_idx int32[n_cand], may be NULL). */
+int binder_state_info(binder_ctx* ctx, int32_t* n_cand, int32_t* total_res, int32_t* orig_idx);
 /* Score every resident candidate against its antigen: LJ + Coulomb + hydrophobic
    (full = 0) or allatom_energy (diffusion.rs:281-283: + H-bond + EEF1 +
    disulfide, full = 1).  out = double[n_cand] (host). */
@@ -258,6 +271,27 @@ int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
    block and reports any device error. */
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_energies, int32_t* out_topk);
 int binder_block_fetch(binder_ctx* ctx, double* out_energies, int32_t* out_topk);
+
+/* run_allatom (diffusion.rs:983-1107) on the resident state: phase 1 runs
+   phase1_steps steps on every candidate in blocks of score_every (score + the
+   survivors lowest per antigen after each block), keeps the last block's
+   survivors, runs phase2_steps Langevin + Metropolis steps on them, scores them
+   with allatom_energy and ranks them (stable, ascending).  out_cand[a * top_n + j]
+   = index (in the last upload) of antigen a's j-th best candidate, -1 past the
+   end; out_energy likewise (NaN past the end).  Afterwards the resident state
+   holds the ranked results, in that order.  Philox step counters: phase 1 uses
+   0..phase1_steps-1, phase 2 continues from phase1_steps. */
+typedef struct binder_run_cfg {
+    int32_t phase1_steps;  /* GPU_STEPS 200 (diffusion.rs:1018) */
+    int32_t score_every;   /* steps per scored block, 10; <= 0 = one block */
+    int32_t survivors;     /* per antigen, population 64 (diffusion.rs:1047) */
+    int32_t phase2_steps;  /* cpu_iterations, 600 */
+    int32_t top_n;         /* results per antigen (diffusion.rs:1098) */
+    int32_t phase1_mc;     /* 1 = Metropolis moves in phase 1 too, as the reference's
+                              loop runs them (diffusion.rs:1023); 0 = gradient only */
+} binder_run_cfg;
+void binder_default_run_cfg(binder_run_cfg* cfg);
+int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg, int32_t* out_cand, double* out_energy);
 
 /* ---- instrumentation (no reference counterpart) --------------------------------
    The context's CUDA stream (cudaStream_t), for callers that time or order work

@@ -171,11 +171,21 @@ void set_ca_pos(Prot& P, int r, const V3& new_pos) {
     }
 }
 
+// Transcendentals of the Metropolis path (acceptance exp, H-bond and disulfide
+// Gaussians, rotation by a random torsion): evaluated in double and rounded once
+// to f32, as the CUDA kernels do.  Both double functions are within 1 ulp of the
+// exact value, so the two f32 results agree unless the exact value lies within
+// about 2^-29 (relative) of an f32 rounding boundary.  Rust's f32 exp/sin/cos
+// (libm) are within 1 ulp of these values.
+inline float mc_exp(float x) { return (float)std::exp((double)x); }
+inline float mc_sin(float x) { return (float)std::sin((double)x); }
+inline float mc_cos(float x) { return (float)std::cos((double)x); }
+
 // rodrigues (allatom.rs:467-479)
 V3 rodrigues(const V3& point, const V3& origin, const V3& axis, float angle) {
     V3 v = sub3(point, origin);
-    float ca = std::cos(angle);
-    float sa = std::sin(angle);
+    float ca = mc_cos(angle);
+    float sa = mc_sin(angle);
     float dot = v[0] * axis[0] + v[1] * axis[1] + v[2] * axis[2];
     V3 cx = cross3(axis, v);
     V3 rotd = {v[0] * ca + cx[0] * sa + axis[0] * dot * (1.0f - ca),
@@ -204,23 +214,27 @@ void perturb_psi(Prot& P, int r, float delta) {
         for (int k = 0; k < P.natoms(q); ++k) P.set(q, k, rodrigues(P.at(q, k), c, axis, delta));
 }
 
-// disulfide_energy (allatom.rs:155-180); SG is topology atom 5 of CYS (sg_pos, :139-150)
-float disulfide(const Prot& P) {
+// disulfide_energy (allatom.rs:155-180); SG is topology atom 5 of CYS (sg_pos, :139-150).
+// Acc = float: the reference's f32 sum; Acc = double: the same f32 pair terms
+// summed in double.
+template <class Acc>
+Acc disulfide_t(const Prot& P) {
     const float D0 = 2.05f, SIGMA = 0.4f, DEPTH = 4.0f, CUT = 4.0f;
     std::vector<V3> sg;
     for (int r = 0; r < P.n; ++r)
         if (P.aa[r] == CYS && P.natoms(r) > 5) sg.push_back(P.at(r, 5));
-    float e = 0.0f;
+    Acc e = 0;
     for (size_t i = 0; i < sg.size(); ++i)
         for (size_t j = i + 1; j < sg.size(); ++j) {
             float dx = sg[i][0] - sg[j][0], dy = sg[i][1] - sg[j][1], dz = sg[i][2] - sg[j][2];
             float d = std::sqrt(dx * dx + dy * dy + dz * dz);
             if (d > CUT) continue;
             float z = (d - D0) / SIGMA;
-            e -= DEPTH * std::exp(-0.5f * z * z);
+            e -= (Acc)(DEPTH * mc_exp(-0.5f * z * z));
         }
     return e;
 }
+float disulfide(const Prot& P) { return disulfide_t<float>(P); }
 
 // hbond_energy (energy.rs:32-39)
 inline float hbond_energy(float r_sq) {
@@ -228,6 +242,12 @@ inline float hbond_energy(float r_sq) {
     float r = std::sqrt(r_sq);
     float z = (r - HB_R0) / HB_SIGMA;
     return -HB_DEPTH * std::exp(-0.5f * z * z);
+}
+inline float hbond_energy_mc(float r_sq) {
+    if (r_sq > HB_CUTOFF_SQ) return 0.0f;
+    float r = std::sqrt(r_sq);
+    float z = (r - HB_R0) / HB_SIGMA;
+    return -HB_DEPTH * mc_exp(-0.5f * z * z);
 }
 inline double hbond_energy64(double r_sq) {
     if (r_sq > (double)HB_CUTOFF_SQ) return 0.0;
@@ -747,7 +767,7 @@ void orc_default_params(orc_params* p) {
     p->step = 0.08f; p->noise_base = 0.25f; p->t_hot = 3.0f; p->t_cold = 0.02f;
     p->mutation_p = 0.08f; p->rotamer_move_p = 0.12f; p->backbone_move_p = 0.04f;
     p->max_torsion_deg = 15.0f; p->iface_cutoff_sq = 64.0f; p->shell_radius = 20.0f;
-    p->max_disp = 2.0f; p->restraint_k = 0.02f; p->ca_cell = 10.0f; p->seed = 0;
+    p->max_disp = 2.0f; p->restraint_k = 0.02f; p->ca_cell = 10.0f; p->accumulate = 0; p->seed = 0;
 }
 
 // temperature (diffusion.rs:102-104)
@@ -784,15 +804,17 @@ void orc_antigen_center(const orc_antigen* A, float out[3]) { out[0] = A->center
 
 namespace {
 // residue_contribution_allatom (diffusion.rs:425-463): Calpha of residue r against
-// every antigen Calpha, AMBER LJ + Coulomb + hydrophobic + H-bond, f32 order.
-float residue_contribution(const orc_antigen* A, const Prot& P, int r) {
+// every antigen Calpha, AMBER LJ + Coulomb + hydrophobic + H-bond.  Acc = float:
+// the reference's f32 sum; Acc = double: the same f32 terms summed in double.
+template <class Acc>
+Acc residue_contribution_t(const orc_antigen* A, const Prot& P, int r) {
     int baa = P.aa[r];
     int bca = T_TOPO_CA[baa];
     V3 p = P.at(r, bca);
     int bt = T_TOPO_TYPE[baa][bca];
     float brm = T_NB[bt][0], be = T_NB[bt][1], bq = T_TOPO_Q[baa][bca];
     uint8_t bh = T_TOPO_HYD[baa][bca];
-    float e = 0.0f;
+    Acc e = 0;
     for (int i = 0; i < A->n_res; ++i) {
         int aaa = A->aa[i];
         int aca = T_TOPO_CA[aaa];
@@ -807,15 +829,30 @@ float residue_contribution(const orc_antigen* A, const Prot& P, int r) {
         float eps = std::sqrt(be * ae);
         float r2 = (r_ij * r_ij) / r_sq;
         float r6 = r2 * r2 * r2;
-        e += eps * (r6 * r6 - 2.0f * r6);
-        if (bq != 0.0f && aq != 0.0f) e += 332.0f * bq * aq / std::sqrt(r_sq);
-        if (bh == 1 && ah == 1 && r_sq < 36.0f) e -= 0.5f;
-        if (hb_pair(bt, at)) e += hbond_energy(r_sq);
+        e += (Acc)(eps * (r6 * r6 - 2.0f * r6));
+        if (bq != 0.0f && aq != 0.0f) e += (Acc)(332.0f * bq * aq / std::sqrt(r_sq));
+        if (bh == 1 && ah == 1 && r_sq < 36.0f) e -= (Acc)0.5f;
+        if (hb_pair(bt, at)) e += (Acc)hbond_energy_mc(r_sq);
     }
     return e;
 }
+float residue_contribution(const orc_antigen* A, const Prot& P, int r) {
+    return residue_contribution_t<float>(A, P, r);
+}
 
-// allatom_diffusion_step (diffusion.rs:290-419) for one candidate
+// Metropolis criterion (diffusion.rs:368, 385, 414-415): accept downhill moves, else
+// with probability exp(-dE/T).  f32: the reference's arithmetic; double: the
+// difference of the double energies and a double exponential.
+inline bool metropolis(float delta_e, float temp, float u) {
+    return delta_e <= 0.0f || u < mc_exp(-delta_e / temp);
+}
+inline bool metropolis(double delta_e, float temp, float u) {
+    return delta_e <= 0.0 || (double)u < std::exp(-delta_e / (double)temp);
+}
+
+// allatom_diffusion_step (diffusion.rs:290-419) for one candidate; Acc is the
+// accumulation type of the Metropolis energies.
+template <class Acc>
 void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t cand, uint32_t step, float temp,
               bool with_noise, bool with_mc, int64_t* stats) {
     const int n = P.n;
@@ -854,6 +891,8 @@ void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t can
         set_ca_pos(P, r, new_ca);
     }
     if (!with_mc) return;
+    auto contrib = [&](int r) { return residue_contribution_t<Acc>(A, P, r); };
+    auto ds = [&]() { return disulfide_t<Acc>(P); };
     // interface mask (diffusion.rs:343-351)
     std::vector<char> iface(n);
     for (int r = 0; r < n; ++r) {
@@ -878,12 +917,11 @@ void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t can
             float old_chi[4];
             for (int k = 0; k < 4; ++k) old_chi[k] = P.chi[r * 4 + k];
             int rot_idx = (int)urange(d4[2], (uint32_t)T_ROT_N[aa]);
-            float old_e = residue_contribution(A, P, r) + disulfide(P);
+            Acc old_e = contrib(r) + ds();
             for (int k = 0; k < 4; ++k) P.chi[r * 4 + k] = T_ROT[aa][rot_idx][k];
             rebuild_side_chain(P, r);
-            float new_e = residue_contribution(A, P, r) + disulfide(P);
-            float delta_e = new_e - old_e;
-            bool accept = delta_e <= 0.0f || u01(d4[3]) < std::exp(-delta_e / temp);
+            Acc new_e = contrib(r) + ds();
+            bool accept = metropolis(new_e - old_e, temp, u01(d4[3]));
             if (stats) { stats[0]++; stats[1] += accept; }
             if (!accept) {
                 for (int k = 0; k < 4; ++k) P.chi[r * 4 + k] = old_chi[k];
@@ -894,14 +932,13 @@ void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t can
             int new_aa = (int)urange(d4[2], 20u);
             float old_chi[4];
             for (int k = 0; k < 4; ++k) old_chi[k] = P.chi[r * 4 + k];
-            float old_e = residue_contribution(A, P, r) + disulfide(P);
+            Acc old_e = contrib(r) + ds();
             float new_chi[4] = {0.f, 0.f, 0.f, 0.f};
             if (T_ROT_N[new_aa] > 0)
                 for (int k = 0; k < 4; ++k) new_chi[k] = T_ROT[new_aa][0][k];
             mutate_residue(P, r, new_aa, new_chi);
-            float new_e = residue_contribution(A, P, r) + disulfide(P);
-            float delta_e = new_e - old_e;
-            bool accept = delta_e <= 0.0f || u01(d4[3]) < std::exp(-delta_e / temp);
+            Acc new_e = contrib(r) + ds();
+            bool accept = metropolis(new_e - old_e, temp, u01(d4[3]));
             if (stats) { stats[0]++; stats[1] += accept; }
             if (!accept) mutate_residue(P, r, old_aa, old_chi);
         }
@@ -913,14 +950,14 @@ void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t can
         if (!(u01(d4[0]) < prm->backbone_move_p)) continue;
         float delta = frange(d4[1], -prm->max_torsion_deg, prm->max_torsion_deg) * RADS_PER_DEG;
         bool do_phi = (d4[2] >> 31) & 1u;
-        float old_e = 0.0f;
-        for (int i = r; i < n; ++i) old_e += residue_contribution(A, P, i);
-        old_e += disulfide(P);
+        Acc old_e = 0;
+        for (int i = r; i < n; ++i) old_e += contrib(i);
+        old_e += ds();
         if (do_phi) perturb_phi(P, r, delta); else perturb_psi(P, r, delta);
-        float new_e = 0.0f;
-        for (int i = r; i < n; ++i) new_e += residue_contribution(A, P, i);
-        new_e += disulfide(P);
-        bool accept = (new_e - old_e) <= 0.0f || u01(d4[3]) < std::exp(-(new_e - old_e) / temp);
+        Acc new_e = 0;
+        for (int i = r; i < n; ++i) new_e += contrib(i);
+        new_e += ds();
+        bool accept = metropolis(new_e - old_e, temp, u01(d4[3]));
         if (stats) { stats[2]++; stats[3] += accept; }
         if (!accept) {
             if (do_phi) perturb_phi(P, r, -delta); else perturb_psi(P, r, -delta);
@@ -950,8 +987,10 @@ void orc_step(const orc_antigen* A, const orc_params* prm, int n_cand, int n_res
               int n_threads) {
     parallel_for(n_cand, n_threads, [&](int64_t c) {
         Prot P{n_res, aa + (size_t)c * n_res, chi + (size_t)c * n_res * 4, pos + (size_t)c * n_res * SLOTS * 3};
-        step_one(A, prm, P, cand_id ? cand_id[c] : (uint32_t)c, step_id, temp, with_noise != 0, with_mc != 0,
-                 stats ? stats + c * 4 : nullptr);
+        const uint32_t id = cand_id ? cand_id[c] : (uint32_t)c;
+        int64_t* st = stats ? stats + c * 4 : nullptr;
+        if (prm->accumulate == 1) step_one<float>(A, prm, P, id, step_id, temp, with_noise != 0, with_mc != 0, st);
+        else step_one<double>(A, prm, P, id, step_id, temp, with_noise != 0, with_mc != 0, st);
     });
 }
 

@@ -120,6 +120,9 @@ void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 typedef struct orc_params {
     float step, noise_base, t_hot, t_cold, mutation_p, rotamer_move_p, backbone_move_p,
           max_torsion_deg, iface_cutoff_sq, shell_radius, max_disp, restraint_k, ca_cell;
+    /* Metropolis energies: 0 = f32 pair terms summed in double (the CUDA default),
+       1 = the reference's f32 sums */
+    int32_t accumulate;
     uint64_t seed;
 } orc_params;
 void orc_default_params(orc_params* p);

@@ -64,7 +64,8 @@ class OrcParams(C.Structure):
     _fields_ = [("step", C.c_float), ("noise_base", C.c_float), ("t_hot", C.c_float), ("t_cold", C.c_float),
                 ("mutation_p", C.c_float), ("rotamer_move_p", C.c_float), ("backbone_move_p", C.c_float),
                 ("max_torsion_deg", C.c_float), ("iface_cutoff_sq", C.c_float), ("shell_radius", C.c_float),
-                ("max_disp", C.c_float), ("restraint_k", C.c_float), ("ca_cell", C.c_float), ("seed", C.c_uint64)]
+                ("max_disp", C.c_float), ("restraint_k", C.c_float), ("ca_cell", C.c_float),
+                ("accumulate", C.c_int32), ("seed", C.c_uint64)]
 
     @classmethod
     def defaults(cls, **kw):
