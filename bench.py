@@ -34,6 +34,8 @@ sys.path.insert(0, str(ROOT))
 
 N_STEPS_PER_BLOCK = 10
 TOP_K = 64
+PHASE1_STEPS = 200   # GPU_STEPS (diffusion.rs:1018)
+PHASE2_STEPS = 600   # Langevin + Metropolis steps on the survivors
 # Algorithmic flops per in-cutoff pair (FADD/FMUL = 1, FFMA = 2, rsqrt/sqrt/div
 # MUFU sequences not counted):
 #  all-atom score pair: dx,dy,dz 3 + r^2 5 + 1/r^2 1 + R 1 + R^2 1 + s2 1 + s6 2 +
@@ -230,6 +232,50 @@ def run_reference(args, rank, world):
     return 0
 
 
+def cpu_mc_sample(orc, cfg, ag_aa, ag_pos, aa, chi, pos, n_res, target_s, threads):
+    """Phase-2 steps (Langevin + Metropolis, diffusion.rs:290-463) of the oracle on
+    the survivors, as many as fit in about target_s seconds."""
+    A = orc.Antigen(ag_aa, ag_pos)
+    prm = orc.OrcParams.defaults(shell_radius=float(cfg["shell"][0]))
+    n_cand = len(aa) // n_res
+    ids = np.arange(n_cand, dtype=np.uint32)
+    aa, chi, pos = aa.copy(), chi.copy(), pos.copy()
+    steps, t0 = 0, time.perf_counter()
+    while steps < PHASE2_STEPS and time.perf_counter() - t0 < target_s:
+        A.step(prm, aa, chi, pos, n_res, ids, steps, orc.temperature(steps, PHASE2_STEPS), True, True,
+               threads=threads)
+        steps += 1
+    return steps, time.perf_counter() - t0
+
+
+def measure_phase2(torch, ctx, ext, survivors, n_res, reps=3):
+    """Phase 2 of run_allatom on the survivors: PHASE2_STEPS Langevin + Metropolis
+    steps (noise on, annealed), one launch, device time on the library stream."""
+    ctx.state_select(np.asarray(survivors, np.int32))
+    aa, chi, pos = ctx.state_download()
+    temps = np.array([np.float32(3.0) * np.power(np.float32(0.02 / 3.0), np.float32(i) / np.float32(PHASE2_STEPS))
+                      for i in range(PHASE2_STEPS)], np.float32)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for rep in range(reps + 1):
+        ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+        torch.cuda.synchronize()
+        a.record(ext)
+        ctx.diffuse(PHASE2_STEPS, PHASE1_STEPS, with_noise=True, with_mc=True, temps=temps)
+        b.record(ext)
+        b.synchronize()
+        if rep:
+            ms.append(a.elapsed_time(b))
+    st = ctx.mc_stats().sum(0)
+    n = len(survivors)
+    t = statistics.mean(ms)
+    return {"candidates": n, "steps": PHASE2_STEPS, "ms": t, "candidate_steps_per_s": n * PHASE2_STEPS / (t * 1e-3),
+            "moves_per_candidate_step": {"mutation_rotamer": float(st[0]) / (n * PHASE2_STEPS),
+                                         "backbone": float(st[2]) / (n * PHASE2_STEPS)},
+            "acceptance": {"mutation_rotamer": float(st[1]) / max(1, st[0]), "backbone": float(st[3]) / max(1, st[2])},
+            "accumulate": "f32 pair terms summed in FP64, FP64 Metropolis test"}, (aa, chi, pos)
+
+
 def workload_config():
     return {"workload": "search block: 1024 antibodies x 20 residues vs 300-residue globule (2505 atoms); "
                         "10 gradient steps + all-atom score + top-64 per step",
@@ -315,6 +361,18 @@ def run_ours(args, rank, world, local_rank):
     h2d = h_aa.nbytes + h_chi.nbytes + h_pos.nbytes
     d2h = h_e.nbytes + h_top.nbytes + h_aa.nbytes + h_chi.nbytes + h_pos.nbytes
 
+    # phase 2 on this rank's survivors, then the whole run_allatom pipeline
+    phase2, surv_state = measure_phase2(torch, ctx, ext, top_last[0], n_res)
+    ctx.state_upload(pop.aa, chi, pos, uniform_n_res=n_res)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run_cand, run_e = ctx.run_allatom(pkg.RunCfg.defaults(phase1_steps=PHASE1_STEPS, score_every=N_STEPS_PER_BLOCK,
+                                                          survivors=TOP_K, phase2_steps=PHASE2_STEPS, top_n=TOP_K))
+    run_ms = 1e3 * (time.perf_counter() - t0)
+    run_allatom = {"ms": run_ms, "phase1_steps": PHASE1_STEPS, "phase2_steps": PHASE2_STEPS, "candidates": n_cand,
+                   "survivors": TOP_K, "best_energy": float(run_e[0][0]), "best_index": int(run_cand[0][0]),
+                   "api": "binder_run_allatom (wall clock, host call to results)"}
+
     peaks, peaks_kind = load_peaks()
     fp32_scalar, fp32_packed = ctx.fp32_peak()
     fp32_peak = max(fp32_scalar, fp32_packed)
@@ -346,6 +404,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks, "gpu_launches": int(launches),
         "survivors": {"best_energy": float(surv_e[0]), "best_index": int(survivors[0])},
         "hbm_peak_gbs": peaks.get("hbm_gbs"), "peaks_file": peaks_kind,
+        "phase2": phase2, "run_allatom": run_allatom,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, str(ROOT / "tests"))
@@ -356,11 +415,37 @@ def run_ours(args, rank, world, local_rank):
                                 "kind": "port",
                                 "sample": f"one block (10 gradient steps + brute-force f32 score + top-64) over "
                                           f"{n} of 1024 candidates, {dt:.1f} s"}
+        ms_steps, mdt = cpu_mc_sample(orc, cfg, ag_aa, np.ascontiguousarray(ag_pos), *surv_state, n_res,
+                                      args.cpu_seconds / 3, threads)
+        cpu_p2 = len(surv_state[0]) // n_res * ms_steps / mdt
+        line["phase2"]["cpu_baseline"] = {
+            "value": cpu_p2, "unit": "candidate-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{ms_steps} of {PHASE2_STEPS} phase-2 steps on the 64 survivors, {mdt:.1f} s"}
+        cpu_run_s = n_cand * PHASE1_STEPS / (n * N_STEPS_PER_BLOCK / dt) + TOP_K * PHASE2_STEPS / cpu_p2
+        line["run_allatom"]["cpu_estimate_ms"] = 1e3 * cpu_run_s
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def run_phase2_only(args):
+    """Small profiling case for the Metropolis kernel (one GPU, one launch timed)."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(0)
+    cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, 0)
+    n_res = int(pop.n_res[0])
+    ctx.state_upload(pop.aa, chi, pos, uniform_n_res=n_res)
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    global PHASE2_STEPS
+    PHASE2_STEPS = args.phase2_only
+    out, _ = measure_phase2(torch, ctx, ext, np.arange(TOP_K), n_res, reps=1)
+    print(json.dumps({"phase2_only": out}), flush=True)
+    ctx.close()
     return 0
 
 
@@ -372,6 +457,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--phase2-only", type=int, default=0, metavar="STEPS",
+                    help="profiling case: one launch of STEPS Langevin + Metropolis steps on 64 candidates")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -380,6 +467,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.phase2_only:
+        return run_phase2_only(args)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -101,6 +101,9 @@ struct State {
     std::vector<uint32_t> h_cand_id;
     std::vector<int> h_orig;  // index of each candidate in the last full upload
     int max_res = 0;
+    // chi sin/cos for the Metropolis kernel, derived from the uploaded chi on first use
+    std::vector<float> h_chi_upload;
+    bool trig_valid = false;
     // Metropolis statistics, 4 per candidate (tried / accepted: mutation+rotamer, backbone)
     DBuf<long long> mc_stats;
     int n_segments = 0;
@@ -945,6 +948,30 @@ int binder_clear_antigens(binder_ctx* ctx) {
 }  // extern "C"
 
 namespace {
+// sin/cos of every chi (the NERF dihedrals of a rejected move's rebuild), computed
+// from the uploaded chi with the C library's sinf/cosf of chi * PI/180 as
+// place_atom does; the Metropolis kernel keeps them current afterwards.
+int ensure_trig(binder_ctx* ctx) {
+    State& S = ctx->st;
+    if (S.trig_valid) return BINDER_OK;
+    const int total = S.total_res;
+    std::vector<float4> trig((size_t)2 * std::max(total, 1));
+    for (int r = 0; r < total; ++r) {
+        float sc[8];
+        for (int k = 0; k < 4; ++k) {
+            const float x = S.h_chi_upload[4 * r + k] * RADS_PER_DEG;
+            sc[2 * k] = std::sin(x);
+            sc[2 * k + 1] = std::cos(x);
+        }
+        trig[2 * r] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+        trig[2 * r + 1] = make_float4(sc[4], sc[5], sc[6], sc[7]);
+    }
+    int s = upload(ctx, S.res_trig, trig.data(), trig.size(), "trig");
+    if (s) return s;
+    S.trig_valid = true;
+    return BINDER_OK;
+}
+
 // Candidate metadata of the resident state: residue offsets, antigen, Philox id,
 // per-antigen candidate groups, sort keys and scratch sizes.
 int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vector<int>& ag,
@@ -1029,22 +1056,10 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
     for (int r = 0; r < total; ++r)
         if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
-    // sin/cos of every chi (the NERF dihedrals of a rejected move's rebuild), with
-    // the C library's sinf/cosf of chi * PI/180 as place_atom computes them
-    std::vector<float4> trig((size_t)2 * total);
-    for (int r = 0; r < total; ++r) {
-        float sc[8];
-        for (int k = 0; k < 4; ++k) {
-            const float x = chi[4 * r + k] * RADS_PER_DEG;
-            sc[2 * k] = std::sin(x);
-            sc[2 * k + 1] = std::cos(x);
-        }
-        trig[2 * r] = make_float4(sc[0], sc[1], sc[2], sc[3]);
-        trig[2 * r + 1] = make_float4(sc[4], sc[5], sc[6], sc[7]);
-    }
     if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
     if ((s = upload(ctx, S.res_aa, aa, (size_t)total, "state"))) return s;
-    if ((s = upload(ctx, S.res_trig, trig.data(), trig.size(), "state"))) return s;
+    S.h_chi_upload.assign(chi, chi + (size_t)4 * total);
+    S.trig_valid = false;
     CK(S.res_chi.ensure(total), "alloc");
     if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
     if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
@@ -1075,6 +1090,7 @@ int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n) {
         for (int r = S.h_res_off[c]; r < S.h_res_off[c + 1]; ++r) map.push_back(r);
     }
     const int total = off[n];
+    if ((s = ensure_trig(ctx))) return s;
     // gather residues (and statistics) into fresh buffers, then swap them in
     DBuf<int> d_map, d_cidx;
     DBuf<uint8_t> aa;
@@ -1188,8 +1204,17 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     if (with_mc) {
         if (S.max_res > ANNEAL_MAX_RES)
             return fail(ctx, BINDER_ERR_ARG, "Metropolis steps hold at most %d residues per candidate", ANNEAL_MAX_RES);
+        int s = ensure_trig(ctx);
+        if (s) return s;
+        int max_ag = 0, max_cells = 0;
+        for (const auto& a : ctx->ags) {
+            const GridView& g = a->view.ca_grid;
+            max_ag = std::max(max_ag, a->n_res);
+            max_cells = std::max(max_cells, g.nx * g.ny * g.nz + 1);
+        }
         CK(launch_anneal(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
-                         temps ? ctx->temps.p : nullptr, ctx->params.accumulate, S.max_res, ctx->errf.p,
+                         temps ? ctx->temps.p : nullptr, ctx->params.accumulate, S.max_res, max_ag, max_cells,
+                         ctx->errf.p,
                          S.mc_stats.p),
            "anneal");
         LAUNCHED("anneal");

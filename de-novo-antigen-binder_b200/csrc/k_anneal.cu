@@ -1,23 +1,27 @@
 // k_anneal.cu — allatom_diffusion_step with its Metropolis moves (diffusion.rs:290-463)
-// on the GPU: one CTA per candidate, the candidate's residues resident in shared
-// memory for all n_steps of the launch.
+// on the GPU: one CTA per candidate, the candidate's residues and its antigen's
+// Calphas resident in shared memory for all n_steps of the launch.
 //
 // Per step, in the reference's order:
-//  1. Langevin: coarse-grained force (the 27-cell walk in the reference's order),
-//     restraint, noise, 2 A clamp, rigid translation (diffusion.rs:306-339).
+//  1. Langevin: coarse-grained force, restraint, noise, 2 A clamp, rigid
+//     translation (diffusion.rs:306-339).  Eight lanes per residue split the 27
+//     probe cells (reference order) into consecutive runs; each lane evaluates
+//     the in-cutoff pair terms of its run and lane 0 adds them lane by lane, which
+//     is the reference's sequential sum.
 //  2. Interface mask: any antigen Calpha within sqrt(iface_cutoff_sq) (:343-351).
 //  3. Mutation / rotamer sweep (:354-399).  A move at residue r changes only
 //     residue r's atoms, and the Calpha-level energy of r depends only on r's
 //     Calpha and amino acid; residues interact only through the disulfide term.
 //     So every residue's proposal, its rejection rebuild and both Calpha energies
-//     are computed in parallel, and one thread then takes the decisions in
-//     residue order, updating the disulfide energy wherever a Cys is involved —
-//     the reference's sequential sweep, exactly.
+//     are computed in parallel (builds on one half of the warps, energies on the
+//     other), and one thread then takes the decisions in residue order, updating
+//     the disulfide energy wherever a Cys is involved — the reference's
+//     sequential sweep, exactly.
 //  4. Backbone phi/psi sweep (:403-418): sequential over the attempted moves;
-//     per move the Calpha energies of residues r..n are evaluated by warps over
-//     the antigen Calphas, the downstream atoms rotated by all threads (Rodrigues,
-//     allatom.rs:397-479), and the decision broadcast; a rejected move is undone
-//     by the opposite rotation, as in the reference.
+//     per move the Calpha energies of residues r..n are evaluated by warps, the
+//     downstream atoms rotated by all threads (Rodrigues, allatom.rs:397-479), and
+//     the decision broadcast; a rejected move is undone by the opposite rotation,
+//     as in the reference.
 // Calpha energies are cached per residue and recomputed whenever the Calpha moved.
 //
 // Accumulation: ACC = float reproduces the reference's f32 sums bit for bit; ACC =
@@ -32,28 +36,46 @@ cudaError_t anneal_init_tables() { return geom_init_tables(); }
 
 constexpr int AN_WARPS = 8;
 constexpr int AN_THREADS = AN_WARPS * 32;
+constexpr int CG_LANES = 8;                          // lanes per residue in the Langevin probe
+constexpr int CG_RES_PER_PASS = AN_THREADS / CG_LANES;
+constexpr int CG_SLOTS = 16;                         // in-cutoff terms a lane holds
+constexpr int STAGE_CAP = 64;                        // staged in-cutoff terms per warp
+constexpr int AG_STAGE_MAX = 1024;                   // antigen Calphas staged in shared memory
+constexpr int CELL_STAGE_MAX = 4096;                 // Calpha-grid cells staged in shared memory
 enum : int { MV_NONE = 0, MV_ROT = 1, MV_MUT = 2 };
 enum : int { SEL_KEEP = 0, SEL_PROP = 1, SEL_REJ = 2 };
+enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3 };
 
-// Shared-memory carve of one CTA for candidates of up to R residues.
+// Shared-memory carve of one CTA for candidates of up to R residues and antigens
+// of up to G staged Calphas.
 struct AnSmem {
     float4 *pos, *prop, *rej;  // R * SLOT_STRIDE each: state, proposal, rejection rebuild
     float4* trig;              // 2R: sin/cos of chi1..4
     float4* chi;               // R (degrees)
     float4* ldelta;            // R: Langevin translation
-    float4* stage;             // AN_WARPS * 32: in-cutoff pair terms of one warp chunk
+    float4* bb_trig;           // R: cos, sin of the torsion step and of its negation
+    float4* terms;             // min(R, 32) * CG_LANES * CG_SLOTS Langevin pair terms
+    float4* stage;             // AN_WARPS * STAGE_CAP: in-cutoff Calpha-energy terms
+    float4 *agq, *agp;         // G staged antigen Calphas: x, y, z, q | r_min_half, eps, hyd, type
+    float4 *cgq, *cgp;         // G staged Calphas in CG-grid order (AgView::ca_pq, ca_prm)
+    int* cgcell;               // C staged CG-grid cell starts
+    AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
-    float *u_acc, *bb_delta, *bb_u;  // R
-    int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface;  // R
-    double* dscal;  // [0] disulfide energy of the current state
-    int* iscal;     // [0] disulfide valid, [1] decision
+    double* dscal;                  // [0] disulfide energy of the current state
+    float *u_acc, *bb_u;            // R
+    int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
+    int* iscal;
 };
-__host__ __device__ inline size_t anneal_smem_bytes(int R) {
-    return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 4 + (size_t)AN_WARPS * 32 * 16 + (size_t)R * 8 * 3 +
-           (size_t)R * 4 * 3 + (size_t)R * 4 * 9 + 16 + 16;
+__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C) {
+    const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
+    return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + (size_t)L * CG_SLOTS * 16 +
+           (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
+           ((sizeof(AgView) + 15) / 16) * 16 +
+           (size_t)R * 8 * 3 + 16 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 + 32;
 }
-__device__ inline AnSmem carve(unsigned char* b, int R) {
+__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C) {
     AnSmem s;
+    const int L = min(R, CG_RES_PER_PASS) * CG_LANES;
     auto take = [&](size_t bytes) { unsigned char* p = b; b += bytes; return p; };
     s.pos = (float4*)take((size_t)R * SLOT_STRIDE * 16);
     s.prop = (float4*)take((size_t)R * SLOT_STRIDE * 16);
@@ -61,13 +83,20 @@ __device__ inline AnSmem carve(unsigned char* b, int R) {
     s.trig = (float4*)take((size_t)R * 32);
     s.chi = (float4*)take((size_t)R * 16);
     s.ldelta = (float4*)take((size_t)R * 16);
-    s.stage = (float4*)take((size_t)AN_WARPS * 32 * 16);
+    s.bb_trig = (float4*)take((size_t)R * 16);
+    s.terms = (float4*)take((size_t)L * CG_SLOTS * 16);
+    s.stage = (float4*)take((size_t)AN_WARPS * STAGE_CAP * 16);
+    s.agq = (float4*)take((size_t)G * 16);
+    s.agp = (float4*)take((size_t)G * 16);
+    s.cgq = (float4*)take((size_t)G * 16);
+    s.cgp = (float4*)take((size_t)G * 16);
+    s.cgcell = (int*)take(((size_t)C * 4 + 15) / 16 * 16);
+    s.ag = (AgView*)take(((sizeof(AgView) + 15) / 16) * 16);
     s.c_cur = (double*)take((size_t)R * 8);
     s.c_old = (double*)take((size_t)R * 8);
     s.c_new = (double*)take((size_t)R * 8);
     s.dscal = (double*)take(16);
     s.u_acc = (float*)take((size_t)R * 4);
-    s.bb_delta = (float*)take((size_t)R * 4);
     s.bb_u = (float*)take((size_t)R * 4);
     s.aa = (int*)take((size_t)R * 4);
     s.kind = (int*)take((size_t)R * 4);
@@ -78,7 +107,8 @@ __device__ inline AnSmem carve(unsigned char* b, int R) {
     s.bb_att = (int*)take((size_t)R * 4);
     s.bb_phi = (int*)take((size_t)R * 4);
     s.iface = (int*)take((size_t)R * 4);
-    s.iscal = (int*)take(16);
+    s.tcount = (int*)take((size_t)L * 4);
+    s.iscal = (int*)take(32);
     return s;
 }
 
@@ -90,27 +120,41 @@ __device__ __forceinline__ float hbond_mc(float r_sq) {
     return xmul(-HB_DEPTH, mc_exp(xmul(xmul(-0.5f, z), z)));
 }
 
-// residue_contribution_allatom (diffusion.rs:425-463) of a Calpha at `ca` of amino
-// acid `aa`, by one warp: lanes evaluate 32 antigen Calphas at a time (in index
-// order); the in-cutoff terms are staged in shared memory and lane 0 adds them in
-// the reference's order.  Result valid in lane 0.
+// Add staged Calpha-energy terms in order (lj; coulomb; hydrophobic; hbond per pair).
 template <class ACC>
-__device__ ACC warp_contribution(const AgView& A, F3 ca, int aa, float4* stage) {
+__device__ __forceinline__ void fold_terms(const float4* stage, int cnt, ACC& e) {
+    for (int j = 0; j < cnt; ++j) {
+        const float4 v = stage[j];
+        const unsigned fl = __float_as_uint(v.w);
+        e += (ACC)v.x;
+        if (fl & 1u) e += (ACC)v.y;
+        if (fl & 2u) e -= (ACC)0.5f;
+        if (fl & 4u) e += (ACC)v.z;
+    }
+}
+
+// residue_contribution_allatom (diffusion.rs:425-463) of a Calpha at `ca` of amino
+// acid `aa`, by one warp: lanes evaluate 32 antigen Calphas at a time (index
+// order), in-cutoff terms are compacted into the warp's stage in that order and
+// lane 0 adds them in the reference's order.  Result valid in lane 0.
+template <class ACC>
+__device__ ACC warp_contribution(const float4* __restrict__ agq, const float4* __restrict__ agp, int nag, F3 ca,
+                                 int aa, float4* stage) {
     const int lane = threadIdx.x & 31;
     const float4 b = s_ca_atom[aa];  // q, r_min_half, epsilon, hydrophobic
-    const int bt = s_ca_type[aa];
-    const int bhb = s_hb_role[bt];
+    const int bhb = s_hb_role[s_ca_type[aa]];
     ACC e = 0;
-    for (int base = 0; base < A.n_res; base += 32) {
+    int cnt = 0;
+    for (int base = 0; base < nag; base += 32) {
         const int i = base + lane;
         bool in = false;
         float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i < A.n_res) {
-            const float4 a = A.ca_atom[i];
-            const float4 ap = A.ca_atom_prm[i];
+        if (i < nag) {
+            const float4 a = agq[i];
             const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
             in = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
             if (in) {
+                const float4 ap = agp[i];
                 unsigned fl = 0;
                 const float r_ij = xadd(b.y, ap.x);
                 const float eps = xsqrt(xmul(b.z, ap.y));
@@ -131,21 +175,18 @@ __device__ ACC warp_contribution(const AgView& A, F3 ca, int aa, float4* stage) 
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
-        if (in) stage[__popc(m & ((1u << lane) - 1u))] = t;
-        __syncwarp();
-        if (lane == 0) {
-            const int cnt = __popc(m);
-            for (int j = 0; j < cnt; ++j) {
-                const float4 v = stage[j];
-                const unsigned fl = __float_as_uint(v.w);
-                e += (ACC)v.x;
-                if (fl & 1u) e += (ACC)v.y;
-                if (fl & 2u) e -= (ACC)0.5f;
-                if (fl & 4u) e += (ACC)v.z;
-            }
+        if (in) stage[cnt + __popc(m & ((1u << lane) - 1u))] = t;
+        cnt += __popc(m);
+        if (cnt > STAGE_CAP - 32) {  // flush before the stage can overflow
+            __syncwarp();
+            if (lane == 0) fold_terms(stage, cnt, e);
+            __syncwarp();
+            cnt = 0;
         }
-        __syncwarp();
     }
+    __syncwarp();
+    if (lane == 0) fold_terms(stage, cnt, e);
+    __syncwarp();
     return e;
 }
 
@@ -157,19 +198,20 @@ __device__ __forceinline__ const float4* cur_slots(const AnSmem& S, int j) {
 }
 
 // disulfide_energy (allatom.rs:155-180) over the SG atoms (topology atom 5 of Cys)
-// in residue order; residue `sub` (>= 0) is taken from `sub_slots` with amino
-// acid `sub_aa` instead.
-template <class ACC>
-__device__ ACC disulfide_sweep(const AnSmem& S, int n, int sub, const float4* sub_slots, int sub_aa) {
+// in residue order.  SWEEP: residues take their slots from cur_slots and residue
+// `sub` (>= 0) is taken from `sub_slots` with amino acid `sub_aa` instead; else
+// every residue is read from the state.
+template <class ACC, bool SWEEP>
+__device__ ACC disulfide_of(const AnSmem& S, int n, int sub, const float4* sub_slots, int sub_aa) {
     ACC e = 0;
     for (int i = 0; i < n; ++i) {
-        const int ai = i == sub ? sub_aa : S.aa[i];
+        const int ai = (SWEEP && i == sub) ? sub_aa : S.aa[i];
         if (ai != CYS) continue;
-        const float4 pi = (i == sub ? sub_slots : cur_slots(S, i))[5];
+        const float4 pi = (SWEEP ? (i == sub ? sub_slots : cur_slots(S, i)) : S.pos + (size_t)i * SLOT_STRIDE)[5];
         for (int j = i + 1; j < n; ++j) {
-            const int aj = j == sub ? sub_aa : S.aa[j];
+            const int aj = (SWEEP && j == sub) ? sub_aa : S.aa[j];
             if (aj != CYS) continue;
-            const float4 pj = (j == sub ? sub_slots : cur_slots(S, j))[5];
+            const float4 pj = (SWEEP ? (j == sub ? sub_slots : cur_slots(S, j)) : S.pos + (size_t)j * SLOT_STRIDE)[5];
             const float d = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
             if (d > 4.0f) continue;
             const float z = xdiv(xsub(d, 2.05f), 0.4f);
@@ -235,13 +277,12 @@ __device__ __forceinline__ float4 rodrigues(float4 p, F3 o, F3 ax, float ca, flo
 
 // Rotate the atoms a phi (about N-CA through CA: residue r's atoms after CA and all
 // later residues) or psi move (about CA-C through C: residue r's O and all later
-// residues) moves; allatom.rs:397-455.
-__device__ void rotate_downstream(const AnSmem& S, int n, int r, bool phi, float angle) {
+// residues) moves, by the angle whose cosine and sine are ca, sa; allatom.rs:397-455.
+__device__ void rotate_downstream(const AnSmem& S, int n, int r, bool phi, float ca, float sa) {
     const float4* rs = S.pos + (size_t)r * SLOT_STRIDE;
     const F3 a0 = f3(rs[phi ? 0 : 1]), a1 = f3(rs[phi ? 1 : 2]);
     const F3 axis = norm3(sub3(a1, a0));
     const F3 origin = a1;
-    const float ca = mc_cos(angle), sa = mc_sin(angle);
     const int n_at_r = s_topo_n[S.aa[r]];
     for (int idx = threadIdx.x; idx < (n - r) * SLOT_STRIDE; idx += AN_THREADS) {
         const int q = r + idx / SLOT_STRIDE, k = idx % SLOT_STRIDE;
@@ -253,21 +294,104 @@ __device__ void rotate_downstream(const AnSmem& S, int n, int r, bool phi, float
     }
 }
 
+// Coarse-grained force on residue r (compute_forces_with_grid, energy.rs:322-398) by
+// its group of CG_LANES lanes (gl = lane in group, all lanes of the group call).
+// Lane gl evaluates the consecutive probe cells [27 gl / 8, 27 (gl + 1) / 8) of the
+// reference's (dx, dy, dz) order into its term slots; lane 0 then adds the terms
+// lane by lane.  A lane with more in-cutoff terms than slots sends the residue to
+// the one-lane walk (same sum).  Result valid in lane 0 of the group.
+__device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigned gmask, float4* my_terms,
+                               int* my_count, const int* group_counts, const float4* group_terms, float& fx,
+                               float& fy, float& fz) {
+    const GridView& g = A.ca_grid;
+    const int cx = cell_coord(body.x, g.inv), cy = cell_coord(body.y, g.inv), cz = cell_coord(body.z, g.inv);
+    const float p[3] = {body.x, body.y, body.z};
+    const int c[3] = {cx, cy, cz};
+    // squared distance to the lower / own / upper slab per dimension (culling only;
+    // the margin covers the f32 rounding of x*inv and of the slab bounds)
+    float sl[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            const float lo = (float)(c[d] + o - 1) * g.cell, hi = lo + g.cell;
+            const float dd = fmaxf(fmaxf(lo - p[d], p[d] - hi), 0.0f);
+            sl[d][o] = dd * dd;
+        }
+    const float reach = 10.001f + 4e-7f * (fabsf(body.x) + fabsf(body.y) + fabsf(body.z));
+    const float reach2 = reach * reach;
+    const int c_lo = (27 * gl) / CG_LANES, c_hi = (27 * (gl + 1)) / CG_LANES;
+    int nt = 0;
+    for (int ci = c_lo; ci < c_hi; ++ci) {
+        const int dx = ci / 9 - 1, dy = (ci / 3) % 3 - 1, dz = ci % 3 - 1;
+        if (sl[0][dx + 1] + sl[1][dy + 1] + sl[2][dz + 1] > reach2) continue;
+        int a0, a1;
+        if (!probe_cell(g, cx, cy, cz, dx, dy, dz, a0, a1)) continue;
+        for (int i = a0; i < a1; ++i) {
+            float tx, ty, tz;
+            if (!cg_term_parts(body, A.ca_pq[i], A.ca_prm[i], tx, ty, tz)) continue;
+            if (nt < CG_SLOTS) my_terms[nt] = make_float4(tx, ty, tz, 0.f);
+            ++nt;
+        }
+    }
+    *my_count = nt;
+    const bool overflow = (__ballot_sync(gmask, nt > CG_SLOTS) & gmask) != 0u;
+    __syncwarp(gmask);
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    if (gl == 0) {
+        if (!overflow) {
+            for (int L = 0; L < CG_LANES; ++L) {
+                const int cnt = group_counts[L];
+                const float4* t = group_terms + L * CG_SLOTS;
+                for (int k = 0; k < cnt; ++k) {
+                    sx = xadd(sx, t[k].x);
+                    sy = xadd(sy, t[k].y);
+                    sz = xadd(sz, t[k].z);
+                }
+            }
+        } else {
+            cg_force(A, body, sx, sy, sz);
+        }
+    }
+    fx = sx; fy = sy; fz = sz;
+}
+
 template <class ACC>
 __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                        int n_steps, uint32_t step0, int with_noise,
-                                                       const float* __restrict__ temps, int R,
+                                                       const float* __restrict__ temps, int R, int G, int C,
                                                        uint32_t* __restrict__ err, long long* __restrict__ stats) {
     extern __shared__ __align__(16) unsigned char an_smem[];
-    const AnSmem S = carve(an_smem, R);
+    const AnSmem S = carve(an_smem, R, G, C);
     const int c = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = st.cand_res_off[c];
     const int n = st.cand_res_off[c + 1] - r0;
     if (n <= 0 || n > R) return;
     const uint32_t cid = st.cand_id[c];
-    const AgView A = ags[st.cand_ag[c]];
-    float4* stage = S.stage + warp * 32;
+    if (tid == 0) *S.ag = ags[st.cand_ag[c]];
+    __syncthreads();
+    const AgView& A = *S.ag;
+    const int nag = A.n_res;
+    const bool staged = nag <= G;
+    const int ncell = A.ca_grid.nx * A.ca_grid.ny * A.ca_grid.nz + 1;
+    const bool cells_staged = staged && ncell <= C;
+    for (int i = tid; staged && i < nag; i += AN_THREADS) {
+        S.agq[i] = A.ca_atom[i];
+        S.agp[i] = A.ca_atom_prm[i];
+        S.cgq[i] = A.ca_pq[i];
+        S.cgp[i] = A.ca_prm[i];
+    }
+    for (int i = tid; cells_staged && i < ncell; i += AN_THREADS) S.cgcell[i] = A.ca_grid.cell_start[i];
+    __syncthreads();
+    if (tid == 0 && cells_staged) {  // the CG probe reads the staged copies through the view
+        S.ag->ca_pq = S.cgq;
+        S.ag->ca_prm = S.cgp;
+        S.ag->ca_grid.cell_start = S.cgcell;
+    }
+    const float4* agq = staged ? S.agq : A.ca_atom;
+    const float4* agp = staged ? S.agp : A.ca_atom_prm;
+    float4* stage = S.stage + warp * STAGE_CAP;
 
     for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
     for (int r = tid; r < n; r += AN_THREADS) {
@@ -275,7 +399,6 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
         S.chi[r] = st.res_chi[r0 + r];
         S.trig[2 * r] = st.res_trig[2 * (r0 + r)];
         S.trig[2 * r + 1] = st.res_trig[2 * (r0 + r) + 1];
-        S.sel[r] = SEL_KEEP;
     }
     long long n_mc = 0, n_mc_acc = 0, n_bb = 0, n_bb_acc = 0;
     __syncthreads();
@@ -283,35 +406,51 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
     for (int s = 0; s < n_steps; ++s) {
         const uint32_t step = step0 + (uint32_t)s;
         const float temp = temps ? temps[s] : p.t_hot;
-        // ---- 1. Langevin (diffusion.rs:306-339) ----
-        for (int r = tid; r < n; r += AN_THREADS) {
-            const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
-            if (err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
-            float fx, fy, fz;
-            cg_force(A, cg_body(ca.x, ca.y, ca.z, S.aa[r]), fx, fy, fz);
-            const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
-            const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
-            const float f_r = xdiv(xmul(-p.restraint_k, xsub(d, p.shell_radius)), d);
-            fx = xadd(fx, xmul(f_r, dx_c));
-            fy = xadd(fy, xmul(f_r, dy_c));
-            fz = xadd(fz, xmul(f_r, dz_c));
-            float nx = 0.f, ny = 0.f, nz = 0.f;
-            if (with_noise) {
-                const float sigma = xmul(p.noise_base, xsqrt(temp));
-                const U4 u = rng_draw(p.seed, cid, step, STREAM_NOISE, (uint32_t)r);
-                nx = frange(u.x, -sigma, sigma);
-                ny = frange(u.y, -sigma, sigma);
-                nz = frange(u.z, -sigma, sigma);
+        // ---- 1. Langevin (diffusion.rs:306-339): CG_LANES lanes per residue ----
+        {
+            const int gl = tid % CG_LANES;
+            const unsigned gmask = ((1u << CG_LANES) - 1u) << (lane & ~(CG_LANES - 1));
+            const int g0 = tid - gl;  // first thread of the group
+            for (int base = 0; base < n; base += CG_RES_PER_PASS) {
+                const int r = base + tid / CG_LANES;
+                if (r >= n) continue;  // whole groups leave together
+                const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
+                if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
+                const CgB body = cg_body(ca.x, ca.y, ca.z, S.aa[r]);
+                float fx, fy, fz;
+                group_cg_force(A, body, gl, gmask, S.terms + (size_t)tid * CG_SLOTS, S.tcount + tid, S.tcount + g0,
+                               S.terms + (size_t)g0 * CG_SLOTS, fx, fy, fz);
+                if (gl == 0) {
+                    const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
+                    const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
+                    const float f_r = xdiv(xmul(-p.restraint_k, xsub(d, p.shell_radius)), d);
+                    fx = xadd(fx, xmul(f_r, dx_c));
+                    fy = xadd(fy, xmul(f_r, dy_c));
+                    fz = xadd(fz, xmul(f_r, dz_c));
+                    float nx = 0.f, ny = 0.f, nz = 0.f;
+                    if (with_noise) {
+                        const float sigma = xmul(p.noise_base, xsqrt(temp));
+                        const U4 u = rng_draw(p.seed, cid, step, STREAM_NOISE, (uint32_t)r);
+                        nx = frange(u.x, -sigma, sigma);
+                        ny = frange(u.y, -sigma, sigma);
+                        nz = frange(u.z, -sigma, sigma);
+                    }
+                    const float md = p.max_disp;
+                    const F3 nca = {xadd(xadd(ca.x, fminf(fmaxf(xmul(p.step, fx), -md), md)), nx),
+                                    xadd(xadd(ca.y, fminf(fmaxf(xmul(p.step, fy), -md), md)), ny),
+                                    xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
+                    const F3 dl = sub3(nca, ca);
+                    S.ldelta[r] = make_float4(dl.x, dl.y, dl.z, 0.f);
+                    S.valid[r] = 0;
+                }
+                __syncwarp(gmask);  // the group's term slots are reused by the next pass
             }
-            const float md = p.max_disp;
-            const F3 nca = {xadd(xadd(ca.x, fminf(fmaxf(xmul(p.step, fx), -md), md)), nx),
-                            xadd(xadd(ca.y, fminf(fmaxf(xmul(p.step, fy), -md), md)), ny),
-                            xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
-            const F3 dl = sub3(nca, ca);
-            S.ldelta[r] = make_float4(dl.x, dl.y, dl.z, 0.f);
-            S.valid[r] = 0;
         }
-        if (tid == 0) S.iscal[0] = 0;  // disulfide energy stale
+        if (tid == 0) {
+            S.iscal[IS_DVALID] = 0;  // disulfide energy stale
+            S.iscal[IS_NCYS] = 0;
+            S.iscal[IS_LASTCYS] = -1;
+        }
         __syncthreads();
         for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) {
             const int r = i / SLOT_STRIDE, k = i % SLOT_STRIDE;
@@ -324,16 +463,19 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
         }
         __syncthreads();
 
-        // ---- 2. interface mask (diffusion.rs:343-351) + backbone draws ----
+        // ---- 2. interface mask (diffusion.rs:343-351) + move draws ----
         for (int r = warp; r < n; r += AN_WARPS) {
             const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
             bool hit = false;
-            for (int base = 0; base < A.n_res && !hit; base += 32) {
-                const int i = base + lane;
+            for (int base = 0; base < nag && !hit; base += 64) {
                 bool h = false;
-                if (i < A.n_res) {
-                    const float4 a = A.ca_atom[i];
-                    h = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z)) < p.iface_cutoff_sq;
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int i = base + u * 32 + lane;
+                    if (i < nag) {
+                        const float4 a = agq[i];
+                        h |= xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z)) < p.iface_cutoff_sq;
+                    }
                 }
                 hit = __any_sync(0xffffffffu, h);
             }
@@ -341,10 +483,15 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
         }
         for (int r = tid; r < n; r += AN_THREADS) {
             const U4 d = rng_draw(p.seed, cid, step, STREAM_BACKBONE, (uint32_t)r);
-            S.bb_att[r] = u01(d.x) < p.backbone_move_p;
-            S.bb_delta[r] = xmul(frange(d.y, -p.max_torsion_deg, p.max_torsion_deg), RADS_PER_DEG);
+            const bool att = u01(d.x) < p.backbone_move_p;
+            S.bb_att[r] = att;
+            if (att) {
+                const float delta = xmul(frange(d.y, -p.max_torsion_deg, p.max_torsion_deg), RADS_PER_DEG);
+                S.bb_trig[r] = make_float4(mc_cos(delta), mc_sin(delta), mc_cos(-delta), mc_sin(-delta));
+            }
             S.bb_phi[r] = (int)((d.z >> 31) & 1u);
             S.bb_u[r] = u01(d.w);
+            S.sel[r] = SEL_KEEP;
         }
         __syncthreads();
 
@@ -354,9 +501,9 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
             const float eff_mut_p = itf ? xmul(p.mutation_p, 3.0f) : xmul(p.mutation_p, 0.4f);
             const float eff_rot_p = itf ? xmul(p.rotamer_move_p, 2.0f) : p.rotamer_move_p;
             const U4 d = rng_draw(p.seed, cid, step, STREAM_MC, (uint32_t)r);
+            const int aa = S.aa[r];
             int kind = MV_NONE;
             if (u01(d.x) < eff_mut_p) {
-                const int aa = S.aa[r];
                 if (u01(d.y) < eff_rot_p) {
                     if (s_rot_n[aa] > 0) {
                         kind = MV_ROT;
@@ -371,47 +518,56 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
             }
             S.kind[r] = kind;
             S.u_acc[r] = u01(d.w);
+            if (aa == CYS) atomicAdd(&S.iscal[IS_NCYS], 1);
         }
         __syncthreads();
-        // proposals and rejection rebuilds (two threads per residue), then the Calpha
-        // energies before / after each move (one warp per energy)
-        for (int t = tid; t < 2 * n; t += AN_THREADS) {
-            const int r = t >> 1;
-            if (S.kind[r] != MV_NONE) build_move(S, r, (t & 1) ? SEL_REJ : SEL_PROP);
-        }
-        for (int t = warp; t < 2 * n; t += AN_WARPS) {
-            const int r = t >> 1, which = t & 1;
-            const int kind = S.kind[r];
-            if (kind == MV_NONE) continue;
-            const bool same = kind == MV_ROT || S.new_aa[r] == S.aa[r];
-            if (which == 1 && same) continue;  // same Calpha, same amino acid: same energy
-            const int a = which ? S.new_aa[r] : S.aa[r];
-            const ACC e = warp_contribution<ACC>(A, f3(S.pos[r * SLOT_STRIDE + 1]), a, stage);
-            if (lane == 0) {
-                if (which == 0) {
-                    S.c_old[r] = (double)e;
-                    if (same) S.c_new[r] = (double)e;
-                } else {
-                    S.c_new[r] = (double)e;
+        // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
+        // the Calpha energies before / after each move on warps 0..3 (one warp each)
+        if (warp >= AN_WARPS / 2) {
+            for (int t = tid - AN_THREADS / 2; t < 2 * n; t += AN_THREADS / 2) {
+                const int r = t >> 1;
+                if (S.kind[r] != MV_NONE) build_move(S, r, (t & 1) ? SEL_REJ : SEL_PROP);
+            }
+        } else {
+            for (int t = warp; t < 2 * n; t += AN_WARPS / 2) {
+                const int r = t >> 1, which = t & 1;
+                const int kind = S.kind[r];
+                if (kind == MV_NONE) continue;
+                const bool same = kind == MV_ROT || S.new_aa[r] == S.aa[r];
+                if (which == 1 && same) continue;  // same Calpha, same amino acid: same energy
+                const int a = which ? S.new_aa[r] : S.aa[r];
+                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[r * SLOT_STRIDE + 1]), a, stage);
+                if (lane == 0) {
+                    if (which == 0) {
+                        S.c_old[r] = (double)e;
+                        if (same) S.c_new[r] = (double)e;
+                    } else {
+                        S.c_new[r] = (double)e;
+                    }
                 }
             }
         }
         __syncthreads();
         // the sweep's decisions, in residue order
         if (tid == 0) {
+            int ncys = S.iscal[IS_NCYS];
             bool have_d = false;
             ACC D = 0;
             for (int r = 0; r < n; ++r) {
                 const int kind = S.kind[r];
                 if (kind == MV_NONE) continue;
                 if (!have_d) {
-                    D = disulfide_sweep<ACC>(S, n, -1, nullptr, 0);
+                    D = ncys >= 2 ? disulfide_of<ACC, true>(S, n, -1, nullptr, 0) : (ACC)0;
                     have_d = true;
                 }
                 const int oa = S.aa[r];
                 const int na = kind == MV_MUT ? S.new_aa[r] : oa;
                 const bool cys = oa == CYS || na == CYS;
-                const ACC Dn = cys ? disulfide_sweep<ACC>(S, n, r, S.prop + (size_t)r * SLOT_STRIDE, na) : D;
+                const int ncys_new = ncys + (na == CYS) - (oa == CYS);
+                ACC Dn = D;
+                if (cys)
+                    Dn = ncys_new >= 2 ? disulfide_of<ACC, true>(S, n, r, S.prop + (size_t)r * SLOT_STRIDE, na)
+                                       : (ACC)0;
                 const ACC old_e = (ACC)S.c_old[r] + D;
                 const ACC new_e = (ACC)S.c_new[r] + Dn;
                 const bool acc = metropolis(new_e - old_e, temp, S.u_acc[r]);
@@ -428,16 +584,17 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                     S.trig[2 * r + 1] = make_float4(t.t[2].x, t.t[2].y, t.t[3].x, t.t[3].y);
                     S.c_cur[r] = S.c_new[r];
                     D = Dn;
+                    ncys = ncys_new;
                 } else {
                     S.sel[r] = SEL_REJ;
                     S.c_cur[r] = S.c_old[r];
-                    if (oa == CYS) D = disulfide_sweep<ACC>(S, n, -1, nullptr, 0);  // SG rebuilt
+                    if (oa == CYS && ncys >= 2) D = disulfide_of<ACC, true>(S, n, -1, nullptr, 0);  // SG rebuilt
                 }
                 S.valid[r] = 1;
             }
             if (have_d) {
                 S.dscal[0] = (double)D;
-                S.iscal[0] = 1;
+                S.iscal[IS_DVALID] = 1;
             }
         }
         __syncthreads();
@@ -446,24 +603,25 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
             const int sl = S.sel[r];
             if (sl == SEL_PROP) S.pos[i] = S.prop[i];
             else if (sl == SEL_REJ) S.pos[i] = S.rej[i];
+            if ((i % SLOT_STRIDE) == 0 && S.aa[r] == CYS) atomicMax(&S.iscal[IS_LASTCYS], r);
         }
-        __syncthreads();
-        for (int r = tid; r < n; r += AN_THREADS) S.sel[r] = SEL_KEEP;
         __syncthreads();
 
         // ---- 4. backbone phi/psi moves (diffusion.rs:403-418) ----
+        const int last_cys = S.iscal[IS_LASTCYS];
         for (int r = 0; r < n; ++r) {
             if (!S.bb_att[r]) continue;
             const bool phi = S.bb_phi[r] != 0;
+            const bool cys_down = r <= last_cys;  // a Cys at or after r: the disulfide term can change
             // Calpha energies of residues r..n at the current positions, and the
             // disulfide energy
-            if (tid == 0 && !S.iscal[0]) {
-                S.dscal[0] = (double)disulfide_sweep<ACC>(S, n, -1, nullptr, 0);
-                S.iscal[0] = 1;
+            if (tid == 0 && !S.iscal[IS_DVALID]) {
+                S.dscal[0] = (double)disulfide_of<ACC, false>(S, n, -1, nullptr, 0);
+                S.iscal[IS_DVALID] = 1;
             }
             for (int i = r + warp; i < n; i += AN_WARPS) {
                 if (S.valid[i]) continue;
-                const ACC e = warp_contribution<ACC>(A, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
+                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
                 if (lane == 0) {
                     S.c_cur[i] = (double)e;
                     S.valid[i] = 1;
@@ -475,17 +633,16 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                 for (int i = r; i < n; ++i) old_e += (ACC)S.c_cur[i];
                 old_e += (ACC)S.dscal[0];
             }
-            bool cys_down = false;  // a Cys at or after r: the disulfide term can change
-            for (int i = r; i < n; ++i) cys_down |= S.aa[i] == CYS;
-            rotate_downstream(S, n, r, phi, S.bb_delta[r]);
+            const float4 bt = S.bb_trig[r];
+            rotate_downstream(S, n, r, phi, bt.x, bt.y);
             __syncthreads();
             for (int i = r + 1 + warp; i < n; i += AN_WARPS) {
-                const ACC e = warp_contribution<ACC>(A, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
+                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
                 if (lane == 0) S.c_new[i] = (double)e;
             }
             __syncthreads();
             if (tid == 0) {
-                const ACC Dn = cys_down ? disulfide_sweep<ACC>(S, n, -1, nullptr, 0) : (ACC)S.dscal[0];
+                const ACC Dn = cys_down ? disulfide_of<ACC, false>(S, n, -1, nullptr, 0) : (ACC)S.dscal[0];
                 ACC new_e = 0;
                 new_e += (ACC)S.c_cur[r];
                 for (int i = r + 1; i < n; ++i) new_e += (ACC)S.c_new[i];
@@ -498,13 +655,13 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                     S.dscal[0] = (double)Dn;
                 } else {
                     for (int i = r + 1; i < n; ++i) S.valid[i] = 0;
-                    if (cys_down) S.iscal[0] = 0;
+                    if (cys_down) S.iscal[IS_DVALID] = 0;
                 }
-                S.iscal[1] = acc;
+                S.iscal[IS_DECISION] = acc;
             }
             __syncthreads();
-            if (!S.iscal[1]) {
-                rotate_downstream(S, n, r, phi, -S.bb_delta[r]);
+            if (!S.iscal[IS_DECISION]) {
+                rotate_downstream(S, n, r, phi, bt.z, bt.w);
                 __syncthreads();
             }
         }
@@ -525,24 +682,29 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
     }
 }
 
-size_t anneal_smem(int max_res) { return anneal_smem_bytes(max_res); }
+size_t anneal_smem(int max_res, int max_ag_res, int max_cells) {
+    const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
+    return anneal_smem_bytes(max_res, G, G && max_cells <= CELL_STAGE_MAX ? max_cells : 0);
+}
 
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          uint32_t* err, long long* stats) {
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats) {
     if (st.n_cand <= 0 || n_steps <= 0 || max_res <= 0) return cudaSuccess;
-    const size_t smem = anneal_smem_bytes(max_res);
+    const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
+    const int C = G && max_cells <= CELL_STAGE_MAX ? max_cells : 0;
+    const size_t smem = anneal_smem_bytes(max_res, G, C);
     cudaError_t e;
     if (accumulate == 1) {
         if ((e = cudaFuncSetAttribute(k_anneal<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
             return e;
-        k_anneal<float><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res,
-                                                           err, stats);
+        k_anneal<float><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G,
+                                                           C, err, stats);
     } else {
         if ((e = cudaFuncSetAttribute(k_anneal<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
             return e;
         k_anneal<double><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res,
-                                                            err, stats);
+                                                            G, C, err, stats);
     }
     return cudaGetLastError();
 }

@@ -81,13 +81,13 @@ void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView*
 // ---- k_anneal.cu: Langevin + Metropolis steps, one CTA per candidate ----
 constexpr int ANNEAL_MAX_RES = 128;  // residues per candidate held in shared memory
 cudaError_t anneal_init_tables();
-size_t anneal_smem(int max_res);
+size_t anneal_smem(int max_res, int max_ag_res, int max_cells);
 // accumulate: 1 = the reference's f32 sums, else f32 terms summed in double.
 // stats (may be null): 4 per candidate, += mutation/rotamer tried, accepted,
 // backbone tried, accepted.
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          uint32_t* err, long long* stats);
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats);
 
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
 double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);
