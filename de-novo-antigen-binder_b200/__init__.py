@@ -63,7 +63,7 @@ class Params(C.Structure):
                 ("mutation_p", C.c_float), ("rotamer_move_p", C.c_float), ("backbone_move_p", C.c_float),
                 ("max_torsion_deg", C.c_float), ("iface_cutoff_sq", C.c_float), ("shell_radius", C.c_float),
                 ("max_disp", C.c_float), ("restraint_k", C.c_float), ("ca_cell", C.c_float),
-                ("score_cell", C.c_float), ("accumulate", C.c_int32), ("_reserved", C.c_int32),
+                ("score_cell", C.c_float), ("accumulate", C.c_int32), ("flags", C.c_int32),
                 ("seed", C.c_uint64)]
 
     @classmethod
@@ -73,6 +73,20 @@ class Params(C.Structure):
         for k, v in kw.items():
             setattr(p, k, v)
         return p
+
+
+class LaunchCfg(C.Structure):
+    """binder_launch_cfg (include/binder_gpu.h): launch shapes of the search block."""
+    _fields_ = [("score_warps", C.c_int32), ("score_ctas_per_sm", C.c_int32), ("cg_warps", C.c_int32),
+                ("_pad", C.c_int32)]
+
+    def as_dict(self):
+        return {"score_warps": self.score_warps, "score_ctas_per_sm": self.score_ctas_per_sm,
+                "cg_warps": self.cg_warps}
+
+
+FLAG_GRAPH = 1
+FLAG_AUTOTUNE = 2
 
 
 class RunCfg(C.Structure):
@@ -145,6 +159,9 @@ _SIGS = {
     "binder_state_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
     "binder_default_run_cfg": (None, [C.c_void_p]),
     "binder_run_allatom": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_get_launch_cfg": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_set_launch_cfg": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
 }
 
 
@@ -516,6 +533,21 @@ class GpuContext:
         self._check(lib().binder_run_allatom(self._h, C.byref(cfg), _ptr(cand), _ptr(e)))
         self._sync_state_info()
         return cand.reshape(n_segments, -1), e.reshape(n_segments, -1)
+
+    def launch_cfg(self):
+        c = LaunchCfg()
+        self._check(lib().binder_get_launch_cfg(self._h, C.byref(c)))
+        return c
+
+    def set_launch_cfg(self, score_warps=8, score_ctas_per_sm=4, cg_warps=4):
+        c = LaunchCfg(score_warps, score_ctas_per_sm, cg_warps, 0)
+        self._check(lib().binder_set_launch_cfg(self._h, C.byref(c)))
+
+    def autotune(self, reps=5):
+        """Pick the fastest launch shapes for the resident state; returns them."""
+        c = LaunchCfg()
+        self._check(lib().binder_autotune(self._h, reps, C.byref(c)))
+        return c
 
     def score_state(self, full=False):
         out = np.zeros(self._state_cand, np.float64)

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -176,7 +177,18 @@ struct binder_ctx {
     int ev_blocks = 0;
     int last_k = 0;
     bool async_pending = false;
+    // launch shapes (autotuned) and the CUDA graph of the search block
+    LaunchCfg cfg;
+    cudaGraphExec_t block_graph = nullptr;
+    std::vector<uint64_t> block_graph_sig;  // what the captured launches baked in
+    int block_graph_launches = 0;
+    std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
+    void drop_graph() {
+        if (block_graph) cudaGraphExecDestroy(block_graph);
+        block_graph = nullptr;
+    }
     ~binder_ctx() {
+        drop_graph();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
     }
@@ -523,6 +535,7 @@ void binder_default_params(binder_params* p) {
     p->ca_cell = 10.0f;
     p->score_cell = 8.0f;
     p->accumulate = BINDER_ACC_KAHAN;
+    p->flags = BINDER_FLAG_GRAPH;
     p->seed = 0;
 }
 
@@ -1223,8 +1236,8 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     }
     int s = enqueue_order(ctx);
     if (s) return s;
-    launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise, with_mc,
-                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p);
+    launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
@@ -1234,7 +1247,7 @@ StateScoreScratch score_scratch(binder_ctx* ctx) {
     return StateScoreScratch{S.order_valid ? S.order.p : nullptr, S.queue.p, S.res_e.p, S.res_abs.p};
 }
 
-int persistent_ctas(binder_ctx* ctx) { return ctx->num_sms * 4; }
+int persistent_ctas(binder_ctx* ctx) { return ctx->num_sms * ctx->cfg.score_ctas_per_sm; }
 
 int enqueue_score_state(binder_ctx* ctx, int full) {
     State& S = ctx->st;
@@ -1245,7 +1258,7 @@ int enqueue_score_state(binder_ctx* ctx, int full) {
     }
     ScoreOut o{ctx->energy.p, nullptr, nullptr, nullptr, ctx->errf.p};
     ctx->launches += launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
-                                        score_scratch(ctx), persistent_ctas(ctx)) - 1;
+                                        score_scratch(ctx), persistent_ctas(ctx), ctx->cfg.score_warps) - 1;
     LAUNCHED("score_state");
     return BINDER_OK;
 }
@@ -1274,32 +1287,245 @@ int binder_score_state(binder_ctx* ctx, int full, double* out) {
     return fetch_energies(ctx, ctx->st.n_cand, out, nullptr, nullptr);
 }
 
+}  // extern "C"
+
+namespace {
+// One search block on the context stream: n_steps gradient steps (no noise, so
+// the steps' Philox counters are not read), one score of every candidate, the k
+// lowest per antigen.  ev (4 events) brackets the phases when timing.
+int enqueue_block(binder_ctx* ctx, int n_steps, int k, cudaEvent_t* ev) {
+    State& S = ctx->st;
+    int s;
+    if (ev) CK(cudaEventRecord(ev[0], ctx->stream), "event");
+    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return s;
+    if (ev) CK(cudaEventRecord(ev[1], ctx->stream), "event");
+    if ((s = enqueue_score_state(ctx, 0))) return s;
+    if (ev) CK(cudaEventRecord(ev[2], ctx->stream), "event");
+    if (k > 0) {
+        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
+                             ctx->topk.p);
+        LAUNCHED("topk");
+    }
+    if (ev) CK(cudaEventRecord(ev[3], ctx->stream), "event");
+    return BINDER_OK;
+}
+
+// Everything a captured block bakes into its launches: sizes, buffer addresses,
+// parameters and launch shapes.  Buffer contents are read at replay time.
+std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
+    const State& S = ctx->st;
+    std::vector<uint64_t> v = {
+        (uint64_t)n_steps, (uint64_t)k, (uint64_t)S.n_cand, (uint64_t)S.total_res, (uint64_t)S.n_segments,
+        (uint64_t)S.n_keys, (uint64_t)ctx->cfg.score_warps, (uint64_t)ctx->cfg.score_ctas_per_sm,
+        (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->ags.size()};
+    const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
+                          S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
+                          S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
+                          ctx->energy.p, ctx->topk.p, ctx->errf.p, ctx->d_views.p};
+    for (const void* q : ptrs) v.push_back((uint64_t)(uintptr_t)q);
+    unsigned char pb[sizeof(binder_params)];
+    std::memcpy(pb, &ctx->params, sizeof(pb));
+    for (size_t i = 0; i < sizeof(pb); i += 8) {
+        uint64_t w = 0;
+        std::memcpy(&w, pb + i, std::min<size_t>(8, sizeof(pb) - i));
+        v.push_back(w);
+    }
+    return v;
+}
+
+// Capture enqueue_block into ctx->block_graph (buffers are sized beforehand, so
+// the capture allocates nothing).
+int capture_block(binder_ctx* ctx, int n_steps, int k) {
+    ctx->drop_graph();
+    const uint64_t l0 = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int s = enqueue_block(ctx, n_steps, k, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (s || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        ctx->launches = l0;
+        return s ? s : cuda_fail(ctx, e, "end capture");
+    }
+    e = cudaGraphInstantiate(&ctx->block_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->block_graph = nullptr;
+        ctx->launches = l0;
+        return cuda_fail(ctx, e, "graph instantiate");
+    }
+    ctx->block_graph_launches = (int)(ctx->launches - l0);
+    ctx->launches = l0;
+    ctx->block_graph_sig = block_sig(ctx, n_steps, k);
+    return BINDER_OK;
+}
+
+std::string tune_key(binder_ctx* ctx) {
+    const State& S = ctx->st;
+    std::string k = "sm" + std::to_string(ctx->num_sms) + ":c" + std::to_string(S.n_cand) + ":r" +
+                    std::to_string(S.total_res) + ":m" + std::to_string(S.max_res);
+    for (const auto& a : ctx->ags) k += ":a" + std::to_string(a->n_atoms) + "/" + std::to_string(a->n_res);
+    return k;
+}
+
+void tune_cache_load(binder_ctx* ctx) {
+    const char* path = std::getenv("BINDER_TUNE_CACHE");
+    if (!path || !ctx->tune_cache.empty()) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[1024];
+    LaunchCfg c;
+    while (std::fscanf(f, "%1023s %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps) == 4)
+        ctx->tune_cache.emplace_back(key, c);
+    std::fclose(f);
+}
+
+void tune_cache_store(binder_ctx* ctx, const std::string& key, const LaunchCfg& c) {
+    ctx->tune_cache.emplace_back(key, c);
+    const char* path = std::getenv("BINDER_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps);
+    std::fclose(f);
+}
+
+// Median device time (ms) of `reps` runs of fn on the context stream.
+template <class F>
+int time_ms(binder_ctx* ctx, int reps, F&& fn, float* out) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a), "event");
+    CK(cudaEventCreate(&b), "event");
+    std::vector<float> t;
+    int s = BINDER_OK;
+    for (int i = 0; i <= reps && !s; ++i) {
+        cudaEventRecord(a, ctx->stream);
+        s = fn();
+        cudaEventRecord(b, ctx->stream);
+        cudaError_t e = cudaEventSynchronize(b);
+        if (!s && e != cudaSuccess) s = cuda_fail(ctx, e, "autotune");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (i) t.push_back(ms);  // the first run warms up
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (s) return s;
+    std::sort(t.begin(), t.end());
+    *out = t[t.size() / 2];
+    return BINDER_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out) {
+    if (!ctx || !out) return BINDER_ERR_ARG;
+    out->score_warps = ctx->cfg.score_warps;
+    out->score_ctas_per_sm = ctx->cfg.score_ctas_per_sm;
+    out->cg_warps = ctx->cfg.cg_warps;
+    out->_pad = 0;
+    return BINDER_OK;
+}
+
+int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
+    if (!ctx || !c) return BINDER_ERR_ARG;
+    if ((c->score_warps != 4 && c->score_warps != 8 && c->score_warps != 16) || c->score_ctas_per_sm < 1 ||
+        c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8))
+        return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
+    ctx->cfg.score_warps = c->score_warps;
+    ctx->cfg.score_ctas_per_sm = c->score_ctas_per_sm;
+    ctx->cfg.cg_warps = c->cg_warps;
+    return BINDER_OK;
+}
+
+int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (reps < 1) reps = 5;
+    tune_cache_load(ctx);
+    const std::string key = tune_key(ctx);
+    for (const auto& e : ctx->tune_cache)
+        if (e.first == key) {
+            ctx->cfg = e.second;
+            return out ? binder_get_launch_cfg(ctx, out) : BINDER_OK;
+        }
+    if ((s = clear_err(ctx))) return s;
+    CK(ctx->energy.ensure(S.n_cand), "alloc");
+    // gradient steps move the candidates: time them on a copy and put the state back
+    DBuf<float4> saved;
+    const size_t n_slots = (size_t)S.total_res * SLOT_STRIDE;
+    CK(saved.ensure(n_slots), "alloc");
+    CK(cudaMemcpyAsync(saved.p, S.res_pos.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    LaunchCfg best = ctx->cfg;
+    float best_ms = 1e30f;
+    for (int w : {2, 4, 8}) {
+        ctx->cfg.cg_warps = w;
+        float ms = 0.f;
+        if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
+        if (ms < best_ms) { best_ms = ms; best.cg_warps = w; }
+        CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream),
+           "copy");
+    }
+    best_ms = 1e30f;
+    for (int nw : {4, 8, 16})
+        for (int per_sm : {1, 2, 4, 8}) {
+            if (s) break;
+            ctx->cfg.score_warps = nw;
+            ctx->cfg.score_ctas_per_sm = per_sm;
+            float ms = 0.f;
+            if ((s = time_ms(ctx, reps, [&] { return enqueue_score_state(ctx, 0); }, &ms))) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.score_warps = nw;
+                best.score_ctas_per_sm = per_sm;
+            }
+        }
+    CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    ctx->cfg = best;
+    if (s) return s;
+    if ((s = check_err(ctx))) return s;
+    tune_cache_store(ctx, key, best);
+    return out ? binder_get_launch_cfg(ctx, out) : BINDER_OK;
+}
+
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_e, int32_t* out_topk) {
+    (void)step0;
     int s = enter(ctx);
     if (s) return s;
     State& S = ctx->st;
     if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
     if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
     const bool async = out_e == nullptr && out_topk == nullptr;
+    if ((ctx->params.flags & BINDER_FLAG_AUTOTUNE) && !ctx->async_pending) {
+        const std::string key = tune_key(ctx);
+        bool known = false;
+        for (const auto& e : ctx->tune_cache) known |= e.first == key;
+        if (!known && (s = binder_autotune(ctx, 5, nullptr))) return s;
+    }
     // the device error word accumulates over a run of enqueued blocks until fetched
     if (!ctx->async_pending && (s = clear_err(ctx))) return s;
     ctx->async_pending = async;
+    CK(ctx->energy.ensure(S.n_cand), "alloc");
+    if (k > 0) CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
     const bool tm = ctx->timing && ctx->ev_blocks < TIMING_RING;
-    cudaEvent_t* ev = tm ? &ctx->ev[4 * ctx->ev_blocks] : nullptr;
-    if (tm) CK(cudaEventRecord(ev[0], ctx->stream), "event");
-    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, step0, 0, 0, nullptr))) return s;
-    if (tm) CK(cudaEventRecord(ev[1], ctx->stream), "event");
-    if ((s = enqueue_score_state(ctx, 0))) return s;
-    if (tm) CK(cudaEventRecord(ev[2], ctx->stream), "event");
-    if (k > 0) {
-        CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
-        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
-                             ctx->topk.p);
-        LAUNCHED("topk");
-    }
     if (tm) {
-        CK(cudaEventRecord(ev[3], ctx->stream), "event");
+        // per-phase events: the launches are issued one by one
+        if ((s = enqueue_block(ctx, n_steps, k, &ctx->ev[4 * ctx->ev_blocks]))) return s;
         ctx->ev_blocks++;
+    } else if (ctx->params.flags & BINDER_FLAG_GRAPH) {
+        if (!ctx->block_graph || ctx->block_graph_sig != block_sig(ctx, n_steps, k)) {
+            if ((s = capture_block(ctx, n_steps, k))) return s;
+        }
+        CK(cudaGraphLaunch(ctx->block_graph, ctx->stream), "graph launch");
+        ctx->launches += ctx->block_graph_launches;
+        S.order_valid = true;
+    } else if ((s = enqueue_block(ctx, n_steps, k, nullptr))) {
+        return s;
     }
     ctx->last_k = k;
     if (async) return BINDER_OK;

@@ -592,21 +592,31 @@ __global__ void k_sum_residues(StateView st, const double* __restrict__ res_e, c
     if (out_abs) out_abs[c] = ea;
 }
 
-int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& o, const StateScoreScratch& scr, int grid_ctas) {
-    if (st.n_cand <= 0) return 0;
-    const bool kahan = accumulate == 0, abs_ = o.abs_sum != nullptr, count = o.pairs != nullptr;
-    const int g = grid_ctas > 0 ? grid_ctas : 148 * 4;
-    cudaMemsetAsync(scr.queue, 0, sizeof(int), s);
+template <int NW>
+static void score_residues_nw(cudaStream_t s, int g, const StateView& st, const AgView* ags, bool kahan, bool full,
+                              bool abs_, bool count, const ScoreOut& o, const StateScoreScratch& scr) {
 #define BINDER_R(K, FU, A, C)                                                                                    \
-    k_score_residues<NW_SCORE, K, FU, A, C><<<g, NW_SCORE * 32, 0, s>>>(st, ags, scr.order, scr.queue,          \
-                                                                      count ? nullptr : scr.res_e,            \
-                                                                      scr.res_abs, o.pairs, o.err)
+    k_score_residues<NW, K, FU, A, C><<<g, NW * 32, 0, s>>>(st, ags, scr.order, scr.queue,                      \
+                                                            count ? nullptr : scr.res_e, scr.res_abs, o.pairs,  \
+                                                            o.err)
     if (count) BINDER_R(true, false, false, true);
     else if (full) BINDER_R(true, true, false, false);
     else if (abs_) { if (kahan) BINDER_R(true, false, true, false); else BINDER_R(false, false, true, false); }
     else { if (kahan) BINDER_R(true, false, false, false); else BINDER_R(false, false, false, false); }
 #undef BINDER_R
+}
+
+int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
+                       const ScoreOut& o, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta) {
+    if (st.n_cand <= 0) return 0;
+    const bool kahan = accumulate == 0, abs_ = o.abs_sum != nullptr, count = o.pairs != nullptr;
+    const int g = grid_ctas > 0 ? grid_ctas : 148 * 4;
+    cudaMemsetAsync(scr.queue, 0, sizeof(int), s);
+    switch (warps_per_cta) {
+        case 4: score_residues_nw<4>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
+        case 16: score_residues_nw<16>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
+        default: score_residues_nw<8>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
+    }
     if (!count)
         k_sum_residues<<<(st.n_cand + 127) / 128, 128, 0, s>>>(st, scr.res_e, abs_ ? scr.res_abs : nullptr, full,
                                                                o.energy, o.abs_sum);
@@ -617,7 +627,7 @@ void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView*
                               uint32_t* err, const StateScoreScratch& scr, int grid_ctas) {
     if (st.n_cand <= 0) return;
     ScoreOut o{nullptr, nullptr, nullptr, pairs, err};
-    launch_score_state(s, st, ags, 0, 0, o, scr, grid_ctas);
+    launch_score_state(s, st, ags, 0, 0, o, scr, grid_ctas, NW_SCORE);
 }
 
 }  // namespace binder

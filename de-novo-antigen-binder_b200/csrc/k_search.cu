@@ -73,17 +73,19 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 // (the same sequence of roundings as set_ca_pos, allatom.rs:279-293).
 // COUNT: count the in-cutoff pairs of the same trajectory, leave the state as is.
 constexpr int CG_GROUP = 4;
-constexpr int CG_TERMS = 24;      // in-cutoff terms a lane holds per step
-constexpr int CG_WARPS = 4;       // warps per CTA
+// in-cutoff terms a lane holds per step (static shared memory stays under 48 KB)
+template <int CG_WARPS>
+constexpr int cg_terms() { return CG_WARPS >= 8 ? 15 : 24; }
 constexpr int CG_MAX_STEPS = 32;  // steps per launch (the host splits longer runs)
 
-template <bool COUNT>
+template <bool COUNT, int CG_WARPS>
 __global__ void __launch_bounds__(CG_WARPS * 32) k_langevin(StateView st, const AgView* __restrict__ ags,
                                                              StepParams p, int n_steps, uint32_t step0,
                                                              int with_noise, const float* __restrict__ temps,
                                                              uint32_t* __restrict__ err,
                                                              long long* __restrict__ pair_count,
                                                              const int* __restrict__ order) {
+    constexpr int CG_TERMS = cg_terms<CG_WARPS>();
     __shared__ float3 s_terms[CG_WARPS * 32][CG_TERMS];
     const int lane = threadIdx.x & 31;
     const int gl = lane & (CG_GROUP - 1);
@@ -269,26 +271,35 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
     k_res_scatter<<<(st.total_res + 255) / 256, 256, 0, s>>>(st.total_res, keys, cursor, order);
 }
 
-void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
-                    uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err,
-                    const int* order) {
-    if (st.total_res <= 0 || n_steps <= 0) return;
-    (void)with_mc;
-    const int threads = CG_WARPS * 32;
+template <int W>
+static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                      uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order) {
+    const int threads = W * 32;
     const long long total = (long long)st.total_res * CG_GROUP;
     for (int s0 = 0; s0 < n_steps; s0 += CG_MAX_STEPS) {
         const int ns = min(CG_MAX_STEPS, n_steps - s0);
-        k_langevin<false><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
+        k_langevin<false, W><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
             st, ags, p, ns, step0 + (uint32_t)s0, with_noise, temps ? temps + s0 : nullptr, err, nullptr, order);
+    }
+}
+
+void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                    uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
+                    int warps_per_cta) {
+    if (st.total_res <= 0 || n_steps <= 0) return;
+    switch (warps_per_cta) {
+        case 2: diffuse_w<2>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+        case 8: diffuse_w<8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+        default: diffuse_w<4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
     }
 }
 
 void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           long long* pairs) {
     if (st.total_res <= 0 || n_steps <= 0) return;
-    const int threads = CG_WARPS * 32;
+    const int threads = 4 * 32;
     const long long total = (long long)st.total_res * CG_GROUP;
-    k_langevin<true><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
+    k_langevin<true, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
         st, ags, p, min(n_steps, CG_MAX_STEPS), 0, 0, nullptr, nullptr, pairs, nullptr);
 }
 
@@ -311,6 +322,7 @@ __global__ void k_unpack_slots(int n_res, const float4* __restrict__ in, float* 
     const float4 v = in[r * SLOT_STRIDE + k];
     out[3 * t] = v.x; out[3 * t + 1] = v.y; out[3 * t + 2] = v.z;
 }
+
 // ---- resident-state gather (survivor selection) -------------------------------------
 __global__ void k_gather_state(int total, const int* __restrict__ map, const uint8_t* __restrict__ aa,
                                const float4* __restrict__ chi, const float4* __restrict__ trig,

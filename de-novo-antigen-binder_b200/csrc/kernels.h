@@ -6,6 +6,15 @@
 
 namespace binder {
 
+// Launch shapes of the search block, chosen by the autotuner (results do not
+// depend on them: every residue is computed by the same lanes with the same
+// arithmetic whatever the grid).
+struct LaunchCfg {
+    int score_warps = 8;         // warps per CTA of the persistent scoring kernel (4, 8, 16)
+    int score_ctas_per_sm = 4;   // persistent scoring CTAs per SM
+    int cg_warps = 4;            // warps per CTA of the gradient-step kernel (2, 4, 8)
+};
+
 // ---- k_grid.cu: SpatialHashGrid ----
 void launch_cell_coords(cudaStream_t s, const float* x, const float* y, const float* z, int n, float inv, int4* cells,
                         int* minmax, uint32_t* err);
@@ -44,7 +53,7 @@ struct StateScoreScratch {
     double* res_abs;   // total_res (abs sums)
 };
 int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& out, const StateScoreScratch& scr, int grid_ctas);
+                       const ScoreOut& out, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta);
 
 void launch_uniform_offsets(cudaStream_t s, long long* off, int n_cand, long long n_ab);
 
@@ -60,8 +69,8 @@ void launch_build_residues(cudaStream_t s, int n, const float* ca_xyz, const uin
 void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const float* by, const float* bz,
                       const uint8_t* baa, int n, float* fx, float* fy, float* fz);
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
-                    uint32_t step0, int with_noise, int with_mc, const float* temps, uint32_t* err,
-                    const int* order);
+                    uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
+                    int warps_per_cta);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);

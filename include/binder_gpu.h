@@ -102,12 +102,17 @@ typedef struct binder_params {
     float ca_cell;          /* Calpha grid cell for the CG force, 10 A */
     float score_cell;       /* all-atom grid cell for scoring, 8 A */
     int32_t accumulate;     /* BINDER_ACC_KAHAN (default) or BINDER_ACC_F32 */
-    int32_t _reserved;
+    int32_t flags;          /* BINDER_FLAG_* (default BINDER_FLAG_GRAPH) */
     uint64_t seed;          /* Philox key for every stochastic move */
 } binder_params;
 
 #define BINDER_ACC_KAHAN 0  /* f32 pair terms, compensated per-lane sums, FP64 cross-lane/block reduction */
 #define BINDER_ACC_F32 1    /* f32 pair terms, plain f32 per-lane sums, FP64 cross-lane/block reduction */
+/* binder_block replays a CUDA graph of its launches (captured on first use,
+   re-captured when the state, parameters or launch shapes change) */
+#define BINDER_FLAG_GRAPH 1
+/* the first binder_block on a new state shape runs binder_autotune */
+#define BINDER_FLAG_AUTOTUNE 2
 
 /* ---- force-field tables compiled into the library (amber.rs, rotamer.rs) ----
    Residue aa: its atom count and per-slot partial charge, AMBER type and
@@ -271,6 +276,24 @@ int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
    block and reports any device error. */
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_energies, int32_t* out_topk);
 int binder_block_fetch(binder_ctx* ctx, double* out_energies, int32_t* out_topk);
+
+/* ---- launch shapes and the autotuner (no reference counterpart) ----------------
+   Results never depend on these: every residue is computed by the same lanes with
+   the same arithmetic whatever the grid. */
+typedef struct binder_launch_cfg {
+    int32_t score_warps;        /* warps per CTA of the persistent scoring kernel: 4, 8, 16 */
+    int32_t score_ctas_per_sm;  /* persistent scoring CTAs per SM: 1..32 */
+    int32_t cg_warps;           /* warps per CTA of the gradient-step kernel: 2, 4, 8 */
+    int32_t _pad;
+} binder_launch_cfg;
+int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
+int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
+/* Time every launch shape on the resident state (median of reps runs each; the
+   gradient steps run on a copy of the positions, which are put back), keep the
+   fastest and remember it per state shape (candidate / residue counts, antigen
+   sizes, SM count).  With the environment variable BINDER_TUNE_CACHE naming a
+   file, choices are read from and appended to it.  out may be NULL. */
+int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out);
 
 /* run_allatom (diffusion.rs:983-1107) on the resident state: phase 1 runs
    phase1_steps steps on every candidate in blocks of score_every (score + the

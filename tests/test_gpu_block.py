@@ -1,0 +1,106 @@
+"""The search block through its CUDA graph, every launch shape and the autotuner:
+results are bit-identical to the eagerly launched block (launch shapes only change
+which warp takes which residue, never the arithmetic)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(ctx, oracle, pkg, n_cand=256, flags=None):
+    cfg = pkg.workloads.config1(n_cand=n_cand)
+    ag_aa, ag_ca = cfg["antigens"][0]
+    ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    kw = {} if flags is None else {"flags": flags}
+    ctx.set_params(pkg.Params.defaults(shell_radius=cfg["shell"][0], seed=5, **kw))
+    ctx.add_antigen(ag_aa, ag_pos)
+    pop = cfg["pop"]
+    n_res = int(pop.n_res[0])
+    aa = pop.aa[: n_cand * n_res].copy()
+    pos, chi = oracle.build_residues(pop.ca[: n_cand * n_res], aa)
+    return aa, chi, pos, n_res
+
+
+def _run_blocks(ctx, aa, chi, pos, n_res, n_blocks=3):
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    outs = [ctx.block(10, 10 * b, k=64) for b in range(n_blocks)]
+    return outs, ctx.state_download()
+
+
+def _same(a, b):
+    (oa, sa), (ob, sb) = a, b
+    for (ea, ta), (eb, tb) in zip(oa, ob):
+        assert np.array_equal(ea, eb) and np.array_equal(ta, tb)
+    for x, y in zip(sa, sb):
+        assert np.array_equal(x, y)
+
+
+def test_graph_block_matches_eager(ctx, oracle, pkg):
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, flags=0)
+    eager = _run_blocks(ctx, aa, chi, pos, n_res)
+    ctx.set_params(pkg.Params.defaults(shell_radius=ctx.params.shell_radius, seed=5, flags=pkg.FLAG_GRAPH))
+    n0 = ctx.launch_count
+    graph = _run_blocks(ctx, aa, chi, pos, n_res)
+    assert ctx.launch_count > n0
+    _same(eager, graph)
+    # a new upload (new buffers) re-captures the graph
+    again = _run_blocks(ctx, aa, chi, pos, n_res)
+    _same(eager, again)
+
+
+@pytest.mark.parametrize("shape", [(4, 1, 2), (16, 8, 8), (8, 2, 4)])
+def test_launch_shapes_bit_identical(ctx, oracle, pkg, shape):
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg)
+    ctx.set_launch_cfg(8, 4, 4)
+    ref = _run_blocks(ctx, aa, chi, pos, n_res)
+    ctx.set_launch_cfg(*shape)
+    got = _run_blocks(ctx, aa, chi, pos, n_res)
+    ctx.set_launch_cfg(8, 4, 4)
+    _same(ref, got)
+
+
+def test_autotune_restores_state_and_caches(ctx, oracle, pkg, tmp_path, monkeypatch):
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg)
+    ref = _run_blocks(ctx, aa, chi, pos, n_res)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    cfg = ctx.autotune(reps=2)
+    assert cfg.score_warps in (4, 8, 16) and cfg.cg_warps in (2, 4, 8) and 1 <= cfg.score_ctas_per_sm <= 8
+    _, _, p_after = ctx.state_download()
+    assert np.array_equal(p_after, pos)  # the timing runs worked on a copy
+    got = [ctx.block(10, 10 * b, k=64) for b in range(3)], ctx.state_download()
+    _same(ref, got)
+    # a fresh context finds the choice in the cache file and does not re-tune
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("BINDER_TUNE_CACHE", str(cache))
+    c2 = pkg.GpuContext.create(0)
+    try:
+        _setup(c2, oracle, pkg)
+        c2.state_upload(aa, chi, pos, uniform_n_res=n_res)
+        first = c2.autotune(reps=2)
+        lines = cache.read_text().splitlines()
+        assert len(lines) == 1
+        c3 = pkg.GpuContext.create(0)
+        try:
+            _setup(c3, oracle, pkg)
+            c3.state_upload(aa, chi, pos, uniform_n_res=n_res)
+            again = c3.autotune(reps=2)
+            assert again.as_dict() == first.as_dict()
+            assert len(cache.read_text().splitlines()) == 1
+        finally:
+            c3.close()
+    finally:
+        c2.close()
+
+
+def test_autotune_flag_in_block(ctx, oracle, pkg):
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, n_cand=128, flags=pkg.FLAG_GRAPH | pkg.FLAG_AUTOTUNE)
+    ref_ctx = pkg.GpuContext.create(0)
+    try:
+        _setup(ref_ctx, oracle, pkg, n_cand=128, flags=0)
+        ref = _run_blocks(ref_ctx, aa, chi, pos, n_res)
+    finally:
+        ref_ctx.close()
+    got = _run_blocks(ctx, aa, chi, pos, n_res)
+    _same(ref, got)
+    ctx.set_params(pkg.Params.defaults(shell_radius=ctx.params.shell_radius, seed=5))
