@@ -6,6 +6,10 @@ candidate (coarse-grained grid force, restraint, 2 A clamp, rigid residue
 translation), one all-atom LJ + Coulomb + hydrophobic score of every candidate,
 and the top-64 survivor selection.  Workload: 1024 antibodies x 20 residues
 against a 300-residue (2505-atom) compact globule, seeded synthetic inputs.
+Steps walk through phase-1 passes: blocks 0..19 (gradient steps 0..199) from
+the initial population, then the population is reset (outside the timed
+events) and the next pass starts, so every timed block is a block of the
+200-step phase the workload defines.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -35,6 +39,7 @@ sys.path.insert(0, str(ROOT))
 N_STEPS_PER_BLOCK = 10
 TOP_K = 64
 PHASE1_STEPS = 200   # GPU_STEPS (diffusion.rs:1018)
+PHASE1_BLOCKS = PHASE1_STEPS // N_STEPS_PER_BLOCK
 PHASE2_STEPS = 600   # Langevin + Metropolis steps on the survivors
 # Algorithmic flops per in-cutoff pair (FADD/FMUL = 1, FFMA = 2, rsqrt/sqrt/div
 # MUFU sequences not counted):
@@ -55,7 +60,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -68,7 +73,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                          "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -173,7 +178,10 @@ def cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, ste
 
 
 def cpu_sample(orc, cfg, ag_aa, ag_pos, pop, target_s, threads, n_max=None):
-    """Time the reference algorithm on a bounded sample of the candidates."""
+    """Time the reference algorithm on a bounded sample: candidates are doubled
+    until one block takes a quarter of target_s (or all are in), then blocks of a
+    phase-1 pass are run until target_s is spent.  Returns (candidates, blocks,
+    seconds, ...)."""
     n_res = int(pop.n_res[0])
     A = orc.Antigen(ag_aa, ag_pos)
     prm = orc.OrcParams.defaults(shell_radius=float(cfg["shell"][0]))
@@ -189,7 +197,13 @@ def cpu_sample(orc, cfg, ag_aa, ag_pos, pop, target_s, threads, n_max=None):
         if dt > 0.25 * target_s or n >= n_total:
             break
         n = min(n_total, max(n * 2, int(n * 0.5 * target_s / max(dt, 1e-6))))
-    return n, dt, A, prm, ag_atoms, n_res
+    blocks = 1
+    while dt < target_s and blocks < PHASE1_BLOCKS:
+        t0 = time.perf_counter()
+        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, blocks * N_STEPS_PER_BLOCK)
+        dt += time.perf_counter() - t0
+        blocks += 1
+    return n, blocks, dt, A, prm, ag_atoms, n_res
 
 
 def run_reference(args, rank, world):
@@ -206,21 +220,23 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     # each step: one block over a sample sized so the whole K+W run stays within minutes
     budget = max(0.5, min(4.0, 150.0 / max(1, args.steps + args.warmup)))
-    n, _, A, prm, ag_atoms, n_res = cpu_sample(orc, cfg, ag_aa, ag_pos, pop, budget, threads)
-    aa = pop.aa[: n * n_res].copy()
-    pos, chi = orc.build_residues(pop.ca[: n * n_res], aa)
-    for w in range(args.warmup):
-        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, w * N_STEPS_PER_BLOCK)
+    n, _, _, A, prm, ag_atoms, n_res = cpu_sample(orc, cfg, ag_aa, ag_pos, pop, budget, threads)
+    aa0 = pop.aa[: n * n_res].copy()
+    pos0, chi0 = orc.build_residues(pop.ca[: n * n_res], aa0)
+    aa, chi, pos = aa0.copy(), chi0.copy(), pos0.copy()
     times = []
-    for k in range(args.steps):
+    for k in range(args.warmup + args.steps):
+        b = k % PHASE1_BLOCKS  # phase-1 passes, as in the GPU arm
+        if b == 0:
+            aa[:], chi[:], pos[:] = aa0, chi0, pos0
         t0 = time.perf_counter()
-        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads,
-                            (args.warmup + k) * N_STEPS_PER_BLOCK)
-        times.append(time.perf_counter() - t0)
+        cpu_reference_block(orc, A, prm, aa, chi, pos, n_res, ag_atoms, threads, b * N_STEPS_PER_BLOCK)
+        if k >= args.warmup:
+            times.append(time.perf_counter() - t0)
     ms = 1e3 * statistics.mean(times)
     value = n * N_STEPS_PER_BLOCK / (ms / 1e3)
     sample = (f"{n} of 1024 candidates per step (10 gradient steps + brute-force f32 score + top-64), "
-              f"CPU restatement of the reference")
+              f"phase-1 passes of 20 blocks, CPU restatement of the reference")
     line = {"impl": "reference", "metric": "candidate-steps/s", "value": value, "unit": "candidate-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -283,6 +299,7 @@ def workload_config():
             "gradient_steps_per_block": N_STEPS_PER_BLOCK, "top_k": TOP_K, "score_cell_A": 8.0,
             "cutoff_A": 10.0, "ca_cell_A": 10.0,
             "l2": "256 MiB buffer written between timed steps (flush); working set 5 MiB",
+            "steps": "blocks 0..19 of 200-step phase-1 passes from the initial population, repeated",
             "precision": "f32 pair terms, Kahan lane sums, FP64 reductions"}
 
 
@@ -302,43 +319,57 @@ def run_ours(args, rank, world, local_rank):
     # launch shapes for this state (autotuner; results do not depend on them), then
     # warm-up (untimed; the first block captures the CUDA graph of a block)
     tuned = ctx.autotune(reps=5).as_dict()
-    for w in range(args.warmup):
-        ctx.block_async(N_STEPS_PER_BLOCK, w * N_STEPS_PER_BLOCK, TOP_K)
-    ctx.block_fetch(TOP_K)
 
-    # algorithmic work of the timed blocks: in-cutoff pairs (counted, untimed, state unchanged)
-    cg_pairs, score_pairs = ctx.state_pair_counts(N_STEPS_PER_BLOCK)
+    def reset():  # start of a phase-1 pass: the initial population (same buffers, same graph)
+        ctx.state_upload(pop.aa, chi, pos, uniform_n_res=n_res)
+
+    for w in range(args.warmup):
+        if w % PHASE1_BLOCKS == 0:
+            reset()
+        ctx.block_async(N_STEPS_PER_BLOCK, (w % PHASE1_BLOCKS) * N_STEPS_PER_BLOCK, TOP_K)
+    ctx.block_fetch(TOP_K)
 
     sampler = ClockSampler(local_rank)
     sampler.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    launches0 = ctx.launch_count
+    launches = 0
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    step0 = args.warmup * N_STEPS_PER_BLOCK
     for k in range(args.steps):
+        b = (args.warmup + k) % PHASE1_BLOCKS
+        if b == 0:
+            reset()  # host upload, before the start event
         with torch.cuda.stream(ext):
             flush.zero_()  # L2 flush between timed steps, outside the timed events
             starts[k].record(ext)
-        ctx.block_async(N_STEPS_PER_BLOCK, step0 + k * N_STEPS_PER_BLOCK, TOP_K)
+        l0 = ctx.launch_count
+        ctx.block_async(N_STEPS_PER_BLOCK, b * N_STEPS_PER_BLOCK, TOP_K)
+        launches += ctx.launch_count - l0
         with torch.cuda.stream(ext):
             stops[k].record(ext)
     e_last, top_last = ctx.block_fetch(TOP_K)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    launches = ctx.launch_count - launches0
     clocks = sampler.stop()
-    # per-phase device times: a second pass of eagerly issued blocks with events
-    # between the phases (the graph replay above has none)
+    # per-phase device times and in-cutoff pair counts over one phase-1 pass: eagerly
+    # issued blocks with events between the phases (the graph replay above has none);
+    # pairs counted before each block on the same state (untimed, state unchanged)
+    reset()
+    cg_pairs = score_pairs = 0
     ctx.set_timing(True)
-    for k in range(min(args.steps, 50)):
-        ctx.block_async(N_STEPS_PER_BLOCK, 0, TOP_K)
+    for b in range(PHASE1_BLOCKS):
+        cg, sc = ctx.state_pair_counts(N_STEPS_PER_BLOCK)
+        cg_pairs += cg
+        score_pairs += sc
+        ctx.block_async(N_STEPS_PER_BLOCK, b * N_STEPS_PER_BLOCK, TOP_K)
     ctx.block_fetch(TOP_K)
     phase_ms, n_blocks = ctx.timing_summary()
     ctx.set_timing(False)
+    cg_pairs /= PHASE1_BLOCKS
+    score_pairs /= PHASE1_BLOCKS
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
     ms_local = statistics.mean(step_ms)
     ms = max_over_ranks(torch, dist, world, ms_local, device)
@@ -353,14 +384,15 @@ def run_ours(args, rank, world, local_rank):
     h_pos = torch.empty((n_cand * n_res, 14, 3), dtype=torch.float32, pin_memory=True).numpy()
     h_e = torch.empty(n_cand, dtype=torch.float64, pin_memory=True).numpy()
     h_top = torch.empty(TOP_K, dtype=torch.int32, pin_memory=True).numpy()
-    a0, c0, p0 = ctx.state_download()
-    h_aa[:], h_chi[:], h_pos[:] = a0, c0, p0
     e2e_steps = max(1, min(args.steps, 200))
     t_e2e = []
     for k in range(e2e_steps + 1):
+        b = k % PHASE1_BLOCKS
+        if b == 0:  # phase-1 pass from the initial population
+            h_aa[:], h_chi[:], h_pos[:] = pop.aa, chi, pos
         t0 = time.perf_counter()
         ctx.state_upload(h_aa, h_chi, h_pos, uniform_n_res=n_res)
-        ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K, out_e=h_e, out_top=h_top)
+        ctx.block(N_STEPS_PER_BLOCK, b * N_STEPS_PER_BLOCK, TOP_K, out_e=h_e, out_top=h_top)
         ctx.state_download(h_aa, h_chi, h_pos)
         if k:  # first iteration warms the pinned paths
             t_e2e.append(time.perf_counter() - t0)
@@ -417,18 +449,18 @@ def run_ours(args, rank, world, local_rank):
         sys.path.insert(0, str(ROOT / "tests"))
         import oracle_ctypes as orc
         threads = os.cpu_count() or 1
-        n, dt, *_ = cpu_sample(orc, cfg, ag_aa, np.ascontiguousarray(ag_pos), pop, args.cpu_seconds, threads)
-        line["cpu_baseline"] = {"value": n * N_STEPS_PER_BLOCK / dt, "unit": "candidate-steps/s", "cores": threads,
-                                "kind": "port",
-                                "sample": f"one block (10 gradient steps + brute-force f32 score + top-64) over "
-                                          f"{n} of 1024 candidates, {dt:.1f} s"}
+        n, nb, dt, *_ = cpu_sample(orc, cfg, ag_aa, np.ascontiguousarray(ag_pos), pop, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": n * nb * N_STEPS_PER_BLOCK / dt, "unit": "candidate-steps/s",
+                                "cores": threads, "kind": "port",
+                                "sample": f"blocks 0..{nb - 1} of a phase-1 pass (10 gradient steps + brute-force "
+                                          f"f32 score + top-64 each) over {n} of 1024 candidates, {dt:.1f} s"}
         ms_steps, mdt = cpu_mc_sample(orc, cfg, ag_aa, np.ascontiguousarray(ag_pos), *surv_state, n_res,
                                       args.cpu_seconds / 3, threads)
         cpu_p2 = len(surv_state[0]) // n_res * ms_steps / mdt
         line["phase2"]["cpu_baseline"] = {
             "value": cpu_p2, "unit": "candidate-steps/s", "cores": threads, "kind": "port",
             "sample": f"{ms_steps} of {PHASE2_STEPS} phase-2 steps on the 64 survivors, {mdt:.1f} s"}
-        cpu_run_s = n_cand * PHASE1_STEPS / (n * N_STEPS_PER_BLOCK / dt) + TOP_K * PHASE2_STEPS / cpu_p2
+        cpu_run_s = n_cand * PHASE1_STEPS / (n * nb * N_STEPS_PER_BLOCK / dt) + TOP_K * PHASE2_STEPS / cpu_p2
         line["run_allatom"]["cpu_estimate_ms"] = 1e3 * cpu_run_s
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -459,7 +491,7 @@ def run_phase2_only(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

@@ -1237,7 +1237,7 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     int s = enqueue_order(ctx);
     if (s) return s;
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
-                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps);
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
@@ -1317,7 +1317,7 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
     std::vector<uint64_t> v = {
         (uint64_t)n_steps, (uint64_t)k, (uint64_t)S.n_cand, (uint64_t)S.total_res, (uint64_t)S.n_segments,
         (uint64_t)S.n_keys, (uint64_t)ctx->cfg.score_warps, (uint64_t)ctx->cfg.score_ctas_per_sm,
-        (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->ags.size()};
+        (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->cfg.cg_lanes, (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
                           S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
@@ -1376,7 +1376,8 @@ void tune_cache_load(binder_ctx* ctx) {
     if (!f) return;
     char key[1024];
     LaunchCfg c;
-    while (std::fscanf(f, "%1023s %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps) == 4)
+    while (std::fscanf(f, "%1023s %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
+                       &c.cg_lanes) == 5)
         ctx->tune_cache.emplace_back(key, c);
     std::fclose(f);
 }
@@ -1387,7 +1388,7 @@ void tune_cache_store(binder_ctx* ctx, const std::string& key, const LaunchCfg& 
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps);
+    std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps, c.cg_lanes);
     std::fclose(f);
 }
 
@@ -1425,18 +1426,20 @@ int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out) {
     out->score_warps = ctx->cfg.score_warps;
     out->score_ctas_per_sm = ctx->cfg.score_ctas_per_sm;
     out->cg_warps = ctx->cfg.cg_warps;
-    out->_pad = 0;
+    out->cg_lanes = ctx->cfg.cg_lanes;
     return BINDER_OK;
 }
 
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
     if (!ctx || !c) return BINDER_ERR_ARG;
     if ((c->score_warps != 4 && c->score_warps != 8 && c->score_warps != 16) || c->score_ctas_per_sm < 1 ||
-        c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8))
+        c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8) ||
+        (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8))
         return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
     ctx->cfg.score_warps = c->score_warps;
     ctx->cfg.score_ctas_per_sm = c->score_ctas_per_sm;
     ctx->cfg.cg_warps = c->cg_warps;
+    ctx->cfg.cg_lanes = c->cg_lanes;
     return BINDER_OK;
 }
 
@@ -1462,14 +1465,19 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
     CK(cudaMemcpyAsync(saved.p, S.res_pos.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     LaunchCfg best = ctx->cfg;
     float best_ms = 1e30f;
-    for (int w : {2, 4, 8}) {
-        ctx->cfg.cg_warps = w;
-        float ms = 0.f;
-        if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
-        if (ms < best_ms) { best_ms = ms; best.cg_warps = w; }
-        CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream),
-           "copy");
-    }
+    for (int lanes : {4, 8})
+        for (int w : {2, 4, 8}) {
+            if (s) break;
+            if (lanes == 4 && w == 8) continue;  // not a supported shape
+            ctx->cfg.cg_warps = w;
+            ctx->cfg.cg_lanes = lanes;
+            float ms = 0.f;
+            if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
+            if (ms < best_ms) { best_ms = ms; best.cg_warps = w; best.cg_lanes = lanes; }
+            CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice,
+                               ctx->stream),
+               "copy");
+        }
     best_ms = 1e30f;
     for (int nw : {4, 8, 16})
         for (int per_sm : {1, 2, 4, 8}) {

@@ -4,8 +4,9 @@
 //    per residue, one thread each.
 //  * compute_forces_with_grid (energy.rs:322-398) for a batch of bodies.
 //  * The Langevin part of allatom_diffusion_step (diffusion.rs:306-339) without
-//    Metropolis moves: four lanes per residue probe the Calpha grid, the pair
-//    terms are folded in the reference's order, and n_steps are fused per launch
+//    Metropolis moves: per-residue Verlet lists of antigen Calphas in the
+//    reference's probe order, four or eight lanes per residue evaluate the pair
+//    terms, lane 0 folds them in that order, and n_steps are fused per launch
 //    since in this phase every residue moves independently.
 //  * The residue visiting order by Calpha cell and the slot packing kernels.
 #include <algorithm>
@@ -61,43 +62,142 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 }
 
 // ---- Langevin steps without Metropolis moves (diffusion.rs:306-339) ----------------
-// Four lanes per residue (eight residues per warp, residues in Calpha-cell order).
-// The 27 probe cells, in the reference's order, are split into four contiguous
-// runs, one per lane; each lane tests its cells' atoms and evaluates the in-cutoff
-// pair terms of its run into shared memory.  The accumulator then passes lane 0 ->
-// 1 -> 2 -> 3 and each lane folds its own terms in order: exactly the reference's
-// sequential sum, with the probing and the IEEE-exact pair math spread over four
-// lanes.  A lane whose run holds more than CG_TERMS in-cutoff pairs sends the
-// residue to the one-lane walk over all 27 cells (same sum).  Per-step translations
-// are recorded and applied to the residue's atoms at the end, atom k on lane k % 4
-// (the same sequence of roundings as set_ca_pos, allatom.rs:279-293).
+// The reference sums the pair terms of compute_forces_with_grid in its probe order:
+// cells (cx+dx, cy+dy, cz+dz) for dx, dy, dz = -1..1 (dz fastest), atoms ascending
+// within a cell.  The antigen Calphas are stored sorted by cell in the same
+// lexicographic order (ascending original index within a cell), so that probe order
+// is ascending position in the sorted array.  Each residue therefore keeps a Verlet
+// list: the positions, ascending, of the antigen Calphas within cutoff + skin of a
+// list centre.  While the Calpha stays within the skin of the centre the list holds
+// every in-cutoff Calpha; a step evaluates the list entries whose cell is adjacent
+// to the Calpha's current cell and whose r^2 passes the reference's cutoff test,
+// and sums their terms in list order -- the reference's pair set in the reference's
+// order, hence the same f32 sum.  A Calpha leaving the skin rebuilds its list.
+//
+// G lanes per residue (G = 4 or 8; residues in Calpha-cell order): the lanes split
+// the list entries, write their terms to shared memory, and lane 0 folds them in
+// order.  A list longer than CG_LIST_MAX, or a cell index near the i32 limits (where
+// the reference's cell arithmetic wraps), sends the residue to the one-lane 27-cell
+// walk (same sum).  The residue's atoms live in registers, atom k on lane k % G, and
+// take every step's translation as set_ca_pos does (allatom.rs:279-293).
 // COUNT: count the in-cutoff pairs of the same trajectory, leave the state as is.
-constexpr int CG_GROUP = 4;
-// in-cutoff terms a lane holds per step (static shared memory stays under 48 KB)
-template <int CG_WARPS>
-constexpr int cg_terms() { return CG_WARPS >= 8 ? 15 : 24; }
-constexpr int CG_MAX_STEPS = 32;  // steps per launch (the host splits longer runs)
+constexpr int CG_LIST_MAX = 64;
+constexpr float CG_SKIN = 2.0f;  // list radius = 10 A cutoff + skin
 
-template <bool COUNT, int CG_WARPS>
-__global__ void __launch_bounds__(CG_WARPS * 32) k_langevin(StateView st, const AgView* __restrict__ ags,
+// The one-lane walk over all 27 cells, out of line: it is rarely taken and must
+// not take registers from the list path.
+template <bool COUNT>
+__device__ __noinline__ void cg_force_walk(const AgView* __restrict__ ag, float x, float y, float z, int aa,
+                                           float3* out, int* n_pairs) {
+    float sx, sy, sz;
+    cg_force<COUNT>(*ag, cg_body(x, y, z, aa), sx, sy, sz, n_pairs);
+    *out = make_float3(sx, sy, sz);
+}
+
+__device__ __forceinline__ bool cell_far(int cx, int cy, int cz) {
+    return abs(cx) > (1 << 29) || abs(cy) > (1 << 29) || abs(cz) > (1 << 29);
+}
+
+// Verlet list of the residue whose group of G lanes calls this (gl = lane in group):
+// positions (ascending) of the antigen Calphas within CG_SKIN + 10 A (+ 10 mA for
+// rounding) of p, found by a walk over the 5 x 5 x 5 cells around p's cell culled by
+// slab distance.  The lanes split the 25 (dx, dy) columns into contiguous runs,
+// count, take offsets by a prefix sum and write.  Returns the list length (all lanes);
+// a length above CG_LIST_MAX leaves the list unwritten.
+template <int G>
+__device__ __noinline__ int build_cg_list(const GridView& g, const float4* __restrict__ ca_pq, F3 p, int gl, unsigned gmask,
+                             int* list) {
+    const float R = 10.0f + CG_SKIN + 0.01f, R2 = R * R;
+    const int c[3] = {cell_coord(p.x, g.inv), cell_coord(p.y, g.inv), cell_coord(p.z, g.inv)};
+    if (cell_far(c[0], c[1], c[2])) return CG_LIST_MAX + 1;
+    const float pp[3] = {p.x, p.y, p.z};
+    float sl[3][5];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int o = 0; o < 5; ++o) {
+            const float lo = (float)(c[d] + o - 2) * g.cell, hi = lo + g.cell;
+            const float dd = fmaxf(fmaxf(lo - pp[d], pp[d] - hi), 0.0f);
+            sl[d][o] = dd * dd;
+        }
+    const int col0 = (25 * gl) / G, col1 = (25 * (gl + 1)) / G;
+    int n_mine = 0, off = 0, total = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        int w = off;
+        for (int col = col0; col < col1; ++col) {
+            const int ox = col / 5, oy = col % 5;
+            const float dxy = sl[0][ox] + sl[1][oy];
+            if (dxy > R2) continue;
+            const int X = c[0] + ox - 2 - g.ox, Y = c[1] + oy - 2 - g.oy;
+            if (X < 0 || Y < 0 || X >= g.nx || Y >= g.ny) continue;
+            int zl = 0, zh = 4;
+            while (zl <= 4 && dxy + sl[2][zl] > R2) ++zl;
+            while (zh >= zl && dxy + sl[2][zh] > R2) --zh;
+            if (zl > zh) continue;
+            const int Z0 = max(c[2] + zl - 2 - g.oz, 0), Z1 = min(c[2] + zh - 2 - g.oz, g.nz - 1);
+            if (Z0 > Z1) continue;
+            const int base = (X * g.ny + Y) * g.nz;
+            const int a1 = g.cell_start[base + Z1 + 1];
+            for (int i = g.cell_start[base + Z0]; i < a1; ++i) {
+                const float4 a = ca_pq[i];
+                const float dx = p.x - a.x, dy = p.y - a.y, dz = p.z - a.z;
+                if (dx * dx + dy * dy + dz * dz > R2) continue;
+                if (pass == 0) ++n_mine;
+                else list[w++] = i;
+            }
+        }
+        if (pass == 0) {
+            int incl = n_mine;
+#pragma unroll
+            for (int d = 1; d < G; d <<= 1) {
+                const int v = __shfl_up_sync(gmask, incl, d, G);
+                if (gl >= d) incl += v;
+            }
+            total = __shfl_sync(gmask, incl, G - 1, G);
+            off = incl - n_mine;
+            if (total > CG_LIST_MAX) return total;
+        }
+    }
+    __syncwarp(gmask);
+    return total;
+}
+
+// resident warps per SM the register budget is set for: about one wave of the
+// benchmark's 20480 residues (4 lanes: 17 warps per SM, 8 lanes: 35)
+template <int G>
+constexpr int cg_warps_per_sm() { return G == 8 ? 36 : 20; }
+
+template <bool COUNT, int CG_WARPS, int G>
+__global__ void __launch_bounds__(CG_WARPS * 32, cg_warps_per_sm<G>() / CG_WARPS) k_langevin(StateView st, const AgView* __restrict__ ags,
                                                              StepParams p, int n_steps, uint32_t step0,
                                                              int with_noise, const float* __restrict__ temps,
                                                              uint32_t* __restrict__ err,
                                                              long long* __restrict__ pair_count,
                                                              const int* __restrict__ order) {
-    constexpr int CG_TERMS = cg_terms<CG_WARPS>();
-    __shared__ float3 s_terms[CG_WARPS * 32][CG_TERMS];
+    constexpr int RPC = CG_WARPS * 32 / G;  // residues per CTA
+    constexpr int NA = (SLOTS + G - 1) / G;  // atoms per lane
+    static_assert(RPC <= 32, "list storage is sized for 32 residues per CTA");
+    __shared__ int s_list[RPC][CG_LIST_MAX];
+    __shared__ float4 s_term[RPC][CG_LIST_MAX];
     const int lane = threadIdx.x & 31;
-    const int gl = lane & (CG_GROUP - 1);
-    const int gshift = lane & ~(CG_GROUP - 1);
-    const unsigned gmask = ((1u << CG_GROUP) - 1u) << gshift;
-    const int slot_id = (blockIdx.x * blockDim.x + threadIdx.x) / CG_GROUP;
+    const int gl = lane & (G - 1);
+    const int gshift = lane & ~(G - 1);
+    const unsigned gmask = ((1u << G) - 1u) << gshift;
+    const int slot_id = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     if (slot_id >= st.total_res) return;  // the whole group leaves together
+    const int rl = threadIdx.x / G;
+    int* list = s_list[rl];
+    float4* terms = s_term[rl];
     const int r = order ? order[slot_id] : slot_id;
     const int c = st.res_cand[r];
     const int r_local = r - st.cand_res_off[c];
     const uint32_t cid = st.cand_id[c];
-    const AgView A = ags[st.cand_ag[c]];  // by value: the fields live in registers
+    const AgView* __restrict__ Ap = ags + st.cand_ag[c];
+    const GridView g = Ap->ca_grid;
+    const float4* __restrict__ ca_pq = Ap->ca_pq;
+    const float4* __restrict__ ca_prm = Ap->ca_prm;
+    const int4* __restrict__ ca_cell = Ap->ca_cell;
+    const float ag_cx = Ap->cx, ag_cy = Ap->cy, ag_cz = Ap->cz;
     const int aa = st.res_aa[r];
     const int n_at = s_topo_n[aa];
     const float4 res = s_res[aa];
@@ -105,81 +205,56 @@ __global__ void __launch_bounds__(CG_WARPS * 32) k_langevin(StateView st, const 
     const float4 v1 = slot[1];  // Calpha = topology atom 1 of every residue (amber.rs:358-377)
     F3 ca = {v1.x, v1.y, v1.z};
     if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
-    float3* my_terms = s_terms[threadIdx.x];
-    const GridView& g = A.ca_grid;
-    // this lane's run of the 9 probe columns (dx, dy), in the reference's order
-    const int c0 = gl == 0 ? 0 : 1 + 2 * gl, c1 = gl == 0 ? 3 : 3 + 2 * gl;
-    F3 delta[CG_MAX_STEPS];
+    float4 at[NA];
+#pragma unroll
+    for (int j = 0; j < NA; ++j) {
+        const int k = gl + G * j;
+        at[j] = (!COUNT && k < n_at) ? slot[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    F3 centre = ca;
+    int nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+    const float skin2 = (CG_SKIN - 0.01f) * (CG_SKIN - 0.01f);
     int n_pairs = 0;
     for (int s = 0; s < n_steps; ++s) {
-        const CgB body{ca.x, ca.y, ca.z, res.x, res.y, res.z, res.w};
         const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
-        // Squared distances from the Calpha to the lower / upper neighbour slab in each
-        // dimension; a cell beyond the cutoff (+1 mA, above the f32 rounding of r^2
-        // and of the slab bounds) holds no in-cutoff atom, so skipping it changes
-        // nothing.  For fixed (dx, dy) the three cells dz = -1..1 are one contiguous
-        // range of the sorted array, visited in the reference's order.
-        const float reach = 10.001f + 4e-7f * (fabsf(ca.x) + fabsf(ca.y) + fabsf(ca.z));
-        const float reach2 = reach * reach;
-        const float xm = fmaxf(ca.x - (float)cx * g.cell, 0.f), xp = fmaxf((float)(cx + 1) * g.cell - ca.x, 0.f);
-        const float ym = fmaxf(ca.y - (float)cy * g.cell, 0.f), yp = fmaxf((float)(cy + 1) * g.cell - ca.y, 0.f);
-        const float zm = fmaxf(ca.z - (float)cz * g.cell, 0.f), zp = fmaxf((float)(cz + 1) * g.cell - ca.z, 0.f);
-        // cell indices near the i32 limits: the one-lane walk reproduces the wrapping
-        const bool far = abs(cx) > (1 << 29) || abs(cy) > (1 << 29) || abs(cz) > (1 << 29);
-        int nt = 0;
-        if (!far) {
-            for (int col = c0; col < c1; ++col) {
-                const int dx = col >= 6 ? 1 : (col >= 3 ? 0 : -1);
-                const int dy = col - 3 * (dx + 1) - 1;
-                const float ddx = dx < 0 ? xm : (dx > 0 ? xp : 0.f);
-                const float ddy = dy < 0 ? ym : (dy > 0 ? yp : 0.f);
-                const float dxy = ddx * ddx + ddy * ddy;
-                if (dxy > reach2) continue;
-                const long long X = (long long)cx + dx - g.ox, Y = (long long)cy + dy - g.oy;
-                if (X < 0 || Y < 0 || X >= g.nx || Y >= g.ny) continue;
-                long long zl = (dxy + zm * zm > reach2) ? cz : (long long)cz - 1;
-                long long zh = (dxy + zp * zp > reach2) ? cz : (long long)cz + 1;
-                zl = max(zl - g.oz, 0ll);
-                zh = min(zh - g.oz, (long long)g.nz - 1);
-                if (zl > zh) continue;
-                const int base = ((int)X * g.ny + (int)Y) * g.nz;
-                const int a1 = g.cell_start[base + (int)zh + 1];
-                for (int i = g.cell_start[base + (int)zl]; i < a1; ++i) {
-                    float tx, ty, tz;
-                    if (!cg_term_parts(body, A.ca_pq[i], A.ca_prm[i], tx, ty, tz)) continue;
-                    if (nt < CG_TERMS) my_terms[nt] = make_float3(tx, ty, tz);
-                    ++nt;
-                }
-            }
-            if (COUNT) n_pairs += nt;
-        }
-        const bool overflow = (__ballot_sync(gmask, far || nt > CG_TERMS) & gmask) != 0u;
         float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        if (!overflow) {
-#pragma unroll
-            for (int L = 0; L < CG_GROUP; ++L) {
-                if (gl == L)
-                    for (int k = 0; k < nt; ++k) {
-                        const float3 t = my_terms[k];
+        if (nl <= CG_LIST_MAX && !cell_far(cx, cy, cz)) {
+            const CgB body{ca.x, ca.y, ca.z, res.x, res.y, res.z, res.w};
+            for (int j = gl; j < nl; j += G) {
+                const int i = list[j];
+                const int4 ce = ca_cell[i];
+                float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
+                    abs((long long)ce.z - cz) <= 1 && cg_term_parts(body, ca_pq[i], ca_prm[i], t.x, t.y, t.z))
+                    t.w = 1.0f;
+                terms[j] = t;
+            }
+            __syncwarp(gmask);
+            if (gl == 0) {
+                for (int j = 0; j < nl; ++j) {
+                    const float4 t = terms[j];
+                    if (t.w != 0.0f) {
                         sx = xadd(sx, t.x);
                         sy = xadd(sy, t.y);
                         sz = xadd(sz, t.z);
+                        if (COUNT) ++n_pairs;
                     }
-                sx = __shfl_sync(gmask, sx, L, CG_GROUP);
-                sy = __shfl_sync(gmask, sy, L, CG_GROUP);
-                sz = __shfl_sync(gmask, sz, L, CG_GROUP);
+                }
             }
+            __syncwarp(gmask);  // term slots are rewritten next step
         } else {
             int np = 0;
-            if (gl == 0) cg_force<COUNT>(A, body, sx, sy, sz, &np);
-            if (COUNT && far) n_pairs += np;  // lanes did not count when far
-            sx = __shfl_sync(gmask, sx, 0, CG_GROUP);
-            sy = __shfl_sync(gmask, sy, 0, CG_GROUP);
-            sz = __shfl_sync(gmask, sz, 0, CG_GROUP);
+            if (gl == 0) {
+                float3 f;
+                cg_force_walk<COUNT>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
+                sx = f.x; sy = f.y; sz = f.z;
+            }
+            if (COUNT) n_pairs += np;
         }
-        float fx = sx, fy = sy, fz = sz;
+        float fx = __shfl_sync(gmask, sx, 0, G), fy = __shfl_sync(gmask, sy, 0, G),
+              fz = __shfl_sync(gmask, sz, 0, G);
         // harmonic restraint toward the shell (diffusion.rs:317-327)
-        const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
+        const float dx_c = xsub(ca.x, ag_cx), dy_c = xsub(ca.y, ag_cy), dz_c = xsub(ca.z, ag_cz);
         const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
         const float excess = xsub(d, p.shell_radius);
         const float f_r = xdiv(xmul(-p.restraint_k, excess), d);
@@ -201,21 +276,31 @@ __global__ void __launch_bounds__(CG_WARPS * 32) k_langevin(StateView st, const 
                            xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
         // set_ca_pos: delta = new - old; every atom (the Calpha included) += delta
         const F3 dl = sub3(new_ca, ca);
-        delta[s] = dl;
+        if (!COUNT) {
+#pragma unroll
+            for (int j = 0; j < NA; ++j) {
+                at[j].x = xadd(at[j].x, dl.x);
+                at[j].y = xadd(at[j].y, dl.y);
+                at[j].z = xadd(at[j].z, dl.z);
+            }
+        }
         ca = {xadd(ca.x, dl.x), xadd(ca.y, dl.y), xadd(ca.z, dl.z)};
+        if (s + 1 < n_steps) {
+            const float mx = ca.x - centre.x, my = ca.y - centre.y, mz = ca.z - centre.z;
+            if (!(mx * mx + my * my + mz * mz <= skin2)) {  // left the skin (or NaN): new list
+                centre = ca;
+                nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+            }
+        }
     }
     if (COUNT) {
-        if (n_pairs) atomicAdd((unsigned long long*)pair_count, (unsigned long long)n_pairs);
+        if (gl == 0 && n_pairs) atomicAdd((unsigned long long*)pair_count, (unsigned long long)n_pairs);
         return;
     }
-    for (int k = gl; k < n_at; k += CG_GROUP) {
-        float4 v = slot[k];
-        for (int s = 0; s < n_steps; ++s) {
-            v.x = xadd(v.x, delta[s].x);
-            v.y = xadd(v.y, delta[s].y);
-            v.z = xadd(v.z, delta[s].z);
-        }
-        slot[k] = v;
+#pragma unroll
+    for (int j = 0; j < NA; ++j) {
+        const int k = gl + G * j;
+        if (k < n_at) slot[k] = at[j];
     }
 }
 
@@ -271,26 +356,28 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
     k_res_scatter<<<(st.total_res + 255) / 256, 256, 0, s>>>(st.total_res, keys, cursor, order);
 }
 
-template <int W>
+template <int W, int G>
 static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                       uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order) {
     const int threads = W * 32;
-    const long long total = (long long)st.total_res * CG_GROUP;
-    for (int s0 = 0; s0 < n_steps; s0 += CG_MAX_STEPS) {
-        const int ns = min(CG_MAX_STEPS, n_steps - s0);
-        k_langevin<false, W><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-            st, ags, p, ns, step0 + (uint32_t)s0, with_noise, temps ? temps + s0 : nullptr, err, nullptr, order);
-    }
+    const long long total = (long long)st.total_res * G;
+    k_langevin<false, W, G><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
+        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order);
 }
 
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta) {
+                    int warps_per_cta, int lanes_per_res) {
     if (st.total_res <= 0 || n_steps <= 0) return;
-    switch (warps_per_cta) {
-        case 2: diffuse_w<2>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
-        case 8: diffuse_w<8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
-        default: diffuse_w<4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+    if (lanes_per_res == 8) {
+        switch (warps_per_cta) {
+            case 2: diffuse_w<2, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+            case 8: diffuse_w<8, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+            default: diffuse_w<4, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+        }
+    } else {  // four lanes: at most four warps per CTA (list storage)
+        if (warps_per_cta == 2) diffuse_w<2, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order);
+        else diffuse_w<4, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order);
     }
 }
 
@@ -298,9 +385,9 @@ void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags
                           long long* pairs) {
     if (st.total_res <= 0 || n_steps <= 0) return;
     const int threads = 4 * 32;
-    const long long total = (long long)st.total_res * CG_GROUP;
-    k_langevin<true, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-        st, ags, p, min(n_steps, CG_MAX_STEPS), 0, 0, nullptr, nullptr, pairs, nullptr);
+    const long long total = (long long)st.total_res * 4;
+    k_langevin<true, 4, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
+        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr);
 }
 
 }  // namespace binder

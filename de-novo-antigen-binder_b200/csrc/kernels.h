@@ -12,7 +12,8 @@ namespace binder {
 struct LaunchCfg {
     int score_warps = 8;         // warps per CTA of the persistent scoring kernel (4, 8, 16)
     int score_ctas_per_sm = 4;   // persistent scoring CTAs per SM
-    int cg_warps = 4;            // warps per CTA of the gradient-step kernel (2, 4, 8)
+    int cg_warps = 8;            // warps per CTA of the gradient-step kernel (2, 4, 8)
+    int cg_lanes = 8;            // lanes per residue of the gradient-step kernel (4, 8)
 };
 
 // ---- k_grid.cu: SpatialHashGrid ----
@@ -70,7 +71,7 @@ void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const f
                       const uint8_t* baa, int n, float* fx, float* fy, float* fz);
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta);
+                    int warps_per_cta, int lanes_per_res);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);

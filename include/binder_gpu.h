@@ -284,7 +284,8 @@ typedef struct binder_launch_cfg {
     int32_t score_warps;        /* warps per CTA of the persistent scoring kernel: 4, 8, 16 */
     int32_t score_ctas_per_sm;  /* persistent scoring CTAs per SM: 1..32 */
     int32_t cg_warps;           /* warps per CTA of the gradient-step kernel: 2, 4, 8 */
-    int32_t _pad;
+    int32_t cg_lanes;           /* lanes per residue of the gradient-step kernel: 4 (with 2 or 4
+                                   warps per CTA) or 8 */
 } binder_launch_cfg;
 int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
