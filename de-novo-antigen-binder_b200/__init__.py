@@ -162,7 +162,43 @@ _SIGS = {
     "binder_get_launch_cfg": (C.c_int, [C.c_void_p, C.c_void_p]),
     "binder_set_launch_cfg": (C.c_int, [C.c_void_p, C.c_void_p]),
     "binder_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "binder_mlp_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "binder_mlp_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_mlp_forward": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "binder_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                                       C.POINTER(C.c_double), C.c_void_p]),
+    "binder_mlp_set_tuples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "binder_mlp_tuple_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "binder_mlp_get_tuples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_mlp_train": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64, C.c_void_p]),
 }
+
+# learned proposal network (include/binder_gpu.h): sizes and the logged-tuple record
+MLP_IN, MLP_OUT, MLP_N_PARAMS = 180, 25, 123424
+MLP_K1, MLP_H, MLP_OUT_PAD = 192, 256, 32
+MLP_OFF = {"w1": 0, "b1": 49152, "w2": 49408, "b2": 114944, "w3": 115200, "b3": 123392}
+MC_TUPLE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("delta_e", "<f4"), ("cand", "<i4"),
+                     ("residue", "<i2"), ("aa", "u1"), ("action", "u1"), ("antigen", "u1"), ("accepted", "u1"),
+                     ("_pad", "u1", (6,))])
+
+
+def mlp_init_params(seed=0):
+    """Initial parameters: uniform(+-1/sqrt(fan_in)) weights (PyTorch's Linear
+    default), zero biases, zero padding rows / columns."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MLP_N_PARAMS, np.float32)
+    w1 = rng.uniform(-1, 1, (MLP_H, MLP_IN)) / np.sqrt(MLP_IN)
+    w2 = rng.uniform(-1, 1, (MLP_H, MLP_H)) / np.sqrt(MLP_H)
+    w3 = rng.uniform(-1, 1, (MLP_OUT, MLP_H)) / np.sqrt(MLP_H)
+    W1 = np.zeros((MLP_H, MLP_K1), np.float32)
+    W1[:, :MLP_IN] = w1
+    W3 = np.zeros((MLP_OUT_PAD, MLP_H), np.float32)
+    W3[:MLP_OUT] = w3
+    p[MLP_OFF["w1"]:MLP_OFF["b1"]] = W1.ravel()
+    p[MLP_OFF["w2"]:MLP_OFF["b2"]] = w2.astype(np.float32).ravel()
+    p[MLP_OFF["w3"]:MLP_OFF["b3"]] = W3.ravel()
+    return p
 
 
 def lib():
@@ -595,6 +631,56 @@ class GpuContext:
         a, b = C.c_double(), C.c_double()
         self._check(lib().binder_fp32_peak(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    # -- learned proposal network --
+    def mlp_set_params(self, params):
+        p = _f32(params)
+        assert p.shape == (MLP_N_PARAMS,)
+        self._check(lib().binder_mlp_set_params(self._h, _ptr(p)))
+
+    def mlp_get_params(self):
+        out = np.zeros(MLP_N_PARAMS, np.float32)
+        self._check(lib().binder_mlp_get_params(self._h, _ptr(out)))
+        return out
+
+    def mlp_features(self, antigen_id, ca, aa):
+        ca, aa = _f32(ca).reshape(-1, 3), _u8(aa)
+        out = np.zeros((len(aa), MLP_IN), np.float32)
+        self._check(lib().binder_mlp_features(self._h, antigen_id, len(aa), _ptr(ca), _ptr(aa), _ptr(out)))
+        return out
+
+    def mlp_forward(self, features):
+        f = _f32(features).reshape(-1, MLP_IN)
+        out = np.zeros((len(f), MLP_OUT), np.float32)
+        self._check(lib().binder_mlp_forward(self._h, len(f), _ptr(f), _ptr(out)))
+        return out
+
+    def mlp_loss_grad(self, features, action, target, huber_delta=1.0):
+        f = _f32(features).reshape(-1, MLP_IN)
+        a = np.ascontiguousarray(action, np.int32)
+        t = _f32(target)
+        loss = C.c_double()
+        g = np.zeros(MLP_N_PARAMS, np.float32)
+        self._check(lib().binder_mlp_loss_grad(self._h, len(f), _ptr(f), _ptr(a), _ptr(t), huber_delta,
+                                               C.byref(loss), _ptr(g)))
+        return loss.value, g
+
+    def mlp_set_tuples(self, tuples):
+        t = np.ascontiguousarray(tuples, MC_TUPLE)
+        self._check(lib().binder_mlp_set_tuples(self._h, _ptr(t), len(t)))
+
+    def mlp_get_tuples(self):
+        n = C.c_size_t()
+        self._check(lib().binder_mlp_tuple_count(self._h, C.byref(n)))
+        out = np.zeros(n.value, MC_TUPLE)
+        self._check(lib().binder_mlp_get_tuples(self._h, _ptr(out), len(out), C.byref(n)))
+        return out
+
+    def mlp_train(self, n_steps, batch=8192, lr=1e-3, huber_delta=1.0, seed=0):
+        """n_steps Adam steps on minibatches of the training set; per-step losses."""
+        out = np.zeros(max(0, n_steps), np.float64)
+        self._check(lib().binder_mlp_train(self._h, n_steps, batch, lr, huber_delta, seed, _ptr(out)))
+        return out
 
 
 def temperature(iteration, total, t_hot=3.0, t_cold=0.02):

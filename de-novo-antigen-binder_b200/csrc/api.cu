@@ -136,6 +136,24 @@ const size_t MAX_GRID_CELLS = (size_t)1 << 24;
 
 }  // namespace
 
+// Learned proposal network: parameters, Adam moments, BF16 copies, the logged
+// Metropolis tuples and the activations of up to `cap` rows.
+struct MlpState {
+    bool ready = false;
+    int adam_t = 0;
+    DBuf<float> w, g, m1, m2;
+    DBuf<__nv_bfloat16> w1, w2, w2t, w3, w3t;
+    int cap = 0;
+    DBuf<__nv_bfloat16> X, Xt, H1, H1t, H2, H2t, dY, dYt, dZ2, dZ2t, dZ1t;
+    DBuf<float> Z1, Z2, Y, part, feat, ca, target;
+    DBuf<uint8_t> aa;
+    DBuf<int> ag, action, idx;
+    DBuf<double> loss;
+    DBuf<MlpTuple> tuples;
+    size_t n_tuples = 0;
+    MlpBf16 bf16() { return MlpBf16{w1.p, w2.p, w2t.p, w3.p, w3t.p}; }
+};
+
 struct binder_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -183,6 +201,7 @@ struct binder_ctx {
     std::vector<uint64_t> block_graph_sig;  // what the captured launches baked in
     int block_graph_launches = 0;
     std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
+    MlpState mlp;
     void drop_graph() {
         if (block_graph) cudaGraphExecDestroy(block_graph);
         block_graph = nullptr;
@@ -229,6 +248,13 @@ int cuda_fail(binder_ctx* ctx, cudaError_t e, const char* what) {
         cudaError_t e__ = cudaGetLastError();               \
         if (e__ != cudaSuccess) return cuda_fail(ctx, e__, what); \
     } while (0)
+
+// log1p(n) of the environment counts, n = 0..255, rounded once to f32
+cudaError_t init_mlp_tables() {
+    float t[MLP_COUNT_CAP + 1];
+    for (int n = 0; n <= MLP_COUNT_CAP; ++n) t[n] = (float)std::log1p((double)n);
+    return mlp_init_tables(t);
+}
 
 int enter(binder_ctx* ctx) {
     if (!ctx) return BINDER_ERR_ARG;
@@ -354,6 +380,7 @@ int build_antigen_ca(binder_ctx* ctx, Antigen& A, const float* x, const float* y
     A.view.ca_pq = A.ca_pq.p;
     A.view.ca_prm = A.ca_prm.p;
     A.view.ca_cell = A.ca_cell.p;
+    A.view.res_aa = A.caa.p;
     A.view.ca_grid = A.ca_grid.view;
     A.view.n_res = (int)n;
     return BINDER_OK;
@@ -565,7 +592,7 @@ binder_ctx* binder_create(int device, const binder_params* params, int* status) 
     else binder_default_params(&ctx->params);
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         score_init_tables() != cudaSuccess || search_init_tables() != cudaSuccess ||
-        anneal_init_tables() != cudaSuccess) {
+        anneal_init_tables() != cudaSuccess || init_mlp_tables() != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
         *status = BINDER_ERR_CUDA;
@@ -1718,6 +1745,354 @@ int binder_fp32_peak(binder_ctx* ctx, double* scalar, double* packed) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return BINDER_OK;
+}
+
+}  // extern "C"
+
+// ---- learned proposal network: host side of k_mlp.cu ----------------------------------
+namespace {
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// activations for up to `rows` rows (rounded up to the 128-row GEMM tile)
+int mlp_reserve(binder_ctx* ctx, int rows) {
+    MlpState& M = ctx->mlp;
+    const int cap = round_up(std::max(rows, 1), 128);
+    if (cap <= M.cap) return BINDER_OK;
+    const size_t c = (size_t)cap;
+    CK(M.X.ensure(c * MLP_K1), "mlp alloc");
+    CK(M.Xt.ensure(c * MLP_K1), "mlp alloc");
+    CK(M.H1.ensure(c * MLP_H), "mlp alloc");
+    CK(M.H1t.ensure(c * MLP_H), "mlp alloc");
+    CK(M.H2.ensure(c * MLP_H), "mlp alloc");
+    CK(M.H2t.ensure(c * MLP_H), "mlp alloc");
+    CK(M.dY.ensure(c * MLP_OUT_PAD), "mlp alloc");
+    CK(M.dYt.ensure(c * MLP_OUT_PAD), "mlp alloc");
+    CK(M.dZ2.ensure(c * MLP_H), "mlp alloc");
+    CK(M.dZ2t.ensure(c * MLP_H), "mlp alloc");
+    CK(M.dZ1t.ensure(c * MLP_H), "mlp alloc");
+    CK(M.Z1.ensure(c * MLP_H), "mlp alloc");
+    CK(M.Z2.ensure(c * MLP_H), "mlp alloc");
+    CK(M.Y.ensure(c * MLP_OUT_PAD), "mlp alloc");
+    CK(M.feat.ensure(c * MLP_IN), "mlp alloc");
+    CK(M.ca.ensure(c * 3), "mlp alloc");
+    CK(M.target.ensure(c), "mlp alloc");
+    CK(M.aa.ensure(c), "mlp alloc");
+    CK(M.ag.ensure(c), "mlp alloc");
+    CK(M.action.ensure(c), "mlp alloc");
+    CK(M.idx.ensure(c), "mlp alloc");
+    M.cap = cap;
+    return BINDER_OK;
+}
+
+constexpr int MLP_KSPLIT = 512;  // batch rows per split-K slice of the weight-gradient GEMMs
+
+int gemm(binder_ctx* ctx, const GemmArgs& g, const char* what) {
+    CK(launch_gemm_tc(ctx->stream, g, ctx->errf.p), what);
+    ctx->launches++;
+    return BINDER_OK;
+}
+
+// Forward pass of rows 0..m-1 of M.X (BF16, rows up to m_pad zero).  train keeps
+// what the backward pass needs (pre-activations and transposed activations).
+int mlp_forward_dev(binder_ctx* ctx, int m, bool train) {
+    MlpState& M = ctx->mlp;
+    const int mp = round_up(m, 128);
+    int s;
+    GemmArgs g;
+    // layer 1: Z1 = X W1^T + b1, H1 = silu(Z1)
+    g.a = M.X.p; g.lda = MLP_K1; g.m = mp;
+    g.b = M.w1.p; g.ldb = MLP_K1; g.n = MLP_H; g.k = MLP_K1; g.k_split = MLP_K1;
+    g.e = GemmEpi{};
+    g.e.mode = EPI_SILU; g.e.bias = M.w.p + MLP_OFF_B1;
+    g.e.c = train ? M.Z1.p : nullptr; g.e.ldc = MLP_H;
+    g.e.h = M.H1.p; g.e.ldh = MLP_H; g.e.h_rows = mp;
+    g.e.ht = train ? M.H1t.p : nullptr; g.e.ldht = mp; g.e.ht_rows = mp;
+    g.e.n_valid = MLP_H; g.e.m_valid = m;
+    if ((s = gemm(ctx, g, "mlp layer 1"))) return s;
+    // layer 2
+    g.a = M.H1.p; g.lda = MLP_H; g.b = M.w2.p; g.ldb = MLP_H; g.k = MLP_H; g.k_split = MLP_H;
+    g.e.bias = M.w.p + MLP_OFF_B2; g.e.c = train ? M.Z2.p : nullptr;
+    g.e.h = M.H2.p; g.e.ht = train ? M.H2t.p : nullptr;
+    if ((s = gemm(ctx, g, "mlp layer 2"))) return s;
+    // layer 3: Y = H2 W3^T + b3 (FP32)
+    g.a = M.H2.p; g.lda = MLP_H; g.b = M.w3.p; g.ldb = MLP_H; g.n = MLP_OUT_PAD; g.k = MLP_H; g.k_split = MLP_H;
+    g.e = GemmEpi{};
+    g.e.mode = EPI_F32; g.e.bias = M.w.p + MLP_OFF_B3; g.e.c = M.Y.p; g.e.ldc = MLP_OUT_PAD;
+    g.e.n_valid = MLP_OUT_PAD; g.e.m_valid = mp;
+    return gemm(ctx, g, "mlp layer 3");
+}
+
+// dW = G^T * A over the batch: G^T [rows][mp] and A^T [n][mp] (BF16), split-K
+// partials reduced in a fixed order into grad (FP32 [rows][n]).
+int mlp_weight_grad(binder_ctx* ctx, const __nv_bfloat16* Gt, int rows, const __nv_bfloat16* At, int n, int mp,
+                    float* grad) {
+    MlpState& M = ctx->mlp;
+    const int slices = (mp + MLP_KSPLIT - 1) / MLP_KSPLIT;
+    const long long stride = (long long)rows * n;
+    CK(M.part.ensure((size_t)slices * stride), "mlp alloc");
+    GemmArgs g;
+    g.a = Gt; g.lda = mp; g.m = rows;
+    g.b = At; g.ldb = mp; g.n = n; g.k = mp; g.k_split = MLP_KSPLIT;
+    g.e.mode = EPI_PARTIAL; g.e.c = M.part.p; g.e.ldc = n; g.e.part_stride = stride;
+    g.e.n_valid = n; g.e.m_valid = rows;
+    int s = gemm(ctx, g, "mlp weight grad");
+    if (s) return s;
+    launch_reduce_partials(ctx->stream, (int)stride, slices, stride, M.part.p, grad);
+    LAUNCHED("mlp reduce");
+    return BINDER_OK;
+}
+
+// Loss and gradient of the batch in M.X / M.action / M.target (m rows) into M.g.
+int mlp_backward_dev(binder_ctx* ctx, int m, float delta) {
+    MlpState& M = ctx->mlp;
+    const int mp = round_up(m, 128);
+    int s;
+    launch_mlp_loss(ctx->stream, m, mp, M.Y.p, M.action.p, M.target.p, delta, M.dY.p, M.dYt.p, M.loss.p);
+    LAUNCHED("mlp loss");
+    // layer 3: dW3 = dY^T H2, db3 = colsum dY, dZ2 = (dY W3) * silu'(Z2)
+    if ((s = mlp_weight_grad(ctx, M.dYt.p, MLP_OUT_PAD, M.H2t.p, MLP_H, mp, M.g.p + MLP_OFF_W3))) return s;
+    launch_rowsum_bf16(ctx->stream, MLP_OUT_PAD, mp, mp, M.dYt.p, M.g.p + MLP_OFF_B3);
+    LAUNCHED("mlp bias grad");
+    GemmArgs g;
+    g.a = M.dY.p; g.lda = MLP_OUT_PAD; g.m = mp;
+    g.b = M.w3t.p; g.ldb = MLP_OUT_PAD; g.n = MLP_H; g.k = MLP_OUT_PAD; g.k_split = 64;
+    g.e.mode = EPI_DSILU; g.e.z = M.Z2.p; g.e.ldz = MLP_H;
+    g.e.h = M.dZ2.p; g.e.ldh = MLP_H; g.e.h_rows = mp;
+    g.e.ht = M.dZ2t.p; g.e.ldht = mp; g.e.ht_rows = mp;
+    g.e.n_valid = MLP_H; g.e.m_valid = m;
+    if ((s = gemm(ctx, g, "mlp dZ2"))) return s;
+    // layer 2: dW2 = dZ2^T H1, db2, dZ1 = (dZ2 W2) * silu'(Z1)
+    if ((s = mlp_weight_grad(ctx, M.dZ2t.p, MLP_H, M.H1t.p, MLP_H, mp, M.g.p + MLP_OFF_W2))) return s;
+    launch_rowsum_bf16(ctx->stream, MLP_H, mp, mp, M.dZ2t.p, M.g.p + MLP_OFF_B2);
+    LAUNCHED("mlp bias grad");
+    g.a = M.dZ2.p; g.lda = MLP_H; g.b = M.w2t.p; g.ldb = MLP_H; g.k = MLP_H; g.k_split = MLP_H;
+    g.e.z = M.Z1.p; g.e.h = nullptr; g.e.ht = M.dZ1t.p;
+    if ((s = gemm(ctx, g, "mlp dZ1"))) return s;
+    // layer 1: dW1 = dZ1^T X, db1
+    if ((s = mlp_weight_grad(ctx, M.dZ1t.p, MLP_H, M.Xt.p, MLP_K1, mp, M.g.p + MLP_OFF_W1))) return s;
+    launch_rowsum_bf16(ctx->stream, MLP_H, mp, mp, M.dZ1t.p, M.g.p + MLP_OFF_B1);
+    LAUNCHED("mlp bias grad");
+    return BINDER_OK;
+}
+
+int mlp_check_ready(binder_ctx* ctx) {
+    if (!ctx->mlp.ready) return fail(ctx, BINDER_ERR_STATE, "proposal network has no parameters (binder_mlp_set_params)");
+    return BINDER_OK;
+}
+
+int mlp_pack(binder_ctx* ctx) {
+    launch_pack_weights(ctx->stream, ctx->mlp.w.p, ctx->mlp.bf16());
+    LAUNCHED("mlp pack weights");
+    return BINDER_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int binder_mlp_set_params(binder_ctx* ctx, const float* params) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!params) return fail(ctx, BINDER_ERR_ARG, "NULL parameters");
+    MlpState& M = ctx->mlp;
+    for (int i = 0; i < MLP_N_PARAMS; ++i)
+        if (!std::isfinite(params[i])) return fail(ctx, BINDER_ERR_NAN, "non-finite parameter %d", i);
+    // padding entries (W1 columns >= 180, W3 rows and b3 entries >= 25) must be zero
+    for (int n = 0; n < MLP_H; ++n)
+        for (int k = MLP_IN; k < MLP_K1; ++k)
+            if (params[MLP_OFF_W1 + n * MLP_K1 + k] != 0.0f) return fail(ctx, BINDER_ERR_ARG, "W1 padding not zero");
+    for (int i = MLP_OUT * MLP_H; i < MLP_OUT_PAD * MLP_H; ++i)
+        if (params[MLP_OFF_W3 + i] != 0.0f) return fail(ctx, BINDER_ERR_ARG, "W3 padding not zero");
+    for (int i = MLP_OUT; i < MLP_OUT_PAD; ++i)
+        if (params[MLP_OFF_B3 + i] != 0.0f) return fail(ctx, BINDER_ERR_ARG, "b3 padding not zero");
+    CK(M.w.ensure(MLP_N_PARAMS), "mlp alloc");
+    CK(M.g.ensure(MLP_N_PARAMS), "mlp alloc");
+    CK(M.m1.ensure(MLP_N_PARAMS), "mlp alloc");
+    CK(M.m2.ensure(MLP_N_PARAMS), "mlp alloc");
+    CK(M.w1.ensure(MLP_H * MLP_K1), "mlp alloc");
+    CK(M.w2.ensure(MLP_H * MLP_H), "mlp alloc");
+    CK(M.w2t.ensure(MLP_H * MLP_H), "mlp alloc");
+    CK(M.w3.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
+    CK(M.w3t.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
+    CK(M.loss.ensure(1), "mlp alloc");
+    CK(cudaMemcpyAsync(M.w.p, params, MLP_N_PARAMS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "mlp H2D");
+    CK(cudaMemsetAsync(M.g.p, 0, MLP_N_PARAMS * sizeof(float), ctx->stream), "mlp memset");
+    CK(cudaMemsetAsync(M.m1.p, 0, MLP_N_PARAMS * sizeof(float), ctx->stream), "mlp memset");
+    CK(cudaMemsetAsync(M.m2.p, 0, MLP_N_PARAMS * sizeof(float), ctx->stream), "mlp memset");
+    M.adam_t = 0;
+    if ((s = mlp_pack(ctx))) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    M.ready = true;
+    return BINDER_OK;
+}
+
+int binder_mlp_get_params(binder_ctx* ctx, float* params) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!params) return fail(ctx, BINDER_ERR_ARG, "NULL output");
+    if ((s = mlp_check_ready(ctx))) return s;
+    CK(cudaMemcpyAsync(params, ctx->mlp.w.p, MLP_N_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
+       "mlp D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_mlp_features(binder_ctx* ctx, int32_t antigen_id, size_t n, const float* ca_xyz, const uint8_t* aa,
+                        float* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n && (!ca_xyz || !aa || !out)) return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    if (antigen_id < 0 || antigen_id >= (int)ctx->ags.size()) return fail(ctx, BINDER_ERR_ARG, "no antigen %d", antigen_id);
+    if (n > (1u << 24)) return fail(ctx, BINDER_ERR_ARG, "too many rows");
+    for (size_t i = 0; i < n; ++i)
+        if (aa[i] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid %d out of range", (int)aa[i]);
+    if (n == 0) return BINDER_OK;
+    MlpState& M = ctx->mlp;
+    if ((s = mlp_reserve(ctx, (int)n))) return s;
+    std::vector<int> agv(n, antigen_id);
+    if ((s = upload(ctx, M.ca, ca_xyz, 3 * n, "features H2D")) || (s = upload(ctx, M.aa, aa, n, "features H2D")) ||
+        (s = upload(ctx, M.ag, agv.data(), n, "features H2D")))
+        return s;
+    launch_features(ctx->stream, (int)n, (int)n, M.ca.p, M.aa.p, M.ag.p, ctx->d_views.p, M.X.p);
+    LAUNCHED("features");
+    std::vector<__nv_bfloat16> h(n * MLP_K1);
+    CK(cudaMemcpyAsync(h.data(), M.X.p, h.size() * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost, ctx->stream),
+       "features D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    for (size_t r = 0; r < n; ++r)
+        for (int j = 0; j < MLP_IN; ++j) out[r * MLP_IN + j] = __bfloat162float(h[r * MLP_K1 + j]);
+    return BINDER_OK;
+}
+
+int binder_mlp_forward(binder_ctx* ctx, size_t n, const float* features, float* out) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n && (!features || !out)) return fail(ctx, BINDER_ERR_ARG, "NULL array");
+    if (n > (1u << 24)) return fail(ctx, BINDER_ERR_ARG, "too many rows");
+    if ((s = mlp_check_ready(ctx))) return s;
+    if (n == 0) return BINDER_OK;
+    MlpState& M = ctx->mlp;
+    if ((s = mlp_reserve(ctx, (int)n)) || (s = clear_err(ctx))) return s;
+    if ((s = upload(ctx, M.feat, features, n * MLP_IN, "mlp H2D"))) return s;
+    const int mp = round_up((int)n, 128);
+    launch_pack_features(ctx->stream, (int)n, mp, M.feat.p, M.X.p);
+    LAUNCHED("mlp pack features");
+    if ((s = mlp_forward_dev(ctx, (int)n, false))) return s;
+    CK(cudaMemcpy2DAsync(out, MLP_OUT * sizeof(float), M.Y.p, MLP_OUT_PAD * sizeof(float), MLP_OUT * sizeof(float), n,
+                         cudaMemcpyDeviceToHost, ctx->stream),
+       "mlp D2H");
+    return check_err(ctx);
+}
+
+int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const int32_t* action,
+                         const float* target, float huber_delta, double* out_loss, float* out_grad) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!n || !features || !action || !target) return fail(ctx, BINDER_ERR_ARG, "empty or NULL batch");
+    if (n > (1u << 24)) return fail(ctx, BINDER_ERR_ARG, "too many rows");
+    if (!(huber_delta > 0.0f)) return fail(ctx, BINDER_ERR_ARG, "huber_delta must be positive");
+    for (size_t i = 0; i < n; ++i)
+        if (action[i] < 0 || action[i] >= MLP_OUT) return fail(ctx, BINDER_ERR_ARG, "action %d out of range", action[i]);
+    if ((s = mlp_check_ready(ctx))) return s;
+    MlpState& M = ctx->mlp;
+    if ((s = mlp_reserve(ctx, (int)n)) || (s = clear_err(ctx))) return s;
+    if ((s = upload(ctx, M.feat, features, n * MLP_IN, "mlp H2D")) ||
+        (s = upload(ctx, M.action, (const int*)action, n, "mlp H2D")) ||
+        (s = upload(ctx, M.target, target, n, "mlp H2D")))
+        return s;
+    const int mp = round_up((int)n, 128);
+    launch_pack_features(ctx->stream, (int)n, mp, M.feat.p, M.X.p);
+    LAUNCHED("mlp pack features");
+    launch_transpose_bf16(ctx->stream, mp, MLP_K1, M.X.p, M.Xt.p);
+    LAUNCHED("mlp transpose");
+    CK(cudaMemsetAsync(M.loss.p, 0, sizeof(double), ctx->stream), "mlp memset");
+    if ((s = mlp_forward_dev(ctx, (int)n, true)) || (s = mlp_backward_dev(ctx, (int)n, huber_delta))) return s;
+    double loss = 0.0;
+    CK(cudaMemcpyAsync(&loss, M.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "mlp D2H");
+    if (out_grad)
+        CK(cudaMemcpyAsync(out_grad, M.g.p, MLP_N_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
+           "mlp D2H");
+    if ((s = check_err(ctx))) return s;
+    if (out_loss) *out_loss = loss;
+    return BINDER_OK;
+}
+
+int binder_mlp_set_tuples(binder_ctx* ctx, const binder_mc_tuple* t, size_t n) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n && !t) return fail(ctx, BINDER_ERR_ARG, "NULL tuples");
+    for (size_t i = 0; i < n; ++i)
+        if (t[i].action >= MLP_OUT || t[i].aa >= N_AA || t[i].antigen >= ctx->ags.size() || !std::isfinite(t[i].x) ||
+            !std::isfinite(t[i].y) || !std::isfinite(t[i].z) || !std::isfinite(t[i].delta_e))
+            return fail(ctx, BINDER_ERR_ARG, "invalid tuple %zu", i);
+    if ((s = upload(ctx, ctx->mlp.tuples, (const MlpTuple*)t, n, "tuples H2D"))) return s;
+    ctx->mlp.n_tuples = n;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_mlp_tuple_count(binder_ctx* ctx, size_t* out_n) {
+    if (!ctx || !out_n) return BINDER_ERR_ARG;
+    *out_n = ctx->mlp.n_tuples;
+    return BINDER_OK;
+}
+
+int binder_mlp_get_tuples(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_t* out_n) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (!out_n) return fail(ctx, BINDER_ERR_ARG, "NULL count");
+    *out_n = ctx->mlp.n_tuples;
+    if (cap < ctx->mlp.n_tuples) return fail(ctx, BINDER_ERR_CAPACITY, "need %zu tuples", ctx->mlp.n_tuples);
+    if (ctx->mlp.n_tuples)
+        CK(cudaMemcpyAsync(out, ctx->mlp.tuples.p, ctx->mlp.n_tuples * sizeof(MlpTuple), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "tuples D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float huber_delta, uint64_t seed,
+                     double* out_losses) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_steps < 0 || batch <= 0 || batch > (1 << 20) || !(lr > 0.0f) || !(huber_delta > 0.0f))
+        return fail(ctx, BINDER_ERR_ARG, "invalid training arguments");
+    if ((s = mlp_check_ready(ctx))) return s;
+    MlpState& M = ctx->mlp;
+    if (M.n_tuples == 0) return fail(ctx, BINDER_ERR_STATE, "no tuples to train on");
+    if ((s = mlp_reserve(ctx, batch)) || (s = clear_err(ctx))) return s;
+    CK(M.loss.ensure((size_t)std::max(1, n_steps)), "mlp alloc");
+    CK(cudaMemsetAsync(M.loss.p, 0, (size_t)std::max(1, n_steps) * sizeof(double), ctx->stream), "mlp memset");
+    const int mp = round_up(batch, 128);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    double* loss_base = M.loss.p;
+    for (int step = 0; step < n_steps; ++step) {
+        launch_draw_batch(ctx->stream, batch, (int)std::min<size_t>(M.n_tuples, INT32_MAX), seed, (uint32_t)M.adam_t,
+                          M.idx.p);
+        LAUNCHED("mlp draw batch");
+        launch_gather_tuples(ctx->stream, batch, M.idx.p, M.tuples.p, M.ca.p, M.aa.p, M.ag.p, M.action.p, M.target.p);
+        LAUNCHED("mlp gather");
+        launch_features(ctx->stream, batch, mp, M.ca.p, M.aa.p, M.ag.p, ctx->d_views.p, M.X.p);
+        LAUNCHED("features");
+        launch_transpose_bf16(ctx->stream, mp, MLP_K1, M.X.p, M.Xt.p);
+        LAUNCHED("mlp transpose");
+        M.loss.p = loss_base + step;  // per-step loss slot
+        s = mlp_forward_dev(ctx, batch, true);
+        if (!s) s = mlp_backward_dev(ctx, batch, huber_delta);
+        M.loss.p = loss_base;
+        if (s) return s;
+        M.adam_t += 1;
+        const float bc1 = 1.0f - std::pow(b1, (float)M.adam_t), bc2 = 1.0f - std::pow(b2, (float)M.adam_t);
+        launch_adam(ctx->stream, MLP_N_PARAMS, M.w.p, M.g.p, M.m1.p, M.m2.p, lr, b1, b2, eps, bc1, bc2);
+        LAUNCHED("mlp adam");
+        if ((s = mlp_pack(ctx))) return s;
+    }
+    if (out_losses && n_steps > 0)
+        CK(cudaMemcpyAsync(out_losses, loss_base, (size_t)n_steps * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "mlp D2H");
+    return check_err(ctx);
 }
 
 }  // extern "C"

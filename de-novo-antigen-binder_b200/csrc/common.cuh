@@ -128,6 +128,7 @@ struct AgView {
     // Calpha atoms in residue order with their AMBER parameters (diffusion.rs:440-446)
     const float4* ca_atom;      // x, y, z, partial charge
     const float4* ca_atom_prm;  // r_min_half, epsilon, hydrophobic, atom type
+    const uint8_t* res_aa;      // amino acid of each antigen residue (residue order)
     int n_res;
     float cx, cy, cz;  // ca_center_of_mass (allatom.rs:183-195)
 };

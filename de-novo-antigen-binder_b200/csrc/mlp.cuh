@@ -1,0 +1,103 @@
+// mlp.cuh — sizes, parameter layout and device views of the learned proposal
+// network (k_mlp.cu), and the environment count shared by the feature kernel and
+// the Metropolis kernel.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace binder {
+
+constexpr int MLP_IN = 180;       // 20 one-hot + 8 shells x 20 amino acids
+constexpr int MLP_K1 = 192;       // first-layer K padded to the MMA K step
+constexpr int MLP_H = 256;        // hidden width
+constexpr int MLP_OUT = 25;       // 20 mutation targets + 5 rotamers
+constexpr int MLP_OUT_PAD = 32;   // output rows of W3 (rows >= 25 stay zero)
+constexpr int MLP_SHELLS = 8;     // radial shells of 1.25 A out to 10 A
+constexpr int MLP_COUNT_CAP = 255;
+
+// flat FP32 parameter vector: W1 [256][192], b1 [256], W2 [256][256], b2 [256],
+// W3 [32][256], b3 [32]
+constexpr int MLP_OFF_W1 = 0;
+constexpr int MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_K1;
+constexpr int MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;
+constexpr int MLP_OFF_B2 = MLP_OFF_W2 + MLP_H * MLP_H;
+constexpr int MLP_OFF_W3 = MLP_OFF_B2 + MLP_H;
+constexpr int MLP_OFF_B3 = MLP_OFF_W3 + MLP_OUT_PAD * MLP_H;
+constexpr int MLP_N_PARAMS = MLP_OFF_B3 + MLP_OUT_PAD;
+
+// Shell of a squared distance r2 < 100: the number of squared shell radii
+// (1.25 k)^2, k = 1..7, that r2 reaches.  Every radius square is exact in f32.
+__host__ __device__ __forceinline__ int mlp_shell(float r2) {
+    return (r2 >= 1.5625f) + (r2 >= 6.25f) + (r2 >= 14.0625f) + (r2 >= 25.0f) + (r2 >= 39.0625f) +
+           (r2 >= 56.25f) + (r2 >= 76.5625f);
+}
+
+// Counts of antigen Calphas by (shell, amino acid) around (x, y, z), by one warp:
+// cnt[shell * 20 + aa] += 1 for every antigen Calpha with r^2 < 100 (the
+// reference's f32 rounding of r^2).  cnt is zeroed by the caller.
+__device__ __forceinline__ void mlp_count_env(const float4* __restrict__ ag_ca, const uint8_t* __restrict__ ag_aa,
+                                              int n, float x, float y, float z, int* cnt) {
+    for (int i = (threadIdx.x & 31); i < n; i += 32) {
+        const float4 a = ag_ca[i];
+        const float r2 = xdist2(xsub(x, a.x), xsub(y, a.y), xsub(z, a.z));
+        if (r2 < 100.0f) atomicAdd(&cnt[mlp_shell(r2) * N_AA + ag_aa[i]], 1);
+    }
+}
+
+enum : int { EPI_F32 = 0, EPI_PARTIAL = 1, EPI_SILU = 2, EPI_DSILU = 3 };
+
+// Epilogue of k_gemm_tc.
+//  EPI_F32:     c[row][col] = acc + bias[col]                (cols < n_valid, rows < m_valid)
+//  EPI_PARTIAL: the same without bias at c + blockIdx.y * part_stride (split-K partials)
+//  EPI_SILU:    z = acc + bias; c[row][col] = z (if c); h = silu(z) as BF16 to h[row][col]
+//               (rows < h_rows) and ht[col][row] (rows < ht_rows); rows >= m_valid store 0
+//  EPI_DSILU:   h = acc * silu'(z[row][col]) as BF16 to h / ht likewise
+struct GemmEpi {
+    int mode = EPI_F32;
+    const float* bias = nullptr;
+    float* c = nullptr;
+    int ldc = 0;
+    long long part_stride = 0;
+    __nv_bfloat16* h = nullptr;
+    int ldh = 0, h_rows = 0;
+    __nv_bfloat16* ht = nullptr;
+    int ldht = 0, ht_rows = 0;
+    const float* z = nullptr;
+    int ldz = 0;
+    int n_valid = 0, m_valid = 0;
+};
+
+// C = A * B^T: A [m][k] (row stride lda), B [n][k] (row stride ldb), BF16, K-major.
+// k and k_split multiples of 16 and 64; n in 16..256, multiple of 16.
+struct GemmArgs {
+    const __nv_bfloat16* a = nullptr;
+    int lda = 0, m = 0;
+    const __nv_bfloat16* b = nullptr;
+    int ldb = 0, n = 0;
+    int k = 0, k_split = 0;
+    GemmEpi e;
+};
+
+// BF16 weight copies used by the GEMMs
+struct MlpBf16 {
+    __nv_bfloat16* w1;   // [256][192]
+    __nv_bfloat16* w2;   // [256][256]
+    __nv_bfloat16* w2t;  // [256][256] transposed
+    __nv_bfloat16* w3;   // [32][256]
+    __nv_bfloat16* w3t;  // [256][32] transposed
+};
+
+// One logged Metropolis proposal (binder_mc_tuple of the C ABI, 32 bytes).
+struct MlpTuple {
+    float x, y, z;   // Calpha when the move was proposed
+    float delta_e;   // exact Metropolis energy change of the move
+    int32_t cand;
+    int16_t residue;
+    uint8_t aa, action, antigen, accepted;
+    uint8_t pad[6];
+};
+static_assert(sizeof(MlpTuple) == 32, "tuple layout");
+
+}  // namespace binder

@@ -317,6 +317,62 @@ typedef struct binder_run_cfg {
 void binder_default_run_cfg(binder_run_cfg* cfg);
 int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg, int32_t* out_cand, double* out_energy);
 
+/* ---- learned mutation / rotamer proposal (no reference counterpart) ------------------
+   A BF16 MLP, 180 -> 256 (SiLU) -> 256 (SiLU) -> 25, FP32 accumulation, trained on
+   the GPU on (environment, energy change) tuples of the plain Metropolis moves and
+   used as a Metropolis-Hastings proposal for the mutation and rotamer moves of
+   binder_diffuse (diffusion.rs:354-399); the exact energy still decides every
+   acceptance.
+   Features of a residue (180): a one-hot of its amino acid (20), then for shells
+   s = 0..7 of 1.25 A around its Calpha and amino acids a = 0..19, log1p of the
+   number of antigen Calphas of amino acid a at a distance in [1.25 s, 1.25 (s+1))
+   (index 20 + 20 s + a), as BF16.
+   Outputs (25): predicted energy change of a mutation to amino acid 0..19, then of
+   a move to rotamer 0..4.
+   Parameters: one FP32 vector of BINDER_MLP_N_PARAMS values, W1 [256][192] (input
+   columns 180..191 zero), b1 [256], W2 [256][256], b2 [256], W3 [32][256] (rows
+   25..31 zero), b3 [32] (entries 25..31 zero); W is [out][in]. */
+#define BINDER_MLP_IN 180
+#define BINDER_MLP_OUT 25
+#define BINDER_MLP_N_PARAMS 123424
+
+/* One logged Metropolis proposal (32 bytes). */
+typedef struct binder_mc_tuple {
+    float x, y, z;     /* Calpha of the residue when the move was proposed */
+    float delta_e;     /* Metropolis energy change of the move (kcal/mol) */
+    int32_t cand;      /* candidate (resident state index) */
+    int16_t residue;   /* residue within the candidate */
+    uint8_t aa;        /* amino acid before the move */
+    uint8_t action;    /* 0..19 mutation to that amino acid, 20..24 rotamer 0..4 */
+    uint8_t antigen;   /* resident antigen id */
+    uint8_t accepted;  /* 1 when the move was accepted */
+    uint8_t _pad[6];
+} binder_mc_tuple;
+
+/* Set the parameters (resets the optimiser) / read them back. */
+int binder_mlp_set_params(binder_ctx* ctx, const float* params);
+int binder_mlp_get_params(binder_ctx* ctx, float* params);
+/* Features of n residues (Calpha xyz float[n][3], amino acids) against resident
+   antigen antigen_id: out float[n][180] (the BF16 values the network sees). */
+int binder_mlp_features(binder_ctx* ctx, int32_t antigen_id, size_t n, const float* ca_xyz, const uint8_t* aa,
+                        float* out);
+/* Network outputs of n feature rows (float[n][180], rounded to BF16): out float[n][25]. */
+int binder_mlp_forward(binder_ctx* ctx, size_t n, const float* features, float* out);
+/* Mean Huber loss (threshold huber_delta) of output action[i] against target[i]
+   over the batch, and its gradient with respect to every parameter
+   (out_grad float[BINDER_MLP_N_PARAMS], may be NULL).  Parameters unchanged. */
+int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const int32_t* action,
+                         const float* target, float huber_delta, double* out_loss, float* out_grad);
+/* The training set: tuples logged by binder_diffuse (binder_mc_log) or given here. */
+int binder_mlp_set_tuples(binder_ctx* ctx, const binder_mc_tuple* tuples, size_t n);
+int binder_mlp_tuple_count(binder_ctx* ctx, size_t* out_n);
+int binder_mlp_get_tuples(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_t* out_n);
+/* n_steps Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on minibatches of `batch`
+   tuples drawn uniformly (Philox, key seed) from the training set; out_losses
+   double[n_steps] (may be NULL) = each step's mean Huber loss. */
+int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float huber_delta, uint64_t seed,
+                     double* out_losses);
+
 /* ---- instrumentation (no reference counterpart) --------------------------------
    The context's CUDA stream (cudaStream_t), for callers that time or order work
    around the library's launches. */
