@@ -172,15 +172,21 @@ _SIGS = {
     "binder_mlp_tuple_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "binder_mlp_get_tuples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "binder_mlp_train": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64, C.c_void_p]),
+    "binder_mc_log": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "binder_mc_log_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "binder_mc_log_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_mlp_take_log": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "binder_set_proposal": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
 }
+PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
 # learned proposal network (include/binder_gpu.h): sizes and the logged-tuple record
 MLP_IN, MLP_OUT, MLP_N_PARAMS = 180, 25, 123424
 MLP_K1, MLP_H, MLP_OUT_PAD = 192, 256, 32
 MLP_OFF = {"w1": 0, "b1": 49152, "w2": 49408, "b2": 114944, "w3": 115200, "b3": 123392}
 MC_TUPLE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("delta_e", "<f4"), ("cand", "<i4"),
-                     ("residue", "<i2"), ("aa", "u1"), ("action", "u1"), ("antigen", "u1"), ("accepted", "u1"),
-                     ("_pad", "u1", (6,))])
+                     ("log_ratio", "<f4"), ("residue", "<i2"), ("aa", "u1"), ("action", "u1"), ("antigen", "u1"),
+                     ("accepted", "u1"), ("_pad", "u1", (2,))])
 
 
 def mlp_init_params(seed=0):
@@ -675,6 +681,33 @@ class GpuContext:
         out = np.zeros(n.value, MC_TUPLE)
         self._check(lib().binder_mlp_get_tuples(self._h, _ptr(out), len(out), C.byref(n)))
         return out
+
+    def set_proposal(self, learned, t_prop_min=0.3):
+        """Mutation / rotamer proposal of diffuse(): uniform (the reference) or the network."""
+        self._check(lib().binder_set_proposal(self._h, PROPOSAL_LEARNED if learned else PROPOSAL_UNIFORM,
+                                              t_prop_min))
+
+    def mc_log(self, capacity):
+        """Log the mutation / rotamer decisions of the following diffuse() calls (0 stops)."""
+        self._check(lib().binder_mc_log(self._h, capacity))
+
+    def mc_log_count(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        self._check(lib().binder_mc_log_count(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def mc_log_fetch(self):
+        n, _ = self.mc_log_count()
+        out = np.zeros(n, MC_TUPLE)
+        got = C.c_size_t()
+        self._check(lib().binder_mc_log_fetch(self._h, _ptr(out), len(out), C.byref(got)))
+        return out[:got.value]
+
+    def mlp_take_log(self):
+        """The logged tuples become the training set; returns their number."""
+        n = C.c_size_t()
+        self._check(lib().binder_mlp_take_log(self._h, C.byref(n)))
+        return n.value
 
     def mlp_train(self, n_steps, batch=8192, lr=1e-3, huber_delta=1.0, seed=0):
         """n_steps Adam steps on minibatches of the training set; per-step losses."""

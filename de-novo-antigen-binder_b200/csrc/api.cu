@@ -151,7 +151,16 @@ struct MlpState {
     DBuf<double> loss;
     DBuf<MlpTuple> tuples;
     size_t n_tuples = 0;
+    // proposal of binder_diffuse's mutation / rotamer moves, and the proposal log
+    bool learned = false;
+    float t_prop_min = 0.3f;
+    DBuf<MlpTuple> log;
+    DBuf<unsigned long long> log_n;
+    size_t log_cap = 0;
     MlpBf16 bf16() { return MlpBf16{w1.p, w2.p, w2t.p, w3.p, w3t.p}; }
+    MlpDev dev() const {
+        return MlpDev{w1.p, w2.p, w3.p, w.p + MLP_OFF_B1, w.p + MLP_OFF_B2, w.p + MLP_OFF_B3, t_prop_min};
+    }
 };
 
 struct binder_ctx {
@@ -253,7 +262,8 @@ int cuda_fail(binder_ctx* ctx, cudaError_t e, const char* what) {
 cudaError_t init_mlp_tables() {
     float t[MLP_COUNT_CAP + 1];
     for (int n = 0; n <= MLP_COUNT_CAP; ++n) t[n] = (float)std::log1p((double)n);
-    return mlp_init_tables(t);
+    cudaError_t e = mlp_init_tables(t);
+    return e ? e : anneal_init_mlp_table(t);
 }
 
 int enter(binder_ctx* ctx) {
@@ -1252,10 +1262,20 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
             max_ag = std::max(max_ag, a->n_res);
             max_cells = std::max(max_cells, g.nx * g.ny * g.nz + 1);
         }
+        AnnealExtras x;
+        if (ctx->mlp.learned) {
+            if (!ctx->mlp.ready) return fail(ctx, BINDER_ERR_STATE, "learned proposal without network parameters");
+            x.learned = true;
+            x.mlp = ctx->mlp.dev();
+        }
+        if (ctx->mlp.log_cap) {
+            x.log = ctx->mlp.log.p;
+            x.log_n = ctx->mlp.log_n.p;
+            x.log_cap = (long long)ctx->mlp.log_cap;
+        }
         CK(launch_anneal(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
                          temps ? ctx->temps.p : nullptr, ctx->params.accumulate, S.max_res, max_ag, max_cells,
-                         ctx->errf.p,
-                         S.mc_stats.p),
+                         ctx->errf.p, S.mc_stats.p, x),
            "anneal");
         LAUNCHED("anneal");
         S.order_valid = false;  // residues moved: the cell order is stale
@@ -2093,6 +2113,83 @@ int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float hu
                            ctx->stream),
            "mlp D2H");
     return check_err(ctx);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (mode != BINDER_PROPOSAL_UNIFORM && mode != BINDER_PROPOSAL_LEARNED)
+        return fail(ctx, BINDER_ERR_ARG, "unknown proposal mode %d", mode);
+    if (!(t_prop_min > 0.0f) || !std::isfinite(t_prop_min)) return fail(ctx, BINDER_ERR_ARG, "t_prop_min must be > 0");
+    if (mode == BINDER_PROPOSAL_LEARNED && (s = mlp_check_ready(ctx))) return s;
+    ctx->mlp.learned = mode == BINDER_PROPOSAL_LEARNED;
+    ctx->mlp.t_prop_min = t_prop_min;
+    return BINDER_OK;
+}
+
+int binder_mc_log(binder_ctx* ctx, size_t capacity) {
+    int s = enter(ctx);
+    if (s) return s;
+    MlpState& M = ctx->mlp;
+    if (capacity == 0) {
+        M.log.release();
+        M.log_n.release();
+        M.log_cap = 0;
+        return BINDER_OK;
+    }
+    CK(M.log.ensure(capacity), "log alloc");
+    CK(M.log_n.ensure(1), "log alloc");
+    CK(cudaMemsetAsync(M.log_n.p, 0, sizeof(unsigned long long), ctx->stream), "log memset");
+    M.log_cap = capacity;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_mc_log_count(binder_ctx* ctx, size_t* out_logged, size_t* out_proposed) {
+    int s = enter(ctx);
+    if (s) return s;
+    unsigned long long n = 0;
+    if (ctx->mlp.log_cap) {
+        CK(cudaMemcpyAsync(&n, ctx->mlp.log_n.p, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream), "log D2H");
+        CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    }
+    if (out_proposed) *out_proposed = (size_t)n;
+    if (out_logged) *out_logged = std::min<size_t>((size_t)n, ctx->mlp.log_cap);
+    return BINDER_OK;
+}
+
+int binder_mc_log_fetch(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_t* out_n) {
+    size_t n = 0;
+    int s = binder_mc_log_count(ctx, &n, nullptr);
+    if (s) return s;
+    if (!out_n) return fail(ctx, BINDER_ERR_ARG, "NULL count");
+    *out_n = n;
+    if (cap < n) return fail(ctx, BINDER_ERR_CAPACITY, "need %zu tuples", n);
+    if (n) {
+        if (!out) return fail(ctx, BINDER_ERR_ARG, "NULL output");
+        CK(cudaMemcpyAsync(out, ctx->mlp.log.p, n * sizeof(MlpTuple), cudaMemcpyDeviceToHost, ctx->stream), "log D2H");
+        CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    }
+    return BINDER_OK;
+}
+
+int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n) {
+    size_t n = 0;
+    int s = binder_mc_log_count(ctx, &n, nullptr);
+    if (s) return s;
+    MlpState& M = ctx->mlp;
+    CK(M.tuples.ensure(std::max<size_t>(n, 1)), "tuples alloc");
+    if (n)
+        CK(cudaMemcpyAsync(M.tuples.p, M.log.p, n * sizeof(MlpTuple), cudaMemcpyDeviceToDevice, ctx->stream),
+           "tuples copy");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    M.n_tuples = n;
+    if (out_n) *out_n = n;
+    return BINDER_OK;
 }
 
 }  // extern "C"

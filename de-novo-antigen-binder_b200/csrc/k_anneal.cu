@@ -29,10 +29,18 @@
 // the double energy difference.
 #include "geom.cuh"
 #include "kernels.h"
+#include "mlp_tile.cuh"
 
 namespace binder {
 
 cudaError_t anneal_init_tables() { return geom_init_tables(); }
+
+// log1p of the environment counts for the in-kernel features (the same host table
+// as the feature kernel's)
+__constant__ float c_an_log1p[MLP_COUNT_CAP + 1];
+cudaError_t anneal_init_mlp_table(const float* t) {
+    return cudaMemcpyToSymbol(c_an_log1p, t, sizeof(float) * (MLP_COUNT_CAP + 1));
+}
 
 constexpr int AN_WARPS = 8;
 constexpr int AN_THREADS = AN_WARPS * 32;
@@ -44,7 +52,7 @@ constexpr int AG_STAGE_MAX = 1024;                   // antigen Calphas staged i
 constexpr int CELL_STAGE_MAX = 4096;                 // Calpha-grid cells staged in shared memory
 enum : int { MV_NONE = 0, MV_ROT = 1, MV_MUT = 2 };
 enum : int { SEL_KEEP = 0, SEL_PROP = 1, SEL_REJ = 2 };
-enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3 };
+enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3, IS_NMV = 4, IS_NMV2 = 5 };
 
 // Shared-memory carve of one CTA for candidates of up to R residues and antigens
 // of up to G staged Calphas.
@@ -54,7 +62,8 @@ struct AnSmem {
     float4* chi;               // R (degrees)
     float4* ldelta;            // R: Langevin translation
     float4* bb_trig;           // R: cos, sin of the torsion step and of its negation
-    float4* terms;             // min(R, 32) * CG_LANES * CG_SLOTS Langevin pair terms
+    float4* terms;             // min(R, 32) * CG_LANES * CG_SLOTS Langevin pair terms; with the learned
+                               // proposal also the network tile (the two are never live together)
     float4* stage;             // AN_WARPS * STAGE_CAP: in-cutoff Calpha-energy terms
     float4 *agq, *agp;         // G staged antigen Calphas: x, y, z, q | r_min_half, eps, hyd, type
     float4 *cgq, *cgp;         // G staged Calphas in CG-grid order (AgView::ca_pq, ca_prm)
@@ -62,18 +71,27 @@ struct AnSmem {
     AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
     double* dscal;                  // [0] disulfide energy of the current state
+    double *lhr, *lqf;              // R: log Hastings ratio of the move, log q of the forward mutation
     float *u_acc, *bb_u;            // R
     int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
+    int *rot, *mvl, *mv2;           // R: rotamer index of the state (-1 unknown), residues with a move
+    uint32_t* dz;                   // R: the move's choice draw
     int* iscal;
 };
-__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C) {
+__host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
-    return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + (size_t)L * CG_SLOTS * 16 +
+    const size_t t = (size_t)L * CG_SLOTS * 16;
+    return learned && t < (size_t)MT_BYTES ? (size_t)MT_BYTES : t;
+}
+__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned) {
+    const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
+    return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + anneal_terms_bytes(R, learned) +
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
-           (size_t)R * 8 * 3 + 16 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 + 32;
+           (size_t)R * 8 * 3 + 16 + (size_t)R * 8 * 2 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
+           (size_t)R * 4 * 4 + 32;
 }
-__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C) {
+__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
     AnSmem s;
     const int L = min(R, CG_RES_PER_PASS) * CG_LANES;
     auto take = [&](size_t bytes) { unsigned char* p = b; b += bytes; return p; };
@@ -84,7 +102,7 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C) {
     s.chi = (float4*)take((size_t)R * 16);
     s.ldelta = (float4*)take((size_t)R * 16);
     s.bb_trig = (float4*)take((size_t)R * 16);
-    s.terms = (float4*)take((size_t)L * CG_SLOTS * 16);
+    s.terms = (float4*)take(anneal_terms_bytes(R, learned));
     s.stage = (float4*)take((size_t)AN_WARPS * STAGE_CAP * 16);
     s.agq = (float4*)take((size_t)G * 16);
     s.agp = (float4*)take((size_t)G * 16);
@@ -96,6 +114,8 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C) {
     s.c_old = (double*)take((size_t)R * 8);
     s.c_new = (double*)take((size_t)R * 8);
     s.dscal = (double*)take(16);
+    s.lhr = (double*)take((size_t)R * 8);
+    s.lqf = (double*)take((size_t)R * 8);
     s.u_acc = (float*)take((size_t)R * 4);
     s.bb_u = (float*)take((size_t)R * 4);
     s.aa = (int*)take((size_t)R * 4);
@@ -108,6 +128,10 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C) {
     s.bb_phi = (int*)take((size_t)R * 4);
     s.iface = (int*)take((size_t)R * 4);
     s.tcount = (int*)take((size_t)L * 4);
+    s.rot = (int*)take((size_t)R * 4);
+    s.mvl = (int*)take((size_t)R * 4);
+    s.mv2 = (int*)take((size_t)R * 4);
+    s.dz = (uint32_t*)take((size_t)R * 4);
     s.iscal = (int*)take(32);
     return s;
 }
@@ -227,6 +251,64 @@ __device__ __forceinline__ bool metropolis(float de, float temp, float u) {
 }
 __device__ __forceinline__ bool metropolis(double de, float temp, float u) {
     return de <= 0.0 || (double)u < exp(-de / (double)temp);
+}
+// Metropolis-Hastings with the log proposal ratio lhr = log q(reverse) - log q(forward):
+// accept when u < exp(-dE/T + lhr).  lhr == 0 (uniform proposal) is exactly the
+// Metropolis criterion above.
+template <class ACC>
+__device__ __forceinline__ bool mh_accept(ACC de, float temp, float u, double lhr) {
+    if (lhr == 0.0) return metropolis(de, temp, u);
+    const double a = -(double)de / (double)temp + lhr;
+    return a >= 0.0 || (double)u < exp(a);
+}
+
+// ---- learned proposal -------------------------------------------------------------
+// Features of the tile rows: row i = residue mvl[base + i] with amino acid
+// (prop ? new_aa : aa); one warp per row (rows i and i + 8).
+__device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* rows_of, int base, int rows,
+                                 const float4* agq, const uint8_t* ag_aa, int nag, bool prop) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = warp; i < MT_ROWS; i += AN_WARPS) {
+        int* cnt = T.cnt + i * MLP_SHELLS * N_AA;
+        __nv_bfloat16* x = T.x + i * MT_XS;
+        if (i >= rows) {
+            for (int j = lane; j < MLP_K1; j += 32) x[j] = __float2bfloat16_rn(0.0f);
+            continue;
+        }
+        const int r = rows_of[base + i];
+        for (int j = lane; j < MLP_SHELLS * N_AA; j += 32) cnt[j] = 0;
+        __syncwarp();
+        const float4 ca = S.pos[r * SLOT_STRIDE + 1];
+        mlp_count_env(agq, ag_aa, nag, ca.x, ca.y, ca.z, cnt);
+        __syncwarp();
+        const int a = prop ? S.new_aa[r] : S.aa[r];
+        for (int j = lane; j < MLP_K1; j += 32) {
+            float v = 0.0f;
+            if (j < N_AA) v = j == a ? 1.0f : 0.0f;
+            else if (j < MLP_IN) v = c_an_log1p[min(cnt[j - N_AA], MLP_COUNT_CAP)];
+            x[j] = __float2bfloat16_rn(v);
+        }
+    }
+}
+
+// Choice among n options with logits l_k = -y[k] / tp by inverse CDF on u = dz / 2^32
+// (for equal logits exactly urange(dz, n)); returns the index, its log probability
+// in *lq and the log normaliser log sum exp(l) in *lz.
+__device__ int an_sample(const float* y, int n, float tp, uint32_t dz, double* lq, double* lz) {
+    double m = -INFINITY;
+    for (int k = 0; k < n; ++k) m = fmax(m, -(double)y[k] / (double)tp);
+    double sum = 0.0;
+    for (int k = 0; k < n; ++k) sum += exp(-(double)y[k] / (double)tp - m);
+    const double target = (double)dz * (1.0 / 4294967296.0) * sum;
+    double cum = 0.0;
+    int pick = n - 1;
+    for (int k = 0; k < n; ++k) {
+        cum += exp(-(double)y[k] / (double)tp - m);
+        if (target < cum) { pick = k; break; }
+    }
+    *lz = m + log(sum);
+    *lq = -(double)y[pick] / (double)tp - *lz;
+    return pick;
 }
 
 // The residue a move leaves: which = SEL_PROP builds the proposal, SEL_REJ the state
@@ -356,13 +438,79 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
     fx = sx; fy = sy; fz = sz;
 }
 
+// The network's choice of every mutation and (known-rotamer) rotamer move drawn
+// this step and the moves' log Hastings ratios (all threads of the CTA call).
+__device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const float4* agq, const uint8_t* ag_aa,
+                                                int nag, const MlpDev& mlp, float temp) {
+    const int tid = threadIdx.x;
+    const MlpTile T = mlp_tile_carve((unsigned char*)S.terms);
+    const float tp = fmaxf(temp, mlp.t_prop_min);
+    if (tid == 0) {  // mutations, and rotamer moves from a known library rotamer
+        int k = 0;
+        for (int r = 0; r < n; ++r)
+            if (S.kind[r] == MV_MUT || (S.kind[r] == MV_ROT && S.rot[r] >= 0)) S.mvl[k++] = r;
+        S.iscal[IS_NMV] = k;
+    }
+    __syncthreads();
+    const int n_mv = S.iscal[IS_NMV];
+    for (int base = 0; base < n_mv; base += MT_ROWS) {
+        const int rows = min(MT_ROWS, n_mv - base);
+        an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag, false);
+        __syncthreads();
+        mlp_tile_forward(mlp, T);
+        if (tid < rows) {
+            const int r = S.mvl[base + tid];
+            const float* y = T.y + tid * MT_YS;
+            double lq, lz;
+            if (S.kind[r] == MV_ROT) {
+                const int nr = s_rot_n[S.aa[r]];
+                const int k = an_sample(y + N_AA, nr, tp, S.dz[r], &lq, &lz);
+                S.new_rot[r] = k;
+                // same features before and after a rotamer move: the normalisers cancel
+                S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
+            } else {
+                S.new_aa[r] = an_sample(y, N_AA, tp, S.dz[r], &lq, &lz);
+                S.lqf[r] = lq;
+            }
+        }
+        __syncthreads();
+    }
+    // reverse probabilities of the mutations: the network at the proposed amino acid
+    if (tid == 0) {
+        int k = 0;
+        for (int j = 0; j < n_mv; ++j)
+            if (S.kind[S.mvl[j]] == MV_MUT) S.mv2[k++] = S.mvl[j];
+        S.iscal[IS_NMV2] = k;
+    }
+    __syncthreads();
+    const int n_mv2 = S.iscal[IS_NMV2];
+    for (int base = 0; base < n_mv2; base += MT_ROWS) {
+        const int rows = min(MT_ROWS, n_mv2 - base);
+        an_tile_features(S, T, S.mv2, base, rows, agq, ag_aa, nag, true);
+        __syncthreads();
+        mlp_tile_forward(mlp, T);
+        if (tid < rows) {
+            const int r = S.mv2[base + tid];
+            const float* y = T.y + tid * MT_YS;
+            double m = -INFINITY, sum = 0.0;
+            for (int k = 0; k < N_AA; ++k) m = fmax(m, -(double)y[k] / (double)tp);
+            for (int k = 0; k < N_AA; ++k) sum += exp(-(double)y[k] / (double)tp - m);
+            const double lq_rev = -(double)y[S.aa[r]] / (double)tp - (m + log(sum));
+            S.lhr[r] = lq_rev - S.lqf[r];
+        }
+        __syncthreads();
+    }
+}
+
 template <class ACC>
 __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                        int n_steps, uint32_t step0, int with_noise,
                                                        const float* __restrict__ temps, int R, int G, int C,
-                                                       uint32_t* __restrict__ err, long long* __restrict__ stats) {
+                                                       uint32_t* __restrict__ err, long long* __restrict__ stats,
+                                                       MlpDev mlp, int learned, MlpTuple* __restrict__ tlog,
+                                                       unsigned long long* __restrict__ log_n, long long log_cap) {
     extern __shared__ __align__(16) unsigned char an_smem[];
-    const AnSmem S = carve(an_smem, R, G, C);
+    const AnSmem S = carve(an_smem, R, G, C, learned);
     const int c = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = st.cand_res_off[c];
@@ -395,10 +543,20 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
 
     for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
     for (int r = tid; r < n; r += AN_THREADS) {
-        S.aa[r] = st.res_aa[r0 + r];
-        S.chi[r] = st.res_chi[r0 + r];
+        const int a = st.res_aa[r0 + r];
+        const float4 chi = st.res_chi[r0 + r];
+        S.aa[r] = a;
+        S.chi[r] = chi;
         S.trig[2 * r] = st.res_trig[2 * (r0 + r)];
         S.trig[2 * r + 1] = st.res_trig[2 * (r0 + r) + 1];
+        // rotamer index of the state: the library entry whose chi it holds, else -1
+        int k = -1;
+        for (int q = 0; q < s_rot_n[a] && k < 0; ++q) {
+            const float4 t = s_rot_chi[a][q];
+            if (t.x == chi.x && t.y == chi.y && t.z == chi.z && t.w == chi.w) k = q;
+        }
+        S.rot[r] = k;
+        S.lhr[r] = 0.0;
     }
     long long n_mc = 0, n_mc_acc = 0, n_bb = 0, n_bb_acc = 0;
     __syncthreads();
@@ -518,9 +676,14 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
             }
             S.kind[r] = kind;
             S.u_acc[r] = u01(d.w);
+            S.dz[r] = d.z;
+            S.lhr[r] = 0.0;
             if (aa == CYS) atomicAdd(&S.iscal[IS_NCYS], 1);
         }
         __syncthreads();
+        // learned proposal: the choice of each drawn move comes from the network
+        // (same draw d.z, inverse CDF) and the move carries its Hastings ratio
+        if (learned) an_learned_choices(S, n, agq, A.res_aa, nag, mlp, temp);
         // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
         // the Calpha energies before / after each move on warps 0..3 (one warp each)
         if (warp >= AN_WARPS / 2) {
@@ -570,10 +733,30 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                                        : (ACC)0;
                 const ACC old_e = (ACC)S.c_old[r] + D;
                 const ACC new_e = (ACC)S.c_new[r] + Dn;
-                const bool acc = metropolis(new_e - old_e, temp, S.u_acc[r]);
+                const double lhr = S.lhr[r];
+                const bool acc = mh_accept(new_e - old_e, temp, S.u_acc[r], lhr);
                 ++n_mc;
                 n_mc_acc += acc;
+                if (tlog) {
+                    const unsigned long long slot = atomicAdd(log_n, 1ull);
+                    if ((long long)slot < log_cap) {
+                        const float4 ca = S.pos[r * SLOT_STRIDE + 1];
+                        MlpTuple t;
+                        t.x = ca.x; t.y = ca.y; t.z = ca.z;
+                        t.delta_e = (float)(new_e - old_e);
+                        t.cand = c;
+                        t.log_ratio = (float)lhr;
+                        t.residue = (int16_t)r;
+                        t.aa = (uint8_t)oa;
+                        t.action = (uint8_t)(kind == MV_MUT ? na : N_AA + S.new_rot[r]);
+                        t.antigen = (uint8_t)st.cand_ag[c];
+                        t.accepted = acc ? 1 : 0;
+                        t.pad[0] = t.pad[1] = 0;
+                        tlog[slot] = t;
+                    }
+                }
                 if (acc) {
+                    S.rot[r] = kind == MV_ROT ? S.new_rot[r] : (s_rot_n[na] > 0 ? 0 : -1);
                     S.sel[r] = SEL_PROP;
                     S.aa[r] = na;
                     const int rot = S.new_rot[r];
@@ -682,29 +865,31 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
     }
 }
 
-size_t anneal_smem(int max_res, int max_ag_res, int max_cells) {
+size_t anneal_smem(int max_res, int max_ag_res, int max_cells, int learned) {
     const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
-    return anneal_smem_bytes(max_res, G, G && max_cells <= CELL_STAGE_MAX ? max_cells : 0);
+    return anneal_smem_bytes(max_res, G, G && max_cells <= CELL_STAGE_MAX ? max_cells : 0, learned);
 }
 
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          int max_ag_res, int max_cells, uint32_t* err, long long* stats) {
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x) {
     if (st.n_cand <= 0 || n_steps <= 0 || max_res <= 0) return cudaSuccess;
     const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
     const int C = G && max_cells <= CELL_STAGE_MAX ? max_cells : 0;
-    const size_t smem = anneal_smem_bytes(max_res, G, C);
+    const int learned = x.learned ? 1 : 0;
+    const size_t smem = anneal_smem_bytes(max_res, G, C, learned);
     cudaError_t e;
     if (accumulate == 1) {
         if ((e = cudaFuncSetAttribute(k_anneal<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
             return e;
         k_anneal<float><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G,
-                                                           C, err, stats);
+                                                           C, err, stats, x.mlp, learned, x.log, x.log_n, x.log_cap);
     } else {
         if ((e = cudaFuncSetAttribute(k_anneal<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
             return e;
         k_anneal<double><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res,
-                                                            G, C, err, stats);
+                                                            G, C, err, stats, x.mlp, learned, x.log, x.log_n,
+                                                            x.log_cap);
     }
     return cudaGetLastError();
 }

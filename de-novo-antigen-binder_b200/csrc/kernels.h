@@ -92,13 +92,24 @@ void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView*
 // ---- k_anneal.cu: Langevin + Metropolis steps, one CTA per candidate ----
 constexpr int ANNEAL_MAX_RES = 128;  // residues per candidate held in shared memory
 cudaError_t anneal_init_tables();
-size_t anneal_smem(int max_res, int max_ag_res, int max_cells);
+cudaError_t anneal_init_mlp_table(const float* log1p_table);
+size_t anneal_smem(int max_res, int max_ag_res, int max_cells, int learned);
+// The learned proposal (mlp, used when learned) and the proposal log (log may be
+// null: every mutation / rotamer decision appends one tuple while *log_n < log_cap;
+// *log_n counts all decisions).
+struct AnnealExtras {
+    MlpDev mlp{};
+    bool learned = false;
+    MlpTuple* log = nullptr;
+    unsigned long long* log_n = nullptr;
+    long long log_cap = 0;
+};
 // accumulate: 1 = the reference's f32 sums, else f32 terms summed in double.
 // stats (may be null): 4 per candidate, += mutation/rotamer tried, accepted,
 // backbone tried, accepted.
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          int max_ag_res, int max_cells, uint32_t* err, long long* stats);
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x);
 
 // ---- k_mlp.cu: the learned proposal network (features, tcgen05 GEMM, training) ----
 cudaError_t mlp_init_tables(const float* log1p_table);

@@ -91,12 +91,24 @@ struct MlpBf16 {
 
 // One logged Metropolis proposal (binder_mc_tuple of the C ABI, 32 bytes).
 struct MlpTuple {
-    float x, y, z;   // Calpha when the move was proposed
-    float delta_e;   // exact Metropolis energy change of the move
+    float x, y, z;      // Calpha when the move was proposed
+    float delta_e;      // exact Metropolis energy change of the move
     int32_t cand;
+    float log_ratio;    // log q(reverse) - log q(forward) of the proposal (0 when uniform)
     int16_t residue;
     uint8_t aa, action, antigen, accepted;
-    uint8_t pad[6];
+    uint8_t pad[2];
+};
+
+// The network as the Metropolis kernel sees it (BF16 weights, FP32 biases).
+struct MlpDev {
+    const __nv_bfloat16* w1;  // [256][192]
+    const __nv_bfloat16* w2;  // [256][256]
+    const __nv_bfloat16* w3;  // [32][256]
+    const float* b1;
+    const float* b2;
+    const float* b3;
+    float t_prop_min;         // proposal temperature = max(T, t_prop_min)
 };
 static_assert(sizeof(MlpTuple) == 32, "tuple layout");
 

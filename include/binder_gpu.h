@@ -341,12 +341,13 @@ typedef struct binder_mc_tuple {
     float x, y, z;     /* Calpha of the residue when the move was proposed */
     float delta_e;     /* Metropolis energy change of the move (kcal/mol) */
     int32_t cand;      /* candidate (resident state index) */
+    float log_ratio;   /* log q(reverse move) - log q(move) of the proposal; 0 when uniform */
     int16_t residue;   /* residue within the candidate */
     uint8_t aa;        /* amino acid before the move */
     uint8_t action;    /* 0..19 mutation to that amino acid, 20..24 rotamer 0..4 */
     uint8_t antigen;   /* resident antigen id */
     uint8_t accepted;  /* 1 when the move was accepted */
-    uint8_t _pad[6];
+    uint8_t _pad[2];
 } binder_mc_tuple;
 
 /* Set the parameters (resets the optimiser) / read them back. */
@@ -367,6 +368,25 @@ int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const
 int binder_mlp_set_tuples(binder_ctx* ctx, const binder_mc_tuple* tuples, size_t n);
 int binder_mlp_tuple_count(binder_ctx* ctx, size_t* out_n);
 int binder_mlp_get_tuples(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_t* out_n);
+/* Log every mutation / rotamer decision of the following binder_diffuse calls with
+   Metropolis moves into a device buffer of `capacity` tuples (0 stops logging and
+   frees it).  Tuples past the capacity are counted, not stored. */
+int binder_mc_log(binder_ctx* ctx, size_t capacity);
+int binder_mc_log_count(binder_ctx* ctx, size_t* out_logged, size_t* out_proposed);
+int binder_mc_log_fetch(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_t* out_n);
+/* The logged tuples become the training set (device copy). */
+int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n);
+/* Proposal of binder_diffuse's mutation and rotamer moves.  UNIFORM: the
+   reference's uniform choice.  LEARNED: the choice drawn from softmax(-y / Tp) of
+   the network outputs y at the residue's environment, Tp = max(T, t_prop_min), by
+   inverse CDF on the same random draw (a network with constant outputs chooses
+   exactly as UNIFORM does), accepted with probability min(1, exp(-dE/T) q(reverse)
+   / q(move)), the reverse probability of a mutation evaluated by the network at
+   the proposed amino acid.  Rotamer moves from a chi that is no library rotamer
+   stay uniform. */
+#define BINDER_PROPOSAL_UNIFORM 0
+#define BINDER_PROPOSAL_LEARNED 1
+int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min);
 /* n_steps Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on minibatches of `batch`
    tuples drawn uniformly (Philox, key seed) from the training set; out_losses
    double[n_steps] (may be NULL) = each step's mean Huber loss. */

@@ -975,6 +975,13 @@ float orc_residue_contribution(const orc_antigen* A, int n_res, const uint8_t* a
     return residue_contribution(A, P, r);
 }
 
+double orc_residue_contribution64(const orc_antigen* A, int n_res, const uint8_t* aa, const float* pos, int r) {
+    std::vector<uint8_t> a(aa, aa + n_res);
+    std::vector<float> chi((size_t)n_res * 4, 0.f);
+    Prot P{n_res, a.data(), chi.data(), const_cast<float*>(pos)};
+    return residue_contribution_t<double>(A, P, r);
+}
+
 float orc_disulfide(int n_res, const uint8_t* aa, const float* pos) {
     std::vector<uint8_t> a(aa, aa + n_res);
     std::vector<float> chi((size_t)n_res * 4, 0.f);

@@ -136,6 +136,8 @@ void orc_antigen_center(const orc_antigen*, float out[3]);
 
 /* residue_contribution_allatom (diffusion.rs:425-463), ref f32 order */
 float orc_residue_contribution(const orc_antigen*, int n_res, const uint8_t* aa, const float* pos, int r);
+/* the same f32 terms summed in double (the GPU's default Metropolis accumulation) */
+double orc_residue_contribution64(const orc_antigen*, int n_res, const uint8_t* aa, const float* pos, int r);
 /* disulfide_energy (allatom.rs:155-180) */
 float orc_disulfide(int n_res, const uint8_t* aa, const float* pos);
 

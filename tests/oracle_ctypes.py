@@ -33,12 +33,13 @@ def lib():
         _L.orc_temperature.restype = C.c_float
         _L.orc_temperature.argtypes = [C.c_int, C.c_int]
         _L.orc_residue_contribution.restype = C.c_float
+        _L.orc_residue_contribution64.restype = C.c_double
         _L.orc_disulfide.restype = C.c_float
         _L.orc_antigen_new.restype = C.c_void_p
         _L.orc_antigen_new.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float]
         _L.orc_antigen_free.argtypes = [C.c_void_p]
         _L.orc_topology_size.restype = C.c_int
-        for fn in ("orc_residue_contribution",):
+        for fn in ("orc_residue_contribution", "orc_residue_contribution64"):
             getattr(_L, fn).argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         _L.orc_disulfide.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         _L.orc_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -307,9 +308,12 @@ class Antigen:
         lib().orc_antigen_center(C.c_void_p(self.h), P(out))
         return out
 
-    def residue_contribution(self, aa, pos, r):
+    def residue_contribution(self, aa, pos, r, f64_sum=False):
+        """residue_contribution_allatom: f32 sum (the reference), or the same f32
+        terms summed in double"""
         aa, pos = u8(aa), f32(pos)
-        return lib().orc_residue_contribution(self.h, len(aa), P(aa), P(pos), r)
+        fn = lib().orc_residue_contribution64 if f64_sum else lib().orc_residue_contribution
+        return fn(self.h, len(aa), P(aa), P(pos), r)
 
     def step(self, params, aa, chi, pos, n_res, cand_id, step_id, temp, with_noise, with_mc, threads=8, stats=None):
         """in-place: aa [n_cand*n_res], chi [..,4], pos [..,14,3]"""
