@@ -462,12 +462,64 @@ def run_ours(args, rank, world, local_rank):
             "sample": f"{ms_steps} of {PHASE2_STEPS} phase-2 steps on the 64 survivors, {mdt:.1f} s"}
         cpu_run_s = n_cand * PHASE1_STEPS / (n * nb * N_STEPS_PER_BLOCK / dt) + TOP_K * PHASE2_STEPS / cpu_p2
         line["run_allatom"]["cpu_estimate_ms"] = 1e3 * cpu_run_s
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned_proposal"] = run_learned(pkg, ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_learned(pkg, ctx, seeds=(21, 22, 23), n_res=20):
+    """The learned proposal (configs of the learned-proposal workload): plain-MC
+    tuples on 4 training antigens, GPU training, then annealed 600-step runs on a
+    held-out antigen, uniform vs learned proposal, time to the uniform method's
+    median final champion (within 0.5 kcal/mol)."""
+    L = pkg.learned
+    cfg = pkg.workloads.config4(n_train=4, n_eval=1)
+    shell = float(cfg["train"][0][1])
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=shell, seed=11))
+    train_ids = L.add_antigens(ctx, [t[0] for t in cfg["train"]])
+    eval_ag, _, eval_pop = cfg["eval"][0]
+    (eval_id,) = L.add_antigens(ctx, [eval_ag])
+    t0 = time.perf_counter()
+    n_tuples = L.generate_tuples(ctx, [t[2] for t in cfg["train"]], train_ids, n_res, gen_steps=300)
+    gen_s = time.perf_counter() - t0
+    train_steps = 1500
+    losses, train_s = L.train(ctx, train_steps, batch=8192, lr=1e-3)
+    agid = L.upload_populations(ctx, [eval_pop], [eval_id], n_res)
+    ctx.diffuse(PHASE1_STEPS, 0)  # phase-1 gradient steps bring the population into contact
+    s0 = ctx.state_download()
+    runs = {"uniform": [], "learned": [], "learned_below_T0.5": []}
+    acc = {k: [] for k in runs}
+    for seed in seeds:
+        ctx.set_params(pkg.Params.defaults(shell_radius=shell, seed=seed))
+        for name, kw in (("uniform", {}), ("learned", {"learned": True, "t_prop_min": 1.0}),
+                         ("learned_below_T0.5", {"learned": True, "t_prop_min": 1.0, "t_max": 0.5})):
+            traj, st = L.anneal_champions(ctx, s0, agid, n_res, n_steps=PHASE2_STEPS, **kw)
+            runs[name].append(traj)
+            acc[name].append(st["mutation_rotamer_acceptance"])
+    out = {"workload": "4 training antigens x 1024 antibodies (plain-MC tuples, 300 annealed steps), held-out "
+                       "300-residue antigen x 1024 antibodies x 20 residues, 600 annealed Langevin + Metropolis "
+                       "steps, 3 seeds", "tuples": int(n_tuples), "tuple_gen_s": gen_s, "train_steps": train_steps,
+           "train_batch": 8192, "train_s": train_s, "loss_first": float(np.mean(losses[:10])),
+           "loss_last": float(np.mean(losses[-50:])), "time_unit": "ms of Metropolis steps (wall clock)"}
+    for name in ("learned", "learned_below_T0.5"):
+        target, tt_u, tt_l = L.time_to_target(runs["uniform"], runs[name])
+        out["target_champion"] = target
+        out["uniform"] = {"time_to_target_ms": tt_u, "median_ms": float(np.median(tt_u)),
+                          "final_champions": [r[-1][1] for r in runs["uniform"]],
+                          "ms_per_run": float(np.mean([r[-1][0] for r in runs["uniform"]])),
+                          "acceptance": float(np.mean(acc["uniform"]))}
+        out[name] = {"time_to_target_ms": tt_l, "median_ms": float(np.median(tt_l)),
+                     "final_champions": [r[-1][1] for r in runs[name]],
+                     "ms_per_run": float(np.mean([r[-1][0] for r in runs[name]])),
+                     "acceptance": float(np.mean(acc[name])),
+                     "speedup_vs_uniform": float(np.median(tt_u) / np.median(tt_l))}
+    return out
 
 
 def run_phase2_only(args):
@@ -496,6 +548,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal time-to-target runs")
     ap.add_argument("--phase2-only", type=int, default=0, metavar="STEPS",
                     help="profiling case: one launch of STEPS Langevin + Metropolis steps on 64 candidates")
     args = ap.parse_args()

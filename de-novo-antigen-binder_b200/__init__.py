@@ -176,7 +176,7 @@ _SIGS = {
     "binder_mc_log_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "binder_mc_log_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "binder_mlp_take_log": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
-    "binder_set_proposal": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "binder_set_proposal": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float]),
 }
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
@@ -596,6 +596,12 @@ class GpuContext:
         self._check(lib().binder_score_state(self._h, int(full), _ptr(out)))
         return out
 
+    def mc_energy(self):
+        """The Metropolis energy of every candidate (Calpha-level contributions + disulfide)."""
+        out = np.zeros(self._state_cand, np.float64)
+        self._check(lib().binder_score_state(self._h, 2, _ptr(out)))
+        return out
+
     def block(self, n_steps, step0=0, k=64, n_segments=1, out_e=None, out_top=None):
         e = np.zeros(self._state_cand, np.float64) if out_e is None else out_e
         top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
@@ -682,10 +688,11 @@ class GpuContext:
         self._check(lib().binder_mlp_get_tuples(self._h, _ptr(out), len(out), C.byref(n)))
         return out
 
-    def set_proposal(self, learned, t_prop_min=0.3):
-        """Mutation / rotamer proposal of diffuse(): uniform (the reference) or the network."""
+    def set_proposal(self, learned, t_prop_min=0.3, t_max=float("inf")):
+        """Mutation / rotamer proposal of diffuse(): uniform (the reference) or the
+        network (at steps with temperature <= t_max)."""
         self._check(lib().binder_set_proposal(self._h, PROPOSAL_LEARNED if learned else PROPOSAL_UNIFORM,
-                                              t_prop_min))
+                                              t_prop_min, t_max))
 
     def mc_log(self, capacity):
         """Log the mutation / rotamer decisions of the following diffuse() calls (0 stops)."""
@@ -723,3 +730,4 @@ def temperature(iteration, total, t_hot=3.0, t_cold=0.02):
 
 
 from . import workloads  # noqa: E402,F401  (seeded synthetic inputs)
+from . import learned  # noqa: E402,F401  (learned-proposal workflow)

@@ -143,6 +143,7 @@ struct MlpState {
     int adam_t = 0;
     DBuf<float> w, g, m1, m2;
     DBuf<__nv_bfloat16> w1, w2, w2t, w3, w3t;
+    DBuf<uint4> f1, f2, f3;
     int cap = 0;
     DBuf<__nv_bfloat16> X, Xt, H1, H1t, H2, H2t, dY, dYt, dZ2, dZ2t, dZ1t;
     DBuf<float> Z1, Z2, Y, part, feat, ca, target;
@@ -153,13 +154,13 @@ struct MlpState {
     size_t n_tuples = 0;
     // proposal of binder_diffuse's mutation / rotamer moves, and the proposal log
     bool learned = false;
-    float t_prop_min = 0.3f;
+    float t_prop_min = 0.3f, t_max = INFINITY;
     DBuf<MlpTuple> log;
     DBuf<unsigned long long> log_n;
     size_t log_cap = 0;
-    MlpBf16 bf16() { return MlpBf16{w1.p, w2.p, w2t.p, w3.p, w3t.p}; }
+    MlpBf16 bf16() { return MlpBf16{w1.p, w2.p, w2t.p, w3.p, w3t.p, f1.p, f2.p, f3.p}; }
     MlpDev dev() const {
-        return MlpDev{w1.p, w2.p, w3.p, w.p + MLP_OFF_B1, w.p + MLP_OFF_B2, w.p + MLP_OFF_B3, t_prop_min};
+        return MlpDev{f1.p, f2.p, f3.p, w.p + MLP_OFF_B1, w.p + MLP_OFF_B2, w.p + MLP_OFF_B3, t_prop_min, t_max};
     }
 };
 
@@ -1299,6 +1300,11 @@ int persistent_ctas(binder_ctx* ctx) { return ctx->num_sms * ctx->cfg.score_ctas
 int enqueue_score_state(binder_ctx* ctx, int full) {
     State& S = ctx->st;
     CK(ctx->energy.ensure(S.n_cand), "alloc");
+    if (full == 2) {
+        launch_mc_energy(ctx->stream, S.view(), ctx->d_views.p, ctx->energy.p);
+        LAUNCHED("mc_energy");
+        return BINDER_OK;
+    }
     if (!S.order_valid) {
         int s = enqueue_order(ctx);
         if (s) return s;
@@ -1329,6 +1335,7 @@ int binder_score_state(binder_ctx* ctx, int full, double* out) {
     if (s) return s;
     if (ctx->st.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
     if (!out) return fail(ctx, BINDER_ERR_ARG, "NULL out");
+    if (full < 0 || full > 2) return fail(ctx, BINDER_ERR_ARG, "unknown score mode %d", full);
     if ((s = clear_err(ctx))) return s;
     if ((s = enqueue_score_state(ctx, full))) return s;
     return fetch_energies(ctx, ctx->st.n_cand, out, nullptr, nullptr);
@@ -1935,6 +1942,9 @@ int binder_mlp_set_params(binder_ctx* ctx, const float* params) {
     CK(M.w2t.ensure(MLP_H * MLP_H), "mlp alloc");
     CK(M.w3.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
     CK(M.w3t.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
+    CK(M.f1.ensure((MLP_H / 8) * (MLP_K1 / 32) * 32), "mlp alloc");
+    CK(M.f2.ensure((MLP_H / 8) * (MLP_H / 32) * 32), "mlp alloc");
+    CK(M.f3.ensure((MLP_OUT_PAD / 8) * (MLP_H / 32) * 32), "mlp alloc");
     CK(M.loss.ensure(1), "mlp alloc");
     CK(cudaMemcpyAsync(M.w.p, params, MLP_N_PARAMS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "mlp H2D");
     CK(cudaMemsetAsync(M.g.p, 0, MLP_N_PARAMS * sizeof(float), ctx->stream), "mlp memset");
@@ -2119,15 +2129,17 @@ int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float hu
 
 extern "C" {
 
-int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min) {
+int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min, float t_max) {
     int s = enter(ctx);
     if (s) return s;
     if (mode != BINDER_PROPOSAL_UNIFORM && mode != BINDER_PROPOSAL_LEARNED)
         return fail(ctx, BINDER_ERR_ARG, "unknown proposal mode %d", mode);
     if (!(t_prop_min > 0.0f) || !std::isfinite(t_prop_min)) return fail(ctx, BINDER_ERR_ARG, "t_prop_min must be > 0");
+    if (!(t_max > 0.0f)) return fail(ctx, BINDER_ERR_ARG, "t_max must be > 0");
     if (mode == BINDER_PROPOSAL_LEARNED && (s = mlp_check_ready(ctx))) return s;
     ctx->mlp.learned = mode == BINDER_PROPOSAL_LEARNED;
     ctx->mlp.t_prop_min = t_prop_min;
+    ctx->mlp.t_max = t_max;
     return BINDER_OK;
 }
 

@@ -291,23 +291,43 @@ __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* r
     }
 }
 
-// Choice among n options with logits l_k = -y[k] / tp by inverse CDF on u = dz / 2^32
-// (for equal logits exactly urange(dz, n)); returns the index, its log probability
-// in *lq and the log normaliser log sum exp(l) in *lz.
-__device__ int an_sample(const float* y, int n, float tp, uint32_t dz, double* lq, double* lz) {
-    double m = -INFINITY;
-    for (int k = 0; k < n; ++k) m = fmax(m, -(double)y[k] / (double)tp);
-    double sum = 0.0;
-    for (int k = 0; k < n; ++k) sum += exp(-(double)y[k] / (double)tp - m);
-    const double target = (double)dz * (1.0 / 4294967296.0) * sum;
-    double cum = 0.0;
-    int pick = n - 1;
-    for (int k = 0; k < n; ++k) {
-        cum += exp(-(double)y[k] / (double)tp - m);
-        if (target < cum) { pick = k; break; }
-    }
+// Softmax of the logits l_k = -y[k] / tp over k < n (n <= 32) by one warp, lane k
+// holding option k: returns lane k's weight w_k = exp(l_k - m) and, in every lane,
+// the log normaliser lz = m + log(sum w).  The same code evaluates the forward and
+// the reverse proposal, so a reverse probability equals, bit for bit, the forward
+// probability the network would give from the proposed state.
+__device__ __forceinline__ double warp_softmax(const float* y, int n, float tp, double* lz) {
+    const int lane = threadIdx.x & 31;
+    const double l = lane < n ? -(double)y[lane] / (double)tp : -INFINITY;
+    double m = l;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const double w = lane < n ? exp(l - m) : 0.0;
+    double sum = w;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     *lz = m + log(sum);
-    *lq = -(double)y[pick] / (double)tp - *lz;
+    return w;
+}
+
+// Choice among n options by inverse CDF on u = dz / 2^32 over the warp's softmax
+// weights (for equal logits exactly urange(dz, n): the prefix sums are then exact
+// integers).  Returns the option (all lanes) and its log probability in *lq.
+__device__ int warp_sample(const float* y, int n, float tp, uint32_t dz, double* lq) {
+    const int lane = threadIdx.x & 31;
+    double lz;
+    const double w = warp_softmax(y, n, tp, &lz);
+    double cum = w;  // inclusive prefix sum in lane order
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, cum, o);
+        if (lane >= o) cum += v;
+    }
+    const double total = __shfl_sync(0xffffffffu, cum, 31);
+    const double target = (double)dz * (1.0 / 4294967296.0) * total;
+    const unsigned hit = __ballot_sync(0xffffffffu, lane < n && target < cum);
+    const int pick = hit ? __ffs(hit) - 1 : n - 1;
+    *lq = -(double)y[pick] / (double)tp - lz;
     return pick;
 }
 
@@ -442,7 +462,7 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
 // this step and the moves' log Hastings ratios (all threads of the CTA call).
 __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const float4* agq, const uint8_t* ag_aa,
                                                 int nag, const MlpDev& mlp, float temp) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const MlpTile T = mlp_tile_carve((unsigned char*)S.terms);
     const float tp = fmaxf(temp, mlp.t_prop_min);
     if (tid == 0) {  // mutations, and rotamer moves from a known library rotamer
@@ -458,19 +478,23 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
         an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag, false);
         __syncthreads();
         mlp_tile_forward(mlp, T);
-        if (tid < rows) {
-            const int r = S.mvl[base + tid];
-            const float* y = T.y + tid * MT_YS;
-            double lq, lz;
+        for (int i = warp; i < rows; i += AN_WARPS) {  // one warp per row
+            const int r = S.mvl[base + i];
+            const float* y = T.y + i * MT_YS;
+            double lq;
             if (S.kind[r] == MV_ROT) {
-                const int nr = s_rot_n[S.aa[r]];
-                const int k = an_sample(y + N_AA, nr, tp, S.dz[r], &lq, &lz);
-                S.new_rot[r] = k;
-                // same features before and after a rotamer move: the normalisers cancel
-                S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
+                const int k = warp_sample(y + N_AA, s_rot_n[S.aa[r]], tp, S.dz[r], &lq);
+                if (lane == 0) {
+                    S.new_rot[r] = k;
+                    // same features before and after a rotamer move: the normalisers cancel
+                    S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
+                }
             } else {
-                S.new_aa[r] = an_sample(y, N_AA, tp, S.dz[r], &lq, &lz);
-                S.lqf[r] = lq;
+                const int a = warp_sample(y, N_AA, tp, S.dz[r], &lq);
+                if (lane == 0) {
+                    S.new_aa[r] = a;
+                    S.lqf[r] = lq;
+                }
             }
         }
         __syncthreads();
@@ -489,21 +513,21 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
         an_tile_features(S, T, S.mv2, base, rows, agq, ag_aa, nag, true);
         __syncthreads();
         mlp_tile_forward(mlp, T);
-        if (tid < rows) {
-            const int r = S.mv2[base + tid];
-            const float* y = T.y + tid * MT_YS;
-            double m = -INFINITY, sum = 0.0;
-            for (int k = 0; k < N_AA; ++k) m = fmax(m, -(double)y[k] / (double)tp);
-            for (int k = 0; k < N_AA; ++k) sum += exp(-(double)y[k] / (double)tp - m);
-            const double lq_rev = -(double)y[S.aa[r]] / (double)tp - (m + log(sum));
-            S.lhr[r] = lq_rev - S.lqf[r];
+        for (int i = warp; i < rows; i += AN_WARPS) {
+            const int r = S.mv2[base + i];
+            const float* y = T.y + i * MT_YS;
+            double lz;
+            warp_softmax(y, N_AA, tp, &lz);
+            if (lane == 0) S.lhr[r] = (-(double)y[S.aa[r]] / (double)tp - lz) - S.lqf[r];
         }
         __syncthreads();
     }
 }
 
-template <class ACC>
-__global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
+// EXT: the learned proposal and the proposal log are compiled in (a separate
+// instance, so the plain kernel carries none of their registers).
+template <class ACC, bool EXT>
+__global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                        int n_steps, uint32_t step0, int with_noise,
                                                        const float* __restrict__ temps, int R, int G, int C,
                                                        uint32_t* __restrict__ err, long long* __restrict__ stats,
@@ -549,14 +573,16 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
         S.chi[r] = chi;
         S.trig[2 * r] = st.res_trig[2 * (r0 + r)];
         S.trig[2 * r + 1] = st.res_trig[2 * (r0 + r) + 1];
-        // rotamer index of the state: the library entry whose chi it holds, else -1
-        int k = -1;
-        for (int q = 0; q < s_rot_n[a] && k < 0; ++q) {
-            const float4 t = s_rot_chi[a][q];
-            if (t.x == chi.x && t.y == chi.y && t.z == chi.z && t.w == chi.w) k = q;
+        if (EXT) {
+            // rotamer index of the state: the library entry whose chi it holds, else -1
+            int k = -1;
+            for (int q = 0; q < s_rot_n[a] && k < 0; ++q) {
+                const float4 t = s_rot_chi[a][q];
+                if (t.x == chi.x && t.y == chi.y && t.z == chi.z && t.w == chi.w) k = q;
+            }
+            S.rot[r] = k;
+            S.lhr[r] = 0.0;
         }
-        S.rot[r] = k;
-        S.lhr[r] = 0.0;
     }
     long long n_mc = 0, n_mc_acc = 0, n_bb = 0, n_bb_acc = 0;
     __syncthreads();
@@ -676,14 +702,16 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
             }
             S.kind[r] = kind;
             S.u_acc[r] = u01(d.w);
-            S.dz[r] = d.z;
-            S.lhr[r] = 0.0;
+            if (EXT) {
+                S.dz[r] = d.z;
+                S.lhr[r] = 0.0;
+            }
             if (aa == CYS) atomicAdd(&S.iscal[IS_NCYS], 1);
         }
         __syncthreads();
         // learned proposal: the choice of each drawn move comes from the network
         // (same draw d.z, inverse CDF) and the move carries its Hastings ratio
-        if (learned) an_learned_choices(S, n, agq, A.res_aa, nag, mlp, temp);
+        if (EXT && learned && temp <= mlp.t_max) an_learned_choices(S, n, agq, A.res_aa, nag, mlp, temp);
         // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
         // the Calpha energies before / after each move on warps 0..3 (one warp each)
         if (warp >= AN_WARPS / 2) {
@@ -733,11 +761,12 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                                        : (ACC)0;
                 const ACC old_e = (ACC)S.c_old[r] + D;
                 const ACC new_e = (ACC)S.c_new[r] + Dn;
-                const double lhr = S.lhr[r];
-                const bool acc = mh_accept(new_e - old_e, temp, S.u_acc[r], lhr);
+                const double lhr = EXT ? S.lhr[r] : 0.0;
+                const bool acc = EXT ? mh_accept(new_e - old_e, temp, S.u_acc[r], lhr)
+                                     : metropolis(new_e - old_e, temp, S.u_acc[r]);
                 ++n_mc;
                 n_mc_acc += acc;
-                if (tlog) {
+                if (EXT && tlog) {
                     const unsigned long long slot = atomicAdd(log_n, 1ull);
                     if ((long long)slot < log_cap) {
                         const float4 ca = S.pos[r * SLOT_STRIDE + 1];
@@ -756,7 +785,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
                     }
                 }
                 if (acc) {
-                    S.rot[r] = kind == MV_ROT ? S.new_rot[r] : (s_rot_n[na] > 0 ? 0 : -1);
+                    if (EXT) S.rot[r] = kind == MV_ROT ? S.new_rot[r] : (s_rot_n[na] > 0 ? 0 : -1);
                     S.sel[r] = SEL_PROP;
                     S.aa[r] = na;
                     const int rot = S.new_rot[r];
@@ -865,6 +894,56 @@ __global__ void __launch_bounds__(AN_THREADS) k_anneal(StateView st, const AgVie
     }
 }
 
+// The Metropolis energy of every resident candidate, the energy whose changes
+// decide the mutation / rotamer / backbone moves: the sum over its residues of
+// residue_contribution_allatom (diffusion.rs:425-463) plus disulfide_energy
+// (allatom.rs:155-180), f32 terms summed in double in residue order (the default
+// accumulation of k_anneal).  One CTA per candidate, one warp per residue.
+__global__ void __launch_bounds__(AN_THREADS) k_mc_energy(StateView st, const AgView* __restrict__ ags,
+                                                          double* __restrict__ out) {
+    __shared__ float4 s_stage[AN_WARPS * STAGE_CAP];
+    __shared__ double s_e[AN_THREADS];
+    __shared__ double s_total;
+    const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = st.cand_res_off[c], n = st.cand_res_off[c + 1] - r0;
+    const AgView& A = ags[st.cand_ag[c]];
+    if (tid == 0) s_total = 0.0;
+    for (int base = 0; base < n; base += AN_THREADS) {
+        const int m = min(AN_THREADS, n - base);
+        for (int i = warp; i < m; i += AN_WARPS) {
+            const int r = r0 + base + i;
+            const double e = warp_contribution<double>(A.ca_atom, A.ca_atom_prm, A.n_res,
+                                                       f3(st.res_pos[(size_t)r * SLOT_STRIDE + 1]), st.res_aa[r],
+                                                       s_stage + warp * STAGE_CAP);
+            if (lane == 0) s_e[i] = e;
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int i = 0; i < m; ++i) s_total += s_e[i];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double d = 0.0;
+        for (int i = 0; i < n; ++i) {
+            if (st.res_aa[r0 + i] != CYS) continue;
+            const float4 pi = st.res_pos[(size_t)(r0 + i) * SLOT_STRIDE + 5];
+            for (int j = i + 1; j < n; ++j) {
+                if (st.res_aa[r0 + j] != CYS) continue;
+                const float4 pj = st.res_pos[(size_t)(r0 + j) * SLOT_STRIDE + 5];
+                const float dd = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
+                if (dd > 4.0f) continue;
+                const float z = xdiv(xsub(dd, 2.05f), 0.4f);
+                d -= (double)xmul(4.0f, mc_exp(xmul(xmul(-0.5f, z), z)));
+            }
+        }
+        out[c] = s_total + d;
+    }
+}
+
+void launch_mc_energy(cudaStream_t s, const StateView& st, const AgView* ags, double* out) {
+    if (st.n_cand > 0) k_mc_energy<<<st.n_cand, AN_THREADS, 0, s>>>(st, ags, out);
+}
+
 size_t anneal_smem(int max_res, int max_ag_res, int max_cells, int learned) {
     const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
     return anneal_smem_bytes(max_res, G, G && max_cells <= CELL_STAGE_MAX ? max_cells : 0, learned);
@@ -878,19 +957,18 @@ cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags
     const int C = G && max_cells <= CELL_STAGE_MAX ? max_cells : 0;
     const int learned = x.learned ? 1 : 0;
     const size_t smem = anneal_smem_bytes(max_res, G, C, learned);
+    const bool ext = x.learned || x.log;
+    auto run = [&](auto kern) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e) return e;
+        kern<<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G, C, err,
+                                                 stats, x.mlp, learned, x.log, x.log_n, x.log_cap);
+        return cudaSuccess;
+    };
     cudaError_t e;
-    if (accumulate == 1) {
-        if ((e = cudaFuncSetAttribute(k_anneal<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-            return e;
-        k_anneal<float><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G,
-                                                           C, err, stats, x.mlp, learned, x.log, x.log_n, x.log_cap);
-    } else {
-        if ((e = cudaFuncSetAttribute(k_anneal<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-            return e;
-        k_anneal<double><<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res,
-                                                            G, C, err, stats, x.mlp, learned, x.log, x.log_n,
-                                                            x.log_cap);
-    }
+    if (accumulate == 1) e = ext ? run(k_anneal<float, true>) : run(k_anneal<float, false>);
+    else e = ext ? run(k_anneal<double, true>) : run(k_anneal<double, false>);
+    if (e) return e;
     return cudaGetLastError();
 }
 

@@ -391,9 +391,38 @@ __global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g
     w[i] -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
 }
 
-// BF16 copies of the weights: W1 [256][192], W2 [256][256] and W2^T, W3 [32][256] and W3^T
+// 16-byte fragment-order element (t, sp, lane) of W [N][K] at w (FP32 master copy)
+__device__ __forceinline__ uint4 pack_frag(const float* __restrict__ w, int K, int t, int sp, int lane) {
+    const int n = t * 8 + lane / 4, g = 2 * (lane % 4);
+    uint32_t v[4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int k0 = (2 * sp + h) * 16;
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(w[(size_t)n * K + k0 + g], w[(size_t)n * K + k0 + g + 1]);
+        const __nv_bfloat162 hi =
+            __floats2bfloat162_rn(w[(size_t)n * K + k0 + 8 + g], w[(size_t)n * K + k0 + 8 + g + 1]);
+        v[2 * h] = *(const uint32_t*)&lo;
+        v[2 * h + 1] = *(const uint32_t*)&hi;
+    }
+    return make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+// BF16 copies of the weights: W1 [256][192], W2 [256][256] and W2^T, W3 [32][256] and
+// W3^T, and the fragment-order copies of W1, W2, W3
 __global__ void k_pack_weights(const float* __restrict__ p, MlpBf16 o) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (MLP_H / 8) * (MLP_K1 / 32) * 32) {
+        const int lane = t % 32, sp = (t / 32) % (MLP_K1 / 32), nt = t / (32 * (MLP_K1 / 32));
+        o.f1[t] = pack_frag(p + MLP_OFF_W1, MLP_K1, nt, sp, lane);
+    }
+    if (t < (MLP_H / 8) * (MLP_H / 32) * 32) {
+        const int lane = t % 32, sp = (t / 32) % (MLP_H / 32), nt = t / (32 * (MLP_H / 32));
+        o.f2[t] = pack_frag(p + MLP_OFF_W2, MLP_H, nt, sp, lane);
+    }
+    if (t < (MLP_OUT_PAD / 8) * (MLP_H / 32) * 32) {
+        const int lane = t % 32, sp = (t / 32) % (MLP_H / 32), nt = t / (32 * (MLP_H / 32));
+        o.f3[t] = pack_frag(p + MLP_OFF_W3, MLP_H, nt, sp, lane);
+    }
     if (t < MLP_H * MLP_K1) o.w1[t] = __float2bfloat16_rn(p[MLP_OFF_W1 + t]);
     if (t < MLP_H * MLP_H) {
         const int n = t / MLP_H, k = t % MLP_H;

@@ -93,6 +93,8 @@ void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView*
 constexpr int ANNEAL_MAX_RES = 128;  // residues per candidate held in shared memory
 cudaError_t anneal_init_tables();
 cudaError_t anneal_init_mlp_table(const float* log1p_table);
+// Metropolis energy (Calpha-level contributions + disulfide) of every candidate
+void launch_mc_energy(cudaStream_t s, const StateView& st, const AgView* ags, double* out);
 size_t anneal_smem(int max_res, int max_ag_res, int max_cells, int learned);
 // The learned proposal (mlp, used when learned) and the proposal log (log may be
 // null: every mutation / rotamer decision appends one tuple while *log_n < log_cap;

@@ -80,13 +80,25 @@ struct GemmArgs {
     GemmEpi e;
 };
 
-// BF16 weight copies used by the GEMMs
+// Fragment order of a BF16 weight matrix W [N][K] for the warp-level MMA
+// (m16n8k16, B operand "col"): element (t, sp, l) (t = n-tile of 8 outputs, sp =
+// pair of 16-wide k-steps, l = lane) is 16 bytes holding, for the k-steps s = 2 sp
+// and 2 sp + 1 (k0 = 16 s), n = 8 t + l / 4, g = 2 (l % 4):
+// {W[n][k0+g], W[n][k0+g+1], W[n][k0+8+g], W[n][k0+8+g+1]} of s = 2 sp, then of
+// s = 2 sp + 1 -- the lane's b0, b1 registers of both k-steps in one 16-byte load,
+// a warp's loads 512 contiguous bytes.
+__host__ __device__ constexpr int frag_index(int t, int sp, int lane, int K) { return (t * (K / 32) + sp) * 32 + lane; }
+
+// BF16 weight copies used by the GEMMs and the Metropolis kernel's network tile
 struct MlpBf16 {
     __nv_bfloat16* w1;   // [256][192]
     __nv_bfloat16* w2;   // [256][256]
     __nv_bfloat16* w2t;  // [256][256] transposed
     __nv_bfloat16* w3;   // [32][256]
     __nv_bfloat16* w3t;  // [256][32] transposed
+    uint4* f1;           // W1 in fragment order (32 x 6 x 32)
+    uint4* f2;           // W2 in fragment order (32 x 8 x 32)
+    uint4* f3;           // W3 in fragment order (4 x 8 x 32)
 };
 
 // One logged Metropolis proposal (binder_mc_tuple of the C ABI, 32 bytes).
@@ -100,15 +112,17 @@ struct MlpTuple {
     uint8_t pad[2];
 };
 
-// The network as the Metropolis kernel sees it (BF16 weights, FP32 biases).
+// The network as the Metropolis kernel sees it (BF16 weights in fragment order,
+// FP32 biases).
 struct MlpDev {
-    const __nv_bfloat16* w1;  // [256][192]
-    const __nv_bfloat16* w2;  // [256][256]
-    const __nv_bfloat16* w3;  // [32][256]
+    const uint4* f1;
+    const uint4* f2;
+    const uint4* f3;
     const float* b1;
     const float* b2;
     const float* b3;
     float t_prop_min;         // proposal temperature = max(T, t_prop_min)
+    float t_max;              // steps at temperatures above t_max use the uniform proposal
 };
 static_assert(sizeof(MlpTuple) == 32, "tuple layout");
 

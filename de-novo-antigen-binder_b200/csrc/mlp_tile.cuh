@@ -2,8 +2,9 @@
 // tile of at most 16 residues (the residues of one candidate that drew a move in
 // a step: a handful of rows, below the 64/128-row tiles of tcgen05.mma, so the
 // CTA's eight warps use the warp-level BF16 MMA, m16n8k16 with FP32 accumulators).
-// Weights are read from global memory (L2-resident, 240 KB); activations stay in
-// shared memory as BF16, the output as FP32.  Same arithmetic as the batched
+// Weights are read from global memory (L2-resident, 240 KB) in fragment order with
+// 16-byte loads, double-buffered in registers; activations stay in shared memory as
+// BF16, the output as FP32.  Same arithmetic as the batched
 // tensor-core path up to the order of the FP32 sums.
 #pragma once
 
@@ -50,32 +51,56 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 }
 
 __device__ __forceinline__ uint32_t ld_s32(const __nv_bfloat16* p) { return *(const uint32_t*)p; }
-__device__ __forceinline__ uint32_t ld_g32(const __nv_bfloat16* p) { return __ldg((const unsigned int*)p); }
+__device__ __forceinline__ uint4 ld_g128(const uint4* p) { return __ldg(p); }
 __device__ __forceinline__ float silu_f(float z) { return z / (1.0f + expf(-z)); }
 
-// One dense layer on the tile: out[16][n_tiles*8 per warp] = act(in[16][K] W^T + b).
-// Warp w computes the n-tiles w*NT .. w*NT+NT-1 (8 columns each); ACT = SiLU to BF16
-// (out_h) or identity to FP32 (out_f).
+// One dense layer on the tile: out[16][cols of the warp] = act(in[16][K] W^T + b).
+// Warp w computes the n-tiles n_tile0 .. n_tile0+NT-1 (8 columns each); ACT = SiLU to
+// BF16 (out_h) or identity to FP32 (out_f).  The warp's weights (fragment order,
+// 16 bytes per lane per pair of k-steps) stream through registers in batches of
+// two pairs, the next batch in flight while the current one is multiplied.
 template <int K, int NT, bool ACT>
-__device__ __forceinline__ void mlp_tile_layer(const __nv_bfloat16* in, int in_stride, const __nv_bfloat16* W,
+__device__ __forceinline__ void mlp_tile_layer(const __nv_bfloat16* in, int in_stride, const uint4* Wf,
                                                const float* bias, __nv_bfloat16* out_h, int out_stride,
                                                float* out_f, int n_tile0) {
+    constexpr int SP = K / 32;   // pairs of k-steps
+    constexpr int PB = 2;        // pairs per batch
+    constexpr int NB = SP / PB;  // batches
+    static_assert(SP % PB == 0, "K must be a multiple of 64");
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
     float acc[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0f;
-#pragma unroll 4
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        uint32_t a[4];
-        a[0] = ld_s32(in + g * in_stride + k0 + 2 * tg);
-        a[1] = ld_s32(in + (g + 8) * in_stride + k0 + 2 * tg);
-        a[2] = ld_s32(in + g * in_stride + k0 + 8 + 2 * tg);
-        a[3] = ld_s32(in + (g + 8) * in_stride + k0 + 8 + 2 * tg);
+    uint4 buf[2][PB][NT];
 #pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const __nv_bfloat16* wr = W + (size_t)((n_tile0 + t) * 8 + g) * K + k0 + 2 * tg;
-            mma_bf16_16816(acc[t], a, ld_g32(wr), ld_g32(wr + 8));
+    for (int p = 0; p < PB; ++p)
+#pragma unroll
+        for (int t = 0; t < NT; ++t) buf[0][p][t] = ld_g128(Wf + frag_index(n_tile0 + t, p, lane, K));
+#pragma unroll
+    for (int bi = 0; bi < NB; ++bi) {
+        if (bi + 1 < NB) {
+#pragma unroll
+            for (int p = 0; p < PB; ++p)
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                    buf[(bi + 1) & 1][p][t] = ld_g128(Wf + frag_index(n_tile0 + t, (bi + 1) * PB + p, lane, K));
         }
+#pragma unroll
+        for (int p = 0; p < PB; ++p)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k0 = ((bi * PB + p) * 2 + h) * 16;
+                uint32_t a[4];
+                a[0] = ld_s32(in + g * in_stride + k0 + 2 * tg);
+                a[1] = ld_s32(in + (g + 8) * in_stride + k0 + 2 * tg);
+                a[2] = ld_s32(in + g * in_stride + k0 + 8 + 2 * tg);
+                a[3] = ld_s32(in + (g + 8) * in_stride + k0 + 8 + 2 * tg);
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    const uint4 v = buf[bi & 1][p][t];
+                    mma_bf16_16816(acc[t], a, h ? v.z : v.x, h ? v.w : v.y);
+                }
+            }
     }
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
@@ -99,11 +124,11 @@ __device__ __forceinline__ void mlp_tile_layer(const __nv_bfloat16* in, int in_s
 // (all threads call; barriers inside).
 __device__ __forceinline__ void mlp_tile_forward(const MlpDev& M, const MlpTile& T) {
     const int warp = threadIdx.x >> 5;
-    mlp_tile_layer<MLP_K1, 4, true>(T.x, MT_XS, M.w1, M.b1, T.h1, MT_HS, nullptr, warp * 4);
+    mlp_tile_layer<MLP_K1, 4, true>(T.x, MT_XS, M.f1, M.b1, T.h1, MT_HS, nullptr, warp * 4);
     __syncthreads();
-    mlp_tile_layer<MLP_H, 4, true>(T.h1, MT_HS, M.w2, M.b2, T.h2, MT_HS, nullptr, warp * 4);
+    mlp_tile_layer<MLP_H, 4, true>(T.h1, MT_HS, M.f2, M.b2, T.h2, MT_HS, nullptr, warp * 4);
     __syncthreads();
-    if (warp < MLP_OUT_PAD / 8) mlp_tile_layer<MLP_H, 1, false>(T.h2, MT_HS, M.w3, M.b3, nullptr, 0, T.y, warp);
+    if (warp < MLP_OUT_PAD / 8) mlp_tile_layer<MLP_H, 1, false>(T.h2, MT_HS, M.f3, M.b3, nullptr, 0, T.y, warp);
     __syncthreads();
 }
 

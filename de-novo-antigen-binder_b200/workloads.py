@@ -15,6 +15,10 @@ allatom.rs:523-541) or by the CPU oracle in tests.  Seeds: 0xB200 + config id.
   config 3  config-1 antigen + 1024 frozen all-atom poses whose atoms sit at
             log-uniform 2.5-12 A from random antigen atoms; 30 % of residues
             charged (K, R, D, E).
+  config 4  learned proposal: training antigens (300-residue globules built as
+            in config 1 from their own seeds) with 1024 x 20-residue antibodies
+            each, and held-out 300-residue antigens of other seeds with 1024 x 20
+            antibodies for the evaluation.
 """
 from __future__ import annotations
 
@@ -187,3 +191,20 @@ def config3_poses(ag_cloud_xyz, tables, n_cand=1024, n_res=20, charged_frac=0.3)
     off = np.concatenate([[0], np.cumsum(per_cand)]).astype(np.int64)
     return g, off, aa
 
+
+
+def _config1_like(rng, n_cand, n_res):
+    ag_aa, ag_ca, radius = _globule_antigen(300, rng)
+    shell = radius + 4.0
+    c = ca_center(ag_ca)
+    ca = sphere_points(n_cand * n_res, shell, c, rng)
+    aa = random_sequence(n_cand * n_res, rng)
+    return (ag_aa, ag_ca), shell, Population(ca, aa, np.full(n_cand, n_res, np.int32), np.zeros(n_cand, np.int32))
+
+
+def config4(n_train=4, n_eval=2, n_cand=1024, n_res=20):
+    """Training antigens (seeds 1..n_train) and held-out antigens (seeds 1001..),
+    each a config-1-style 300-residue globule with its own population."""
+    train = [_config1_like(rng_for(4, salt=s), n_cand, n_res) for s in range(1, n_train + 1)]
+    held = [_config1_like(rng_for(4, salt=1000 + s), n_cand, n_res) for s in range(1, n_eval + 1)]
+    return dict(name="config4", train=train, eval=held)

@@ -265,8 +265,11 @@ int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n);
    last binder_state_upload (orig_idx int32[n_cand], may be NULL). */
 int binder_state_info(binder_ctx* ctx, int32_t* n_cand, int32_t* total_res, int32_t* orig_idx);
 /* Score every resident candidate against its antigen: LJ + Coulomb + hydrophobic
-   (full = 0) or allatom_energy (diffusion.rs:281-283: + H-bond + EEF1 +
-   disulfide, full = 1).  out = double[n_cand] (host). */
+   (full = 0), allatom_energy (diffusion.rs:281-283: + H-bond + EEF1 +
+   disulfide, full = 1), or the Metropolis energy whose changes decide the moves
+   (full = 2: the sum over residues of residue_contribution_allatom,
+   diffusion.rs:425-463, plus disulfide_energy, f32 terms summed in double).
+   out = double[n_cand] (host). */
 int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
 /* The phase-1 block: n_steps gradient-only steps, one score of every candidate,
    then the k lowest per antigen (diffusion.rs:1018-1057 with scoring every
@@ -383,10 +386,12 @@ int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n);
    exactly as UNIFORM does), accepted with probability min(1, exp(-dE/T) q(reverse)
    / q(move)), the reverse probability of a mutation evaluated by the network at
    the proposed amino acid.  Rotamer moves from a chi that is no library rotamer
-   stay uniform. */
+   stay uniform, and so do all moves of steps whose temperature is above t_max
+   (INFINITY: none) -- each step is a Metropolis-Hastings step at its temperature
+   either way. */
 #define BINDER_PROPOSAL_UNIFORM 0
 #define BINDER_PROPOSAL_LEARNED 1
-int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min);
+int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min, float t_max);
 /* n_steps Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on minibatches of `batch`
    tuples drawn uniformly (Philox, key seed) from the training set; out_losses
    double[n_steps] (may be NULL) = each step's mean Huber loss. */
