@@ -463,6 +463,7 @@ def run_ours(args, rank, world, local_rank):
         cpu_run_s = n_cand * PHASE1_STEPS / (n * nb * N_STEPS_PER_BLOCK / dt) + TOP_K * PHASE2_STEPS / cpu_p2
         line["run_allatom"]["cpu_estimate_ms"] = 1e3 * cpu_run_s
     if rank == 0 and world == 1 and not args.no_learned:
+        line["batched_uneven"] = run_batched(pkg, ctx, torch, ext)
         line["learned_proposal"] = run_learned(pkg, ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -470,6 +471,46 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_batched(pkg, ctx, torch, ext):
+    """The batched uneven workload: 8 antigens of 50..800 residues resident
+    together, 4096 antibodies of 10..30 residues assigned round-robin, one phase-1
+    pass (20 blocks of 10 gradient steps + score + per-antigen top-64, CUDA graph,
+    autotuned launch shapes), device time per block."""
+    cfg = pkg.workloads.config2()
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=26.0))
+    pop = cfg["pop"]
+    # the restraint radius is per context: the antigens' shells differ, so each
+    # candidate keeps the radius of the config-1 globule (26 A); the grid, scoring
+    # and top-k are per antigen
+    for ag_aa, ag_ca in cfg["antigens"]:
+        pos_a, _ = ctx.build_residues(ag_ca, ag_aa)
+        ctx.add_antigen(ag_aa, pos_a)
+    pos, chi = ctx.build_residues(pop.ca, pop.aa)
+    ctx.state_upload(pop.aa, chi, pos, n_res=pop.n_res, antigen_id=pop.antigen_id)
+    tuned = ctx.autotune(reps=3).as_dict()
+    n_seg = len(cfg["antigens"])
+    times = []
+    for p in range(2):  # pass 0 warms up (graph capture), pass 1 is timed
+        ctx.state_upload(pop.aa, chi, pos, n_res=pop.n_res, antigen_id=pop.antigen_id)
+        for b in range(PHASE1_BLOCKS):
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ext)
+            ctx.block_async(N_STEPS_PER_BLOCK, b * N_STEPS_PER_BLOCK, TOP_K)
+            e.record(ext)
+            if p:
+                times.append((a, e))
+        e_last, top = ctx.block_fetch(TOP_K, n_segments=n_seg)
+    ms = [a.elapsed_time(e) for a, e in times]
+    mean_ms = float(np.mean(ms))
+    return {"workload": "8 globules of 50..800 residues resident together, 4096 antibodies of 10..30 residues "
+                        "(round-robin), one phase-1 pass: 20 x (10 gradient steps + all-atom score + top-64 per "
+                        "antigen), CUDA graph", "candidates": int(pop.n_cand), "residues": int(pop.n_res.sum()),
+            "ms_per_block": mean_ms, "candidate_steps_per_s": pop.n_cand * N_STEPS_PER_BLOCK / (mean_ms * 1e-3),
+            "launch": tuned, "survivors_per_antigen": [int((t >= 0).sum()) for t in top],
+            "best_energy_per_antigen": [float(e_last[t[0]]) for t in top]}
 
 
 def run_learned(pkg, ctx, seeds=(21, 22, 23), n_res=20):
@@ -522,6 +563,45 @@ def run_learned(pkg, ctx, seeds=(21, 22, 23), n_res=20):
     return out
 
 
+def run_block_only(args):
+    """Small profiling case for the search block: 3 eagerly issued blocks of the
+    bench workload at launch shape (cg_warps, cg_lanes)."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(0)
+    ctx.set_params(pkg.Params.defaults(flags=0))
+    cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, 0)
+    w, lanes = (int(x) for x in args.block_only.split(","))
+    ctx.set_launch_cfg(8, 4, w, lanes)
+    ctx.state_upload(pop.aa, chi, pos, uniform_n_res=int(pop.n_res[0]))
+    for k in range(3):
+        ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K)
+    torch.cuda.synchronize()
+    print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "blocks": 3}}), flush=True)
+    ctx.close()
+    return 0
+
+
+def run_mlp_only(args):
+    """Small profiling case for the proposal network's tensor-core GEMMs: 3 loss +
+    gradient passes on `rows` random feature rows."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(0)
+    rng = np.random.default_rng(0)
+    n = args.mlp_only
+    f = np.zeros((n, pkg.MLP_IN), np.float32)
+    f[np.arange(n), rng.integers(0, 20, n)] = 1.0
+    f[:, 20:] = np.log1p(rng.poisson(0.6, (n, pkg.MLP_IN - 20))).astype(np.float32)
+    ctx.mlp_set_params(pkg.mlp_init_params(0))
+    for _ in range(3):
+        loss, _ = ctx.mlp_loss_grad(f, rng.integers(0, 25, n).astype(np.int32), rng.normal(size=n).astype(np.float32))
+    print(json.dumps({"mlp_only": {"rows": n, "loss": loss}}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_phase2_only(args):
     """Small profiling case for the Metropolis kernel (one GPU, one launch timed)."""
     import torch
@@ -551,6 +631,10 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal time-to-target runs")
     ap.add_argument("--phase2-only", type=int, default=0, metavar="STEPS",
                     help="profiling case: one launch of STEPS Langevin + Metropolis steps on 64 candidates")
+    ap.add_argument("--block-only", default="", metavar="WARPS,LANES",
+                    help="profiling case: 3 search blocks at this gradient-step launch shape")
+    ap.add_argument("--mlp-only", type=int, default=0, metavar="ROWS",
+                    help="profiling case: 3 loss + gradient passes of the proposal network on ROWS rows")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -561,6 +645,10 @@ def main():
         return run_reference(args, rank, world)
     if args.phase2_only:
         return run_phase2_only(args)
+    if args.block_only:
+        return run_block_only(args)
+    if args.mlp_only:
+        return run_mlp_only(args)
     return run_ours(args, rank, world, local_rank)
 
 
