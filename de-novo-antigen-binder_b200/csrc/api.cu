@@ -112,6 +112,11 @@ struct State {
     DBuf<int> key_base, keys, key_counts, key_cursor, order;
     int n_keys = 0;
     bool order_valid = false;
+    // the gradient-step kernel's Verlet lists (csrc/k_search.cu), valid per residue
+    DBuf<int> cg_list;
+    DBuf<float4> cg_centre;
+    DBuf<int4> cg_meta;
+    const int* ag_epoch = nullptr;  // the context's device epoch word
     // scoring work queue and per-residue energies
     DBuf<int> queue;
     DBuf<double> res_e, res_abs;
@@ -127,6 +132,10 @@ struct State {
         v.res_pos = res_pos.p;
         v.res_trig = res_trig.p;
         v.res_cand = res_cand.p;
+        v.cg_list = cg_list.p;
+        v.cg_centre = cg_centre.p;
+        v.cg_meta = cg_meta.p;
+        v.ag_epoch = ag_epoch;
         return v;
     }
 };
@@ -212,6 +221,9 @@ struct binder_ctx {
     int block_graph_launches = 0;
     std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
     MlpState mlp;
+    // antigen-set epoch (device word read by the gradient-step kernel)
+    DBuf<int> d_ag_epoch;
+    int ag_epoch = 0;
     void drop_graph() {
         if (block_graph) cudaGraphExecDestroy(block_graph);
         block_graph = nullptr;
@@ -298,6 +310,16 @@ template <class T>
 int upload(binder_ctx* ctx, DBuf<T>& d, const T* h, size_t n, const char* what) {
     CK(d.ensure(n), what);
     if (n) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream), what);
+    return BINDER_OK;
+}
+
+// New antigen set: every stored Verlet list of the gradient-step kernel is stale.
+int bump_antigen_epoch(binder_ctx* ctx) {
+    CK(ctx->d_ag_epoch.ensure(1), "alloc");
+    ++ctx->ag_epoch;
+    CK(cudaMemcpyAsync(ctx->d_ag_epoch.p, &ctx->ag_epoch, sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+       "epoch H2D");
+    ctx->st.ag_epoch = ctx->d_ag_epoch.p;
     return BINDER_OK;
 }
 
@@ -976,6 +998,7 @@ int binder_add_antigen(binder_ctx* ctx, size_t n_res, const uint8_t* aa, const f
     A->view.cy = sy / nf;
     A->view.cz = sz / nf;
     ctx->ags.push_back(std::move(A));
+    if ((s = bump_antigen_epoch(ctx))) return s;
     std::vector<AgView> views;
     refresh_views(ctx, views);
     CK(ctx->d_views.ensure(views.size()), "alloc");
@@ -993,7 +1016,7 @@ int binder_clear_antigens(binder_ctx* ctx) {
     ctx->ags.clear();
     ctx->st.n_cand = 0;
     ctx->st.total_res = 0;
-    return BINDER_OK;
+    return bump_antigen_epoch(ctx);
 }
 
 }  // extern "C"
@@ -1115,6 +1138,12 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
     if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
     CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
+    if (S.cg_meta.n < (size_t)total || !S.cg_meta.p) {  // fresh list storage: every list invalid
+        CK(S.cg_list.ensure((size_t)total * CG_LIST_CAP), "alloc");
+        CK(S.cg_centre.ensure(total), "alloc");
+        CK(S.cg_meta.ensure(total), "alloc");
+        CK(cudaMemsetAsync(S.cg_meta.p, 0xFF, S.cg_meta.n * sizeof(int4), ctx->stream), "memset");
+    }
     launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
     if (total) LAUNCHED("pack_slots");
     CK(S.mc_stats.ensure(4 * n_cand), "alloc");
@@ -1284,8 +1313,15 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     }
     int s = enqueue_order(ctx);
     if (s) return s;
+    int max_ag = 0, max_cells = 0;
+    for (const auto& a : ctx->ags) {
+        const GridView& gv = a->view.ca_grid;
+        max_ag = std::max(max_ag, a->n_res);
+        max_cells = std::max(max_cells, gv.nx * gv.ny * gv.nz);
+    }
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
-                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes);
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
+                   max_ag, max_cells);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }

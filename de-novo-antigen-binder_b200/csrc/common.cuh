@@ -36,6 +36,9 @@ constexpr float CA_C_BOND = 1.52f;
 constexpr float C_O_BOND = 1.23f;
 constexpr float CA_CB_BOND = 1.52f;
 
+// entries of a residue's Verlet list in the gradient-step kernel (k_search.cu)
+constexpr int CG_LIST_CAP = 128;
+
 // residue sort keys cover the antigen's Calpha-grid box widened by this many cells
 constexpr int RES_KEY_MARGIN = 3;
 
@@ -145,6 +148,11 @@ struct StateView {
     float4* res_trig;         // 2 * total_res: sin/cos of chi1, chi2 | chi3, chi4
     float4* res_pos;          // total_res * SLOT_STRIDE
     const int* res_cand;      // total_res
+    // Verlet lists of the gradient-step kernel kept between launches
+    int* cg_list;             // total_res * CG list capacity: sorted antigen Calpha positions
+    float4* cg_centre;        // total_res: list centre
+    int4* cg_meta;            // total_res: {length, antigen, antigen-set epoch, 0}
+    const int* ag_epoch;      // device word: the antigen-set epoch (bumped when antigens change)
 };
 
 // spatial.rs:61-67: (x * inv).floor() as i32 — one f32 multiply, floor, saturating cast

@@ -81,7 +81,7 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 // walk (same sum).  The residue's atoms live in registers, atom k on lane k % G, and
 // take every step's translation as set_ca_pos does (allatom.rs:279-293).
 // COUNT: count the in-cutoff pairs of the same trajectory, leave the state as is.
-constexpr int CG_LIST_MAX = 64;
+constexpr int CG_LIST_MAX = CG_LIST_CAP;
 constexpr float CG_SKIN = 2.0f;  // list radius = 10 A cutoff + skin
 
 // The one-lane walk over all 27 cells, out of line: it is rarely taken and must
@@ -162,97 +162,218 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
     return total;
 }
 
-// resident warps per SM the register budget is set for: about one wave of the
-// benchmark's 20480 residues (4 lanes: 17 warps per SM, 8 lanes: 35)
-template <int G>
-constexpr int cg_warps_per_sm() { return G == 8 ? 36 : 20; }
+constexpr int CG_IN_MAX = 48;  // in-cutoff list entries a residue holds per step
 
+// register budget: 24 resident warps per SM (80 registers a thread)
+// Dynamic shared memory of the antigen staging: Calphas (pq, prm, cell) and the
+// grid's cell starts of an antigen with n Calphas and ncell cells.
+__host__ __device__ inline size_t cg_stage_bytes(int n, int ncell) {
+    return (size_t)n * 48 + ((size_t)(ncell + 1) * 4 + 15) / 16 * 16;
+}
+
+// The antigen Calphas a CTA's residues probe (their pq / prm / cell arrays and the
+// CG grid's cell starts) are copied to shared memory at the start of the launch
+// when every residue of the CTA belongs to one antigen that fits the dynamic
+// shared memory the launch reserved (residues are ordered by antigen, then cell);
+// otherwise the kernel reads them from global memory.  Same values either way.
 template <bool COUNT, int CG_WARPS, int G>
-__global__ void __launch_bounds__(CG_WARPS * 32, cg_warps_per_sm<G>() / CG_WARPS) k_langevin(StateView st, const AgView* __restrict__ ags,
+__global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(StateView st, const AgView* __restrict__ ags,
                                                              StepParams p, int n_steps, uint32_t step0,
                                                              int with_noise, const float* __restrict__ temps,
                                                              uint32_t* __restrict__ err,
                                                              long long* __restrict__ pair_count,
-                                                             const int* __restrict__ order) {
+                                                             const int* __restrict__ order, int stage_cap) {
     constexpr int RPC = CG_WARPS * 32 / G;  // residues per CTA
-    constexpr int NA = (SLOTS + G - 1) / G;  // atoms per lane
+    constexpr int NG = 32 / G;              // residues (lane groups) per warp
+    constexpr int NA = (SLOTS + G - 1) / G; // atoms per lane
     static_assert(RPC <= 32, "list storage is sized for 32 residues per CTA");
     __shared__ int s_list[RPC][CG_LIST_MAX];
-    __shared__ float4 s_term[RPC][CG_LIST_MAX];
+    __shared__ int s_in[RPC][CG_IN_MAX];
+    __shared__ float3 s_term[RPC][CG_IN_MAX];
     const int lane = threadIdx.x & 31;
     const int gl = lane & (G - 1);
     const int gshift = lane & ~(G - 1);
     const unsigned gmask = ((1u << G) - 1u) << gshift;
+    const int rl = threadIdx.x / G;                  // this group's residue slot in the CTA
+    const int rl0 = (threadIdx.x & ~31) / G;         // the warp's first residue slot
     const int slot_id = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-    if (slot_id >= st.total_res) return;  // the whole group leaves together
-    const int rl = threadIdx.x / G;
+    // every lane of a warp stays to the end: the pair evaluation is warp-wide
+    const bool valid = slot_id < st.total_res;
     int* list = s_list[rl];
-    float4* terms = s_term[rl];
-    const int r = order ? order[slot_id] : slot_id;
-    const int c = st.res_cand[r];
-    const int r_local = r - st.cand_res_off[c];
-    const uint32_t cid = st.cand_id[c];
-    const AgView* __restrict__ Ap = ags + st.cand_ag[c];
-    const GridView g = Ap->ca_grid;
+    int* in = s_in[rl];
+    float3* terms = s_term[rl];
+    const int r = valid ? (order ? order[slot_id] : slot_id) : 0;
+    const int c = valid ? st.res_cand[r] : 0;
+    const int r_local = valid ? r - st.cand_res_off[c] : 0;
+    const uint32_t cid = valid ? st.cand_id[c] : 0u;
+    const AgView* __restrict__ Ap = ags + (valid ? st.cand_ag[c] : 0);
+    GridView g = Ap->ca_grid;
     const float4* __restrict__ ca_pq = Ap->ca_pq;
     const float4* __restrict__ ca_prm = Ap->ca_prm;
     const int4* __restrict__ ca_cell = Ap->ca_cell;
     const float ag_cx = Ap->cx, ag_cy = Ap->cy, ag_cz = Ap->cz;
-    const int aa = st.res_aa[r];
-    const int n_at = s_topo_n[aa];
+    {
+        // stage the antigen when the CTA's first and last residues share it
+        extern __shared__ __align__(16) unsigned char cg_dyn[];
+        __shared__ int s_stage_ag;
+        const int first = blockIdx.x * (CG_WARPS * 32 / G);
+        const int last = min(first + CG_WARPS * 32 / G, st.total_res) - 1;
+        if (threadIdx.x == 0) {
+            const int ra = order ? order[first] : first, rb = order ? order[last] : last;
+            const int a0 = st.cand_ag[st.res_cand[ra]], a1 = st.cand_ag[st.res_cand[rb]];
+            const GridView& gv = ags[a0].ca_grid;
+            const bool fits = a0 == a1 &&
+                              cg_stage_bytes(ags[a0].n_res, gv.nx * gv.ny * gv.nz) <= (size_t)stage_cap;
+            s_stage_ag = fits ? a0 : -1;
+        }
+        __syncthreads();
+        const int sa = s_stage_ag;
+        if (sa >= 0) {
+            const AgView& S = ags[sa];
+            const int n = S.n_res, ncell = S.ca_grid.nx * S.ca_grid.ny * S.ca_grid.nz;
+            float4* spq = (float4*)cg_dyn;
+            float4* sprm = spq + n;
+            int4* scell = (int4*)(sprm + n);
+            int* sstart = (int*)(scell + n);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                spq[i] = S.ca_pq[i];
+                sprm[i] = S.ca_prm[i];
+                scell[i] = S.ca_cell[i];
+            }
+            for (int i = threadIdx.x; i <= ncell; i += blockDim.x) sstart[i] = S.ca_grid.cell_start[i];
+            __syncthreads();
+            if (valid) {  // every valid residue of the CTA probes antigen sa
+                ca_pq = spq;
+                ca_prm = sprm;
+                ca_cell = scell;
+                g.cell_start = sstart;
+            }
+        }
+    }
+    const int aa = valid ? st.res_aa[r] : 0;
+    const int n_at = valid ? s_topo_n[aa] : 0;
     const float4 res = s_res[aa];
     float4* slot = st.res_pos + (size_t)r * SLOT_STRIDE;
-    const float4 v1 = slot[1];  // Calpha = topology atom 1 of every residue (amber.rs:358-377)
-    F3 ca = {v1.x, v1.y, v1.z};
-    if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
+    F3 ca = {0.f, 0.f, 0.f};
+    if (valid) {
+        const float4 v1 = slot[1];  // Calpha = topology atom 1 of every residue (amber.rs:358-377)
+        ca = {v1.x, v1.y, v1.z};
+        if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
+    }
     float4 at[NA];
 #pragma unroll
     for (int j = 0; j < NA; ++j) {
         const int k = gl + G * j;
         at[j] = (!COUNT && k < n_at) ? slot[k] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    F3 centre = ca;
-    int nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+    // the residue's list from the previous launch when it was built for this antigen
+    // set and antigen and still covers the Calpha, else a new one
     const float skin2 = (CG_SKIN - 0.01f) * (CG_SKIN - 0.01f);
+    F3 centre = ca;
+    int nl = 0;
+    bool dirty = false;
+    if (valid) {
+        const int ep = st.ag_epoch ? *st.ag_epoch : -2;
+        const int4 meta = st.cg_meta ? st.cg_meta[r] : make_int4(-1, -1, -1, -1);
+        bool reuse = false;
+        float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ep >= 0 && meta.z == ep && meta.y == st.cand_ag[c] && meta.x >= 0 && meta.x <= CG_LIST_MAX) {
+            cc = st.cg_centre[r];
+            const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
+            reuse = mx * mx + my * my + mz * mz <= skin2;
+        }
+        if (reuse) {
+            centre = {cc.x, cc.y, cc.z};
+            nl = meta.x;
+            for (int j = gl; j < nl; j += G) list[j] = st.cg_list[(size_t)r * CG_LIST_MAX + j];
+            __syncwarp(gmask);
+        } else {
+            nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+            dirty = true;
+        }
+    }
     int n_pairs = 0;
     for (int s = 0; s < n_steps; ++s) {
         const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
+        bool use_list = valid && nl <= CG_LIST_MAX && !cell_far(cx, cy, cz);
+        // A-C in rounds: each round a group compacts its next in-cutoff list entries
+        // (adjacent cell, r^2 passing the reference's cutoff test; list order) up to
+        // CG_IN_MAX, the warp evaluates every group's compacted pairs one pair per lane,
+        // and lane 0 of each group continues its sum in order -- the reference's sum,
+        // however many rounds a residue needs.
         float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        if (nl <= CG_LIST_MAX && !cell_far(cx, cy, cz)) {
-            const CgB body{ca.x, ca.y, ca.z, res.x, res.y, res.z, res.w};
-            for (int j = gl; j < nl; j += G) {
-                const int i = list[j];
-                const int4 ce = ca_cell[i];
-                float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
-                    abs((long long)ce.z - cz) <= 1 && cg_term_parts(body, ca_pq[i], ca_prm[i], t.x, t.y, t.z))
-                    t.w = 1.0f;
-                terms[j] = t;
-            }
-            __syncwarp(gmask);
-            if (gl == 0) {
-                for (int j = 0; j < nl; ++j) {
-                    const float4 t = terms[j];
-                    if (t.w != 0.0f) {
-                        sx = xadd(sx, t.x);
-                        sy = xadd(sy, t.y);
-                        sz = xadd(sz, t.z);
-                        if (COUNT) ++n_pairs;
+        int from = 0;  // next list entry of this group
+        bool more = use_list;
+        while (__any_sync(0xffffffffu, more)) {
+            int n_in = 0;
+            if (more) {
+                while (from < nl && n_in + G <= CG_IN_MAX) {
+                    const int j = from + gl;
+                    bool ok = false;
+                    int i = 0;
+                    if (j < nl) {
+                        i = list[j];
+                        const int4 ce = ca_cell[i];
+                        if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
+                            abs((long long)ce.z - cz) <= 1) {
+                            const float4 a = ca_pq[i];
+                            const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
+                            ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                        }
                     }
+                    const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << G) - 1u);
+                    if (ok) in[n_in + __popc(m & ((1u << gl) - 1u))] = i;
+                    n_in += __popc(m);
+                    from += G;
+                }
+                if (COUNT && gl == 0) n_pairs += n_in;
+            }
+            // B. the round's pair terms of every residue of the warp, one pair per lane
+            int pre[NG + 1];
+            pre[0] = 0;
+#pragma unroll
+            for (int q = 0; q < NG; ++q) pre[q + 1] = pre[q] + __shfl_sync(0xffffffffu, n_in, q * G);
+            const int total = pre[NG];
+            for (int base = 0; base < total; base += 32) {
+                const int pidx = base + lane;
+                int q = 0;
+#pragma unroll
+                for (int t = 1; t < NG; ++t) q += pidx >= pre[t] ? 1 : 0;
+                const int src = q * G;
+                const CgB body{__shfl_sync(0xffffffffu, ca.x, src), __shfl_sync(0xffffffffu, ca.y, src),
+                               __shfl_sync(0xffffffffu, ca.z, src), __shfl_sync(0xffffffffu, res.x, src),
+                               __shfl_sync(0xffffffffu, res.y, src), __shfl_sync(0xffffffffu, res.z, src),
+                               __shfl_sync(0xffffffffu, res.w, src)};
+                if (pidx < total) {
+                    const int k = pidx - pre[q];
+                    const int i = s_in[rl0 + q][k];
+                    float tx, ty, tz;
+                    cg_term_parts(body, ca_pq[i], ca_prm[i], tx, ty, tz);
+                    s_term[rl0 + q][k] = make_float3(tx, ty, tz);
                 }
             }
-            __syncwarp(gmask);  // term slots are rewritten next step
-        } else {
+            __syncwarp();
+            // C. lane 0 of each group continues its sum in order
+            if (gl == 0)
+                for (int k = 0; k < n_in; ++k) {
+                    const float3 t = terms[k];
+                    sx = xadd(sx, t.x);
+                    sy = xadd(sy, t.y);
+                    sz = xadd(sz, t.z);
+                }
+            __syncwarp();  // term slots are rewritten next round
+            more = more && from < nl;
+        }
+        if (gl == 0 && valid && !use_list) {  // list overflow or cells near the i32 limits
             int np = 0;
-            if (gl == 0) {
-                float3 f;
-                cg_force_walk<COUNT>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
-                sx = f.x; sy = f.y; sz = f.z;
-            }
+            float3 f;
+            cg_force_walk<COUNT>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
+            sx = f.x; sy = f.y; sz = f.z;
             if (COUNT) n_pairs += np;
         }
-        float fx = __shfl_sync(gmask, sx, 0, G), fy = __shfl_sync(gmask, sy, 0, G),
-              fz = __shfl_sync(gmask, sz, 0, G);
+        float fx = __shfl_sync(0xffffffffu, sx, gshift), fy = __shfl_sync(0xffffffffu, sy, gshift),
+              fz = __shfl_sync(0xffffffffu, sz, gshift);
+        if (!valid) continue;  // uniform per group; the warp-wide shuffles above were all taken
         // harmonic restraint toward the shell (diffusion.rs:317-327)
         const float dx_c = xsub(ca.x, ag_cx), dy_c = xsub(ca.y, ag_cy), dz_c = xsub(ca.z, ag_cz);
         const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
@@ -290,7 +411,16 @@ __global__ void __launch_bounds__(CG_WARPS * 32, cg_warps_per_sm<G>() / CG_WARPS
             if (!(mx * mx + my * my + mz * mz <= skin2)) {  // left the skin (or NaN): new list
                 centre = ca;
                 nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+                dirty = true;
             }
+        }
+    }
+    if (!valid) return;
+    if (!COUNT && dirty && st.cg_meta) {  // keep the list for the next launch
+        for (int j = gl; j < min(nl, CG_LIST_MAX); j += G) st.cg_list[(size_t)r * CG_LIST_MAX + j] = list[j];
+        if (gl == 0) {
+            st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, 0.f);
+            st.cg_meta[r] = make_int4(nl, st.cand_ag[c], st.ag_epoch ? *st.ag_epoch : -2, 0);
         }
     }
     if (COUNT) {
@@ -358,26 +488,32 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
 
 template <int W, int G>
 static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
-                      uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order) {
+                      uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
+                      int stage_bytes) {
     const int threads = W * 32;
     const long long total = (long long)st.total_res * G;
-    k_langevin<false, W, G><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order);
+    if (stage_bytes > 0)
+        cudaFuncSetAttribute(k_langevin<false, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
+    k_langevin<false, W, G><<<(int)((total + threads - 1) / threads), threads, stage_bytes, s>>>(
+        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order, stage_bytes);
 }
 
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta, int lanes_per_res) {
+                    int warps_per_cta, int lanes_per_res, int max_ag_res, int max_ag_cells) {
     if (st.total_res <= 0 || n_steps <= 0) return;
+    // antigen staging: up to 96 KB of dynamic shared memory per CTA
+    const size_t sb = cg_stage_bytes(max_ag_res, max_ag_cells);
+    const int stage = sb <= 96 * 1024 ? (int)sb : 0;
     if (lanes_per_res == 8) {
         switch (warps_per_cta) {
-            case 2: diffuse_w<2, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
-            case 8: diffuse_w<8, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
-            default: diffuse_w<4, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order); break;
+            case 2: diffuse_w<2, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
+            case 8: diffuse_w<8, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
+            default: diffuse_w<4, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
         }
     } else {  // four lanes: at most four warps per CTA (list storage)
-        if (warps_per_cta == 2) diffuse_w<2, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order);
-        else diffuse_w<4, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order);
+        if (warps_per_cta == 2) diffuse_w<2, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage);
+        else diffuse_w<4, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage);
     }
 }
 
@@ -387,7 +523,7 @@ void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags
     const int threads = 4 * 32;
     const long long total = (long long)st.total_res * 4;
     k_langevin<true, 4, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr);
+        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr, 0);
 }
 
 }  // namespace binder
