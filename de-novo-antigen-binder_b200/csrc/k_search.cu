@@ -82,7 +82,8 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 // take every step's translation as set_ca_pos does (allatom.rs:279-293).
 // COUNT: count the in-cutoff pairs of the same trajectory, leave the state as is.
 constexpr int CG_LIST_MAX = CG_LIST_CAP;
-constexpr float CG_SKIN = 2.0f;  // list radius = 10 A cutoff + skin
+constexpr float CG_SKIN = 2.0f;      // list radius = 10 A cutoff + skin; a residue's first skin
+constexpr float CG_SKIN_MAX = 5.0f;  // a residue that outruns its list gets twice the skin, up to this
 
 // The one-lane walk over all 27 cells, out of line: it is rarely taken and must
 // not take registers from the list path.
@@ -99,42 +100,41 @@ __device__ __forceinline__ bool cell_far(int cx, int cy, int cz) {
 }
 
 // Verlet list of the residue whose group of G lanes calls this (gl = lane in group):
-// positions (ascending) of the antigen Calphas within CG_SKIN + 10 A (+ 10 mA for
-// rounding) of p, found by a walk over the 5 x 5 x 5 cells around p's cell culled by
-// slab distance.  The lanes split the 25 (dx, dy) columns into contiguous runs,
-// count, take offsets by a prefix sum and write.  Returns the list length (all lanes);
-// a length above CG_LIST_MAX leaves the list unwritten.
+// positions (ascending) of the antigen Calphas within skin + 10 A (+ 10 mA for
+// rounding) of p, found by a walk over the (2K+1)^3 cells around p's cell, K =
+// ceil(radius / cell), culled by slab distance.  The lanes split the (2K+1)^2
+// (dx, dy) columns into contiguous runs (for fixed (dx, dy) the cells along z are
+// one contiguous range of the sorted array), count, take offsets by a prefix sum
+// and write.  Returns the list length (all lanes); a length above CG_LIST_MAX (or a
+// grid finer than radius / 8) leaves the list unusable.
 template <int G>
-__device__ __noinline__ int build_cg_list(const GridView& g, const float4* __restrict__ ca_pq, F3 p, int gl, unsigned gmask,
-                             int* list) {
-    const float R = 10.0f + CG_SKIN + 0.01f, R2 = R * R;
+__device__ __noinline__ int build_cg_list(const GridView& g, const float4* __restrict__ ca_pq, F3 p, int gl,
+                                          unsigned gmask, int* list, float skin) {
+    const float R = 10.0f + skin + 0.01f, R2 = R * R;
     const int c[3] = {cell_coord(p.x, g.inv), cell_coord(p.y, g.inv), cell_coord(p.z, g.inv)};
-    if (cell_far(c[0], c[1], c[2])) return CG_LIST_MAX + 1;
+    if (cell_far(c[0], c[1], c[2]) || !(R <= 8.0f * g.cell)) return CG_LIST_MAX + 1;
+    const int K = (int)ceilf(R / g.cell), W = 2 * K + 1, ncol = W * W;
     const float pp[3] = {p.x, p.y, p.z};
-    float sl[3][5];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int o = 0; o < 5; ++o) {
-            const float lo = (float)(c[d] + o - 2) * g.cell, hi = lo + g.cell;
-            const float dd = fmaxf(fmaxf(lo - pp[d], pp[d] - hi), 0.0f);
-            sl[d][o] = dd * dd;
-        }
-    const int col0 = (25 * gl) / G, col1 = (25 * (gl + 1)) / G;
+    auto slab2 = [&](int d, int o) {  // squared distance from p to the cell slab c[d] + o along d
+        const float lo = (float)(c[d] + o) * g.cell, hi = lo + g.cell;
+        const float dd = fmaxf(fmaxf(lo - pp[d], pp[d] - hi), 0.0f);
+        return dd * dd;
+    };
+    const int col0 = (ncol * gl) / G, col1 = (ncol * (gl + 1)) / G;
     int n_mine = 0, off = 0, total = 0;
     for (int pass = 0; pass < 2; ++pass) {
         int w = off;
         for (int col = col0; col < col1; ++col) {
-            const int ox = col / 5, oy = col % 5;
-            const float dxy = sl[0][ox] + sl[1][oy];
+            const int ox = col / W - K, oy = col % W - K;
+            const float dxy = slab2(0, ox) + slab2(1, oy);
             if (dxy > R2) continue;
-            const int X = c[0] + ox - 2 - g.ox, Y = c[1] + oy - 2 - g.oy;
+            const int X = c[0] + ox - g.ox, Y = c[1] + oy - g.oy;
             if (X < 0 || Y < 0 || X >= g.nx || Y >= g.ny) continue;
-            int zl = 0, zh = 4;
-            while (zl <= 4 && dxy + sl[2][zl] > R2) ++zl;
-            while (zh >= zl && dxy + sl[2][zh] > R2) --zh;
+            int zl = -K, zh = K;
+            while (zl <= K && dxy + slab2(2, zl) > R2) ++zl;
+            while (zh >= zl && dxy + slab2(2, zh) > R2) --zh;
             if (zl > zh) continue;
-            const int Z0 = max(c[2] + zl - 2 - g.oz, 0), Z1 = min(c[2] + zh - 2 - g.oz, g.nz - 1);
+            const int Z0 = max(c[2] + zl - g.oz, 0), Z1 = min(c[2] + zh - g.oz, g.nz - 1);
             if (Z0 > Z1) continue;
             const int base = (X * g.ny + Y) * g.nz;
             const int a1 = g.cell_start[base + Z1 + 1];
@@ -268,10 +268,10 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
     }
     // the residue's list from the previous launch when it was built for this antigen
     // set and antigen and still covers the Calpha, else a new one
-    const float skin2 = (CG_SKIN - 0.01f) * (CG_SKIN - 0.01f);
     F3 centre = ca;
     int nl = 0;
     bool dirty = false;
+    float skin = CG_SKIN;
     if (valid) {
         const int ep = st.ag_epoch ? *st.ag_epoch : -2;
         const int4 meta = st.cg_meta ? st.cg_meta[r] : make_int4(-1, -1, -1, -1);
@@ -279,8 +279,10 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ep >= 0 && meta.z == ep && meta.y == st.cand_ag[c] && meta.x >= 0 && meta.x <= CG_LIST_MAX) {
             cc = st.cg_centre[r];
+            skin = fminf(fmaxf(cc.w, CG_SKIN), CG_SKIN_MAX);
             const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
-            reuse = mx * mx + my * my + mz * mz <= skin2;
+            reuse = mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f);
+            if (!reuse) skin = fminf(2.0f * skin, CG_SKIN_MAX);  // it outran the list
         }
         if (reuse) {
             centre = {cc.x, cc.y, cc.z};
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
             for (int j = gl; j < nl; j += G) list[j] = st.cg_list[(size_t)r * CG_LIST_MAX + j];
             __syncwarp(gmask);
         } else {
-            nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+            nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list, skin);
             dirty = true;
         }
     }
@@ -408,9 +410,11 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         ca = {xadd(ca.x, dl.x), xadd(ca.y, dl.y), xadd(ca.z, dl.z)};
         if (s + 1 < n_steps) {
             const float mx = ca.x - centre.x, my = ca.y - centre.y, mz = ca.z - centre.z;
-            if (!(mx * mx + my * my + mz * mz <= skin2)) {  // left the skin (or NaN): new list
+            if (!(mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f))) {
+                // left the skin (or NaN): a new list with twice the skin
+                skin = fminf(2.0f * skin, CG_SKIN_MAX);
                 centre = ca;
-                nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list);
+                nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list, skin);
                 dirty = true;
             }
         }
@@ -419,7 +423,7 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
     if (!COUNT && dirty && st.cg_meta) {  // keep the list for the next launch
         for (int j = gl; j < min(nl, CG_LIST_MAX); j += G) st.cg_list[(size_t)r * CG_LIST_MAX + j] = list[j];
         if (gl == 0) {
-            st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, 0.f);
+            st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
             st.cg_meta[r] = make_int4(nl, st.cand_ag[c], st.ag_epoch ? *st.ag_epoch : -2, 0);
         }
     }
