@@ -164,7 +164,6 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
 
 constexpr int CG_IN_MAX = 48;  // in-cutoff list entries a residue holds per step
 
-// register budget: 24 resident warps per SM (80 registers a thread)
 // Dynamic shared memory of the antigen staging: Calphas (pq, prm, cell) and the
 // grid's cell starts of an antigen with n Calphas and ncell cells.
 __host__ __device__ inline size_t cg_stage_bytes(int n, int ncell) {
@@ -176,6 +175,8 @@ __host__ __device__ inline size_t cg_stage_bytes(int n, int ncell) {
 // when every residue of the CTA belongs to one antigen that fits the dynamic
 // shared memory the launch reserved (residues are ordered by antigen, then cell);
 // otherwise the kernel reads them from global memory.  Same values either way.
+// register budget: 24 resident warps per SM (80 registers a thread; a 64-register
+// budget spills more than the extra occupancy gains)
 template <bool COUNT, int CG_WARPS, int G>
 __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(StateView st, const AgView* __restrict__ ags,
                                                              StepParams p, int n_steps, uint32_t step0,
