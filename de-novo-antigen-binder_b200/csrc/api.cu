@@ -154,8 +154,8 @@ struct MlpState {
     DBuf<__nv_bfloat16> w1, w2, w2t, w3, w3t;
     DBuf<uint4> f1, f2, f3;
     int cap = 0;
-    DBuf<__nv_bfloat16> X, Xt, H1, H1t, H2, H2t, dY, dYt, dZ2, dZ2t, dZ1t;
-    DBuf<float> Z1, Z2, Y, part, feat, ca, target;
+    DBuf<__nv_bfloat16> X, Xt, H1, H1t, H2, H2t, dY, dYt, dZ2, dZ2t, dZ1t, S1, S2;
+    DBuf<float> Y, part, feat, ca, target;
     DBuf<uint8_t> aa;
     DBuf<int> ag, action, idx;
     DBuf<double> loss;
@@ -1834,8 +1834,8 @@ int mlp_reserve(binder_ctx* ctx, int rows) {
     CK(M.dZ2.ensure(c * MLP_H), "mlp alloc");
     CK(M.dZ2t.ensure(c * MLP_H), "mlp alloc");
     CK(M.dZ1t.ensure(c * MLP_H), "mlp alloc");
-    CK(M.Z1.ensure(c * MLP_H), "mlp alloc");
-    CK(M.Z2.ensure(c * MLP_H), "mlp alloc");
+    CK(M.S1.ensure(c * MLP_H), "mlp alloc");
+    CK(M.S2.ensure(c * MLP_H), "mlp alloc");
     CK(M.Y.ensure(c * MLP_OUT_PAD), "mlp alloc");
     CK(M.feat.ensure(c * MLP_IN), "mlp alloc");
     CK(M.ca.ensure(c * 3), "mlp alloc");
@@ -1868,14 +1868,14 @@ int mlp_forward_dev(binder_ctx* ctx, int m, bool train) {
     g.b = M.w1.p; g.ldb = MLP_K1; g.n = MLP_H; g.k = MLP_K1; g.k_split = MLP_K1;
     g.e = GemmEpi{};
     g.e.mode = EPI_SILU; g.e.bias = M.w.p + MLP_OFF_B1;
-    g.e.c = train ? M.Z1.p : nullptr; g.e.ldc = MLP_H;
+    g.e.sp = train ? M.S1.p : nullptr; g.e.ldsp = MLP_H;
     g.e.h = M.H1.p; g.e.ldh = MLP_H; g.e.h_rows = mp;
     g.e.ht = train ? M.H1t.p : nullptr; g.e.ldht = mp; g.e.ht_rows = mp;
     g.e.n_valid = MLP_H; g.e.m_valid = m;
     if ((s = gemm(ctx, g, "mlp layer 1"))) return s;
     // layer 2
     g.a = M.H1.p; g.lda = MLP_H; g.b = M.w2.p; g.ldb = MLP_H; g.k = MLP_H; g.k_split = MLP_H;
-    g.e.bias = M.w.p + MLP_OFF_B2; g.e.c = train ? M.Z2.p : nullptr;
+    g.e.bias = M.w.p + MLP_OFF_B2; g.e.sp = train ? M.S2.p : nullptr;
     g.e.h = M.H2.p; g.e.ht = train ? M.H2t.p : nullptr;
     if ((s = gemm(ctx, g, "mlp layer 2"))) return s;
     // layer 3: Y = H2 W3^T + b3 (FP32)
@@ -1920,7 +1920,7 @@ int mlp_backward_dev(binder_ctx* ctx, int m, float delta) {
     GemmArgs g;
     g.a = M.dY.p; g.lda = MLP_OUT_PAD; g.m = mp;
     g.b = M.w3t.p; g.ldb = MLP_OUT_PAD; g.n = MLP_H; g.k = MLP_OUT_PAD; g.k_split = 64;
-    g.e.mode = EPI_DSILU; g.e.z = M.Z2.p; g.e.ldz = MLP_H;
+    g.e.mode = EPI_DSILU; g.e.sp = M.S2.p; g.e.ldsp = MLP_H;
     g.e.h = M.dZ2.p; g.e.ldh = MLP_H; g.e.h_rows = mp;
     g.e.ht = M.dZ2t.p; g.e.ldht = mp; g.e.ht_rows = mp;
     g.e.n_valid = MLP_H; g.e.m_valid = m;
@@ -1930,7 +1930,7 @@ int mlp_backward_dev(binder_ctx* ctx, int m, float delta) {
     launch_rowsum_bf16(ctx->stream, MLP_H, mp, mp, M.dZ2t.p, M.g.p + MLP_OFF_B2);
     LAUNCHED("mlp bias grad");
     g.a = M.dZ2.p; g.lda = MLP_H; g.b = M.w2t.p; g.ldb = MLP_H; g.k = MLP_H; g.k_split = MLP_H;
-    g.e.z = M.Z1.p; g.e.h = nullptr; g.e.ht = M.dZ1t.p;
+    g.e.sp = M.S1.p; g.e.h = nullptr; g.e.ht = M.dZ1t.p;
     if ((s = gemm(ctx, g, "mlp dZ1"))) return s;
     // layer 1: dW1 = dZ1^T X, db1
     if ((s = mlp_weight_grad(ctx, M.dZ1t.p, MLP_H, M.Xt.p, MLP_K1, mp, M.g.p + MLP_OFF_W1))) return s;

@@ -176,17 +176,15 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + expf(-z));
-    return s * (1.0f + z * (1.0f - s));
-}
+// logistic sigmoid with the fast exponential (the results are rounded to BF16)
+__device__ __forceinline__ float sigmoid_fast(float z) { return __frcp_rn(1.0f + __expf(-z)); }
 
 // ---- C[M x N] = A[M x K] * B[N x K]^T on the tensor cores ----------------------------
-// One CTA of 128 threads per 128-row tile of A (blockIdx.x) and K slice (blockIdx.y,
+// One CTA of 256 threads per 128-row tile of A (blockIdx.x) and K slice (blockIdx.y,
 // split-K); the whole N (16..256, multiple of 16) in one tensor-memory accumulator.
-// A rows >= m and K beyond the slice are zero-filled in shared memory.
-constexpr int G_M = 128, G_K = 64, G_THREADS = 128;
+// A rows >= m and K beyond the slice are zero-filled in shared memory.  Warps w and
+// w + 4 read the accumulator lanes 32 (w % 4) .. +31 and split its columns.
+constexpr int G_M = 128, G_K = 64, G_THREADS = 256;
 constexpr int G_STAGE_A = G_M * G_K * 2;                       // 16 KB
 __host__ __device__ constexpr int gemm_stage_bytes(int n) { return G_STAGE_A + n * G_K * 2; }
 __host__ __device__ constexpr int gemm_smem_bytes(int n) { return 2 * gemm_stage_bytes(n) + 1024; }
@@ -269,13 +267,18 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm_tc(GemmArgs g, uint32_t* __r
     if (!ok && err) atomicOr(err, ERRF_TIMEOUT);
     tc_fence_after();
 
-    // ---- epilogue: warp w owns accumulator lanes (rows) 32w .. 32w+31 ----
-    const int row = m0 + warp * 32 + lane;
+    // ---- epilogue: warp w owns accumulator lanes (rows) 32 (w % 4) .. +31, columns
+    //      [n/2 * (w / 4), n/2 * (w / 4 + 1)) (multiples of 8) ----
+    const int wl = warp & 3, half = warp >> 2;
+    const int row = m0 + wl * 32 + lane;
     const bool row_ok = row < g.e.m_valid;
     const GemmEpi& e = g.e;
-    for (int c0 = 0; c0 < g.n && ok; c0 += 8) {
+    const int n8 = g.n / 8;                        // column groups of 8
+    const int cg0 = (n8 * half) / 2, cg1 = (n8 * (half + 1)) / 2;
+    for (int cgi = cg0; cgi < cg1 && ok; ++cgi) {
+        const int c0 = cgi * 8;
         float v[8];
-        if (n_chunks > 0) tc_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        if (n_chunks > 0) tc_ld8(tmem + ((uint32_t)(wl * 32) << 16) + (uint32_t)c0, v);
         else {
 #pragma unroll
             for (int i = 0; i < 8; ++i) v[i] = 0.0f;
@@ -290,22 +293,28 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm_tc(GemmArgs g, uint32_t* __r
             }
         } else {
             __align__(16) __nv_bfloat16 h[8];
+            __align__(16) __nv_bfloat16 dz[8];
+            if (e.mode == EPI_DSILU && row_ok) *(uint4*)dz = *(const uint4*)(e.sp + (size_t)row * e.ldsp + c0);
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                float o = 0.0f;
+                float o = 0.0f, d = 0.0f;
                 if (row_ok) {
                     if (e.mode == EPI_SILU) {
                         const float z = v[i] + (e.bias ? e.bias[c0 + i] : 0.0f);
-                        if (e.c) e.c[(size_t)row * e.ldc + c0 + i] = z;
-                        o = silu(z);
+                        const float sg = sigmoid_fast(z);
+                        o = z * sg;
+                        d = sg * (1.0f + z * (1.0f - sg));
                     } else {  // EPI_DSILU
-                        o = v[i] * dsilu(e.z[(size_t)row * e.ldz + c0 + i]);
+                        o = v[i] * __bfloat162float(dz[i]);
                     }
                 }
                 h[i] = __float2bfloat16_rn(o);
+                dz[i] = __float2bfloat16_rn(d);
                 if (e.ht && row < e.ht_rows) e.ht[(size_t)(c0 + i) * e.ldht + row] = h[i];
             }
             if (e.h && row < e.h_rows) *(uint4*)(e.h + (size_t)row * e.ldh + c0) = *(const uint4*)h;
+            if (e.mode == EPI_SILU && e.sp && row < e.h_rows)
+                *(uint4*)(e.sp + (size_t)row * e.ldsp + c0) = *(const uint4*)dz;
         }
     }
     tc_fence_before();

@@ -51,9 +51,10 @@ enum : int { EPI_F32 = 0, EPI_PARTIAL = 1, EPI_SILU = 2, EPI_DSILU = 3 };
 // Epilogue of k_gemm_tc.
 //  EPI_F32:     c[row][col] = acc + bias[col]                (cols < n_valid, rows < m_valid)
 //  EPI_PARTIAL: the same without bias at c + blockIdx.y * part_stride (split-K partials)
-//  EPI_SILU:    z = acc + bias; c[row][col] = z (if c); h = silu(z) as BF16 to h[row][col]
-//               (rows < h_rows) and ht[col][row] (rows < ht_rows); rows >= m_valid store 0
-//  EPI_DSILU:   h = acc * silu'(z[row][col]) as BF16 to h / ht likewise
+//  EPI_SILU:    z = acc + bias; h = silu(z) as BF16 to h[row][col] (rows < h_rows) and
+//               ht[col][row] (rows < ht_rows); silu'(z) as BF16 to sp[row][col] (if sp);
+//               rows >= m_valid store 0
+//  EPI_DSILU:   h = acc * sp[row][col] (the saved BF16 silu'(z)) as BF16 to h / ht likewise
 struct GemmEpi {
     int mode = EPI_F32;
     const float* bias = nullptr;
@@ -64,8 +65,8 @@ struct GemmEpi {
     int ldh = 0, h_rows = 0;
     __nv_bfloat16* ht = nullptr;
     int ldht = 0, ht_rows = 0;
-    const float* z = nullptr;
-    int ldz = 0;
+    __nv_bfloat16* sp = nullptr;  // silu'(z), BF16 [rows][ldsp]
+    int ldsp = 0;
     int n_valid = 0, m_valid = 0;
 };
 

@@ -11,8 +11,9 @@ the GPU kernels in de-novo-antigen-binder_b200/csrc/k_mlp.cu:
     With bf16=True the BF16 roundings of the GPU path are applied (weights, input
     rows, hidden activations, output and hidden gradients) and only the sums are
     exact, so the GPU's FP32 sums are compared against exact sums of the same
-    BF16 operands; with bf16=False it is the plain float64 network whose analytic
-    gradient is checked against central finite differences.
+    BF16 operands (the SiLU' factors the forward pass keeps are BF16 too); with
+    bf16=False it is the plain float64 network whose analytic gradient is checked
+    against central finite differences.
 
 Only tests/ import this module.
 """
@@ -115,10 +116,11 @@ def loss_grad(params, X, action, target, delta=1.0, bf16_path=True):
     dY = _b(dY, bf16_path)
     gW3 = dY.T @ H2
     gb3 = dY.sum(0)
-    dZ2 = _b((dY @ W3) * (_sig(Z2) * (1 + Z2 * (1 - _sig(Z2)))), bf16_path)
+    # the GPU keeps silu'(z) of the forward pass as BF16
+    dZ2 = _b((dY @ W3) * _b(_sig(Z2) * (1 + Z2 * (1 - _sig(Z2))), bf16_path), bf16_path)
     gW2 = dZ2.T @ H1
     gb2 = dZ2.sum(0)
-    dZ1 = _b((dZ2 @ W2) * (_sig(Z1) * (1 + Z1 * (1 - _sig(Z1)))), bf16_path)
+    dZ1 = _b((dZ2 @ W2) * _b(_sig(Z1) * (1 + Z1 * (1 - _sig(Z1))), bf16_path), bf16_path)
     gW1 = dZ1.T @ Xb
     gb1 = dZ1.sum(0)
     g = np.zeros(N_PARAMS, np.float64)
