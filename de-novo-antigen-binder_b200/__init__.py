@@ -177,6 +177,8 @@ _SIGS = {
     "binder_mc_log_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "binder_mlp_take_log": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "binder_set_proposal": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float]),
+    "binder_selftest_wait": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "binder_debug_fail_alloc": (C.c_int, [C.c_int64]),
 }
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 

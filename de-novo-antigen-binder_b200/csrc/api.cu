@@ -23,6 +23,19 @@ using namespace binder;
 
 namespace {
 
+// Host-side fault injection for the tests: the device allocation that brings the
+// countdown to zero fails as if the device were out of memory (no GPU fault).
+long long g_alloc_countdown = -1;
+bool injected_alloc_failure() {
+    if (g_alloc_countdown < 0) return false;
+    if (g_alloc_countdown == 0) {
+        g_alloc_countdown = -1;
+        return true;
+    }
+    --g_alloc_countdown;
+    return false;
+}
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -43,6 +56,7 @@ struct DBuf {
     cudaError_t ensure(size_t m) {
         if (m <= n && p) return cudaSuccess;
         release();
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T));
         if (e == cudaSuccess) n = std::max<size_t>(m, 1);
         else p = nullptr;
@@ -2238,6 +2252,24 @@ int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n) {
     M.n_tuples = n;
     if (out_n) *out_n = n;
     return BINDER_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int binder_debug_fail_alloc(int64_t n) {
+    g_alloc_countdown = n < 0 ? -1 : n;
+    return BINDER_OK;
+}
+
+int binder_selftest_wait(binder_ctx* ctx, uint32_t max_polls) {
+    int s = enter(ctx);
+    if (s) return s;
+    if ((s = clear_err(ctx))) return s;
+    CK(launch_wait_selftest(ctx->stream, max_polls, ctx->errf.p), "wait self-test");
+    ctx->launches++;
+    return check_err(ctx);
 }
 
 }  // extern "C"

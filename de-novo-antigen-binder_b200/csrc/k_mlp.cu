@@ -113,8 +113,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait for phase `parity` of barrier b; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 22); ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint32_t max_polls = 1u << 22) {
+    for (uint32_t i = 0; i < max_polls; ++i) {
         if (mbar_try_wait(b, parity)) return true;
         if (i > 64) __nanosleep(64);
     }
@@ -323,6 +323,21 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm_tc(GemmArgs g, uint32_t* __r
         tc_fence_after();
         tmem_dealloc(tmem, ncols);
     }
+}
+
+// The bounded wait on a barrier nothing arrives on: raises ERRF_TIMEOUT after
+// max_polls polls and returns (the error path of every tcgen05 wait, exercised
+// without a fault).
+__global__ void k_wait_selftest(uint32_t max_polls, uint32_t* __restrict__ err) {
+    __shared__ __align__(8) uint64_t bar;
+    mbar_init(&bar, 1);
+    __syncwarp();
+    if (!mbar_wait(&bar, 0, max_polls) && err) atomicOr(err, ERRF_TIMEOUT);
+}
+
+cudaError_t launch_wait_selftest(cudaStream_t s, uint32_t max_polls, uint32_t* err) {
+    k_wait_selftest<<<1, 1, 0, s>>>(max_polls, err);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_gemm_tc(cudaStream_t s, const GemmArgs& g, uint32_t* err) {

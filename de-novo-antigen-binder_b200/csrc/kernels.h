@@ -120,6 +120,7 @@ void launch_features(cudaStream_t s, int n, int n_pad, const float* ca, const ui
 void launch_pack_features(cudaStream_t s, int n, int n_pad, const float* f, __nv_bfloat16* X);
 void launch_transpose_bf16(cudaStream_t s, int rows, int cols, const __nv_bfloat16* in, __nv_bfloat16* out);
 cudaError_t launch_gemm_tc(cudaStream_t s, const GemmArgs& g, uint32_t* err);
+cudaError_t launch_wait_selftest(cudaStream_t s, uint32_t max_polls, uint32_t* err);
 void launch_mlp_loss(cudaStream_t s, int m, int m_pad, const float* Y, const int* action, const float* target,
                      float delta, __nv_bfloat16* dY, __nv_bfloat16* dYt, double* loss);
 void launch_rowsum_bf16(cudaStream_t s, int rows, int m, int ld, const __nv_bfloat16* G, float* out);

@@ -414,6 +414,14 @@ int binder_state_pair_counts(binder_ctx* ctx, int n_steps, int64_t* out_cg_pairs
 /* FP32 FMA throughput of the device (TFLOP/s), scalar and packed f32x2. */
 int binder_fp32_peak(binder_ctx* ctx, double* out_tflops_scalar, double* out_tflops_packed);
 
+/* ---- failure injection (no reference counterpart; tests) ------------------------
+   The bounded device wait every tcgen05 GEMM uses, on a barrier nothing arrives on:
+   returns BINDER_ERR_TIMEOUT after max_polls polls and leaves the context usable. */
+int binder_selftest_wait(binder_ctx* ctx, uint32_t max_polls);
+/* The n-th following device allocation of any context (0 = the next) fails as if
+   the device were out of memory (BINDER_ERR_OOM); n < 0 disarms. */
+int binder_debug_fail_alloc(int64_t n);
+
 #ifdef __cplusplus
 }
 #endif
