@@ -565,20 +565,22 @@ def run_learned(pkg, ctx, seeds=(21, 22, 23), n_res=20):
 
 def run_block_only(args):
     """Small profiling case for the search block: 3 eagerly issued blocks of the
-    bench workload at launch shape (cg_warps, cg_lanes)."""
+    bench workload at launch shape (cg_warps, cg_lanes[, cg_order])."""
     import torch
     from __graft_entry__ import load_package
     pkg = load_package()
     ctx = pkg.GpuContext.create(0)
     ctx.set_params(pkg.Params.defaults(flags=0))
     cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, 0)
-    w, lanes = (int(x) for x in args.block_only.split(","))
-    ctx.set_launch_cfg(8, 4, w, lanes)
+    shape = [int(x) for x in args.block_only.split(",")]
+    w, lanes, order = (shape + [1])[:3]
+    ctx.set_launch_cfg(8, 4, w, lanes, order)
     ctx.state_upload(pop.aa, chi, pos, uniform_n_res=int(pop.n_res[0]))
     for k in range(3):
         ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K)
     torch.cuda.synchronize()
-    print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "blocks": 3}}), flush=True)
+    print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "cg_order": order, "blocks": 3}}),
+          flush=True)
     ctx.close()
     return 0
 
@@ -631,7 +633,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal time-to-target runs")
     ap.add_argument("--phase2-only", type=int, default=0, metavar="STEPS",
                     help="profiling case: one launch of STEPS Langevin + Metropolis steps on 64 candidates")
-    ap.add_argument("--block-only", default="", metavar="WARPS,LANES",
+    ap.add_argument("--block-only", default="", metavar="WARPS,LANES[,ORDER]",
                     help="profiling case: 3 search blocks at this gradient-step launch shape")
     ap.add_argument("--mlp-only", type=int, default=0, metavar="ROWS",
                     help="profiling case: 3 loss + gradient passes of the proposal network on ROWS rows")

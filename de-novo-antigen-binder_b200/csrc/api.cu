@@ -1325,8 +1325,8 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
         S.order_valid = false;  // residues moved: the cell order is stale
         return BINDER_OK;
     }
-    int s = enqueue_order(ctx);
-    if (s) return s;
+    int s;
+    if (ctx->cfg.cg_order == 0 && (s = enqueue_order(ctx))) return s;
     int max_ag = 0, max_cells = 0;
     for (const auto& a : ctx->ags) {
         const GridView& gv = a->view.ca_grid;
@@ -1335,7 +1335,7 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     }
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
                    temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
-                   max_ag, max_cells);
+                   ctx->cfg.cg_order, max_ag, max_cells);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
@@ -1421,7 +1421,8 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
     std::vector<uint64_t> v = {
         (uint64_t)n_steps, (uint64_t)k, (uint64_t)S.n_cand, (uint64_t)S.total_res, (uint64_t)S.n_segments,
         (uint64_t)S.n_keys, (uint64_t)ctx->cfg.score_warps, (uint64_t)ctx->cfg.score_ctas_per_sm,
-        (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->cfg.cg_lanes, (uint64_t)ctx->ags.size()};
+        (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->cfg.cg_lanes, (uint64_t)ctx->cfg.cg_order,
+        (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
                           S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
@@ -1480,8 +1481,8 @@ void tune_cache_load(binder_ctx* ctx) {
     if (!f) return;
     char key[1024];
     LaunchCfg c;
-    while (std::fscanf(f, "%1023s %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
-                       &c.cg_lanes) == 5)
+    while (std::fscanf(f, "%1023s %d %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
+                       &c.cg_lanes, &c.cg_order) == 6)
         ctx->tune_cache.emplace_back(key, c);
     std::fclose(f);
 }
@@ -1492,7 +1493,8 @@ void tune_cache_store(binder_ctx* ctx, const std::string& key, const LaunchCfg& 
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps, c.cg_lanes);
+    std::fprintf(f, "%s %d %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps, c.cg_lanes,
+                 c.cg_order);
     std::fclose(f);
 }
 
@@ -1531,6 +1533,7 @@ int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out) {
     out->score_ctas_per_sm = ctx->cfg.score_ctas_per_sm;
     out->cg_warps = ctx->cfg.cg_warps;
     out->cg_lanes = ctx->cfg.cg_lanes;
+    out->cg_order = ctx->cfg.cg_order;
     return BINDER_OK;
 }
 
@@ -1538,12 +1541,14 @@ int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
     if (!ctx || !c) return BINDER_ERR_ARG;
     if ((c->score_warps != 4 && c->score_warps != 8 && c->score_warps != 16) || c->score_ctas_per_sm < 1 ||
         c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8) ||
-        (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8))
+        (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8) || c->cg_order < 0 ||
+        c->cg_order > 2)
         return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
     ctx->cfg.score_warps = c->score_warps;
     ctx->cfg.score_ctas_per_sm = c->score_ctas_per_sm;
     ctx->cfg.cg_warps = c->cg_warps;
     ctx->cfg.cg_lanes = c->cg_lanes;
+    ctx->cfg.cg_order = c->cg_order;
     return BINDER_OK;
 }
 
@@ -1569,15 +1574,17 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
     CK(cudaMemcpyAsync(saved.p, S.res_pos.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     LaunchCfg best = ctx->cfg;
     float best_ms = 1e30f;
+    for (int order : {0, 1, 2})
     for (int lanes : {4, 8})
         for (int w : {2, 4, 8}) {
             if (s) break;
             if (lanes == 4 && w == 8) continue;  // not a supported shape
             ctx->cfg.cg_warps = w;
             ctx->cfg.cg_lanes = lanes;
+            ctx->cfg.cg_order = order;
             float ms = 0.f;
             if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
-            if (ms < best_ms) { best_ms = ms; best.cg_warps = w; best.cg_lanes = lanes; }
+            if (ms < best_ms) { best_ms = ms; best.cg_warps = w; best.cg_lanes = lanes; best.cg_order = order; }
             CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice,
                                ctx->stream),
                "copy");

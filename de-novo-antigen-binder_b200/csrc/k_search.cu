@@ -164,6 +164,18 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
 
 constexpr int CG_IN_MAX = 48;  // in-cutoff list entries a residue holds per step
 
+// Residue of a lane group's slot: the cell-sorted permutation (order_mode 0), the
+// state's own order (1: candidate after candidate), or a stride through it (2:
+// slot * CG_STRIDE mod total, a bijection when total is coprime to the prime
+// CG_STRIDE) that spreads each warp's residues over unrelated candidates, so the
+// costly residues in contact are shared out evenly.  Results never depend on it.
+constexpr long long CG_STRIDE = 1000003;
+__device__ __forceinline__ int res_of_slot(const int* __restrict__ order, int mode, int slot, int total) {
+    if (mode == 2) return (int)(((long long)slot * CG_STRIDE) % total);
+    if (mode == 1 || !order) return slot;
+    return order[slot];
+}
+
 // Dynamic shared memory of the antigen staging: Calphas (pq, prm, cell) and the
 // grid's cell starts of an antigen with n Calphas and ncell cells.
 __host__ __device__ inline size_t cg_stage_bytes(int n, int ncell) {
@@ -183,7 +195,8 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
                                                              int with_noise, const float* __restrict__ temps,
                                                              uint32_t* __restrict__ err,
                                                              long long* __restrict__ pair_count,
-                                                             const int* __restrict__ order, int stage_cap) {
+                                                             const int* __restrict__ order, int order_mode,
+                                                             int stage_cap) {
     constexpr int RPC = CG_WARPS * 32 / G;  // residues per CTA
     constexpr int NG = 32 / G;              // residues (lane groups) per warp
     constexpr int NA = (SLOTS + G - 1) / G; // atoms per lane
@@ -203,7 +216,7 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
     int* list = s_list[rl];
     int* in = s_in[rl];
     float3* terms = s_term[rl];
-    const int r = valid ? (order ? order[slot_id] : slot_id) : 0;
+    const int r = valid ? res_of_slot(order, order_mode, slot_id, st.total_res) : 0;
     const int c = valid ? st.res_cand[r] : 0;
     const int r_local = valid ? r - st.cand_res_off[c] : 0;
     const uint32_t cid = valid ? st.cand_id[c] : 0u;
@@ -220,8 +233,15 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         const int first = blockIdx.x * (CG_WARPS * 32 / G);
         const int last = min(first + CG_WARPS * 32 / G, st.total_res) - 1;
         if (threadIdx.x == 0) {
-            const int ra = order ? order[first] : first, rb = order ? order[last] : last;
-            const int a0 = st.cand_ag[st.res_cand[ra]], a1 = st.cand_ag[st.res_cand[rb]];
+            // one antigen for the whole CTA: every residue's (orders 0 and 1 sort by
+            // antigen: the first and last tell; order 2 mixes them: check all)
+            const int ra = res_of_slot(order, order_mode, first, st.total_res);
+            const int rb = res_of_slot(order, order_mode, last, st.total_res);
+            const int a0 = st.cand_ag[st.res_cand[ra]];
+            int a1 = st.cand_ag[st.res_cand[rb]];
+            if (order_mode == 2)
+                for (int q = first; q <= last && a1 == a0; ++q)
+                    a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, q, st.total_res)]];
             const GridView& gv = ags[a0].ca_grid;
             const bool fits = a0 == a1 &&
                               cg_stage_bytes(ags[a0].n_res, gv.nx * gv.ny * gv.nz) <= (size_t)stage_cap;
@@ -494,32 +514,35 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
 template <int W, int G>
 static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                       uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                      int stage_bytes) {
+                      int order_mode, int stage_bytes) {
     const int threads = W * 32;
     const long long total = (long long)st.total_res * G;
     if (stage_bytes > 0)
         cudaFuncSetAttribute(k_langevin<false, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
     k_langevin<false, W, G><<<(int)((total + threads - 1) / threads), threads, stage_bytes, s>>>(
-        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order, stage_bytes);
+        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order, order_mode, stage_bytes);
 }
 
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta, int lanes_per_res, int max_ag_res, int max_ag_cells) {
+                    int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells) {
     if (st.total_res <= 0 || n_steps <= 0) return;
+    if (order_mode == 2 && st.total_res % CG_STRIDE == 0) order_mode = 1;  // stride not a bijection
     // antigen staging: up to 96 KB of dynamic shared memory per CTA
     const size_t sb = cg_stage_bytes(max_ag_res, max_ag_cells);
     const int stage = sb <= 96 * 1024 ? (int)sb : 0;
+#define BINDER_DIFFUSE(W, G) diffuse_w<W, G>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage)
     if (lanes_per_res == 8) {
         switch (warps_per_cta) {
-            case 2: diffuse_w<2, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
-            case 8: diffuse_w<8, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
-            default: diffuse_w<4, 8>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage); break;
+            case 2: BINDER_DIFFUSE(2, 8); break;
+            case 8: BINDER_DIFFUSE(8, 8); break;
+            default: BINDER_DIFFUSE(4, 8); break;
         }
     } else {  // four lanes: at most four warps per CTA (list storage)
-        if (warps_per_cta == 2) diffuse_w<2, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage);
-        else diffuse_w<4, 4>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, stage);
+        if (warps_per_cta == 2) BINDER_DIFFUSE(2, 4);
+        else BINDER_DIFFUSE(4, 4);
     }
+#undef BINDER_DIFFUSE
 }
 
 void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
@@ -528,7 +551,7 @@ void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags
     const int threads = 4 * 32;
     const long long total = (long long)st.total_res * 4;
     k_langevin<true, 4, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr, 0);
+        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr, 1, 0);
 }
 
 }  // namespace binder

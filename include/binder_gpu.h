@@ -289,6 +289,8 @@ typedef struct binder_launch_cfg {
     int32_t cg_warps;           /* warps per CTA of the gradient-step kernel: 2, 4, 8 */
     int32_t cg_lanes;           /* lanes per residue of the gradient-step kernel: 4 (with 2 or 4
                                    warps per CTA) or 8 */
+    int32_t cg_order;           /* residue order of the gradient-step kernel: 0 by Calpha cell,
+                                   1 candidate after candidate, 2 strided (work spread out) */
 } binder_launch_cfg;
 int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
