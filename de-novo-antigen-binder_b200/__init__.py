@@ -78,11 +78,13 @@ class Params(C.Structure):
 class LaunchCfg(C.Structure):
     """binder_launch_cfg (include/binder_gpu.h): launch shapes of the search block."""
     _fields_ = [("score_warps", C.c_int32), ("score_ctas_per_sm", C.c_int32), ("cg_warps", C.c_int32),
-                ("cg_lanes", C.c_int32), ("cg_order", C.c_int32)]
+                ("cg_lanes", C.c_int32), ("cg_order", C.c_int32), ("score_order", C.c_int32),
+                ("cg_queue", C.c_int32)]
 
     def as_dict(self):
         return {"score_warps": self.score_warps, "score_ctas_per_sm": self.score_ctas_per_sm,
-                "cg_warps": self.cg_warps, "cg_lanes": self.cg_lanes, "cg_order": self.cg_order}
+                "cg_warps": self.cg_warps, "cg_lanes": self.cg_lanes, "cg_order": self.cg_order,
+                "score_order": self.score_order, "cg_queue": self.cg_queue}
 
 
 FLAG_GRAPH = 1
@@ -583,8 +585,9 @@ class GpuContext:
         self._check(lib().binder_get_launch_cfg(self._h, C.byref(c)))
         return c
 
-    def set_launch_cfg(self, score_warps=8, score_ctas_per_sm=4, cg_warps=8, cg_lanes=8, cg_order=1):
-        c = LaunchCfg(score_warps, score_ctas_per_sm, cg_warps, cg_lanes, cg_order)
+    def set_launch_cfg(self, score_warps=8, score_ctas_per_sm=4, cg_warps=8, cg_lanes=8, cg_order=1, score_order=0,
+                       cg_queue=1):
+        c = LaunchCfg(score_warps, score_ctas_per_sm, cg_warps, cg_lanes, cg_order, score_order, cg_queue)
         self._check(lib().binder_set_launch_cfg(self._h, C.byref(c)))
 
     def autotune(self, reps=5):

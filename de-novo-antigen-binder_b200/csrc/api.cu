@@ -233,6 +233,7 @@ struct binder_ctx {
     cudaGraphExec_t block_graph = nullptr;
     std::vector<uint64_t> block_graph_sig;  // what the captured launches baked in
     int block_graph_launches = 0;
+    bool block_graph_order = false;  // the residue order is valid after a replay
     std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
     MlpState mlp;
     // antigen-set epoch (device word read by the gradient-step kernel)
@@ -1111,7 +1112,7 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     CK(S.order.ensure(std::max(total, 1)), "alloc");
     CK(S.key_counts.ensure(nk + 1), "alloc");
     CK(S.key_cursor.ensure(nk + 1), "alloc");
-    CK(S.queue.ensure(1), "alloc");
+    CK(S.queue.ensure(2), "alloc");  // scoring and gradient-step work queues
     CK(S.res_e.ensure(std::max(total, 1)), "alloc");
     CK(S.res_abs.ensure(std::max(total, 1)), "alloc");
     S.order_valid = false;
@@ -1326,23 +1327,35 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
         return BINDER_OK;
     }
     int s;
-    if (ctx->cfg.cg_order == 0 && (s = enqueue_order(ctx))) return s;
+    if (ctx->cfg.cg_order == 0) {
+        if ((s = enqueue_order(ctx))) return s;  // sorted before the steps, kept for the score
+    } else {
+        S.order_valid = false;  // residues move: the cell order is stale
+    }
     int max_ag = 0, max_cells = 0;
     for (const auto& a : ctx->ags) {
         const GridView& gv = a->view.ca_grid;
         max_ag = std::max(max_ag, a->n_res);
         max_cells = std::max(max_cells, gv.nx * gv.ny * gv.nz);
     }
+    // the antigen every candidate probes, if they share one (staged in shared memory)
+    int stage_ag = S.h_cand_ag.empty() ? -1 : S.h_cand_ag[0];
+    for (int a : S.h_cand_ag)
+        if (a != stage_ag) {
+            stage_ag = -1;
+            break;
+        }
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
                    temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
-                   ctx->cfg.cg_order, max_ag, max_cells);
+                   ctx->cfg.cg_order, max_ag, max_cells, stage_ag, ctx->cfg.cg_queue ? S.queue.p + 1 : nullptr);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
 
 StateScoreScratch score_scratch(binder_ctx* ctx) {
     State& S = ctx->st;
-    return StateScoreScratch{S.order_valid ? S.order.p : nullptr, S.queue.p, S.res_e.p, S.res_abs.p};
+    const bool cell = S.order_valid && ctx->cfg.score_order == 0;
+    return StateScoreScratch{cell ? S.order.p : nullptr, S.queue.p, S.res_e.p, S.res_abs.p};
 }
 
 int persistent_ctas(binder_ctx* ctx) { return ctx->num_sms * ctx->cfg.score_ctas_per_sm; }
@@ -1355,7 +1368,7 @@ int enqueue_score_state(binder_ctx* ctx, int full) {
         LAUNCHED("mc_energy");
         return BINDER_OK;
     }
-    if (!S.order_valid) {
+    if (!S.order_valid && ctx->cfg.score_order == 0) {
         int s = enqueue_order(ctx);
         if (s) return s;
     }
@@ -1422,7 +1435,7 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
         (uint64_t)n_steps, (uint64_t)k, (uint64_t)S.n_cand, (uint64_t)S.total_res, (uint64_t)S.n_segments,
         (uint64_t)S.n_keys, (uint64_t)ctx->cfg.score_warps, (uint64_t)ctx->cfg.score_ctas_per_sm,
         (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->cfg.cg_lanes, (uint64_t)ctx->cfg.cg_order,
-        (uint64_t)ctx->ags.size()};
+        (uint64_t)ctx->cfg.score_order, (uint64_t)ctx->cfg.cg_queue, (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
                           S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
@@ -1461,6 +1474,7 @@ int capture_block(binder_ctx* ctx, int n_steps, int k) {
         return cuda_fail(ctx, e, "graph instantiate");
     }
     ctx->block_graph_launches = (int)(ctx->launches - l0);
+    ctx->block_graph_order = ctx->st.order_valid;
     ctx->launches = l0;
     ctx->block_graph_sig = block_sig(ctx, n_steps, k);
     return BINDER_OK;
@@ -1481,8 +1495,8 @@ void tune_cache_load(binder_ctx* ctx) {
     if (!f) return;
     char key[1024];
     LaunchCfg c;
-    while (std::fscanf(f, "%1023s %d %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
-                       &c.cg_lanes, &c.cg_order) == 6)
+    while (std::fscanf(f, "%1023s %d %d %d %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
+                       &c.cg_lanes, &c.cg_order, &c.score_order, &c.cg_queue) == 8)
         ctx->tune_cache.emplace_back(key, c);
     std::fclose(f);
 }
@@ -1493,8 +1507,8 @@ void tune_cache_store(binder_ctx* ctx, const std::string& key, const LaunchCfg& 
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps, c.cg_lanes,
-                 c.cg_order);
+    std::fprintf(f, "%s %d %d %d %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps,
+                 c.cg_lanes, c.cg_order, c.score_order, c.cg_queue);
     std::fclose(f);
 }
 
@@ -1534,6 +1548,8 @@ int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out) {
     out->cg_warps = ctx->cfg.cg_warps;
     out->cg_lanes = ctx->cfg.cg_lanes;
     out->cg_order = ctx->cfg.cg_order;
+    out->score_order = ctx->cfg.score_order;
+    out->cg_queue = ctx->cfg.cg_queue;
     return BINDER_OK;
 }
 
@@ -1542,13 +1558,16 @@ int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
     if ((c->score_warps != 4 && c->score_warps != 8 && c->score_warps != 16) || c->score_ctas_per_sm < 1 ||
         c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8) ||
         (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8) || c->cg_order < 0 ||
-        c->cg_order > 2)
+        c->cg_order > 2 || c->score_order < 0 || c->score_order > 1 ||
+        c->cg_queue < 0 || c->cg_queue > 1)
         return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
     ctx->cfg.score_warps = c->score_warps;
     ctx->cfg.score_ctas_per_sm = c->score_ctas_per_sm;
     ctx->cfg.cg_warps = c->cg_warps;
     ctx->cfg.cg_lanes = c->cg_lanes;
     ctx->cfg.cg_order = c->cg_order;
+    ctx->cfg.score_order = c->score_order;
+    ctx->cfg.cg_queue = c->cg_queue;
     return BINDER_OK;
 }
 
@@ -1574,6 +1593,7 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
     CK(cudaMemcpyAsync(saved.p, S.res_pos.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     LaunchCfg best = ctx->cfg;
     float best_ms = 1e30f;
+    for (int queue : {0, 1})
     for (int order : {0, 1, 2})
     for (int lanes : {4, 8})
         for (int w : {2, 4, 8}) {
@@ -1582,25 +1602,40 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
             ctx->cfg.cg_warps = w;
             ctx->cfg.cg_lanes = lanes;
             ctx->cfg.cg_order = order;
+            ctx->cfg.cg_queue = queue;
             float ms = 0.f;
             if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
-            if (ms < best_ms) { best_ms = ms; best.cg_warps = w; best.cg_lanes = lanes; best.cg_order = order; }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.cg_warps = w;
+                best.cg_lanes = lanes;
+                best.cg_order = order;
+                best.cg_queue = queue;
+            }
             CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice,
                                ctx->stream),
                "copy");
         }
     best_ms = 1e30f;
+    // the cell order is timed with its sorting launches, as a block after moves runs it
+    for (int order : {0, 1})
     for (int nw : {4, 8, 16})
         for (int per_sm : {1, 2, 4, 8}) {
             if (s) break;
             ctx->cfg.score_warps = nw;
             ctx->cfg.score_ctas_per_sm = per_sm;
+            ctx->cfg.score_order = order;
             float ms = 0.f;
-            if ((s = time_ms(ctx, reps, [&] { return enqueue_score_state(ctx, 0); }, &ms))) break;
+            auto one = [&] {
+                S.order_valid = false;
+                return enqueue_score_state(ctx, 0);
+            };
+            if ((s = time_ms(ctx, reps, one, &ms))) break;
             if (ms < best_ms) {
                 best_ms = ms;
                 best.score_warps = nw;
                 best.score_ctas_per_sm = per_sm;
+                best.score_order = order;
             }
         }
     CK(cudaMemcpyAsync(S.res_pos.p, saved.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
@@ -1642,7 +1677,7 @@ int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* ou
         }
         CK(cudaGraphLaunch(ctx->block_graph, ctx->stream), "graph launch");
         ctx->launches += ctx->block_graph_launches;
-        S.order_valid = true;
+        S.order_valid = ctx->block_graph_order;
     } else if ((s = enqueue_block(ctx, n_steps, k, nullptr))) {
         return s;
     }

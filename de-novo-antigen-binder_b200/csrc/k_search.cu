@@ -184,9 +184,14 @@ __host__ __device__ inline size_t cg_stage_bytes(int n, int ncell) {
 
 // The antigen Calphas a CTA's residues probe (their pq / prm / cell arrays and the
 // CG grid's cell starts) are copied to shared memory at the start of the launch
-// when every residue of the CTA belongs to one antigen that fits the dynamic
-// shared memory the launch reserved (residues are ordered by antigen, then cell);
-// otherwise the kernel reads them from global memory.  Same values either way.
+// when that antigen fits the dynamic shared memory the launch reserved; residues
+// of other antigens read theirs from global memory.  Same values either way.
+//
+// Work: a warp takes NG = 32 / G residue slots at a time.  Static grid (queue
+// null): one task per warp, as many CTAs as tasks need.  Persistent grid: the
+// resident CTAs only, each warp taking tasks from the queue counter (zeroed before
+// the launch) until none is left, so that warps with residues out of contact pick
+// up the slack of those in contact.
 // register budget: 24 resident warps per SM (80 registers a thread; a 64-register
 // budget spills more than the extra occupancy gains)
 template <bool COUNT, int CG_WARPS, int G>
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
                                                              uint32_t* __restrict__ err,
                                                              long long* __restrict__ pair_count,
                                                              const int* __restrict__ order, int order_mode,
-                                                             int stage_cap) {
+                                                             int stage_cap, int stage_ag, int* __restrict__ queue) {
     constexpr int RPC = CG_WARPS * 32 / G;  // residues per CTA
     constexpr int NG = 32 / G;              // residues (lane groups) per warp
     constexpr int NA = (SLOTS + G - 1) / G; // atoms per lane
@@ -210,252 +215,273 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
     const unsigned gmask = ((1u << G) - 1u) << gshift;
     const int rl = threadIdx.x / G;                  // this group's residue slot in the CTA
     const int rl0 = (threadIdx.x & ~31) / G;         // the warp's first residue slot
-    const int slot_id = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-    // every lane of a warp stays to the end: the pair evaluation is warp-wide
-    const bool valid = slot_id < st.total_res;
-    int* list = s_list[rl];
-    int* in = s_in[rl];
-    float3* terms = s_term[rl];
-    const int r = valid ? res_of_slot(order, order_mode, slot_id, st.total_res) : 0;
-    const int c = valid ? st.res_cand[r] : 0;
-    const int r_local = valid ? r - st.cand_res_off[c] : 0;
-    const uint32_t cid = valid ? st.cand_id[c] : 0u;
-    const AgView* __restrict__ Ap = ags + (valid ? st.cand_ag[c] : 0);
-    GridView g = Ap->ca_grid;
-    const float4* __restrict__ ca_pq = Ap->ca_pq;
-    const float4* __restrict__ ca_prm = Ap->ca_prm;
-    const int4* __restrict__ ca_cell = Ap->ca_cell;
-    const float ag_cx = Ap->cx, ag_cy = Ap->cy, ag_cz = Ap->cz;
-    {
-        // stage the antigen when the CTA's first and last residues share it
-        extern __shared__ __align__(16) unsigned char cg_dyn[];
-        __shared__ int s_stage_ag;
-        const int first = blockIdx.x * (CG_WARPS * 32 / G);
-        const int last = min(first + CG_WARPS * 32 / G, st.total_res) - 1;
-        if (threadIdx.x == 0) {
-            // one antigen for the whole CTA: every residue's (orders 0 and 1 sort by
-            // antigen: the first and last tell; order 2 mixes them: check all)
-            const int ra = res_of_slot(order, order_mode, first, st.total_res);
-            const int rb = res_of_slot(order, order_mode, last, st.total_res);
-            const int a0 = st.cand_ag[st.res_cand[ra]];
-            int a1 = st.cand_ag[st.res_cand[rb]];
+    extern __shared__ __align__(16) unsigned char cg_dyn[];
+    __shared__ int s_stage_ag;
+    // stage one antigen: stage_ag when every residue of the state probes it, else
+    // (static grid) the antigen of the CTA's residues when its first and last share it
+    if (threadIdx.x == 0) {
+        int a0 = stage_ag, a1 = stage_ag;
+        if (a0 < 0 && !queue) {
+            const int first = blockIdx.x * RPC;
+            const int last = min(first + RPC, st.total_res) - 1;
+            // orders 0 and 1 sort by antigen: the first and last tell; order 2 mixes them
+            a0 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, first, st.total_res)]];
+            a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, last, st.total_res)]];
             if (order_mode == 2)
                 for (int q = first; q <= last && a1 == a0; ++q)
                     a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, q, st.total_res)]];
+        }
+        bool fits = a0 >= 0 && a0 == a1;
+        if (fits) {
             const GridView& gv = ags[a0].ca_grid;
-            const bool fits = a0 == a1 &&
-                              cg_stage_bytes(ags[a0].n_res, gv.nx * gv.ny * gv.nz) <= (size_t)stage_cap;
-            s_stage_ag = fits ? a0 : -1;
+            fits = cg_stage_bytes(ags[a0].n_res, gv.nx * gv.ny * gv.nz) <= (size_t)stage_cap;
         }
+        s_stage_ag = fits ? a0 : -1;
+    }
+    __syncthreads();
+    const int sa = s_stage_ag;
+    float4* spq = (float4*)cg_dyn;
+    float4* sprm = spq;
+    int4* scell = (int4*)cg_dyn;
+    int* sstart = (int*)cg_dyn;
+    if (sa >= 0) {
+        const AgView& S = ags[sa];
+        const int n = S.n_res, ncell = S.ca_grid.nx * S.ca_grid.ny * S.ca_grid.nz;
+        sprm = spq + n;
+        scell = (int4*)(sprm + n);
+        sstart = (int*)(scell + n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            spq[i] = S.ca_pq[i];
+            sprm[i] = S.ca_prm[i];
+            scell[i] = S.ca_cell[i];
+        }
+        for (int i = threadIdx.x; i <= ncell; i += blockDim.x) sstart[i] = S.ca_grid.cell_start[i];
         __syncthreads();
-        const int sa = s_stage_ag;
-        if (sa >= 0) {
-            const AgView& S = ags[sa];
-            const int n = S.n_res, ncell = S.ca_grid.nx * S.ca_grid.ny * S.ca_grid.nz;
-            float4* spq = (float4*)cg_dyn;
-            float4* sprm = spq + n;
-            int4* scell = (int4*)(sprm + n);
-            int* sstart = (int*)(scell + n);
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                spq[i] = S.ca_pq[i];
-                sprm[i] = S.ca_prm[i];
-                scell[i] = S.ca_cell[i];
-            }
-            for (int i = threadIdx.x; i <= ncell; i += blockDim.x) sstart[i] = S.ca_grid.cell_start[i];
-            __syncthreads();
-            if (valid) {  // every valid residue of the CTA probes antigen sa
-                ca_pq = spq;
-                ca_prm = sprm;
-                ca_cell = scell;
-                g.cell_start = sstart;
-            }
-        }
     }
-    const int aa = valid ? st.res_aa[r] : 0;
-    const int n_at = valid ? s_topo_n[aa] : 0;
-    const float4 res = s_res[aa];
-    float4* slot = st.res_pos + (size_t)r * SLOT_STRIDE;
-    F3 ca = {0.f, 0.f, 0.f};
-    if (valid) {
-        const float4 v1 = slot[1];  // Calpha = topology atom 1 of every residue (amber.rs:358-377)
-        ca = {v1.x, v1.y, v1.z};
-        if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
-    }
-    float4 at[NA];
+    // one task: the residue of this lane group's slot, n_steps gradient steps
+    auto residue_task = [&](const int slot_id) {
+        // every lane of a warp stays to the end: the pair evaluation is warp-wide
+        const bool valid = slot_id < st.total_res;
+        int* list = s_list[rl];
+        int* in = s_in[rl];
+        float3* terms = s_term[rl];
+        const int r = valid ? res_of_slot(order, order_mode, slot_id, st.total_res) : 0;
+        const int c = valid ? st.res_cand[r] : 0;
+        const int r_local = valid ? r - st.cand_res_off[c] : 0;
+        const uint32_t cid = valid ? st.cand_id[c] : 0u;
+        const AgView* __restrict__ Ap = ags + (valid ? st.cand_ag[c] : 0);
+        GridView g = Ap->ca_grid;
+        const float4* __restrict__ ca_pq = Ap->ca_pq;
+        const float4* __restrict__ ca_prm = Ap->ca_prm;
+        const int4* __restrict__ ca_cell = Ap->ca_cell;
+        const float ag_cx = Ap->cx, ag_cy = Ap->cy, ag_cz = Ap->cz;
+        if (valid && st.cand_ag[c] == sa) {  // the staged antigen
+            ca_pq = spq;
+            ca_prm = sprm;
+            ca_cell = scell;
+            g.cell_start = sstart;
+        }
+        const int aa = valid ? st.res_aa[r] : 0;
+        const int n_at = valid ? s_topo_n[aa] : 0;
+        const float4 res = s_res[aa];
+        float4* slot = st.res_pos + (size_t)r * SLOT_STRIDE;
+        F3 ca = {0.f, 0.f, 0.f};
+        if (valid) {
+            const float4 v1 = slot[1];  // Calpha = topology atom 1 of every residue (amber.rs:358-377)
+            ca = {v1.x, v1.y, v1.z};
+            if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
+        }
+        float4 at[NA];
 #pragma unroll
-    for (int j = 0; j < NA; ++j) {
-        const int k = gl + G * j;
-        at[j] = (!COUNT && k < n_at) ? slot[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    // the residue's list from the previous launch when it was built for this antigen
-    // set and antigen and still covers the Calpha, else a new one
-    F3 centre = ca;
-    int nl = 0;
-    bool dirty = false;
-    float skin = CG_SKIN;
-    if (valid) {
-        const int ep = st.ag_epoch ? *st.ag_epoch : -2;
-        const int4 meta = st.cg_meta ? st.cg_meta[r] : make_int4(-1, -1, -1, -1);
-        bool reuse = false;
-        float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ep >= 0 && meta.z == ep && meta.y == st.cand_ag[c] && meta.x >= 0 && meta.x <= CG_LIST_MAX) {
-            cc = st.cg_centre[r];
-            skin = fminf(fmaxf(cc.w, CG_SKIN), CG_SKIN_MAX);
-            const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
-            reuse = mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f);
-            if (!reuse) skin = fminf(2.0f * skin, CG_SKIN_MAX);  // it outran the list
+        for (int j = 0; j < NA; ++j) {
+            const int k = gl + G * j;
+            at[j] = (!COUNT && k < n_at) ? slot[k] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (reuse) {
-            centre = {cc.x, cc.y, cc.z};
-            nl = meta.x;
-            for (int j = gl; j < nl; j += G) list[j] = st.cg_list[(size_t)r * CG_LIST_MAX + j];
-            __syncwarp(gmask);
-        } else {
-            nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list, skin);
-            dirty = true;
-        }
-    }
-    int n_pairs = 0;
-    for (int s = 0; s < n_steps; ++s) {
-        const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
-        bool use_list = valid && nl <= CG_LIST_MAX && !cell_far(cx, cy, cz);
-        // A-C in rounds: each round a group compacts its next in-cutoff list entries
-        // (adjacent cell, r^2 passing the reference's cutoff test; list order) up to
-        // CG_IN_MAX, the warp evaluates every group's compacted pairs one pair per lane,
-        // and lane 0 of each group continues its sum in order -- the reference's sum,
-        // however many rounds a residue needs.
-        float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        int from = 0;  // next list entry of this group
-        bool more = use_list;
-        while (__any_sync(0xffffffffu, more)) {
-            int n_in = 0;
-            if (more) {
-                while (from < nl && n_in + G <= CG_IN_MAX) {
-                    const int j = from + gl;
-                    bool ok = false;
-                    int i = 0;
-                    if (j < nl) {
-                        i = list[j];
-                        const int4 ce = ca_cell[i];
-                        if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
-                            abs((long long)ce.z - cz) <= 1) {
-                            const float4 a = ca_pq[i];
-                            const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
-                            ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
-                        }
-                    }
-                    const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << G) - 1u);
-                    if (ok) in[n_in + __popc(m & ((1u << gl) - 1u))] = i;
-                    n_in += __popc(m);
-                    from += G;
-                }
-                if (COUNT && gl == 0) n_pairs += n_in;
+        // the residue's list from the previous launch when it was built for this antigen
+        // set and antigen and still covers the Calpha, else a new one
+        F3 centre = ca;
+        int nl = 0;
+        bool dirty = false;
+        float skin = CG_SKIN;
+        if (valid) {
+            const int ep = st.ag_epoch ? *st.ag_epoch : -2;
+            const int4 meta = st.cg_meta ? st.cg_meta[r] : make_int4(-1, -1, -1, -1);
+            bool reuse = false;
+            float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ep >= 0 && meta.z == ep && meta.y == st.cand_ag[c] && meta.x >= 0 && meta.x <= CG_LIST_MAX) {
+                cc = st.cg_centre[r];
+                skin = fminf(fmaxf(cc.w, CG_SKIN), CG_SKIN_MAX);
+                const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
+                reuse = mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f);
+                if (!reuse) skin = fminf(2.0f * skin, CG_SKIN_MAX);  // it outran the list
             }
-            // B. the round's pair terms of every residue of the warp, one pair per lane
-            int pre[NG + 1];
-            pre[0] = 0;
-#pragma unroll
-            for (int q = 0; q < NG; ++q) pre[q + 1] = pre[q] + __shfl_sync(0xffffffffu, n_in, q * G);
-            const int total = pre[NG];
-            for (int base = 0; base < total; base += 32) {
-                const int pidx = base + lane;
-                int q = 0;
-#pragma unroll
-                for (int t = 1; t < NG; ++t) q += pidx >= pre[t] ? 1 : 0;
-                const int src = q * G;
-                const CgB body{__shfl_sync(0xffffffffu, ca.x, src), __shfl_sync(0xffffffffu, ca.y, src),
-                               __shfl_sync(0xffffffffu, ca.z, src), __shfl_sync(0xffffffffu, res.x, src),
-                               __shfl_sync(0xffffffffu, res.y, src), __shfl_sync(0xffffffffu, res.z, src),
-                               __shfl_sync(0xffffffffu, res.w, src)};
-                if (pidx < total) {
-                    const int k = pidx - pre[q];
-                    const int i = s_in[rl0 + q][k];
-                    float tx, ty, tz;
-                    cg_term_parts(body, ca_pq[i], ca_prm[i], tx, ty, tz);
-                    s_term[rl0 + q][k] = make_float3(tx, ty, tz);
-                }
-            }
-            __syncwarp();
-            // C. lane 0 of each group continues its sum in order
-            if (gl == 0)
-                for (int k = 0; k < n_in; ++k) {
-                    const float3 t = terms[k];
-                    sx = xadd(sx, t.x);
-                    sy = xadd(sy, t.y);
-                    sz = xadd(sz, t.z);
-                }
-            __syncwarp();  // term slots are rewritten next round
-            more = more && from < nl;
-        }
-        if (gl == 0 && valid && !use_list) {  // list overflow or cells near the i32 limits
-            int np = 0;
-            float3 f;
-            cg_force_walk<COUNT>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
-            sx = f.x; sy = f.y; sz = f.z;
-            if (COUNT) n_pairs += np;
-        }
-        float fx = __shfl_sync(0xffffffffu, sx, gshift), fy = __shfl_sync(0xffffffffu, sy, gshift),
-              fz = __shfl_sync(0xffffffffu, sz, gshift);
-        if (!valid) continue;  // uniform per group; the warp-wide shuffles above were all taken
-        // harmonic restraint toward the shell (diffusion.rs:317-327)
-        const float dx_c = xsub(ca.x, ag_cx), dy_c = xsub(ca.y, ag_cy), dz_c = xsub(ca.z, ag_cz);
-        const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
-        const float excess = xsub(d, p.shell_radius);
-        const float f_r = xdiv(xmul(-p.restraint_k, excess), d);
-        fx = xadd(fx, xmul(f_r, dx_c));
-        fy = xadd(fy, xmul(f_r, dy_c));
-        fz = xadd(fz, xmul(f_r, dz_c));
-        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
-        if (with_noise) {
-            const float temp = temps ? temps[s] : p.t_hot;
-            const float sigma = xmul(p.noise_base, xsqrt(temp));
-            const U4 u = rng_draw(p.seed, cid, step0 + (uint32_t)s, STREAM_NOISE, (uint32_t)r_local);
-            nx = frange(u.x, -sigma, sigma);
-            ny = frange(u.y, -sigma, sigma);
-            nz = frange(u.z, -sigma, sigma);
-        }
-        const float md = p.max_disp;
-        const F3 new_ca = {xadd(xadd(ca.x, fminf(fmaxf(xmul(p.step, fx), -md), md)), nx),
-                           xadd(xadd(ca.y, fminf(fmaxf(xmul(p.step, fy), -md), md)), ny),
-                           xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
-        // set_ca_pos: delta = new - old; every atom (the Calpha included) += delta
-        const F3 dl = sub3(new_ca, ca);
-        if (!COUNT) {
-#pragma unroll
-            for (int j = 0; j < NA; ++j) {
-                at[j].x = xadd(at[j].x, dl.x);
-                at[j].y = xadd(at[j].y, dl.y);
-                at[j].z = xadd(at[j].z, dl.z);
-            }
-        }
-        ca = {xadd(ca.x, dl.x), xadd(ca.y, dl.y), xadd(ca.z, dl.z)};
-        if (s + 1 < n_steps) {
-            const float mx = ca.x - centre.x, my = ca.y - centre.y, mz = ca.z - centre.z;
-            if (!(mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f))) {
-                // left the skin (or NaN): a new list with twice the skin
-                skin = fminf(2.0f * skin, CG_SKIN_MAX);
-                centre = ca;
+            if (reuse) {
+                centre = {cc.x, cc.y, cc.z};
+                nl = meta.x;
+                for (int j = gl; j < nl; j += G) list[j] = st.cg_list[(size_t)r * CG_LIST_MAX + j];
+                __syncwarp(gmask);
+            } else {
                 nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list, skin);
                 dirty = true;
             }
         }
-    }
-    if (!valid) return;
-    if (!COUNT && dirty && st.cg_meta) {  // keep the list for the next launch
-        for (int j = gl; j < min(nl, CG_LIST_MAX); j += G) st.cg_list[(size_t)r * CG_LIST_MAX + j] = list[j];
-        if (gl == 0) {
-            st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
-            st.cg_meta[r] = make_int4(nl, st.cand_ag[c], st.ag_epoch ? *st.ag_epoch : -2, 0);
-        }
-    }
-    if (COUNT) {
-        if (gl == 0 && n_pairs) atomicAdd((unsigned long long*)pair_count, (unsigned long long)n_pairs);
-        return;
-    }
+        int n_pairs = 0;
+        for (int s = 0; s < n_steps; ++s) {
+            const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
+            bool use_list = valid && nl <= CG_LIST_MAX && !cell_far(cx, cy, cz);
+            // A-C in rounds: each round a group compacts its next in-cutoff list entries
+            // (adjacent cell, r^2 passing the reference's cutoff test; list order) up to
+            // CG_IN_MAX, the warp evaluates every group's compacted pairs one pair per lane,
+            // and lane 0 of each group continues its sum in order -- the reference's sum,
+            // however many rounds a residue needs.
+            float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+            int from = 0;  // next list entry of this group
+            bool more = use_list;
+            while (__any_sync(0xffffffffu, more)) {
+                int n_in = 0;
+                if (more) {
+                    while (from < nl && n_in + G <= CG_IN_MAX) {
+                        const int j = from + gl;
+                        bool ok = false;
+                        int i = 0;
+                        if (j < nl) {
+                            i = list[j];
+                            const int4 ce = ca_cell[i];
+                            if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
+                                abs((long long)ce.z - cz) <= 1) {
+                                const float4 a = ca_pq[i];
+                                const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
+                                ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                            }
+                        }
+                        const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << G) - 1u);
+                        if (ok) in[n_in + __popc(m & ((1u << gl) - 1u))] = i;
+                        n_in += __popc(m);
+                        from += G;
+                    }
+                    if (COUNT && gl == 0) n_pairs += n_in;
+                }
+                // B. the round's pair terms of every residue of the warp, one pair per lane
+                int pre[NG + 1];
+                pre[0] = 0;
 #pragma unroll
-    for (int j = 0; j < NA; ++j) {
-        const int k = gl + G * j;
-        if (k < n_at) slot[k] = at[j];
+                for (int q = 0; q < NG; ++q) pre[q + 1] = pre[q] + __shfl_sync(0xffffffffu, n_in, q * G);
+                const int total = pre[NG];
+                for (int base = 0; base < total; base += 32) {
+                    const int pidx = base + lane;
+                    int q = 0;
+#pragma unroll
+                    for (int t = 1; t < NG; ++t) q += pidx >= pre[t] ? 1 : 0;
+                    const int src = q * G;
+                    const CgB body{__shfl_sync(0xffffffffu, ca.x, src), __shfl_sync(0xffffffffu, ca.y, src),
+                                   __shfl_sync(0xffffffffu, ca.z, src), __shfl_sync(0xffffffffu, res.x, src),
+                                   __shfl_sync(0xffffffffu, res.y, src), __shfl_sync(0xffffffffu, res.z, src),
+                                   __shfl_sync(0xffffffffu, res.w, src)};
+                    if (pidx < total) {
+                        const int k = pidx - pre[q];
+                        const int i = s_in[rl0 + q][k];
+                        float tx, ty, tz;
+                        cg_term_parts(body, ca_pq[i], ca_prm[i], tx, ty, tz);
+                        s_term[rl0 + q][k] = make_float3(tx, ty, tz);
+                    }
+                }
+                __syncwarp();
+                // C. lane 0 of each group continues its sum in order
+                if (gl == 0)
+                    for (int k = 0; k < n_in; ++k) {
+                        const float3 t = terms[k];
+                        sx = xadd(sx, t.x);
+                        sy = xadd(sy, t.y);
+                        sz = xadd(sz, t.z);
+                    }
+                __syncwarp();  // term slots are rewritten next round
+                more = more && from < nl;
+            }
+            if (gl == 0 && valid && !use_list) {  // list overflow or cells near the i32 limits
+                int np = 0;
+                float3 f;
+                cg_force_walk<COUNT>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
+                sx = f.x; sy = f.y; sz = f.z;
+                if (COUNT) n_pairs += np;
+            }
+            float fx = __shfl_sync(0xffffffffu, sx, gshift), fy = __shfl_sync(0xffffffffu, sy, gshift),
+                  fz = __shfl_sync(0xffffffffu, sz, gshift);
+            if (!valid) continue;  // uniform per group; the warp-wide shuffles above were all taken
+            // harmonic restraint toward the shell (diffusion.rs:317-327)
+            const float dx_c = xsub(ca.x, ag_cx), dy_c = xsub(ca.y, ag_cy), dz_c = xsub(ca.z, ag_cz);
+            const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
+            const float excess = xsub(d, p.shell_radius);
+            const float f_r = xdiv(xmul(-p.restraint_k, excess), d);
+            fx = xadd(fx, xmul(f_r, dx_c));
+            fy = xadd(fy, xmul(f_r, dy_c));
+            fz = xadd(fz, xmul(f_r, dz_c));
+            float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+            if (with_noise) {
+                const float temp = temps ? temps[s] : p.t_hot;
+                const float sigma = xmul(p.noise_base, xsqrt(temp));
+                const U4 u = rng_draw(p.seed, cid, step0 + (uint32_t)s, STREAM_NOISE, (uint32_t)r_local);
+                nx = frange(u.x, -sigma, sigma);
+                ny = frange(u.y, -sigma, sigma);
+                nz = frange(u.z, -sigma, sigma);
+            }
+            const float md = p.max_disp;
+            const F3 new_ca = {xadd(xadd(ca.x, fminf(fmaxf(xmul(p.step, fx), -md), md)), nx),
+                               xadd(xadd(ca.y, fminf(fmaxf(xmul(p.step, fy), -md), md)), ny),
+                               xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
+            // set_ca_pos: delta = new - old; every atom (the Calpha included) += delta
+            const F3 dl = sub3(new_ca, ca);
+            if (!COUNT) {
+#pragma unroll
+                for (int j = 0; j < NA; ++j) {
+                    at[j].x = xadd(at[j].x, dl.x);
+                    at[j].y = xadd(at[j].y, dl.y);
+                    at[j].z = xadd(at[j].z, dl.z);
+                }
+            }
+            ca = {xadd(ca.x, dl.x), xadd(ca.y, dl.y), xadd(ca.z, dl.z)};
+            if (s + 1 < n_steps) {
+                const float mx = ca.x - centre.x, my = ca.y - centre.y, mz = ca.z - centre.z;
+                if (!(mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f))) {
+                    // left the skin (or NaN): a new list with twice the skin
+                    skin = fminf(2.0f * skin, CG_SKIN_MAX);
+                    centre = ca;
+                    nl = build_cg_list<G>(g, ca_pq, centre, gl, gmask, list, skin);
+                    dirty = true;
+                }
+            }
+        }
+        if (!valid) return;  // ends this task
+        if (!COUNT && dirty && st.cg_meta) {  // keep the list for the next launch
+            for (int j = gl; j < min(nl, CG_LIST_MAX); j += G) st.cg_list[(size_t)r * CG_LIST_MAX + j] = list[j];
+            if (gl == 0) {
+                st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
+                st.cg_meta[r] = make_int4(nl, st.cand_ag[c], st.ag_epoch ? *st.ag_epoch : -2, 0);
+            }
+        }
+        if (COUNT) {
+            if (gl == 0 && n_pairs) atomicAdd((unsigned long long*)pair_count, (unsigned long long)n_pairs);
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < NA; ++j) {
+            const int k = gl + G * j;
+            if (k < n_at) slot[k] = at[j];
+        }
+    };
+    // tasks of NG residue slots, one per warp: the warp's own (static grid) or taken
+    // from the work queue until it runs dry (persistent grid); warp-uniform
+    int task = blockIdx.x * CG_WARPS + (int)(threadIdx.x >> 5);
+    for (;;) {
+        if (queue) {
+            __syncwarp();  // the last task's list reads are done before the next writes
+            int t = 0;
+            if (lane == 0) t = atomicAdd(queue, 1);
+            task = __shfl_sync(0xffffffffu, t, 0);
+        }
+        if ((long long)task * NG >= st.total_res) break;
+        const int slot_id = task * NG + lane / G;
+        residue_task(slot_id);
+        if (!queue) break;
     }
 }
 
@@ -514,24 +540,36 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
 template <int W, int G>
 static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                       uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                      int order_mode, int stage_bytes) {
+                      int order_mode, int stage_bytes, int stage_ag, int* queue) {
     const int threads = W * 32;
     const long long total = (long long)st.total_res * G;
-    if (stage_bytes > 0)
-        cudaFuncSetAttribute(k_langevin<false, W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
-    k_langevin<false, W, G><<<(int)((total + threads - 1) / threads), threads, stage_bytes, s>>>(
-        st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order, order_mode, stage_bytes);
+    long long ctas = (total + threads - 1) / threads;
+    auto kern = k_langevin<false, W, G>;
+    if (stage_bytes > 0) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
+    if (queue) {  // persistent: the CTAs that are resident at once
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, stage_bytes);
+        ctas = std::min(ctas, (long long)std::max(1, sms * std::max(per_sm, 1)));
+        cudaMemsetAsync(queue, 0, sizeof(int), s);
+    }
+    kern<<<(int)ctas, threads, stage_bytes, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order,
+                                                 order_mode, stage_bytes, stage_ag, queue);
 }
 
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells) {
+                    int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
+                    int stage_ag, int* queue) {
     if (st.total_res <= 0 || n_steps <= 0) return;
     if (order_mode == 2 && st.total_res % CG_STRIDE == 0) order_mode = 1;  // stride not a bijection
     // antigen staging: up to 96 KB of dynamic shared memory per CTA
     const size_t sb = cg_stage_bytes(max_ag_res, max_ag_cells);
     const int stage = sb <= 96 * 1024 ? (int)sb : 0;
-#define BINDER_DIFFUSE(W, G) diffuse_w<W, G>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage)
+#define BINDER_DIFFUSE(W, G)                                                                                 \
+    diffuse_w<W, G>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage,               \
+                    stage ? stage_ag : -1, queue)
     if (lanes_per_res == 8) {
         switch (warps_per_cta) {
             case 2: BINDER_DIFFUSE(2, 8); break;
@@ -551,7 +589,7 @@ void launch_diffuse_count(cudaStream_t s, const StateView& st, const AgView* ags
     const int threads = 4 * 32;
     const long long total = (long long)st.total_res * 4;
     k_langevin<true, 4, 4><<<(int)((total + threads - 1) / threads), threads, 0, s>>>(
-        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr, 1, 0);
+        st, ags, p, n_steps, 0, 0, nullptr, nullptr, pairs, nullptr, 1, 0, -1, nullptr);
 }
 
 }  // namespace binder

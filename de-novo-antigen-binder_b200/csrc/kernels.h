@@ -16,6 +16,8 @@ struct LaunchCfg {
     int cg_warps = 8;            // warps per CTA of the gradient-step kernel (2, 4, 8)
     int cg_lanes = 8;            // lanes per residue of the gradient-step kernel (4, 8)
     int cg_order = 1;            // residue order of the gradient-step kernel: 0 cell, 1 candidate, 2 strided
+    int score_order = 0;         // work-queue order of the scoring kernel: 0 cell, 1 residue index
+    int cg_queue = 1;            // gradient-step kernel: 0 static grid, 1 persistent CTAs on a work queue
 };
 
 // ---- k_grid.cu: SpatialHashGrid ----
@@ -73,7 +75,8 @@ void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const f
                       const uint8_t* baa, int n, float* fx, float* fy, float* fz);
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
-                    int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells);
+                    int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
+                    int stage_ag, int* queue);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);

@@ -291,6 +291,10 @@ typedef struct binder_launch_cfg {
                                    warps per CTA) or 8 */
     int32_t cg_order;           /* residue order of the gradient-step kernel: 0 by Calpha cell,
                                    1 candidate after candidate, 2 strided (work spread out) */
+    int32_t score_order;        /* work-queue order of the scoring kernel: 0 by Calpha cell (three
+                                   sorting launches after every move), 1 residue index */
+    int32_t cg_queue;           /* gradient-step kernel: 0 one CTA per residue batch, 1 persistent
+                                   CTAs whose warps take residue batches from a work queue */
 } binder_launch_cfg;
 int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
