@@ -36,10 +36,10 @@ namespace binder {
 cudaError_t anneal_init_tables() { return geom_init_tables(); }
 
 // log1p of the environment counts for the in-kernel features (the same host table
-// as the feature kernel's)
-__constant__ float c_an_log1p[MLP_COUNT_CAP + 1];
+// as the feature kernel's); global memory, since the lanes of a warp index it apart
+__device__ float g_an_log1p[MLP_COUNT_CAP + 1];
 cudaError_t anneal_init_mlp_table(const float* t) {
-    return cudaMemcpyToSymbol(c_an_log1p, t, sizeof(float) * (MLP_COUNT_CAP + 1));
+    return cudaMemcpyToSymbol(g_an_log1p, t, sizeof(float) * (MLP_COUNT_CAP + 1));
 }
 
 constexpr int AN_WARPS = 8;
@@ -52,7 +52,7 @@ constexpr int AG_STAGE_MAX = 1024;                   // antigen Calphas staged i
 constexpr int CELL_STAGE_MAX = 4096;                 // Calpha-grid cells staged in shared memory
 enum : int { MV_NONE = 0, MV_ROT = 1, MV_MUT = 2 };
 enum : int { SEL_KEEP = 0, SEL_PROP = 1, SEL_REJ = 2 };
-enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3, IS_NMV = 4, IS_NMV2 = 5 };
+enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3, IS_NMV = 4 };
 
 // Shared-memory carve of one CTA for candidates of up to R residues and antigens
 // of up to G staged Calphas.
@@ -74,7 +74,7 @@ struct AnSmem {
     double *lhr, *lqf;              // R: log Hastings ratio of the move, log q of the forward mutation
     float *u_acc, *bb_u;            // R
     int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
-    int *rot, *mvl, *mv2;           // R: rotamer index of the state (-1 unknown), residues with a move
+    int *rot, *mvl;                 // R: rotamer index of the state (-1 unknown), residues with a move
     uint32_t* dz;                   // R: the move's choice draw
     int* iscal;
 };
@@ -89,7 +89,7 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 * 2 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
-           (size_t)R * 4 * 4 + 32;
+           (size_t)R * 4 * 3 + 32;
 }
 __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
     AnSmem s;
@@ -130,7 +130,6 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.tcount = (int*)take((size_t)L * 4);
     s.rot = (int*)take((size_t)R * 4);
     s.mvl = (int*)take((size_t)R * 4);
-    s.mv2 = (int*)take((size_t)R * 4);
     s.dz = (uint32_t*)take((size_t)R * 4);
     s.iscal = (int*)take(32);
     return s;
@@ -263,10 +262,10 @@ __device__ __forceinline__ bool mh_accept(ACC de, float temp, float u, double lh
 }
 
 // ---- learned proposal -------------------------------------------------------------
-// Features of the tile rows: row i = residue mvl[base + i] with amino acid
-// (prop ? new_aa : aa); one warp per row (rows i and i + 8).
+// Features of the tile rows: row i = residue mvl[base + i] with its amino acid; one
+// warp per row (rows i and i + 8).
 __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* rows_of, int base, int rows,
-                                 const float4* agq, const uint8_t* ag_aa, int nag, bool prop) {
+                                 const float4* agq, const uint8_t* ag_aa, int nag) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = warp; i < MT_ROWS; i += AN_WARPS) {
         int* cnt = T.cnt + i * MLP_SHELLS * N_AA;
@@ -281,11 +280,11 @@ __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* r
         const float4 ca = S.pos[r * SLOT_STRIDE + 1];
         mlp_count_env(agq, ag_aa, nag, ca.x, ca.y, ca.z, cnt);
         __syncwarp();
-        const int a = prop ? S.new_aa[r] : S.aa[r];
+        const int a = S.aa[r];
         for (int j = lane; j < MLP_K1; j += 32) {
             float v = 0.0f;
             if (j < N_AA) v = j == a ? 1.0f : 0.0f;
-            else if (j < MLP_IN) v = c_an_log1p[min(cnt[j - N_AA], MLP_COUNT_CAP)];
+            else if (j < MLP_IN) v = __ldg(&g_an_log1p[min(cnt[j - N_AA], MLP_COUNT_CAP)]);
             x[j] = __float2bfloat16_rn(v);
         }
     }
@@ -459,12 +458,18 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
 }
 
 // The network's choice of every mutation and (known-rotamer) rotamer move drawn
-// this step and the moves' log Hastings ratios (all threads of the CTA call).
+// this step and the moves' log Hastings ratios (all threads of the CTA call).  Per
+// tile of moves: features, a forward pass, the draws; then the mutation rows' one-hot
+// moved to the drawn amino acid in place -- the features of the proposed state, the
+// environment counts being the same -- and a second pass gives their reverse
+// probabilities by the same code.  Each pass's first weights are fetched ahead.
 __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const float4* agq, const uint8_t* ag_aa,
                                                 int nag, const MlpDev& mlp, float temp) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const MlpTile T = mlp_tile_carve((unsigned char*)S.terms);
     const float tp = fmaxf(temp, mlp.t_prop_min);
+    uint4 w[MT_WREGS];
+    mlp_tile_prefetch(mlp, w);
     if (tid == 0) {  // mutations, and rotamer moves from a known library rotamer
         int k = 0;
         for (int r = 0; r < n; ++r)
@@ -475,9 +480,12 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
     const int n_mv = S.iscal[IS_NMV];
     for (int base = 0; base < n_mv; base += MT_ROWS) {
         const int rows = min(MT_ROWS, n_mv - base);
-        an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag, false);
+        if (base > 0) mlp_tile_prefetch(mlp, w);
+        an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag);
         __syncthreads();
-        mlp_tile_forward(mlp, T);
+        mlp_tile_forward(mlp, T, w, rows);
+        mlp_tile_prefetch(mlp, w);  // the reverse pass's
+        bool mut = false;
         for (int i = warp; i < rows; i += AN_WARPS) {  // one warp per row
             const int r = S.mvl[base + i];
             const float* y = T.y + i * MT_YS;
@@ -494,33 +502,26 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
                 if (lane == 0) {
                     S.new_aa[r] = a;
                     S.lqf[r] = lq;
+                    __nv_bfloat16* x = T.x + i * MT_XS;
+                    x[S.aa[r]] = __float2bfloat16_rn(0.0f);
+                    x[a] = __float2bfloat16_rn(1.0f);
                 }
+                mut = true;
             }
         }
-        __syncthreads();
-    }
-    // reverse probabilities of the mutations: the network at the proposed amino acid
-    if (tid == 0) {
-        int k = 0;
-        for (int j = 0; j < n_mv; ++j)
-            if (S.kind[S.mvl[j]] == MV_MUT) S.mv2[k++] = S.mvl[j];
-        S.iscal[IS_NMV2] = k;
-    }
-    __syncthreads();
-    const int n_mv2 = S.iscal[IS_NMV2];
-    for (int base = 0; base < n_mv2; base += MT_ROWS) {
-        const int rows = min(MT_ROWS, n_mv2 - base);
-        an_tile_features(S, T, S.mv2, base, rows, agq, ag_aa, nag, true);
-        __syncthreads();
-        mlp_tile_forward(mlp, T);
-        for (int i = warp; i < rows; i += AN_WARPS) {
-            const int r = S.mv2[base + i];
-            const float* y = T.y + i * MT_YS;
-            double lz;
-            warp_softmax(y, N_AA, tp, &lz);
-            if (lane == 0) S.lhr[r] = (-(double)y[S.aa[r]] / (double)tp - lz) - S.lqf[r];
+        // reverse probabilities of the mutations: the network at the proposed amino acid
+        if (__syncthreads_or(mut)) {
+            mlp_tile_forward(mlp, T, w, rows);
+            for (int i = warp; i < rows; i += AN_WARPS) {
+                const int r = S.mvl[base + i];
+                if (S.kind[r] != MV_MUT) continue;
+                const float* y = T.y + i * MT_YS;
+                double lz;
+                warp_softmax(y, N_AA, tp, &lz);
+                if (lane == 0) S.lhr[r] = (-(double)y[S.aa[r]] / (double)tp - lz) - S.lqf[r];
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 

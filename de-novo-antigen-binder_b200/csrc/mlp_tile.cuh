@@ -3,8 +3,8 @@
 // a step: a handful of rows, below the 64/128-row tiles of tcgen05.mma, so the
 // CTA's eight warps use the warp-level BF16 MMA, m16n8k16 with FP32 accumulators).
 // Weights are read from global memory (L2-resident, 240 KB) in fragment order with
-// 16-byte loads, double-buffered in registers; activations stay in shared memory as
-// BF16, the output as FP32.  Same arithmetic as the batched
+// 16-byte loads, in a few large register batches per layer; activations stay in
+// shared memory as BF16, the output as FP32.  Same arithmetic as the batched
 // tensor-core path up to the order of the FP32 sums.
 #pragma once
 
@@ -52,39 +52,50 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 
 __device__ __forceinline__ uint32_t ld_s32(const __nv_bfloat16* p) { return *(const uint32_t*)p; }
 __device__ __forceinline__ uint4 ld_g128(const uint4* p) { return __ldg(p); }
-__device__ __forceinline__ float silu_f(float z) { return z / (1.0f + expf(-z)); }
+// SiLU as the batched GEMM epilogue computes it: z * sigmoid, sigmoid = 1 / (1 + e^-z)
+// with the fast exponential and a correctly rounded reciprocal
+__device__ __forceinline__ float silu_f(float z) { return z * __frcp_rn(1.0f + __expf(-z)); }
+
+// Weight registers of a lane: one batch of a layer's fragments (16 bytes per n-tile
+// per pair of k-steps), at most MT_WREGS of them.
+constexpr int MT_WREGS = 16;
+
+// Batch bi of a layer's weights for the warp's n-tiles n_tile0 .. n_tile0+NT-1:
+// pairs of k-steps bi*PB .. bi*PB+PB-1.
+template <int K, int NT, int PB>
+__device__ __forceinline__ void mlp_tile_fetch(uint4 (&w)[MT_WREGS], const uint4* __restrict__ Wf, int n_tile0,
+                                               int bi) {
+    static_assert(NT * PB <= MT_WREGS, "weight batch larger than the registers");
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int p = 0; p < PB; ++p)
+#pragma unroll
+        for (int t = 0; t < NT; ++t) w[p * NT + t] = ld_g128(Wf + frag_index(n_tile0 + t, bi * PB + p, lane, K));
+}
 
 // One dense layer on the tile: out[16][cols of the warp] = act(in[16][K] W^T + b).
 // Warp w computes the n-tiles n_tile0 .. n_tile0+NT-1 (8 columns each); ACT = SiLU to
-// BF16 (out_h) or identity to FP32 (out_f).  The warp's weights (fragment order,
-// 16 bytes per lane per pair of k-steps) stream through registers in batches of
-// two pairs, the next batch in flight while the current one is multiplied.
-template <int K, int NT, bool ACT>
-__device__ __forceinline__ void mlp_tile_layer(const __nv_bfloat16* in, int in_stride, const uint4* Wf,
-                                               const float* bias, __nv_bfloat16* out_h, int out_stride,
-                                               float* out_f, int n_tile0) {
+// BF16 (out_h) or identity to FP32 (out_f).  The weights (fragment order, L2-resident)
+// come in batches of PB pairs of k-steps: w holds batch 0 on entry; each batch is
+// multiplied, then the registers are refilled with the next one -- after the last
+// batch with batch 0 of the next layer (Wn: K2 / NT2 / PB2 at n-tile n_next; none
+// when null), so that its latency hides behind this layer's epilogue and barrier.
+// Rows >= rows hold no move: the epilogue writes them as zeros without evaluating
+// the activation (the MMA rows are independent of each other).
+template <int K, int NT, int PB, bool ACT, int K2, int NT2, int PB2>
+__device__ __forceinline__ void mlp_tile_layer(uint4 (&w)[MT_WREGS], const __nv_bfloat16* in, int in_stride,
+                                               const uint4* __restrict__ Wf, int n_tile0, const float* bias,
+                                               __nv_bfloat16* out_h, int out_stride, float* out_f,
+                                               const uint4* __restrict__ Wn, int n_next, int rows) {
     constexpr int SP = K / 32;   // pairs of k-steps
-    constexpr int PB = 2;        // pairs per batch
     constexpr int NB = SP / PB;  // batches
-    static_assert(SP % PB == 0, "K must be a multiple of 64");
+    static_assert(SP % PB == 0, "batches must split the k-step pairs evenly");
     const int lane = threadIdx.x & 31, g = lane >> 2, tg = lane & 3;
     float acc[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0f;
-    uint4 buf[2][PB][NT];
-#pragma unroll
-    for (int p = 0; p < PB; ++p)
-#pragma unroll
-        for (int t = 0; t < NT; ++t) buf[0][p][t] = ld_g128(Wf + frag_index(n_tile0 + t, p, lane, K));
 #pragma unroll
     for (int bi = 0; bi < NB; ++bi) {
-        if (bi + 1 < NB) {
-#pragma unroll
-            for (int p = 0; p < PB; ++p)
-#pragma unroll
-                for (int t = 0; t < NT; ++t)
-                    buf[(bi + 1) & 1][p][t] = ld_g128(Wf + frag_index(n_tile0 + t, (bi + 1) * PB + p, lane, K));
-        }
 #pragma unroll
         for (int p = 0; p < PB; ++p)
 #pragma unroll
@@ -97,38 +108,61 @@ __device__ __forceinline__ void mlp_tile_layer(const __nv_bfloat16* in, int in_s
                 a[3] = ld_s32(in + (g + 8) * in_stride + k0 + 8 + 2 * tg);
 #pragma unroll
                 for (int t = 0; t < NT; ++t) {
-                    const uint4 v = buf[bi & 1][p][t];
+                    const uint4 v = w[p * NT + t];
                     mma_bf16_16816(acc[t], a, h ? v.z : v.x, h ? v.w : v.y);
                 }
             }
+        if (bi + 1 < NB) mlp_tile_fetch<K, NT, PB>(w, Wf, n_tile0, bi + 1);
+        else if (Wn) mlp_tile_fetch<K2, NT2, PB2>(w, Wn, n_next, 0);
     }
+    const bool lo = g < rows, hi = g + 8 < rows;
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
         const int c = (n_tile0 + t) * 8 + 2 * tg;
         const float b0 = bias[c], b1 = bias[c + 1];
         if (ACT) {
-            out_h[g * out_stride + c] = __float2bfloat16_rn(silu_f(acc[t][0] + b0));
-            out_h[g * out_stride + c + 1] = __float2bfloat16_rn(silu_f(acc[t][1] + b1));
-            out_h[(g + 8) * out_stride + c] = __float2bfloat16_rn(silu_f(acc[t][2] + b0));
-            out_h[(g + 8) * out_stride + c + 1] = __float2bfloat16_rn(silu_f(acc[t][3] + b1));
+            __nv_bfloat162 v0 = __floats2bfloat162_rn(0.0f, 0.0f), v1 = v0;
+            if (lo) v0 = __floats2bfloat162_rn(silu_f(acc[t][0] + b0), silu_f(acc[t][1] + b1));
+            if (hi) v1 = __floats2bfloat162_rn(silu_f(acc[t][2] + b0), silu_f(acc[t][3] + b1));
+            *(__nv_bfloat162*)(out_h + g * out_stride + c) = v0;
+            *(__nv_bfloat162*)(out_h + (g + 8) * out_stride + c) = v1;
         } else {
-            out_f[g * MT_YS + c] = acc[t][0] + b0;
-            out_f[g * MT_YS + c + 1] = acc[t][1] + b1;
-            out_f[(g + 8) * MT_YS + c] = acc[t][2] + b0;
-            out_f[(g + 8) * MT_YS + c + 1] = acc[t][3] + b1;
+            if (lo) {
+                out_f[g * MT_YS + c] = acc[t][0] + b0;
+                out_f[g * MT_YS + c + 1] = acc[t][1] + b1;
+            }
+            if (hi) {
+                out_f[(g + 8) * MT_YS + c] = acc[t][2] + b0;
+                out_f[(g + 8) * MT_YS + c + 1] = acc[t][3] + b1;
+            }
         }
     }
 }
 
-// Network outputs of the 16 rows of T.x into T.y, by the 8 warps of the CTA
-// (all threads call; barriers inside).
-__device__ __forceinline__ void mlp_tile_forward(const MlpDev& M, const MlpTile& T) {
+// Batches: layer 1 (K 192) two of three k-step pairs, layer 2 (K 256) two of four,
+// both over four n-tiles per warp; layer 3 (32 outputs, warps 0-3) one of eight.
+constexpr int MT_PB1 = 3, MT_PB2 = 4, MT_PB3 = 8;
+
+// Batch 0 of layer 1 into w: issue it before the tile's inputs are ready.
+__device__ __forceinline__ void mlp_tile_prefetch(const MlpDev& M, uint4 (&w)[MT_WREGS]) {
+    mlp_tile_fetch<MLP_K1, 4, MT_PB1>(w, M.f1, (int)(threadIdx.x >> 5) * 4, 0);
+}
+
+// Network outputs of rows 0 .. rows-1 of T.x into T.y, by the 8 warps of the CTA
+// (all threads call; barriers inside).  w holds layer 1's batch 0 (mlp_tile_prefetch).
+__device__ __forceinline__ void mlp_tile_forward(const MlpDev& M, const MlpTile& T, uint4 (&w)[MT_WREGS],
+                                                 int rows) {
     const int warp = threadIdx.x >> 5;
-    mlp_tile_layer<MLP_K1, 4, true>(T.x, MT_XS, M.f1, M.b1, T.h1, MT_HS, nullptr, warp * 4);
+    const bool out_warp = warp < MLP_OUT_PAD / 8;
+    mlp_tile_layer<MLP_K1, 4, MT_PB1, true, MLP_H, 4, MT_PB2>(w, T.x, MT_XS, M.f1, warp * 4, M.b1, T.h1, MT_HS,
+                                                               nullptr, M.f2, warp * 4, rows);
     __syncthreads();
-    mlp_tile_layer<MLP_H, 4, true>(T.h1, MT_HS, M.f2, M.b2, T.h2, MT_HS, nullptr, warp * 4);
+    mlp_tile_layer<MLP_H, 4, MT_PB2, true, MLP_H, 1, MT_PB3>(w, T.h1, MT_HS, M.f2, warp * 4, M.b2, T.h2, MT_HS,
+                                                              nullptr, out_warp ? M.f3 : nullptr, warp, rows);
     __syncthreads();
-    if (warp < MLP_OUT_PAD / 8) mlp_tile_layer<MLP_H, 1, false>(T.h2, MT_HS, M.f3, M.b3, nullptr, 0, T.y, warp);
+    if (out_warp)
+        mlp_tile_layer<MLP_H, 1, MT_PB3, false, MLP_H, 1, MT_PB3>(w, T.h2, MT_HS, M.f3, warp, M.b3, nullptr, 0, T.y,
+                                                                  nullptr, 0, rows);
     __syncthreads();
 }
 
