@@ -168,8 +168,8 @@ _SIGS = {
     "binder_mlp_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
     "binder_mlp_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
     "binder_mlp_forward": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
-    "binder_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
-                                       C.POINTER(C.c_double), C.c_void_p]),
+    "binder_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_float, C.POINTER(C.c_double), C.c_void_p]),
     "binder_mlp_set_tuples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "binder_mlp_tuple_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "binder_mlp_get_tuples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -186,6 +186,7 @@ PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
 # learned proposal network (include/binder_gpu.h): sizes and the logged-tuple record
 MLP_IN, MLP_OUT, MLP_N_PARAMS = 180, 25, 123424
+MLP_NO_AA = 255  # amino-acid input of a mutation query (no one-hot)
 MLP_K1, MLP_H, MLP_OUT_PAD = 192, 256, 32
 MLP_OFF = {"w1": 0, "b1": 49152, "w2": 49408, "b2": 114944, "w3": 115200, "b3": 123392}
 MC_TUPLE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("delta_e", "<f4"), ("cand", "<i4"),
@@ -672,13 +673,16 @@ class GpuContext:
         self._check(lib().binder_mlp_forward(self._h, len(f), _ptr(f), _ptr(out)))
         return out
 
-    def mlp_loss_grad(self, features, action, target, huber_delta=1.0):
+    def mlp_loss_grad(self, features, action, target, huber_delta=1.0, ref=None):
+        """Mean Huber loss of y[action] - y[ref] (y[action] where ref is None or -1)
+        against target, and the parameter gradient."""
         f = _f32(features).reshape(-1, MLP_IN)
         a = np.ascontiguousarray(action, np.int32)
+        r = None if ref is None else np.ascontiguousarray(ref, np.int32)
         t = _f32(target)
         loss = C.c_double()
         g = np.zeros(MLP_N_PARAMS, np.float32)
-        self._check(lib().binder_mlp_loss_grad(self._h, len(f), _ptr(f), _ptr(a), _ptr(t), huber_delta,
+        self._check(lib().binder_mlp_loss_grad(self._h, len(f), _ptr(f), _ptr(a), _ptr(r), _ptr(t), huber_delta,
                                                C.byref(loss), _ptr(g)))
         return loss.value, g
 

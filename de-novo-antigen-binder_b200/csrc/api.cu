@@ -171,7 +171,7 @@ struct MlpState {
     DBuf<__nv_bfloat16> X, Xt, H1, H1t, H2, H2t, dY, dYt, dZ2, dZ2t, dZ1t, S1, S2;
     DBuf<float> Y, part, feat, ca, target;
     DBuf<uint8_t> aa;
-    DBuf<int> ag, action, idx;
+    DBuf<int> ag, action, ref, idx;
     DBuf<double> loss;
     DBuf<MlpTuple> tuples;
     size_t n_tuples = 0;
@@ -1899,6 +1899,7 @@ int mlp_reserve(binder_ctx* ctx, int rows) {
     CK(M.aa.ensure(c), "mlp alloc");
     CK(M.ag.ensure(c), "mlp alloc");
     CK(M.action.ensure(c), "mlp alloc");
+    CK(M.ref.ensure(c), "mlp alloc");
     CK(M.idx.ensure(c), "mlp alloc");
     M.cap = cap;
     return BINDER_OK;
@@ -1962,12 +1963,14 @@ int mlp_weight_grad(binder_ctx* ctx, const __nv_bfloat16* Gt, int rows, const __
     return BINDER_OK;
 }
 
-// Loss and gradient of the batch in M.X / M.action / M.target (m rows) into M.g.
-int mlp_backward_dev(binder_ctx* ctx, int m, float delta) {
+// Loss and gradient of the batch in M.X / M.action / M.target (m rows; reference
+// outputs in M.ref when with_ref) into M.g.
+int mlp_backward_dev(binder_ctx* ctx, int m, float delta, bool with_ref) {
     MlpState& M = ctx->mlp;
     const int mp = round_up(m, 128);
     int s;
-    launch_mlp_loss(ctx->stream, m, mp, M.Y.p, M.action.p, M.target.p, delta, M.dY.p, M.dYt.p, M.loss.p);
+    launch_mlp_loss(ctx->stream, m, mp, M.Y.p, M.action.p, with_ref ? M.ref.p : nullptr, M.target.p, delta, M.dY.p,
+                    M.dYt.p, M.loss.p);
     LAUNCHED("mlp loss");
     // layer 3: dW3 = dY^T H2, db3 = colsum dY, dZ2 = (dY W3) * silu'(Z2)
     if ((s = mlp_weight_grad(ctx, M.dYt.p, MLP_OUT_PAD, M.H2t.p, MLP_H, mp, M.g.p + MLP_OFF_W3))) return s;
@@ -2068,7 +2071,8 @@ int binder_mlp_features(binder_ctx* ctx, int32_t antigen_id, size_t n, const flo
     if (antigen_id < 0 || antigen_id >= (int)ctx->ags.size()) return fail(ctx, BINDER_ERR_ARG, "no antigen %d", antigen_id);
     if (n > (1u << 24)) return fail(ctx, BINDER_ERR_ARG, "too many rows");
     for (size_t i = 0; i < n; ++i)
-        if (aa[i] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid %d out of range", (int)aa[i]);
+        if (aa[i] >= N_AA && aa[i] != MLP_NO_AA)
+            return fail(ctx, BINDER_ERR_ARG, "amino acid %d out of range", (int)aa[i]);
     if (n == 0) return BINDER_OK;
     MlpState& M = ctx->mlp;
     if ((s = mlp_reserve(ctx, (int)n))) return s;
@@ -2108,20 +2112,25 @@ int binder_mlp_forward(binder_ctx* ctx, size_t n, const float* features, float* 
 }
 
 int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const int32_t* action,
-                         const float* target, float huber_delta, double* out_loss, float* out_grad) {
+                         const int32_t* ref, const float* target, float huber_delta, double* out_loss,
+                         float* out_grad) {
     int s = enter(ctx);
     if (s) return s;
     if (!n || !features || !action || !target) return fail(ctx, BINDER_ERR_ARG, "empty or NULL batch");
     if (n > (1u << 24)) return fail(ctx, BINDER_ERR_ARG, "too many rows");
     if (!(huber_delta > 0.0f)) return fail(ctx, BINDER_ERR_ARG, "huber_delta must be positive");
-    for (size_t i = 0; i < n; ++i)
+    for (size_t i = 0; i < n; ++i) {
         if (action[i] < 0 || action[i] >= MLP_OUT) return fail(ctx, BINDER_ERR_ARG, "action %d out of range", action[i]);
+        if (ref && (ref[i] < -1 || ref[i] >= MLP_OUT))
+            return fail(ctx, BINDER_ERR_ARG, "reference output %d out of range", ref[i]);
+    }
     if ((s = mlp_check_ready(ctx))) return s;
     MlpState& M = ctx->mlp;
     if ((s = mlp_reserve(ctx, (int)n)) || (s = clear_err(ctx))) return s;
     if ((s = upload(ctx, M.feat, features, n * MLP_IN, "mlp H2D")) ||
         (s = upload(ctx, M.action, (const int*)action, n, "mlp H2D")) ||
-        (s = upload(ctx, M.target, target, n, "mlp H2D")))
+        (s = upload(ctx, M.target, target, n, "mlp H2D")) ||
+        (ref && (s = upload(ctx, M.ref, (const int*)ref, n, "mlp H2D"))))
         return s;
     const int mp = round_up((int)n, 128);
     launch_pack_features(ctx->stream, (int)n, mp, M.feat.p, M.X.p);
@@ -2129,7 +2138,8 @@ int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const
     launch_transpose_bf16(ctx->stream, mp, MLP_K1, M.X.p, M.Xt.p);
     LAUNCHED("mlp transpose");
     CK(cudaMemsetAsync(M.loss.p, 0, sizeof(double), ctx->stream), "mlp memset");
-    if ((s = mlp_forward_dev(ctx, (int)n, true)) || (s = mlp_backward_dev(ctx, (int)n, huber_delta))) return s;
+    if ((s = mlp_forward_dev(ctx, (int)n, true)) || (s = mlp_backward_dev(ctx, (int)n, huber_delta, ref != nullptr)))
+        return s;
     double loss = 0.0;
     CK(cudaMemcpyAsync(&loss, M.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "mlp D2H");
     if (out_grad)
@@ -2193,7 +2203,8 @@ int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float hu
         launch_draw_batch(ctx->stream, batch, (int)std::min<size_t>(M.n_tuples, INT32_MAX), seed, (uint32_t)M.adam_t,
                           M.idx.p);
         LAUNCHED("mlp draw batch");
-        launch_gather_tuples(ctx->stream, batch, M.idx.p, M.tuples.p, M.ca.p, M.aa.p, M.ag.p, M.action.p, M.target.p);
+        launch_gather_tuples(ctx->stream, batch, M.idx.p, M.tuples.p, M.ca.p, M.aa.p, M.ag.p, M.action.p, M.ref.p,
+                             M.target.p);
         LAUNCHED("mlp gather");
         launch_features(ctx->stream, batch, mp, M.ca.p, M.aa.p, M.ag.p, ctx->d_views.p, M.X.p);
         LAUNCHED("features");
@@ -2201,7 +2212,7 @@ int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float hu
         LAUNCHED("mlp transpose");
         M.loss.p = loss_base + step;  // per-step loss slot
         s = mlp_forward_dev(ctx, batch, true);
-        if (!s) s = mlp_backward_dev(ctx, batch, huber_delta);
+        if (!s) s = mlp_backward_dev(ctx, batch, huber_delta, true);
         M.loss.p = loss_base;
         if (s) return s;
         M.adam_t += 1;

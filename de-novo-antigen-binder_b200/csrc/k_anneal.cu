@@ -36,7 +36,7 @@ namespace binder {
 cudaError_t anneal_init_tables() { return geom_init_tables(); }
 
 // log1p of the environment counts for the in-kernel features (the same host table
-// as the feature kernel's); global memory, since the lanes of a warp index it apart
+// as the feature kernel's); copied to shared memory by each learned-proposal CTA
 __device__ float g_an_log1p[MLP_COUNT_CAP + 1];
 cudaError_t anneal_init_mlp_table(const float* t) {
     return cudaMemcpyToSymbol(g_an_log1p, t, sizeof(float) * (MLP_COUNT_CAP + 1));
@@ -71,12 +71,14 @@ struct AnSmem {
     AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
     double* dscal;                  // [0] disulfide energy of the current state
-    double *lhr, *lqf;              // R: log Hastings ratio of the move, log q of the forward mutation
+    double* lhr;                    // R: log Hastings ratio of the move
     float *u_acc, *bb_u;            // R
     int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
     int *rot, *mvl;                 // R: rotamer index of the state (-1 unknown), residues with a move
     uint32_t* dz;                   // R: the move's choice draw
     int* iscal;
+    uint8_t* agaa;                  // learned proposal: G staged antigen amino acids
+    float* lg1p;                    // learned proposal: the log1p count table
 };
 __host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
@@ -88,8 +90,8 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
     return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + anneal_terms_bytes(R, learned) +
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
-           (size_t)R * 8 * 3 + 16 + (size_t)R * 8 * 2 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
-           (size_t)R * 4 * 3 + 32;
+           (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
+           (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1) * 4 : 0);
 }
 __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
     AnSmem s;
@@ -115,7 +117,6 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.c_new = (double*)take((size_t)R * 8);
     s.dscal = (double*)take(16);
     s.lhr = (double*)take((size_t)R * 8);
-    s.lqf = (double*)take((size_t)R * 8);
     s.u_acc = (float*)take((size_t)R * 4);
     s.bb_u = (float*)take((size_t)R * 4);
     s.aa = (int*)take((size_t)R * 4);
@@ -132,6 +133,8 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.mvl = (int*)take((size_t)R * 4);
     s.dz = (uint32_t*)take((size_t)R * 4);
     s.iscal = (int*)take(32);
+    s.agaa = learned ? (uint8_t*)take(((size_t)G + 15) / 16 * 16) : nullptr;
+    s.lg1p = learned ? (float*)take((MLP_COUNT_CAP + 1) * 4) : nullptr;
     return s;
 }
 
@@ -262,10 +265,13 @@ __device__ __forceinline__ bool mh_accept(ACC de, float temp, float u, double lh
 }
 
 // ---- learned proposal -------------------------------------------------------------
-// Features of the tile rows: row i = residue mvl[base + i] with its amino acid; one
-// warp per row (rows i and i + 8).
+// Features of the tile rows: row i = residue mvl[base + i]; the one-hot of its amino
+// acid for a rotamer query, none for a mutation query (the network's mutation
+// outputs then depend on the environment alone, the same before and after the
+// move); one warp per row (rows i and i + 8).  ag_aa and the log1p table are the
+// shared-memory copies when staged.
 __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* rows_of, int base, int rows,
-                                 const float4* agq, const uint8_t* ag_aa, int nag) {
+                                 const float4* agq, const uint8_t* ag_aa, int nag, const float* lg1p) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = warp; i < MT_ROWS; i += AN_WARPS) {
         int* cnt = T.cnt + i * MLP_SHELLS * N_AA;
@@ -280,11 +286,11 @@ __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* r
         const float4 ca = S.pos[r * SLOT_STRIDE + 1];
         mlp_count_env(agq, ag_aa, nag, ca.x, ca.y, ca.z, cnt);
         __syncwarp();
-        const int a = S.aa[r];
+        const int a = S.kind[r] == MV_MUT ? -1 : S.aa[r];
         for (int j = lane; j < MLP_K1; j += 32) {
             float v = 0.0f;
             if (j < N_AA) v = j == a ? 1.0f : 0.0f;
-            else if (j < MLP_IN) v = __ldg(&g_an_log1p[min(cnt[j - N_AA], MLP_COUNT_CAP)]);
+            else if (j < MLP_IN) v = lg1p[min(cnt[j - N_AA], MLP_COUNT_CAP)];
             x[j] = __float2bfloat16_rn(v);
         }
     }
@@ -458,18 +464,18 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
 }
 
 // The network's choice of every mutation and (known-rotamer) rotamer move drawn
-// this step and the moves' log Hastings ratios (all threads of the CTA call).  Per
-// tile of moves: features, a forward pass, the draws; then the mutation rows' one-hot
-// moved to the drawn amino acid in place -- the features of the proposed state, the
-// environment counts being the same -- and a second pass gives their reverse
-// probabilities by the same code.  Each pass's first weights are fetched ahead.
+// this step and the moves' log Hastings ratios (all threads of the CTA call), one
+// network pass per tile of moves.  A move changes neither the residue's environment
+// nor its query (mutation: no amino-acid input; rotamer: the unchanged amino acid),
+// so the reverse move's proposal is the same softmax: log q(reverse) - log q(move)
+// = (y[move] - y[back]) / Tp, the normalisers cancelling.
 __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const float4* agq, const uint8_t* ag_aa,
                                                 int nag, const MlpDev& mlp, float temp) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const MlpTile T = mlp_tile_carve((unsigned char*)S.terms);
     const float tp = fmaxf(temp, mlp.t_prop_min);
     uint4 w[MT_WREGS];
-    mlp_tile_prefetch(mlp, w);
+    mlp_tile_prefetch(mlp, w);  // the first weights are on their way during the features
     if (tid == 0) {  // mutations, and rotamer moves from a known library rotamer
         int k = 0;
         for (int r = 0; r < n; ++r)
@@ -481,11 +487,9 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
     for (int base = 0; base < n_mv; base += MT_ROWS) {
         const int rows = min(MT_ROWS, n_mv - base);
         if (base > 0) mlp_tile_prefetch(mlp, w);
-        an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag);
+        an_tile_features(S, T, S.mvl, base, rows, agq, ag_aa, nag, S.lg1p);
         __syncthreads();
         mlp_tile_forward(mlp, T, w, rows);
-        mlp_tile_prefetch(mlp, w);  // the reverse pass's
-        bool mut = false;
         for (int i = warp; i < rows; i += AN_WARPS) {  // one warp per row
             const int r = S.mvl[base + i];
             const float* y = T.y + i * MT_YS;
@@ -494,34 +498,17 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
                 const int k = warp_sample(y + N_AA, s_rot_n[S.aa[r]], tp, S.dz[r], &lq);
                 if (lane == 0) {
                     S.new_rot[r] = k;
-                    // same features before and after a rotamer move: the normalisers cancel
                     S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
                 }
             } else {
                 const int a = warp_sample(y, N_AA, tp, S.dz[r], &lq);
                 if (lane == 0) {
                     S.new_aa[r] = a;
-                    S.lqf[r] = lq;
-                    __nv_bfloat16* x = T.x + i * MT_XS;
-                    x[S.aa[r]] = __float2bfloat16_rn(0.0f);
-                    x[a] = __float2bfloat16_rn(1.0f);
+                    S.lhr[r] = -(double)y[S.aa[r]] / (double)tp + (double)y[a] / (double)tp;
                 }
-                mut = true;
             }
         }
-        // reverse probabilities of the mutations: the network at the proposed amino acid
-        if (__syncthreads_or(mut)) {
-            mlp_tile_forward(mlp, T, w, rows);
-            for (int i = warp; i < rows; i += AN_WARPS) {
-                const int r = S.mvl[base + i];
-                if (S.kind[r] != MV_MUT) continue;
-                const float* y = T.y + i * MT_YS;
-                double lz;
-                warp_softmax(y, N_AA, tp, &lz);
-                if (lane == 0) S.lhr[r] = (-(double)y[S.aa[r]] / (double)tp - lz) - S.lqf[r];
-            }
-            __syncthreads();
-        }
+        __syncthreads();
     }
 }
 
@@ -556,6 +543,10 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         S.cgp[i] = A.ca_prm[i];
     }
     for (int i = tid; cells_staged && i < ncell; i += AN_THREADS) S.cgcell[i] = A.ca_grid.cell_start[i];
+    if (EXT && learned) {  // the network's features read these every step
+        for (int i = tid; staged && i < nag; i += AN_THREADS) S.agaa[i] = A.res_aa[i];
+        for (int i = tid; i <= MLP_COUNT_CAP; i += AN_THREADS) S.lg1p[i] = g_an_log1p[i];
+    }
     __syncthreads();
     if (tid == 0 && cells_staged) {  // the CG probe reads the staged copies through the view
         S.ag->ca_pq = S.cgq;
@@ -712,7 +703,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         __syncthreads();
         // learned proposal: the choice of each drawn move comes from the network
         // (same draw d.z, inverse CDF) and the move carries its Hastings ratio
-        if (EXT && learned && temp <= mlp.t_max) an_learned_choices(S, n, agq, A.res_aa, nag, mlp, temp);
+        if (EXT && learned && temp <= mlp.t_max)
+            an_learned_choices(S, n, agq, staged ? S.agaa : A.res_aa, nag, mlp, temp);
         // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
         // the Calpha energies before / after each move on warps 0..3 (one warp each)
         if (warp >= AN_WARPS / 2) {

@@ -354,25 +354,33 @@ cudaError_t launch_gemm_tc(cudaStream_t s, const GemmArgs& g, uint32_t* err) {
 }
 
 // ---- training kernels -------------------------------------------------------------
-// Huber loss of the taken action's output against its energy change; writes the
+// Huber loss of the predicted energy change against the logged one; writes the
 // output gradient dY (BF16 [m_pad][32] and its transpose [32][m_pad]) and adds the
-// batch loss.  Rows >= m get zero gradients.
+// batch loss.  Prediction: y[action] - y[ref] with a reference output (ref >= 0:
+// a mutation query, ref = the amino acid before the move; a row with ref == action
+// carries nothing), else y[action].  Rows >= m get zero gradients.
 __global__ void k_mlp_loss(int m, int m_pad, const float* __restrict__ Y, const int* __restrict__ action,
-                           const float* __restrict__ target, float delta, __nv_bfloat16* __restrict__ dY,
-                           __nv_bfloat16* __restrict__ dYt, double* __restrict__ loss) {
+                           const int* __restrict__ ref, const float* __restrict__ target, float delta,
+                           __nv_bfloat16* __restrict__ dY, __nv_bfloat16* __restrict__ dYt, double* __restrict__ loss) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m_pad) return;
-    int a = -1;
+    int a = -1, b = -1;
     float g = 0.0f, l = 0.0f;
     if (r < m) {
         a = action[r];
-        const float d = Y[(size_t)r * MLP_OUT_PAD + a] - target[r];
-        const float ad = fabsf(d);
-        l = ad <= delta ? 0.5f * d * d : delta * (ad - 0.5f * delta);
-        g = fminf(fmaxf(d, -delta), delta) / (float)m;
+        b = ref ? ref[r] : -1;
+        if (b == a) {
+            a = b = -1;
+        } else {
+            const float* y = Y + (size_t)r * MLP_OUT_PAD;
+            const float d = (b >= 0 ? y[a] - y[b] : y[a]) - target[r];
+            const float ad = fabsf(d);
+            l = ad <= delta ? 0.5f * d * d : delta * (ad - 0.5f * delta);
+            g = fminf(fmaxf(d, -delta), delta) / (float)m;
+        }
     }
     for (int j = 0; j < MLP_OUT_PAD; ++j) {
-        const __nv_bfloat16 v = __float2bfloat16_rn(j == a ? g : 0.0f);
+        const __nv_bfloat16 v = __float2bfloat16_rn(j == a ? g : (j == b ? -g : 0.0f));
         dY[(size_t)r * MLP_OUT_PAD + j] = v;
         dYt[(size_t)j * m_pad + r] = v;
     }
@@ -462,19 +470,24 @@ __global__ void k_pack_weights(const float* __restrict__ p, MlpBf16 o) {
     }
 }
 
-// Gather a minibatch of logged tuples: features input rows, action, target.
+// Gather a minibatch of logged tuples: features input rows, action, reference
+// output, target.  A mutation is a query without amino acid (MLP_NO_AA) whose
+// energy change is predicted as y[new] - y[old]; a rotamer move queries with its
+// amino acid and is predicted by y[20 + rotamer].
 __global__ void k_gather_tuples(int m, const int* __restrict__ idx, const MlpTuple* __restrict__ tup,
                                 float* __restrict__ ca, uint8_t* __restrict__ aa, int* __restrict__ ag,
-                                int* __restrict__ action, float* __restrict__ target) {
+                                int* __restrict__ action, int* __restrict__ ref, float* __restrict__ target) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= m) return;
     const MlpTuple t = tup[idx[r]];
+    const bool mut = t.action < N_AA;
     ca[3 * r] = t.x;
     ca[3 * r + 1] = t.y;
     ca[3 * r + 2] = t.z;
-    aa[r] = t.aa;
+    aa[r] = mut ? (uint8_t)MLP_NO_AA : t.aa;
     ag[r] = t.antigen;
     action[r] = t.action;
+    ref[r] = mut ? (int)t.aa : -1;
     target[r] = t.delta_e;
 }
 // minibatch indices drawn with the Philox generator: idx[r] = uniform in [0, n_tuples)
@@ -497,9 +510,10 @@ void launch_pack_features(cudaStream_t s, int n, int n_pad, const float* f, __nv
 void launch_transpose_bf16(cudaStream_t s, int rows, int cols, const __nv_bfloat16* in, __nv_bfloat16* out) {
     if (rows > 0 && cols > 0) k_transpose_bf16<<<dim3((cols + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, s>>>(rows, cols, in, out);
 }
-void launch_mlp_loss(cudaStream_t s, int m, int m_pad, const float* Y, const int* action, const float* target,
-                     float delta, __nv_bfloat16* dY, __nv_bfloat16* dYt, double* loss) {
-    if (m_pad > 0) k_mlp_loss<<<(m_pad + 255) / 256, 256, 0, s>>>(m, m_pad, Y, action, target, delta, dY, dYt, loss);
+void launch_mlp_loss(cudaStream_t s, int m, int m_pad, const float* Y, const int* action, const int* ref,
+                     const float* target, float delta, __nv_bfloat16* dY, __nv_bfloat16* dYt, double* loss) {
+    if (m_pad > 0)
+        k_mlp_loss<<<(m_pad + 255) / 256, 256, 0, s>>>(m, m_pad, Y, action, ref, target, delta, dY, dYt, loss);
 }
 void launch_rowsum_bf16(cudaStream_t s, int rows, int m, int ld, const __nv_bfloat16* G, float* out) {
     if (rows > 0) k_rowsum_bf16<<<(rows + 7) / 8, 256, 0, s>>>(rows, m, ld, G, out);
@@ -515,8 +529,8 @@ void launch_pack_weights(cudaStream_t s, const float* p, const MlpBf16& o) {
     k_pack_weights<<<(MLP_H * MLP_H + 255) / 256, 256, 0, s>>>(p, o);
 }
 void launch_gather_tuples(cudaStream_t s, int m, const int* idx, const MlpTuple* tup, float* ca, uint8_t* aa, int* ag,
-                          int* action, float* target) {
-    if (m > 0) k_gather_tuples<<<(m + 255) / 256, 256, 0, s>>>(m, idx, tup, ca, aa, ag, action, target);
+                          int* action, int* ref, float* target) {
+    if (m > 0) k_gather_tuples<<<(m + 255) / 256, 256, 0, s>>>(m, idx, tup, ca, aa, ag, action, ref, target);
 }
 void launch_draw_batch(cudaStream_t s, int m, int n_tuples, uint64_t seed, uint32_t step, int* idx) {
     if (m > 0) k_draw_batch<<<(m + 255) / 256, 256, 0, s>>>(m, n_tuples, seed, step, idx);

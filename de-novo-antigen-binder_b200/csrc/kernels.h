@@ -125,15 +125,15 @@ void launch_pack_features(cudaStream_t s, int n, int n_pad, const float* f, __nv
 void launch_transpose_bf16(cudaStream_t s, int rows, int cols, const __nv_bfloat16* in, __nv_bfloat16* out);
 cudaError_t launch_gemm_tc(cudaStream_t s, const GemmArgs& g, uint32_t* err);
 cudaError_t launch_wait_selftest(cudaStream_t s, uint32_t max_polls, uint32_t* err);
-void launch_mlp_loss(cudaStream_t s, int m, int m_pad, const float* Y, const int* action, const float* target,
-                     float delta, __nv_bfloat16* dY, __nv_bfloat16* dYt, double* loss);
+void launch_mlp_loss(cudaStream_t s, int m, int m_pad, const float* Y, const int* action, const int* ref,
+                     const float* target, float delta, __nv_bfloat16* dY, __nv_bfloat16* dYt, double* loss);
 void launch_rowsum_bf16(cudaStream_t s, int rows, int m, int ld, const __nv_bfloat16* G, float* out);
 void launch_reduce_partials(cudaStream_t s, int n, int n_part, long long stride, const float* part, float* out);
 void launch_adam(cudaStream_t s, int n, float* w, const float* g, float* m1, float* m2, float lr, float b1, float b2,
                  float eps, float bc1, float bc2);
 void launch_pack_weights(cudaStream_t s, const float* p, const MlpBf16& o);
 void launch_gather_tuples(cudaStream_t s, int m, const int* idx, const MlpTuple* tup, float* ca, uint8_t* aa, int* ag,
-                          int* action, float* target);
+                          int* action, int* ref, float* target);
 void launch_draw_batch(cudaStream_t s, int m, int n_tuples, uint64_t seed, uint32_t step, int* idx);
 
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----

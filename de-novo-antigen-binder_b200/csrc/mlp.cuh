@@ -16,6 +16,7 @@ constexpr int MLP_OUT = 25;       // 20 mutation targets + 5 rotamers
 constexpr int MLP_OUT_PAD = 32;   // output rows of W3 (rows >= 25 stay zero)
 constexpr int MLP_SHELLS = 8;     // radial shells of 1.25 A out to 10 A
 constexpr int MLP_COUNT_CAP = 255;
+constexpr int MLP_NO_AA = 255;    // amino-acid input of a mutation query: none (no one-hot)
 
 // flat FP32 parameter vector: W1 [256][192], b1 [256], W2 [256][256], b2 [256],
 // W3 [32][256], b3 [32]

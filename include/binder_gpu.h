@@ -362,17 +362,28 @@ typedef struct binder_mc_tuple {
 /* Set the parameters (resets the optimiser) / read them back. */
 int binder_mlp_set_params(binder_ctx* ctx, const float* params);
 int binder_mlp_get_params(binder_ctx* ctx, float* params);
-/* Features of n residues (Calpha xyz float[n][3], amino acids) against resident
-   antigen antigen_id: out float[n][180] (the BF16 values the network sees). */
+/* Amino-acid input of a mutation query: no one-hot.  The network answers a mutation
+   query (a residue's environment alone) with outputs 0..19, whose differences
+   y[new] - y[old] predict the energy change of mutating old -> new, and a rotamer
+   query (environment + the residue's amino acid) with outputs 20..24, the energy
+   change of moving to rotamer 0..4. */
+#define BINDER_MLP_NO_AA 255
+/* Features of n residues (Calpha xyz float[n][3], amino acids or BINDER_MLP_NO_AA)
+   against resident antigen antigen_id: out float[n][180] (the BF16 values the
+   network sees). */
 int binder_mlp_features(binder_ctx* ctx, int32_t antigen_id, size_t n, const float* ca_xyz, const uint8_t* aa,
                         float* out);
 /* Network outputs of n feature rows (float[n][180], rounded to BF16): out float[n][25]. */
 int binder_mlp_forward(binder_ctx* ctx, size_t n, const float* features, float* out);
-/* Mean Huber loss (threshold huber_delta) of output action[i] against target[i]
-   over the batch, and its gradient with respect to every parameter
-   (out_grad float[BINDER_MLP_N_PARAMS], may be NULL).  Parameters unchanged. */
+/* Mean Huber loss (threshold huber_delta) of the prediction y[action[i]] -
+   y[ref[i]] (ref NULL or ref[i] = -1: y[action[i]]) against target[i] over the
+   batch -- rows with ref[i] == action[i] contribute zero -- and its gradient with
+   respect to every parameter (out_grad float[BINDER_MLP_N_PARAMS], may be NULL).
+   Parameters unchanged.  Training on logged tuples uses ref = the amino acid
+   before a mutation and -1 for rotamer moves. */
 int binder_mlp_loss_grad(binder_ctx* ctx, size_t n, const float* features, const int32_t* action,
-                         const float* target, float huber_delta, double* out_loss, float* out_grad);
+                         const int32_t* ref, const float* target, float huber_delta, double* out_loss,
+                         float* out_grad);
 /* The training set: tuples logged by binder_diffuse (binder_mc_log) or given here. */
 int binder_mlp_set_tuples(binder_ctx* ctx, const binder_mc_tuple* tuples, size_t n);
 int binder_mlp_tuple_count(binder_ctx* ctx, size_t* out_n);
@@ -387,11 +398,13 @@ int binder_mc_log_fetch(binder_ctx* ctx, binder_mc_tuple* out, size_t cap, size_
 int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n);
 /* Proposal of binder_diffuse's mutation and rotamer moves.  UNIFORM: the
    reference's uniform choice.  LEARNED: the choice drawn from softmax(-y / Tp) of
-   the network outputs y at the residue's environment, Tp = max(T, t_prop_min), by
-   inverse CDF on the same random draw (a network with constant outputs chooses
-   exactly as UNIFORM does), accepted with probability min(1, exp(-dE/T) q(reverse)
-   / q(move)), the reverse probability of a mutation evaluated by the network at
-   the proposed amino acid.  Rotamer moves from a chi that is no library rotamer
+   the network outputs y of the residue's query (mutation: outputs 0..19 of the
+   environment; rotamer: outputs 20..24 given the amino acid), Tp = max(T,
+   t_prop_min), by inverse CDF on the same random draw (a network with constant
+   outputs chooses exactly as UNIFORM does), accepted with probability
+   min(1, exp(-dE/T) q(reverse) / q(move)).  The move leaves the query unchanged, so
+   q(reverse) / q(move) = exp((y[move] - y[back]) / Tp) exactly, from one network
+   evaluation.  Rotamer moves from a chi that is no library rotamer
    stay uniform, and so do all moves of steps whose temperature is above t_max
    (INFINITY: none) -- each step is a Metropolis-Hastings step at its temperature
    either way. */
@@ -399,8 +412,10 @@ int binder_mlp_take_log(binder_ctx* ctx, size_t* out_n);
 #define BINDER_PROPOSAL_LEARNED 1
 int binder_set_proposal(binder_ctx* ctx, int mode, float t_prop_min, float t_max);
 /* n_steps Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on minibatches of `batch`
-   tuples drawn uniformly (Philox, key seed) from the training set; out_losses
-   double[n_steps] (may be NULL) = each step's mean Huber loss. */
+   tuples drawn uniformly (Philox, key seed) from the training set -- mutations as
+   queries without amino acid against y[new] - y[old], rotamer moves as queries
+   with it against y[20 + rotamer]; out_losses double[n_steps] (may be NULL) =
+   each step's mean Huber loss. */
 int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float huber_delta, uint64_t seed,
                      double* out_losses);
 

@@ -6,7 +6,9 @@ the GPU kernels in de-novo-antigen-binder_b200/csrc/k_mlp.cu:
 
   * features(): the 180 environment features of a residue, bit for bit (f32
     squared distances with the reference's rounding, exact shell radii squared,
-    log1p table rounded once to f32, BF16 round-to-nearest-even);
+    log1p table rounded once to f32, BF16 round-to-nearest-even); a mutation
+    query (amino acid NO_AA) carries no one-hot;
+  * loss_grad(ref=...): mutation rows predict y[new] - y[old];
   * forward() / loss_grad(): the MLP 180 -> 256 -> 256 -> 25 with SiLU in float64.
     With bf16=True the BF16 roundings of the GPU path are applied (weights, input
     rows, hidden activations, output and hidden gradients) and only the sums are
@@ -56,12 +58,18 @@ def env_counts(ag_ca, ag_aa, ca):
     return cnt
 
 
+NO_AA = 255  # amino-acid input of a mutation query: no one-hot
+
+
 def features(ag_ca, ag_aa, ca, aa):
-    """float32 [n][180]: one-hot of aa, then log1p(count[shell][aa']) at 20 + 20*shell + aa'."""
+    """float32 [n][180]: one-hot of aa (none for NO_AA), then log1p(count[shell][aa'])
+    at 20 + 20*shell + aa'."""
     cnt = env_counts(ag_ca, ag_aa, ca)
     n = len(cnt)
     f = np.zeros((n, MLP_IN), np.float32)
-    f[np.arange(n), np.asarray(aa, np.int64)] = 1.0
+    a = np.asarray(aa, np.int64)
+    has = a < N_AA
+    f[np.arange(n)[has], a[has]] = 1.0
     f[:, N_AA:] = LOG1P[np.minimum(cnt.reshape(n, -1), 255)]
     return bf16(f)
 
@@ -99,20 +107,29 @@ def forward(params, X, bf16_path=True):
     return Y, (X, Z1, H1, Z2, H2)
 
 
-def loss_grad(params, X, action, target, delta=1.0, bf16_path=True):
-    """Mean Huber loss of Y[i, action[i]] against target[i] and the gradient with
-    respect to the flat parameter vector (float64, padding entries zero)."""
+def loss_grad(params, X, action, target, delta=1.0, bf16_path=True, ref=None):
+    """Mean Huber loss of Y[i, action[i]] - Y[i, ref[i]] (Y[i, action[i]] where ref is
+    None or -1; rows with ref[i] == action[i] contribute zero) against target[i] and
+    the gradient with respect to the flat parameter vector (float64, padding entries
+    zero)."""
     W1, b1, W2, b2, W3, b3 = unpack(params)
     if bf16_path:
         W1, W2, W3 = _b(W1, 1), _b(W2, 1), _b(W3, 1)
     Y, (Xb, Z1, H1, Z2, H2) = forward(params, X, bf16_path)
     m = len(Y)
     a = np.asarray(action, np.int64)
-    d = Y[np.arange(m), a] - np.asarray(target, np.float64)
+    b = np.full(m, -1, np.int64) if ref is None else np.asarray(ref, np.int64)
+    keep = b != a
+    pred = Y[np.arange(m), a] - np.where(b >= 0, Y[np.arange(m), np.maximum(b, 0)], 0.0)
+    d = np.where(keep, pred - np.asarray(target, np.float64), 0.0)
     ad = np.abs(d)
     loss = float(np.where(ad <= delta, 0.5 * d * d, delta * (ad - 0.5 * delta)).mean())
+    g = np.clip(d, -delta, delta) / m
     dY = np.zeros_like(Y)
-    dY[np.arange(m), a] = np.clip(d, -delta, delta) / m
+    rows = np.arange(m)
+    dY[rows[keep], a[keep]] += g[keep]
+    withb = keep & (b >= 0)
+    dY[rows[withb], b[withb]] -= g[withb]
     dY = _b(dY, bf16_path)
     gW3 = dY.T @ H2
     gb3 = dY.sum(0)

@@ -45,20 +45,25 @@ def _params(pkg, seed=0, scale=1.0):
 
 
 # ---- oracle self-checks (CPU) ------------------------------------------------------
-def test_oracle_gradient_matches_finite_differences(pkg):
+@pytest.mark.parametrize("with_ref", [False, True])
+def test_oracle_gradient_matches_finite_differences(pkg, with_ref):
     rng = np.random.default_rng(1)
     X = rng.normal(size=(12, mo.MLP_IN))
     a = rng.integers(0, 25, 12)
     t = rng.normal(scale=2.0, size=12)
+    # reference outputs: mutation rows (y[action] - y[ref]), rotamer rows (-1), a no-op row
+    ref = np.where(a < 20, rng.integers(0, 20, 12), -1) if with_ref else None
+    if with_ref:
+        ref[0], a[0] = 3, 3
     p = _params(pkg, 3).astype(np.float64)
-    _, g = mo.loss_grad(p, X, a, t, delta=1.0, bf16_path=False)
+    _, g = mo.loss_grad(p, X, a, t, delta=1.0, bf16_path=False, ref=ref)
     idx = np.concatenate([rng.integers(mo.OFF[a_], mo.OFF[b_] if b_ else mo.OFF["b3"] + 25, 8) for a_, b_ in BLOCKS])
     h = 1e-6
     for i in idx:
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        fd = (mo.loss_grad(pp, X, a, t, 1.0, False)[0] - mo.loss_grad(pm, X, a, t, 1.0, False)[0]) / (2 * h)
+        fd = (mo.loss_grad(pp, X, a, t, 1.0, False, ref)[0] - mo.loss_grad(pm, X, a, t, 1.0, False, ref)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (i, fd, g[i])
 
 
@@ -108,10 +113,12 @@ def test_features_bit_exact(ctx, pkg):
     # points exactly on shell radii from an antigen Calpha
     ca[:8] = (ag_ca[0] + np.array([[1.25 * k, 0, 0] for k in range(1, 9)])).astype(np.float32)
     aa = rng.integers(0, 20, 500).astype(np.uint8)
+    aa[::3] = pkg.MLP_NO_AA  # mutation queries: no one-hot
     got = ctx.mlp_features(0, ca, aa)
     ref = mo.features(ag_ca, ag_aa, ca, aa)
     assert got.dtype == np.float32 and got.shape == (500, 180)
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert not got[::3, :20].any() and np.all(got[1::3, :20].sum(1) == 1.0)
 
 
 @pytest.mark.gpu
@@ -132,16 +139,20 @@ def test_forward_matches_oracle(ctx, pkg, n):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [128, 1000])
-def test_loss_grad_matches_oracle(ctx, pkg, n):
+@pytest.mark.parametrize("n,with_ref", [(128, False), (1000, False), (1000, True)])
+def test_loss_grad_matches_oracle(ctx, pkg, n, with_ref):
     rng = np.random.default_rng(11 + n)
     p = _params(pkg, 8)
     ctx.mlp_set_params(p)
     X = _random_features(rng, n)
     a = rng.integers(0, 25, n).astype(np.int32)
     t = rng.normal(scale=1.5, size=n).astype(np.float32)
-    loss, g = ctx.mlp_loss_grad(X, a, t, 1.0)
-    rloss, rg = mo.loss_grad(p, X, a, t, 1.0, bf16_path=True)
+    ref = None
+    if with_ref:  # mutation rows against the amino acid before the move, some of them no-ops
+        ref = np.where(a < 20, rng.integers(0, 20, n), -1).astype(np.int32)
+        ref[:10] = a[:10] = 7
+    loss, g = ctx.mlp_loss_grad(X, a, t, 1.0, ref=ref)
+    rloss, rg = mo.loss_grad(p, X, a, t, 1.0, bf16_path=True, ref=ref)
     assert abs(loss - rloss) <= 1e-3 * max(1.0, abs(rloss))
     for a_, b_ in BLOCKS:
         gg, rr = _block(g, a_, b_).astype(np.float64), _block(rg, a_, b_)
@@ -157,8 +168,9 @@ def test_loss_grad_matches_oracle(ctx, pkg, n):
 
 @pytest.mark.gpu
 def test_training_fits_a_learnable_target(ctx, pkg):
-    """Tuples whose energy change is a fixed function of the environment: Adam on
-    the GPU drives the loss down by an order of magnitude."""
+    """Tuples whose energy change is a fixed function of the environment (a mutation
+    old -> new: f_new(env) - f_old(env), as the network's mutation queries model it):
+    Adam on the GPU drives the loss down by an order of magnitude."""
     ag_aa, ag_ca = _antigen(ctx, pkg)
     rng = np.random.default_rng(21)
     n = 20000
@@ -170,7 +182,8 @@ def test_training_fits_a_learnable_target(ctx, pkg):
     act = rng.integers(0, 20, n).astype(np.uint8)
     feats = mo.features(ag_ca, ag_aa, ca, aa)
     w = np.random.default_rng(3).normal(size=(160, 20)) * 0.3
-    target = (feats[:, 20:] @ w)[np.arange(n), act] * 0.5
+    f_env = feats[:, 20:] @ w
+    target = (f_env[np.arange(n), act] - f_env[np.arange(n), aa]) * 0.5
     tup = np.zeros(n, pkg.MC_TUPLE)
     tup["x"], tup["y"], tup["z"] = ca[:, 0], ca[:, 1], ca[:, 2]
     tup["delta_e"] = target.astype(np.float32)
