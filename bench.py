@@ -513,16 +513,17 @@ def run_batched(pkg, ctx, torch, ext):
             "best_energy_per_antigen": [float(e_last[t[0]]) for t in top]}
 
 
-SCHEDULES = (150, 300, 600)  # annealed schedule lengths of the learned-proposal study
+SCHEDULES = (150, 200, 300, 450, 600)  # annealed schedule lengths of the learned-proposal study
 
 
-def run_learned(pkg, ctx, seeds=(21, 22, 23), n_res=20):
+def run_learned(pkg, ctx, seeds=(21, 22, 23, 24, 25), n_res=20):
     """The learned proposal (configs of the learned-proposal workload): plain-MC
     tuples on 4 training antigens, GPU training, then annealed runs on a held-out
     antigen, uniform vs learned proposal.  Time to target = first wall time at which
     a run's champion is within 0.5 kcal/mol of the uniform proposal's median final
-    champion on the 600-step schedule; reported per schedule length (150 / 300 /
-    600 steps) and for each method at its best length (median over seeds)."""
+    champion on the 600-step schedule; reported per schedule length (SCHEDULES, the
+    same grid for every method) and for each method at its best length (median over
+    the seeds)."""
     L = pkg.learned
     cfg = pkg.workloads.config4(n_train=4, n_eval=1)
     shell = float(cfg["train"][0][1])

@@ -296,33 +296,19 @@ __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* r
     }
 }
 
-// Softmax of the logits l_k = -y[k] / tp over k < n (n <= 32) by one warp, lane k
-// holding option k: returns lane k's weight w_k = exp(l_k - m) and, in every lane,
-// the log normaliser lz = m + log(sum w).  The same code evaluates the forward and
-// the reverse proposal, so a reverse probability equals, bit for bit, the forward
-// probability the network would give from the proposed state.
-__device__ __forceinline__ double warp_softmax(const float* y, int n, float tp, double* lz) {
+// Choice among n options (n <= 32) with probabilities softmax(-y / tp), by one
+// warp, lane k holding option k: weights w_k = exp(l_k - m), l_k = -y[k] / tp,
+// m = max l, and the inverse CDF on u = dz / 2^32 over their prefix sums (for equal
+// logits exactly urange(dz, n): the prefix sums are then exact integers).  Returns
+// the option (all lanes).  Its log probability is never needed: a move's Hastings
+// ratio is a difference of two logits of the same softmax.
+__device__ int warp_sample(const float* y, int n, float tp, uint32_t dz) {
     const int lane = threadIdx.x & 31;
     const double l = lane < n ? -(double)y[lane] / (double)tp : -INFINITY;
     double m = l;
 #pragma unroll
     for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const double w = lane < n ? exp(l - m) : 0.0;
-    double sum = w;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    *lz = m + log(sum);
-    return w;
-}
-
-// Choice among n options by inverse CDF on u = dz / 2^32 over the warp's softmax
-// weights (for equal logits exactly urange(dz, n): the prefix sums are then exact
-// integers).  Returns the option (all lanes) and its log probability in *lq.
-__device__ int warp_sample(const float* y, int n, float tp, uint32_t dz, double* lq) {
-    const int lane = threadIdx.x & 31;
-    double lz;
-    const double w = warp_softmax(y, n, tp, &lz);
-    double cum = w;  // inclusive prefix sum in lane order
+    double cum = lane < n ? exp(l - m) : 0.0;  // inclusive prefix sum in lane order
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const double v = __shfl_up_sync(0xffffffffu, cum, o);
@@ -331,9 +317,7 @@ __device__ int warp_sample(const float* y, int n, float tp, uint32_t dz, double*
     const double total = __shfl_sync(0xffffffffu, cum, 31);
     const double target = (double)dz * (1.0 / 4294967296.0) * total;
     const unsigned hit = __ballot_sync(0xffffffffu, lane < n && target < cum);
-    const int pick = hit ? __ffs(hit) - 1 : n - 1;
-    *lq = -(double)y[pick] / (double)tp - lz;
-    return pick;
+    return hit ? __ffs(hit) - 1 : n - 1;
 }
 
 // The residue a move leaves: which = SEL_PROP builds the proposal, SEL_REJ the state
@@ -493,15 +477,14 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
         for (int i = warp; i < rows; i += AN_WARPS) {  // one warp per row
             const int r = S.mvl[base + i];
             const float* y = T.y + i * MT_YS;
-            double lq;
             if (S.kind[r] == MV_ROT) {
-                const int k = warp_sample(y + N_AA, s_rot_n[S.aa[r]], tp, S.dz[r], &lq);
+                const int k = warp_sample(y + N_AA, s_rot_n[S.aa[r]], tp, S.dz[r]);
                 if (lane == 0) {
                     S.new_rot[r] = k;
                     S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
                 }
             } else {
-                const int a = warp_sample(y, N_AA, tp, S.dz[r], &lq);
+                const int a = warp_sample(y, N_AA, tp, S.dz[r]);
                 if (lane == 0) {
                     S.new_aa[r] = a;
                     S.lhr[r] = -(double)y[S.aa[r]] / (double)tp + (double)y[a] / (double)tp;

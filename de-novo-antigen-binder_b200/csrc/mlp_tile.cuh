@@ -2,8 +2,8 @@
 // tile of at most 16 residues (the residues of one candidate that drew a move in
 // a step: a handful of rows, below the 64/128-row tiles of tcgen05.mma, so the
 // CTA's eight warps use the warp-level BF16 MMA, m16n8k16 with FP32 accumulators).
-// Weights are read from global memory (L2-resident, 240 KB) in fragment order with
-// 16-byte loads, in a few large register batches per layer; activations stay in
+// Weights are read from global memory (L2-resident, 240 KB, not cached in L1) in
+// fragment order with 16-byte loads, in a few large register batches per layer; activations stay in
 // shared memory as BF16, the output as FP32.  Same arithmetic as the batched
 // tensor-core path up to the order of the FP32 sums.
 #pragma once
@@ -51,7 +51,9 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a
 }
 
 __device__ __forceinline__ uint32_t ld_s32(const __nv_bfloat16* p) { return *(const uint32_t*)p; }
-__device__ __forceinline__ uint4 ld_g128(const uint4* p) { return __ldg(p); }
+// weights are cached in L2 only: streamed through L1 they would evict the antigen
+// atoms that the CTA's energy evaluations read from it
+__device__ __forceinline__ uint4 ld_g128(const uint4* p) { return __ldcg(p); }
 // SiLU as the batched GEMM epilogue computes it: z * sigmoid, sigmoid = 1 / (1 + e^-z)
 // with the fast exponential and a correctly rounded reciprocal
 __device__ __forceinline__ float silu_f(float z) { return z * __frcp_rn(1.0f + __expf(-z)); }
