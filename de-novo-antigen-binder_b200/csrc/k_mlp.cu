@@ -1,6 +1,6 @@
 // k_mlp.cu — the learned mutation / rotamer proposal network on sm_100a.
 //
-// Network: 180 environment features -> 256 (SiLU) -> 256 (SiLU) -> 25 outputs
+// Network: 180 environment features -> 128 (SiLU) -> 128 (SiLU) -> 25 outputs
 // (predicted Metropolis energy change of a mutation to each of the 20 amino acids
 // and of each of the 5 rotamers).  Weights and activations are BF16, every sum is
 // FP32.  The dense layers of training and of batched inference run on the 5th-gen
@@ -17,6 +17,8 @@
 // Shell membership compares r^2 (the reference's f32 rounding) with the exact
 // f32 squares of the shell radii, and log1p comes from a table filled on the
 // host, so the features are bit-identical wherever they are computed.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 
 #include "kernels.h"
@@ -439,8 +441,9 @@ __device__ __forceinline__ uint4 pack_frag(const float* __restrict__ w, int K, i
     return make_uint4(v[0], v[1], v[2], v[3]);
 }
 
-// BF16 copies of the weights: W1 [256][192], W2 [256][256] and W2^T, W3 [32][256] and
-// W3^T, and the fragment-order copies of W1, W2, W3
+// BF16 copies of the weights: W1 [H][192], W2 [H][H] and W2^T, W3 [32][H] and W3^T,
+// and the fragment-order copies of W1, W2, W3 (one thread per element of the
+// largest of them)
 __global__ void k_pack_weights(const float* __restrict__ p, MlpBf16 o) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < (MLP_H / 8) * (MLP_K1 / 32) * 32) {
@@ -526,7 +529,8 @@ void launch_adam(cudaStream_t s, int n, float* w, const float* g, float* m1, flo
     if (n > 0) k_adam<<<(n + 255) / 256, 256, 0, s>>>(n, w, g, m1, m2, lr, b1, b2, eps, bc1, bc2);
 }
 void launch_pack_weights(cudaStream_t s, const float* p, const MlpBf16& o) {
-    k_pack_weights<<<(MLP_H * MLP_H + 255) / 256, 256, 0, s>>>(p, o);
+    const int n = std::max(MLP_H * MLP_K1, std::max(MLP_H * MLP_H, MLP_OUT_PAD * MLP_H));
+    k_pack_weights<<<(n + 255) / 256, 256, 0, s>>>(p, o);
 }
 void launch_gather_tuples(cudaStream_t s, int m, const int* idx, const MlpTuple* tup, float* ca, uint8_t* aa, int* ag,
                           int* action, int* ref, float* target) {

@@ -11,15 +11,15 @@ namespace binder {
 
 constexpr int MLP_IN = 180;       // 20 one-hot + 8 shells x 20 amino acids
 constexpr int MLP_K1 = 192;       // first-layer K padded to the MMA K step
-constexpr int MLP_H = 256;        // hidden width
+constexpr int MLP_H = 128;        // hidden width
 constexpr int MLP_OUT = 25;       // 20 mutation targets + 5 rotamers
 constexpr int MLP_OUT_PAD = 32;   // output rows of W3 (rows >= 25 stay zero)
 constexpr int MLP_SHELLS = 8;     // radial shells of 1.25 A out to 10 A
 constexpr int MLP_COUNT_CAP = 255;
 constexpr int MLP_NO_AA = 255;    // amino-acid input of a mutation query: none (no one-hot)
 
-// flat FP32 parameter vector: W1 [256][192], b1 [256], W2 [256][256], b2 [256],
-// W3 [32][256], b3 [32]
+// flat FP32 parameter vector: W1 [128][192], b1 [128], W2 [128][128], b2 [128],
+// W3 [32][128], b3 [32]
 constexpr int MLP_OFF_W1 = 0;
 constexpr int MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_K1;
 constexpr int MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;
@@ -93,14 +93,14 @@ __host__ __device__ constexpr int frag_index(int t, int sp, int lane, int K) { r
 
 // BF16 weight copies used by the GEMMs and the Metropolis kernel's network tile
 struct MlpBf16 {
-    __nv_bfloat16* w1;   // [256][192]
-    __nv_bfloat16* w2;   // [256][256]
-    __nv_bfloat16* w2t;  // [256][256] transposed
-    __nv_bfloat16* w3;   // [32][256]
-    __nv_bfloat16* w3t;  // [256][32] transposed
-    uint4* f1;           // W1 in fragment order (32 x 6 x 32)
-    uint4* f2;           // W2 in fragment order (32 x 8 x 32)
-    uint4* f3;           // W3 in fragment order (4 x 8 x 32)
+    __nv_bfloat16* w1;   // [H][192]
+    __nv_bfloat16* w2;   // [H][H]
+    __nv_bfloat16* w2t;  // [H][H] transposed
+    __nv_bfloat16* w3;   // [32][H]
+    __nv_bfloat16* w3t;  // [H][32] transposed
+    uint4* f1;           // W1 in fragment order (H/8 n-tiles x 6 k-step pairs x 32 lanes)
+    uint4* f2;           // W2 in fragment order (H/8 x H/32 x 32)
+    uint4* f3;           // W3 in fragment order (4 x H/32 x 32)
 };
 
 // One logged Metropolis proposal (binder_mc_tuple of the C ABI, 32 bytes).

@@ -2,7 +2,7 @@
 // tile of at most 16 residues (the residues of one candidate that drew a move in
 // a step: a handful of rows, below the 64/128-row tiles of tcgen05.mma, so the
 // CTA's eight warps use the warp-level BF16 MMA, m16n8k16 with FP32 accumulators).
-// Weights are read from global memory (L2-resident, 240 KB, not cached in L1) in
+// Weights are read from global memory (L2-resident, 88 KB, not cached in L1) in
 // fragment order with 16-byte loads, in a few large register batches per layer; activations stay in
 // shared memory as BF16, the output as FP32.  Same arithmetic as the batched
 // tensor-core path up to the order of the FP32 sums.
@@ -16,7 +16,7 @@ namespace binder {
 
 constexpr int MT_ROWS = 16;
 constexpr int MT_XS = 200;  // X row stride (BF16): 100 words, rows land on distinct banks
-constexpr int MT_HS = 264;  // H row stride (BF16): 132 words
+constexpr int MT_HS = MLP_H + 8;  // H row stride (BF16): 4 words mod 32, rows land on distinct banks
 constexpr int MT_YS = MLP_OUT_PAD;
 // shared-memory bytes of a tile: X, H1, H2 (BF16), Y (FP32), environment counts (int)
 constexpr int MT_X_BYTES = MT_ROWS * MT_XS * 2;
@@ -60,7 +60,7 @@ __device__ __forceinline__ float silu_f(float z) { return z * __frcp_rn(1.0f + _
 
 // Weight registers of a lane: one batch of a layer's fragments (16 bytes per n-tile
 // per pair of k-steps), at most MT_WREGS of them.
-constexpr int MT_WREGS = 16;
+constexpr int MT_WREGS = 12;
 
 // Batch bi of a layer's weights for the warp's n-tiles n_tile0 .. n_tile0+NT-1:
 // pairs of k-steps bi*PB .. bi*PB+PB-1.
@@ -141,13 +141,18 @@ __device__ __forceinline__ void mlp_tile_layer(uint4 (&w)[MT_WREGS], const __nv_
     }
 }
 
-// Batches: layer 1 (K 192) two of three k-step pairs, layer 2 (K 256) two of four,
-// both over four n-tiles per warp; layer 3 (32 outputs, warps 0-3) one of eight.
-constexpr int MT_PB1 = 3, MT_PB2 = 4, MT_PB3 = 8;
+// Shapes: layers 1 and 2 over MT_NT n-tiles of 8 columns per warp (the 8 warps
+// cover the hidden width), each in one batch of all its k-step pairs (layer 1:
+// 6 pairs x 2 n-tiles, layer 2: 4 x 2 -- one L2 round trip per layer); layer 3
+// (32 outputs) on warps 0-3, one n-tile and 4 pairs each.
+constexpr int MT_NT = MLP_H / 64;
+constexpr int MT_PB1 = MLP_K1 / 32, MT_PB2 = MLP_H / 32, MT_PB3 = MLP_H / 32;
+static_assert(MT_NT * MT_PB1 <= MT_WREGS && MT_NT * MT_PB2 <= MT_WREGS && MT_PB3 <= MT_WREGS,
+              "weight batches must fit the registers");
 
 // Batch 0 of layer 1 into w: issue it before the tile's inputs are ready.
 __device__ __forceinline__ void mlp_tile_prefetch(const MlpDev& M, uint4 (&w)[MT_WREGS]) {
-    mlp_tile_fetch<MLP_K1, 4, MT_PB1>(w, M.f1, (int)(threadIdx.x >> 5) * 4, 0);
+    mlp_tile_fetch<MLP_K1, MT_NT, MT_PB1>(w, M.f1, (int)(threadIdx.x >> 5) * MT_NT, 0);
 }
 
 // Network outputs of rows 0 .. rows-1 of T.x into T.y, by the 8 warps of the CTA
@@ -156,11 +161,12 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpDev& M, const MlpTile&
                                                  int rows) {
     const int warp = threadIdx.x >> 5;
     const bool out_warp = warp < MLP_OUT_PAD / 8;
-    mlp_tile_layer<MLP_K1, 4, MT_PB1, true, MLP_H, 4, MT_PB2>(w, T.x, MT_XS, M.f1, warp * 4, M.b1, T.h1, MT_HS,
-                                                               nullptr, M.f2, warp * 4, rows);
+    mlp_tile_layer<MLP_K1, MT_NT, MT_PB1, true, MLP_H, MT_NT, MT_PB2>(w, T.x, MT_XS, M.f1, warp * MT_NT, M.b1, T.h1,
+                                                                       MT_HS, nullptr, M.f2, warp * MT_NT, rows);
     __syncthreads();
-    mlp_tile_layer<MLP_H, 4, MT_PB2, true, MLP_H, 1, MT_PB3>(w, T.h1, MT_HS, M.f2, warp * 4, M.b2, T.h2, MT_HS,
-                                                              nullptr, out_warp ? M.f3 : nullptr, warp, rows);
+    mlp_tile_layer<MLP_H, MT_NT, MT_PB2, true, MLP_H, 1, MT_PB3>(w, T.h1, MT_HS, M.f2, warp * MT_NT, M.b2, T.h2,
+                                                                  MT_HS, nullptr, out_warp ? M.f3 : nullptr, warp,
+                                                                  rows);
     __syncthreads();
     if (out_warp)
         mlp_tile_layer<MLP_H, 1, MT_PB3, false, MLP_H, 1, MT_PB3>(w, T.h2, MT_HS, M.f3, warp, M.b3, nullptr, 0, T.y,

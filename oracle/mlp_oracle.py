@@ -9,7 +9,7 @@ the GPU kernels in de-novo-antigen-binder_b200/csrc/k_mlp.cu:
     log1p table rounded once to f32, BF16 round-to-nearest-even); a mutation
     query (amino acid NO_AA) carries no one-hot;
   * loss_grad(ref=...): mutation rows predict y[new] - y[old];
-  * forward() / loss_grad(): the MLP 180 -> 256 -> 256 -> 25 with SiLU in float64.
+  * forward() / loss_grad(): the MLP 180 -> 128 -> 128 -> 25 with SiLU in float64.
     With bf16=True the BF16 roundings of the GPU path are applied (weights, input
     rows, hidden activations, output and hidden gradients) and only the sums are
     exact, so the GPU's FP32 sums are compared against exact sums of the same
@@ -23,10 +23,14 @@ from __future__ import annotations
 
 import numpy as np
 
-MLP_IN, MLP_K1, MLP_H, MLP_OUT, MLP_OUT_PAD = 180, 192, 256, 25, 32
+MLP_IN, MLP_K1, MLP_H, MLP_OUT, MLP_OUT_PAD = 180, 192, 128, 25, 32
 N_AA, SHELLS = 20, 8
-OFF = {"w1": 0, "b1": 49152, "w2": 49408, "b2": 114944, "w3": 115200, "b3": 123392}
-N_PARAMS = 123424
+OFF = {"w1": 0, "b1": MLP_H * MLP_K1}
+OFF["w2"] = OFF["b1"] + MLP_H
+OFF["b2"] = OFF["w2"] + MLP_H * MLP_H
+OFF["w3"] = OFF["b2"] + MLP_H
+OFF["b3"] = OFF["w3"] + MLP_OUT_PAD * MLP_H
+N_PARAMS = OFF["b3"] + MLP_OUT_PAD
 SHELL_R2 = np.array([1.5625, 6.25, 14.0625, 25.0, 39.0625, 56.25, 76.5625], np.float32)
 LOG1P = np.array([np.float32(np.log1p(np.float64(n))) for n in range(256)], np.float32)
 

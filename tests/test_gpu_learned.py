@@ -55,7 +55,7 @@ def test_constant_network_reproduces_uniform_proposal(ctx, pkg):
     ctx.set_proposal(False)
     (a0, c0, p0), s0 = _run(ctx, aa, chi, pos, n_res, temps=temps)
     p = np.zeros(pkg.MLP_N_PARAMS, np.float32)
-    p[pkg.MLP_OFF["b1"]:pkg.MLP_OFF["b1"] + 256] = 0.3  # hidden units active, output weights zero
+    p[pkg.MLP_OFF["b1"]:pkg.MLP_OFF["b1"] + pkg.MLP_H] = 0.3  # hidden units active, output weights zero
     ctx.mlp_set_params(p)
     ctx.set_proposal(True, t_prop_min=0.5)
     (a1, c1, p1), s1 = _run(ctx, aa, chi, pos, n_res, temps=temps)

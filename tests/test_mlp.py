@@ -38,7 +38,7 @@ def _params(pkg, seed=0, scale=1.0):
     rng = np.random.default_rng(seed + 99)
     nz = np.zeros(mo.N_PARAMS, bool)
     for name in ("b1", "b2"):
-        nz[mo.OFF[name]:mo.OFF[name] + 256] = True
+        nz[mo.OFF[name]:mo.OFF[name] + mo.MLP_H] = True
     p[nz] = rng.uniform(-0.1, 0.1, nz.sum()).astype(np.float32)
     p[mo.OFF["b3"]:mo.OFF["b3"] + 25] = rng.uniform(-0.1, 0.1, 25).astype(np.float32)
     return (p * scale).astype(np.float32)
@@ -159,9 +159,9 @@ def test_loss_grad_matches_oracle(ctx, pkg, n, with_ref):
         assert np.linalg.norm(gg - rr) <= 3e-2 * np.linalg.norm(rr) + 1e-7, (a_, np.linalg.norm(gg - rr),
                                                                              np.linalg.norm(rr))
     # padding stays exactly zero
-    W1 = _block(g, "w1", "b1").reshape(256, 192)
+    W1 = _block(g, "w1", "b1").reshape(mo.MLP_H, 192)
     assert not W1[:, 180:].any()
-    assert not _block(g, "w3", "b3").reshape(32, 256)[25:].any()
+    assert not _block(g, "w3", "b3").reshape(32, mo.MLP_H)[25:].any()
     assert not g[mo.OFF["b3"] + 25:].any()
     assert np.array_equal(ctx.mlp_get_params(), p)  # no update
 
@@ -196,4 +196,4 @@ def test_training_fits_a_learnable_target(ctx, pkg):
     assert np.all(np.isfinite(losses))
     assert losses[-20:].mean() < 0.1 * losses[:5].mean(), (losses[:5], losses[-20:])
     p = ctx.mlp_get_params()
-    assert not p.reshape(-1)[mo.OFF["w1"]:mo.OFF["b1"]].reshape(256, 192)[:, 180:].any()
+    assert not p.reshape(-1)[mo.OFF["w1"]:mo.OFF["b1"]].reshape(mo.MLP_H, 192)[:, 180:].any()
