@@ -391,9 +391,8 @@ def run_ours(args, rank, world, local_rank):
         if b == 0:  # phase-1 pass from the initial population
             h_aa[:], h_chi[:], h_pos[:] = pop.aa, chi, pos
         t0 = time.perf_counter()
-        ctx.state_upload(h_aa, h_chi, h_pos, uniform_n_res=n_res)
-        ctx.block(N_STEPS_PER_BLOCK, b * N_STEPS_PER_BLOCK, TOP_K, out_e=h_e, out_top=h_top)
-        ctx.state_download(h_aa, h_chi, h_pos)
+        # upload, block, write-back of the moved residues (copied beside the score)
+        ctx.block_io(h_aa, h_chi, h_pos, N_STEPS_PER_BLOCK, TOP_K, uniform_n_res=n_res, out_e=h_e, out_top=h_top)
         if k:  # first iteration warms the pinned paths
             t_e2e.append(time.perf_counter() - t0)
     e2e_ms = max_over_ranks(torch, dist, world, 1e3 * statistics.mean(t_e2e), device)
@@ -439,7 +438,7 @@ def run_ours(args, rank, world, local_rank):
         "kernels": kern,
         "e2e": {"value": total_cand * N_STEPS_PER_BLOCK / (e2e_ms / 1e3), "unit": "candidate-steps/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "api": "binder_state_upload + binder_block + binder_state_download, pinned host buffers"},
+                "api": "binder_block_io (state upload, block, state write-back), pinned host buffers"},
         "clocks": clocks, "gpu_launches": int(launches),
         "survivors": {"best_energy": float(surv_e[0]), "best_index": int(survivors[0])},
         "hbm_peak_gbs": peaks.get("hbm_gbs"), "peaks_file": peaks_kind,

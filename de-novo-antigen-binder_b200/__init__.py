@@ -154,6 +154,8 @@ _SIGS = {
     "binder_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "binder_timing_summary": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
     "binder_block_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_block_io": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "binder_state_pair_counts": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "binder_fp32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "binder_mc_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
@@ -618,6 +620,26 @@ class GpuContext:
         e = np.zeros(self._state_cand, np.float64) if out_e is None else out_e
         top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
         self._check(lib().binder_block(self._h, n_steps, step0, k, _ptr(e), _ptr(top)))
+        return e, (top.reshape(n_segments, k) if k else None)
+
+    def block_io(self, aa, chi, pos, n_steps, k=64, uniform_n_res=0, n_res=None, n_segments=1, out_e=None,
+                 out_top=None):
+        """Upload the population (aa uint8[R], chi float32[R][4], pos float32[R][14][3]),
+        run one block and write the moved residues back into the same arrays (they
+        must be C-contiguous arrays of those types: pinned ones copy fastest);
+        returns the energies and the top-k as block() does (n_segments = the number of
+        resident antigens)."""
+        for a, t in ((aa, np.uint8), (chi, np.float32), (pos, np.float32)):
+            if not (isinstance(a, np.ndarray) and a.dtype == t and a.flags["C_CONTIGUOUS"] and a.flags["WRITEABLE"]):
+                raise TypeError("block_io needs writable C-contiguous %s arrays" % np.dtype(t).name)
+        nr = None if n_res is None else np.ascontiguousarray(n_res, np.int32)
+        n_cand = len(nr) if nr is not None else len(aa) // max(1, uniform_n_res)
+        e = np.zeros(n_cand, np.float64) if out_e is None else out_e
+        top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
+        self._check(lib().binder_block_io(self._h, n_cand, _ptr(nr), uniform_n_res, None, None, _ptr(aa), _ptr(chi),
+                                          _ptr(pos), n_steps, k, _ptr(e), _ptr(top)))
+        self._state_res = len(aa)
+        self._state_cand = n_cand
         return e, (top.reshape(n_segments, k) if k else None)
 
     def block_async(self, n_steps, step0=0, k=64):

@@ -115,9 +115,9 @@ struct State {
     std::vector<int> h_res_off, h_cand_ag;
     std::vector<uint32_t> h_cand_id;
     std::vector<int> h_orig;  // index of each candidate in the last full upload
+    int meta_epoch = -1;      // the antigen-set epoch the device metadata was built for
     int max_res = 0;
     // chi sin/cos for the Metropolis kernel, derived from the uploaded chi on first use
-    std::vector<float> h_chi_upload;
     bool trig_valid = false;
     // Metropolis statistics, 4 per candidate (tried / accepted: mutation+rotamer, backbone)
     DBuf<long long> mc_stats;
@@ -239,6 +239,9 @@ struct binder_ctx {
     // antigen-set epoch (device word read by the gradient-step kernel)
     DBuf<int> d_ag_epoch;
     int ag_epoch = 0;
+    // binder_block_io: the state download runs on a second stream beside the score
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void drop_graph() {
         if (block_graph) cudaGraphExecDestroy(block_graph);
         block_graph = nullptr;
@@ -247,6 +250,9 @@ struct binder_ctx {
         drop_graph();
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
     }
 };
 static const int TIMING_RING = 4096;
@@ -1044,11 +1050,18 @@ int ensure_trig(binder_ctx* ctx) {
     State& S = ctx->st;
     if (S.trig_valid) return BINDER_OK;
     const int total = S.total_res;
+    // the device chi are still the uploaded ones: only Metropolis steps change chi,
+    // and they run after this
+    std::vector<float> chi((size_t)4 * std::max(total, 1));
+    if (total) {
+        CK(cudaMemcpyAsync(chi.data(), S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    }
     std::vector<float4> trig((size_t)2 * std::max(total, 1));
     for (int r = 0; r < total; ++r) {
         float sc[8];
         for (int k = 0; k < 4; ++k) {
-            const float x = S.h_chi_upload[4 * r + k] * RADS_PER_DEG;
+            const float x = chi[4 * r + k] * RADS_PER_DEG;
             sc[2 * k] = std::sin(x);
             sc[2 * k + 1] = std::cos(x);
         }
@@ -1116,6 +1129,7 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     CK(S.res_e.ensure(std::max(total, 1)), "alloc");
     CK(S.res_abs.ensure(std::max(total, 1)), "alloc");
     S.order_valid = false;
+    S.meta_epoch = ctx->ag_epoch;
     return BINDER_OK;
 }
 }  // namespace
@@ -1145,9 +1159,13 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
     for (int r = 0; r < total; ++r)
         if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
-    if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
+    // a population of the same shape (candidates, residue counts, antigens, ids)
+    // against the same antigen set keeps the device metadata; only the residues move
+    const bool same_meta = S.n_cand == (int)n_cand && S.meta_epoch == ctx->ag_epoch && S.h_res_off == off &&
+                           S.h_cand_ag == ag && S.h_cand_id == ids && S.h_orig == orig;
+    if (same_meta) S.order_valid = false;
+    else if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
     if ((s = upload(ctx, S.res_aa, aa, (size_t)total, "state"))) return s;
-    S.h_chi_upload.assign(chi, chi + (size_t)4 * total);
     S.trig_valid = false;
     CK(S.res_chi.ensure(total), "alloc");
     if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
@@ -1697,6 +1715,56 @@ int binder_block_fetch(binder_ctx* ctx, double* out_e, int32_t* out_topk) {
                            cudaMemcpyDeviceToHost, ctx->stream),
            "D2H");
     return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);
+}
+
+int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                    const int32_t* antigen_id, const uint32_t* cand_id, uint8_t* aa, float* chi, float* pos,
+                    int n_steps, int k, double* out_e, int32_t* out_topk) {
+    if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
+    int s = binder_state_upload(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos);
+    if (s) return s;
+    State& S = ctx->st;
+    if (!ctx->side) {
+        CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking), "stream");
+        CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event");
+        CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "event");
+    }
+    if (ctx->params.flags & BINDER_FLAG_AUTOTUNE) {
+        const std::string key = tune_key(ctx);
+        bool known = false;
+        for (const auto& e : ctx->tune_cache) known |= e.first == key;
+        if (!known && (s = binder_autotune(ctx, 5, nullptr))) return s;
+    }
+    ctx->async_pending = false;  // any enqueued blocks ran on the replaced state
+    if ((s = clear_err(ctx))) return s;
+    CK(ctx->energy.ensure(S.n_cand), "alloc");
+    if (k > 0) CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
+    ctx->last_k = k;
+    const int total = S.total_res;
+    CK(S.stage.ensure((size_t)total * SLOTS * 3), "alloc");
+    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return s;
+    // the moved residues go back to the host on the second stream while this one
+    // scores them (both only read the positions)
+    CK(cudaEventRecord(ctx->ev_fork, ctx->stream), "event");
+    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0), "event");
+    launch_unpack_slots(ctx->side, total, S.res_pos.p, S.stage.p);
+    LAUNCHED("unpack_slots");
+    CK(cudaMemcpyAsync(pos, S.stage.p, (size_t)total * SLOTS * 3 * 4, cudaMemcpyDeviceToHost, ctx->side), "D2H");
+    CK(cudaMemcpyAsync(chi, S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->side), "D2H");
+    CK(cudaMemcpyAsync(aa, S.res_aa.p, total, cudaMemcpyDeviceToHost, ctx->side), "D2H");
+    CK(cudaEventRecord(ctx->ev_join, ctx->side), "event");
+    if ((s = enqueue_score_state(ctx, 0))) return s;
+    if (k > 0) {
+        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
+                             ctx->topk.p);
+        LAUNCHED("topk");
+        if (out_topk)
+            CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * k * sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream),
+               "D2H");
+    }
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0), "event");
+    return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);  // synchronises both streams
 }
 
 void binder_default_run_cfg(binder_run_cfg* c) {

@@ -279,6 +279,16 @@ int binder_score_state(binder_ctx* ctx, int full, double* out_energies);
    block and reports any device error. */
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_energies, int32_t* out_topk);
 int binder_block_fetch(binder_ctx* ctx, double* out_energies, int32_t* out_topk);
+/* One search block on a population that lives in host memory (no reference
+   counterpart; the host side of diffusion.rs:1018-1057 when the caller keeps the
+   population): binder_state_upload of (n_cand, n_res, uniform_n_res, antigen_id,
+   cand_id, aa, chi, pos), binder_block(n_steps, 0, k, out_energies, out_topk),
+   then the moved residues written back into aa, chi and pos -- the same results as
+   the three calls, with the write-back copied on a second stream while the
+   candidates are scored.  Pinned host arrays give the copies full speed. */
+int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                    const int32_t* antigen_id, const uint32_t* cand_id, uint8_t* aa, float* chi, float* pos,
+                    int n_steps, int k, double* out_energies, int32_t* out_topk);
 
 /* ---- launch shapes and the autotuner (no reference counterpart) ----------------
    Results never depend on these: every residue is computed by the same lanes with

@@ -107,3 +107,26 @@ def test_autotune_flag_in_block(ctx, oracle, pkg):
     got = _run_blocks(ctx, aa, chi, pos, n_res)
     _same(ref, got)
     ctx.set_params(pkg.Params.defaults(shell_radius=ctx.params.shell_radius, seed=5))
+
+
+def test_block_io_matches_upload_block_download(ctx, oracle, pkg):
+    """binder_block_io (upload, block, write-back with the copy beside the score) gives
+    the results of binder_state_upload + binder_block + binder_state_download, block
+    after block on the written-back population, and leaves the same resident state."""
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg)
+    ref = []
+    a, c, p = aa.copy(), np.ascontiguousarray(chi, np.float32), np.ascontiguousarray(pos, np.float32)
+    for b in range(3):
+        ctx.state_upload(a, c, p, uniform_n_res=n_res)
+        e, t = ctx.block(10, 0, k=64)
+        a, c, p = ctx.state_download()
+        ref.append((e, t, a.copy(), c.copy(), p.copy()))
+    a, c, p = aa.copy(), np.array(chi, np.float32), np.array(pos, np.float32)
+    for b in range(3):
+        e, t = ctx.block_io(a, c, p, 10, k=64, uniform_n_res=n_res)
+        re, rt, ra, rc, rp = ref[b]
+        assert np.array_equal(e, re) and np.array_equal(t, rt)
+        assert np.array_equal(a, ra) and np.array_equal(c, rc) and np.array_equal(p, rp)
+    # the resident state is the written-back one
+    da, dc, dp = ctx.state_download()
+    assert np.array_equal(da, a) and np.array_equal(dc, c) and np.array_equal(dp, p)
