@@ -122,7 +122,8 @@ struct State {
     // Metropolis statistics, 4 per candidate (tried / accepted: mutation+rotamer, backbone)
     DBuf<long long> mc_stats;
     int n_segments = 0;
-    // residue order by Calpha cell for the Langevin kernel
+    // residue order by Calpha cell (an autotuned order of the gradient-step and
+    // scoring kernels)
     DBuf<int> key_base, keys, key_counts, key_cursor, order;
     int n_keys = 0;
     bool order_valid = false;
@@ -1136,9 +1137,10 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
 
 extern "C" {
 
-int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
-                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
-                        const float* pos) {
+// The upload; sync = wait for the copies (the caller may reuse its arrays at once).
+static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                             const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa,
+                             const float* chi, const float* pos, bool sync) {
     int s = enter(ctx);
     if (s) return s;
     if (ctx->ags.empty()) return fail(ctx, BINDER_ERR_STATE, "no antigen added");
@@ -1181,8 +1183,14 @@ int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, in
     if (total) LAUNCHED("pack_slots");
     CK(S.mc_stats.ensure(4 * n_cand), "alloc");
     CK(cudaMemsetAsync(S.mc_stats.p, 0, 4 * n_cand * sizeof(long long), ctx->stream), "memset");
-    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    if (sync) CK(cudaStreamSynchronize(ctx->stream), "synchronize");
     return BINDER_OK;
+}
+
+int binder_state_upload(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
+                        const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa, const float* chi,
+                        const float* pos) {
+    return state_upload_impl(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos, true);
 }
 
 int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n) {
@@ -1721,7 +1729,9 @@ int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_
                     const int32_t* antigen_id, const uint32_t* cand_id, uint8_t* aa, float* chi, float* pos,
                     int n_steps, int k, double* out_e, int32_t* out_topk) {
     if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
-    int s = binder_state_upload(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos);
+    // no wait after the upload: the write-back into the same arrays comes later on
+    // the streams, after the kernels that follow the copies
+    int s = state_upload_impl(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos, false);
     if (s) return s;
     State& S = ctx->st;
     if (!ctx->side) {

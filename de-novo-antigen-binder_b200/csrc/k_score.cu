@@ -365,8 +365,8 @@ __device__ __forceinline__ void score_group(const AgView* __restrict__ Ap, Group
 }
 
 // Resident state: persistent warps take residues from a work queue (an atomic
-// counter, residues in Calpha-cell order so neighbouring warps share antigen atoms
-// in L1) and write one FP64 energy per residue; k_sum_residues adds a candidate's
+// counter; residues in index order, or in Calpha-cell order so that neighbouring
+// warps share antigen atoms in L1 -- whichever the autotuner timed faster) and write one FP64 energy per residue; k_sum_residues adds a candidate's
 // residues in index order.  No CTA barrier: warps never wait for each other.
 template <int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
 __global__ void __launch_bounds__(NW * 32) k_score_residues(StateView st, const AgView* __restrict__ ags,

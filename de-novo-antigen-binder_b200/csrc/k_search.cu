@@ -8,7 +8,8 @@
 //    reference's probe order, four or eight lanes per residue evaluate the pair
 //    terms, lane 0 folds them in that order, and n_steps are fused per launch
 //    since in this phase every residue moves independently.
-//  * The residue visiting order by Calpha cell and the slot packing kernels.
+//  * The residue visiting order by Calpha cell (one of the autotuned orders of the
+//    gradient-step and scoring kernels) and the slot packing kernels.
 #include <algorithm>
 
 #include "geom.cuh"
@@ -74,7 +75,8 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 // and sums their terms in list order -- the reference's pair set in the reference's
 // order, hence the same f32 sum.  A Calpha leaving the skin rebuilds its list.
 //
-// G lanes per residue (G = 4 or 8; residues in Calpha-cell order): the lanes split
+// G lanes per residue (G = 4 or 8; residue order and schedule autotuned, see
+// res_of_slot and the work description below): the lanes split
 // the list entries, write their terms to shared memory, and lane 0 folds them in
 // order.  A list longer than CG_LIST_MAX, or a cell index near the i32 limits (where
 // the reference's cell arithmetic wraps), sends the residue to the one-lane 27-cell
