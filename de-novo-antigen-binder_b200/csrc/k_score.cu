@@ -201,11 +201,51 @@ __device__ __forceinline__ float warp_max_f(float v) {
 constexpr int GMAX = 16;
 constexpr int FLAT_GROUP = 8;
 
+// Group atom coordinates also as separate x / y / z arrays, so that the pair test
+// reads two atoms' coordinates as one 8-byte word; entries n..GMAX-1 hold GROUP_PAD.
+constexpr float GROUP_PAD = 1e30f;  // its squared distance to any atom overflows to +inf
+
 struct GroupSmem {
     float4 pos[GMAX];  // x, y, z, q*sqrt(332)
     float4 prm[GMAX];  // r_min_half, sqrt(epsilon), hydrophobic, AMBER type
+    __align__(8) float sx[GMAX];
+    __align__(8) float sy[GMAX];
+    __align__(8) float sz[GMAX];
     int q[64];         // queued antigen atom indices
 };
+
+__device__ __forceinline__ void group_xyz(GroupSmem& s, int lane, int n, float x, float y, float z) {
+    if (lane < n) {
+        s.sx[lane] = x;
+        s.sy[lane] = y;
+        s.sz[lane] = z;
+    } else if (lane < GMAX) {
+        s.sx[lane] = s.sy[lane] = s.sz[lane] = GROUP_PAD;
+    }
+}
+
+// Packed pairs of f32 (element 0 in the low word) and the sm_100 two-wide FP32
+// instructions; each element is rounded exactly as the scalar instruction rounds it.
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+    return (uint64_t)__float_as_uint(lo) | ((uint64_t)__float_as_uint(hi) << 32);
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float f2_lo(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float f2_hi(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
 
 struct SrcStateG {
     StateView st;
@@ -221,6 +261,9 @@ struct SrcStateG {
             bad = !finite3(p.x, p.y, p.z);
             s.pos[lane] = make_float4(p.x, p.y, p.z, m.x);
             s.prm[lane] = make_float4(m.y, m.z, m.w, (float)c_slot_type[aa][lane]);
+            group_xyz(s, lane, n, p.x, p.y, p.z);
+        } else {
+            group_xyz(s, lane, n, 0.f, 0.f, 0.f);
         }
         return n;
     }
@@ -243,12 +286,18 @@ struct SrcFlatG {
             bad = !finite3(p0.x, p0.y, p0.z);
             s.pos[lane] = make_float4(p0.x, p0.y, p0.z, p0.w * SQRT_COULOMB_K);
             s.prm[lane] = make_float4(p1.x, sqrtf(p1.y), p1.z > 0.5f ? 1.0f : 0.0f, 0.0f);
+            group_xyz(s, lane, n, p0.x, p0.y, p0.z);
+        } else {
+            group_xyz(s, lane, n, 0.f, 0.f, 0.f);
         }
         return n;
     }
 };
 
-// One antigen atom (this lane's) against the n group atoms in shared memory.
+// One antigen atom (this lane's) against the n group atoms in shared memory, two
+// group atoms per step: dx = b - a and r^2 = (dx*dx + dy*dy) + dz*dz in packed
+// f32x2 arithmetic, the reference's roundings, hence its pair set; the terms of
+// the pairs within the cutoff are added in group-atom order.
 template <bool KAHAN, bool FULL, bool ABS, bool COUNT>
 __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const float4* __restrict__ prm,
                                             const GroupSmem& s, int n, int idx, Acc& acc) {
@@ -256,40 +305,46 @@ __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const
     const float4 ap = __ldg(&prm[idx]);
     float part = 0.0f, pabs = 0.0f;
     int np = 0;
-    for (int j = 0; j < n; ++j) {
+    auto term = [&](int j, float r2) {
         const float4 b = s.pos[j];
         const float4 bp = s.prm[j];
-        const float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
-        const float r2 = xdist2(dx, dy, dz);  // reference rounding: same pair set
-        if (r2 <= CUTOFF_SQ && r2 >= MIN_R_SQ) {
-            const float ir = rsqrtf(r2);
-            const float ir2 = ir * ir;
-            const float R = bp.x + ap.x;
-            const float s2 = R * R * ir2;
-            const float s6 = s2 * s2 * s2;
-            const float lj = (bp.y * ap.y) * (s6 * (s6 - 2.0f));
-            const float coul = (b.w * a.w) * ir;
-            const float hyd = (r2 < HYDRO_CUTOFF_SQ) ? HYDRO_BONUS * (bp.z * ap.z) : 0.0f;
-            float e = lj + coul + hyd;
-            if (FULL) {
-                const int bt = (int)bp.w, at = (int)ap.w;
-                if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) &&
-                    r2 <= HB_CUTOFF_SQ) {
-                    const float z = (r2 * ir - HB_R0) / HB_SIGMA;
-                    e += -HB_DEPTH * __expf(-0.5f * z * z);
-                }
-                const float4 ej = c_eef1[bt];
-                if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
-                    const float4 ei = c_eef1[at];
-                    const float r = r2 * ir;
-                    const float xi = r / ei.z, xj = r / ej.z;
-                    e += -(ei.x * ej.y * __expf(-(xi * xi)) * ei.w + ej.x * ei.y * __expf(-(xj * xj)) * ej.w);
-                }
+        const float ir = rsqrtf(r2);
+        const float ir2 = ir * ir;
+        const float R = bp.x + ap.x;
+        const float s2 = R * R * ir2;
+        const float s6 = s2 * s2 * s2;
+        const float lj = (bp.y * ap.y) * (s6 * (s6 - 2.0f));
+        const float coul = (b.w * a.w) * ir;
+        const float hyd = (r2 < HYDRO_CUTOFF_SQ) ? HYDRO_BONUS * (bp.z * ap.z) : 0.0f;
+        float e = lj + coul + hyd;
+        if (FULL) {
+            const int bt = (int)bp.w, at = (int)ap.w;
+            if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) &&
+                r2 <= HB_CUTOFF_SQ) {
+                const float z = (r2 * ir - HB_R0) / HB_SIGMA;
+                e += -HB_DEPTH * __expf(-0.5f * z * z);
             }
-            part += e;
-            if (ABS) pabs += fabsf(lj) + fabsf(coul) + fabsf(hyd);
-            if (COUNT) ++np;
+            const float4 ej = c_eef1[bt];
+            if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
+                const float4 ei = c_eef1[at];
+                const float r = r2 * ir;
+                const float xi = r / ei.z, xj = r / ej.z;
+                e += -(ei.x * ej.y * __expf(-(xi * xi)) * ei.w + ej.x * ei.y * __expf(-(xj * xj)) * ej.w);
+            }
         }
+        part += e;
+        if (ABS) pabs += fabsf(lj) + fabsf(coul) + fabsf(hyd);
+        if (COUNT) ++np;
+    };
+    const uint64_t ax = f2_pack(a.x, a.x), ay = f2_pack(a.y, a.y), az = f2_pack(a.z, a.z);
+    for (int j = 0; j < n; j += 2) {
+        const uint64_t dx = f2_sub(*(const uint64_t*)&s.sx[j], ax);
+        const uint64_t dy = f2_sub(*(const uint64_t*)&s.sy[j], ay);
+        const uint64_t dz = f2_sub(*(const uint64_t*)&s.sz[j], az);
+        const uint64_t r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
+        const float r2a = f2_lo(r2), r2b = f2_hi(r2);
+        if (r2a <= CUTOFF_SQ && r2a >= MIN_R_SQ) term(j, r2a);
+        if (r2b <= CUTOFF_SQ && r2b >= MIN_R_SQ) term(j + 1, r2b);  // j + 1 = n: a pad, +inf
     }
     acc_add<KAHAN>(acc, part);
     if (ABS) acc.abs_s += pabs;
