@@ -164,7 +164,8 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
     return total;
 }
 
-constexpr int CG_IN_MAX = 48;  // in-cutoff list entries a residue holds per step
+constexpr int CG_IN_MAX = 48;      // in-cutoff list entries a residue holds per step
+constexpr float CG_NEAR_SQ = 99.0f;  // r^2 below which a pair is in adjacent 10 A cells
 
 // Residue of a lane group's slot: the cell-sorted permutation (order_mode 0), the
 // state's own order (1: candidate after candidate), or a stride through it (2:
@@ -331,8 +332,14 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         for (int s = 0; s < n_steps; ++s) {
             const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
             bool use_list = valid && nl <= CG_LIST_MAX && !cell_far(cx, cy, cz);
+            // Cells at least as wide as the cutoff and coordinates below 1e4 A: a pair
+            // whose r^2 (reference rounding) is <= CG_NEAR_SQ is then in adjacent cells
+            // (distance <= 9.95 A, under 0.995 cell edges however x * inv rounds), so the
+            // reference's cell test only decides the entries closer to the cutoff.
+            const bool near_adjacent = g.cell >= 10.0f && fabsf(ca.x) < 1e4f && fabsf(ca.y) < 1e4f &&
+                                       fabsf(ca.z) < 1e4f;
             // A-C in rounds: each round a group compacts its next in-cutoff list entries
-            // (adjacent cell, r^2 passing the reference's cutoff test; list order) up to
+            // (r^2 passing the reference's cutoff test, adjacent cell; list order) up to
             // CG_IN_MAX, the warp evaluates every group's compacted pairs one pair per lane,
             // and lane 0 of each group continues its sum in order -- the reference's sum,
             // however many rounds a residue needs.
@@ -348,12 +355,13 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
                         int i = 0;
                         if (j < nl) {
                             i = list[j];
-                            const int4 ce = ca_cell[i];
-                            if (abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
-                                abs((long long)ce.z - cz) <= 1) {
-                                const float4 a = ca_pq[i];
-                                const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
-                                ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                            const float4 a = ca_pq[i];
+                            const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
+                            ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                            if (ok && !(near_adjacent && r_sq <= CG_NEAR_SQ)) {  // the reference's cell test
+                                const int4 ce = ca_cell[i];
+                                ok = abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
+                                     abs((long long)ce.z - cz) <= 1;
                             }
                         }
                         const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << G) - 1u);
