@@ -6,7 +6,8 @@
 // (-0.0 folded onto +0.0, NaN after every number) and paired with their index,
 // so a plain lexicographic (key, index) order is exactly the stable sort.  The
 // CTA keeps a running best-k list in shared memory and merges the segment in
-// chunks with a bitonic sort of (chunk + best-k) elements.
+// chunks with a bitonic sort of (chunk + best-k) elements, its short-stride stages
+// in registers.
 #include "kernels.h"
 
 namespace binder {
@@ -20,6 +21,32 @@ __device__ __forceinline__ unsigned long long order_key(double e) {
     e = e + 0.0;                               // -0.0 -> +0.0
     unsigned long long b = (unsigned long long)__double_as_longlong(e);
     return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// Bitonic stages with stride < 32 for sizes size_lo..size_hi (powers of two): every
+// position p < N (N a multiple of 32, so whole warps take part or none) is held by
+// lane p % 32 of a warp, whose partner p ^ stride is a lane of the same warp.  The
+// lower position of a pair keeps the smaller (key, index) when the pair sorts
+// ascending (bit `size` of p clear), the larger otherwise.
+__device__ __forceinline__ void register_stages(unsigned long long* key, int* idx, int N, int size_lo, int size_hi) {
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        unsigned long long k = key[p];
+        int i = idx[p];
+        for (int size = size_lo; size <= size_hi; size <<= 1) {
+            for (int stride = min(size >> 1, 16); stride > 0; stride >>= 1) {
+                const unsigned long long ko = __shfl_xor_sync(0xffffffffu, k, stride);
+                const int io = __shfl_xor_sync(0xffffffffu, i, stride);
+                const bool lower = (p & stride) == 0, up = (p & size) == 0;
+                const bool other_less = (ko < k) || (ko == k && io < i);
+                if (other_less == (lower == up)) {  // take the partner's element
+                    k = ko;
+                    i = io;
+                }
+            }
+        }
+        key[p] = k;
+        idx[p] = i;
+    }
 }
 
 __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict__ e,
@@ -53,8 +80,14 @@ __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict_
             }
         }
         __syncthreads();
-        for (int size = 2; size <= N; size <<= 1) {
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        // bitonic sort of [0, N): the stages with stride >= 32 exchange through shared
+        // memory (a barrier each); those with stride < 32 pair lanes of one warp and run
+        // in registers with shuffles -- sizes 2..32 entirely, then the five last
+        // strides of every larger size
+        register_stages(key, idx, N, 2, 32);
+        __syncthreads();
+        for (int size = 64; size <= N; size <<= 1) {
+            for (int stride = size >> 1; stride >= 32; stride >>= 1) {
                 for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
                     const int lo = 2 * t - (t & (stride - 1));
                     const int hi = lo + stride;
@@ -69,6 +102,8 @@ __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict_
                 }
                 __syncthreads();
             }
+            register_stages(key, idx, N, size, size);
+            __syncthreads();
         }
         kept = (int)min((long long)k, (long long)kept + take);
         if (take <= 0) break;
