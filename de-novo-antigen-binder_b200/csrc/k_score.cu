@@ -380,19 +380,34 @@ __device__ __forceinline__ void score_group(const AgView* __restrict__ Ap, Group
     const float rc = reach * inv, rc2 = rc * rc;
     const int i0 = max(0, (int)floorf(ux - rc)), i1 = min(gnx - 1, (int)floorf(ux + rc));
     const int j0 = max(0, (int)floorf(uy - rc)), j1 = min(gny - 1, (int)floorf(uy + rc));
+    // the columns (i, j) in x-major order, 32 at a time: each lane finds one column's
+    // atom range (z-run of cells within reach) in parallel, then the warp takes the
+    // non-empty ranges in column order
+    const int nj = j1 - j0 + 1;
+    const int ncol = (i1 >= i0 && j1 >= j0) ? (i1 - i0 + 1) * nj : 0;
     int qn = 0;
-    for (int i = i0; i <= i1; ++i) {
-        const float ddx = fmaxf(fmaxf((float)i - ux, ux - (float)(i + 1)), 0.0f);
-        for (int j = j0; j <= j1; ++j) {
+    for (int c0 = 0; c0 < ncol; c0 += 32) {
+        int ra0 = 0, ra1 = 0;
+        if (c0 + lane < ncol) {
+            const int i = i0 + (c0 + lane) / nj, j = j0 + (c0 + lane) % nj;
+            const float ddx = fmaxf(fmaxf((float)i - ux, ux - (float)(i + 1)), 0.0f);
             const float ddy = fmaxf(fmaxf((float)j - uy, uy - (float)(j + 1)), 0.0f);
             const float rem2 = rc2 - ddx * ddx - ddy * ddy;
-            if (rem2 < 0.0f) continue;
-            const float rem = sqrtf(rem2);
-            const int k0 = max(0, (int)floorf(uz - rem)), k1 = min(gnz - 1, (int)floorf(uz + rem));
-            if (k0 > k1) continue;
-            const int base = (i * gny + j) * gnz;
-            const int a0 = __ldg(&cell_start[base + k0]);
-            const int a1 = __ldg(&cell_start[base + k1 + 1]);
+            if (rem2 >= 0.0f) {
+                const float rem = sqrtf(rem2);
+                const int k0 = max(0, (int)floorf(uz - rem)), k1 = min(gnz - 1, (int)floorf(uz + rem));
+                if (k0 <= k1) {
+                    const int base = (i * gny + j) * gnz;
+                    ra0 = __ldg(&cell_start[base + k0]);
+                    ra1 = __ldg(&cell_start[base + k1 + 1]);
+                }
+            }
+        }
+        unsigned live = __ballot_sync(0xffffffffu, ra1 > ra0);
+        while (live) {
+            const int src = __ffs(live) - 1;
+            live &= live - 1;
+            const int a0 = __shfl_sync(0xffffffffu, ra0, src), a1 = __shfl_sync(0xffffffffu, ra1, src);
             for (int t0 = a0; t0 < a1; t0 += 32) {
                 const int t = t0 + lane;
                 bool pass = false;
@@ -421,8 +436,9 @@ __device__ __forceinline__ void score_group(const AgView* __restrict__ Ap, Group
 
 // Resident state: persistent warps take residues from a work queue (an atomic
 // counter; residues in index order, or in Calpha-cell order so that neighbouring
-// warps share antigen atoms in L1 -- whichever the autotuner timed faster) and write one FP64 energy per residue; k_sum_residues adds a candidate's
-// residues in index order.  No CTA barrier: warps never wait for each other.
+// warps share antigen atoms in L1 -- whichever the autotuner timed faster) and
+// write one FP64 energy per residue; k_sum_residues adds a candidate's residues in
+// index order.  No CTA barrier: warps never wait for each other.
 template <int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
 __global__ void __launch_bounds__(NW * 32) k_score_residues(StateView st, const AgView* __restrict__ ags,
                                                              const int* __restrict__ order, int* __restrict__ queue,
