@@ -622,8 +622,8 @@ class GpuContext:
         self._check(lib().binder_block(self._h, n_steps, step0, k, _ptr(e), _ptr(top)))
         return e, (top.reshape(n_segments, k) if k else None)
 
-    def block_io(self, aa, chi, pos, n_steps, k=64, uniform_n_res=0, n_res=None, n_segments=1, out_e=None,
-                 out_top=None):
+    def block_io(self, aa, chi, pos, n_steps, k=64, uniform_n_res=0, n_res=None, antigen_id=None, cand_id=None,
+                 n_segments=1, out_e=None, out_top=None):
         """Upload the population (aa uint8[R], chi float32[R][4], pos float32[R][14][3]),
         run one block and write the moved residues back into the same arrays (they
         must be C-contiguous arrays of those types: pinned ones copy fastest);
@@ -634,10 +634,12 @@ class GpuContext:
                 raise TypeError("block_io needs writable C-contiguous %s arrays" % np.dtype(t).name)
         nr = None if n_res is None else np.ascontiguousarray(n_res, np.int32)
         n_cand = len(nr) if nr is not None else len(aa) // max(1, uniform_n_res)
+        agi = None if antigen_id is None else np.ascontiguousarray(antigen_id, np.int32)
+        cid = None if cand_id is None else np.ascontiguousarray(cand_id, np.uint32)
         e = np.zeros(n_cand, np.float64) if out_e is None else out_e
         top = (np.zeros(n_segments * k, np.int32) if k else None) if out_top is None else out_top
-        self._check(lib().binder_block_io(self._h, n_cand, _ptr(nr), uniform_n_res, None, None, _ptr(aa), _ptr(chi),
-                                          _ptr(pos), n_steps, k, _ptr(e), _ptr(top)))
+        self._check(lib().binder_block_io(self._h, n_cand, _ptr(nr), uniform_n_res, _ptr(agi), _ptr(cid), _ptr(aa),
+                                          _ptr(chi), _ptr(pos), n_steps, k, _ptr(e), _ptr(top)))
         self._state_res = len(aa)
         self._state_cand = n_cand
         return e, (top.reshape(n_segments, k) if k else None)

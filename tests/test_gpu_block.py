@@ -130,3 +130,27 @@ def test_block_io_matches_upload_block_download(ctx, oracle, pkg):
     # the resident state is the written-back one
     da, dc, dp = ctx.state_download()
     assert np.array_equal(da, a) and np.array_equal(dc, c) and np.array_equal(dp, p)
+
+
+def test_block_io_ragged_antigens(ctx, pkg):
+    """Ragged candidates over several resident antigens: binder_block_io's energies,
+    per-antigen top-k and written-back residues equal those of the three separate
+    calls."""
+    cfg = pkg.workloads.config2(n_cand=256)
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=26.0, seed=6))
+    for ag_aa, ag_ca in cfg["antigens"]:
+        p_a, _ = ctx.build_residues(ag_ca, ag_aa)
+        ctx.add_antigen(ag_aa, p_a)
+    pop = cfg["pop"]
+    pos, chi = ctx.build_residues(pop.ca, pop.aa)
+    n_seg = len(cfg["antigens"])
+    ctx.state_upload(pop.aa, chi, pos, n_res=pop.n_res, antigen_id=pop.antigen_id)
+    e0, t0 = ctx.block(10, 0, k=16, n_segments=n_seg)
+    a0, c0, p0 = ctx.state_download()
+    a = pop.aa.copy()
+    c = np.array(chi, np.float32)
+    p = np.array(pos, np.float32)
+    e1, t1 = ctx.block_io(a, c, p, 10, k=16, n_res=pop.n_res, antigen_id=pop.antigen_id, n_segments=n_seg)
+    assert np.array_equal(e0, e1) and np.array_equal(t0, t1)
+    assert np.array_equal(a0, a) and np.array_equal(c0, c) and np.array_equal(p0, p)
