@@ -387,11 +387,17 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
                                    __shfl_sync(0xffffffffu, ca.z, src), __shfl_sync(0xffffffffu, res.x, src),
                                    __shfl_sync(0xffffffffu, res.y, src), __shfl_sync(0xffffffffu, res.z, src),
                                    __shfl_sync(0xffffffffu, res.w, src)};
+                    // the antigen Calphas of the pair's own residue: the groups of a warp
+                    // may probe different antigens
+                    const float4* q_pq = reinterpret_cast<const float4*>(
+                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(ca_pq), src));
+                    const float4* q_prm = reinterpret_cast<const float4*>(
+                        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(ca_prm), src));
                     if (pidx < total) {
                         const int k = pidx - pre[q];
                         const int i = s_in[rl0 + q][k];
                         float tx, ty, tz;
-                        cg_term_parts(body, ca_pq[i], ca_prm[i], tx, ty, tz);
+                        cg_term_parts(body, q_pq[i], q_prm[i], tx, ty, tz);
                         s_term[rl0 + q][k] = make_float3(tx, ty, tz);
                     }
                 }

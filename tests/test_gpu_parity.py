@@ -249,6 +249,41 @@ def test_langevin_steps_bit_exact(ctx, oracle, pkg, with_noise):
     assert np.array_equal(g_aa, aa) and np.array_equal(g_pos, pos)
 
 
+@pytest.mark.parametrize("with_noise", [False, True])
+def test_langevin_steps_bit_exact_mixed_antigens(ctx, oracle, pkg, with_noise):
+    """Ragged candidates of 8 antigens interleaved, so that the warps of the
+    gradient-step kernel hold residues of different antigens: every candidate's
+    trajectory equals the oracle's against its own antigen, under the default
+    schedule (candidate order, work queue) and the Calpha-cell order on a static grid."""
+    cfg = pkg.workloads.config2(n_cand=48)
+    pop = cfg["pop"]
+    As = []
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=26.0, seed=1234))
+    for ag_aa, ag_ca in cfg["antigens"]:
+        ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+        ctx.add_antigen(ag_aa, ag_pos)
+        As.append(oracle.Antigen(ag_aa, ag_pos))
+    pos0, chi0 = oracle.build_residues(pop.ca, pop.aa)
+    off = np.concatenate([[0], np.cumsum(pop.n_res)])
+    n_steps = 10
+    temps = np.array([oracle.temperature(i, 600) for i in range(n_steps)], np.float32)
+    aa, chi, pos = pop.aa.copy(), chi0.copy(), pos0.copy()
+    prm = oracle.OrcParams.defaults(shell_radius=26.0, seed=1234)
+    for s in range(n_steps):
+        for c in range(len(pop.n_res)):
+            o0, o1 = off[c], off[c + 1]
+            As[pop.antigen_id[c]].step(prm, aa[o0:o1], chi[o0:o1], pos[o0:o1], int(pop.n_res[c]), [c], s,
+                                       temps[s], with_noise, False)
+    for shape in ((8, 4, 8, 8, 1, 1, 1), (8, 4, 8, 8, 0, 0, 0)):
+        ctx.set_launch_cfg(*shape)
+        ctx.state_upload(pop.aa, chi0, pos0, n_res=pop.n_res, antigen_id=pop.antigen_id)
+        ctx.diffuse(n_steps, step0=0, with_noise=with_noise, temps=temps)
+        g_aa, g_chi, g_pos = ctx.state_download()
+        assert np.array_equal(g_aa, aa) and np.array_equal(g_pos, pos), shape
+    ctx.set_launch_cfg()
+
+
 def test_block_scores_and_survivors(ctx, oracle, pkg):
     cfg = pkg.workloads.config1(n_cand=256)
     A, aa, chi, pos, n_res = _setup_search(ctx, oracle, pkg, cfg, 256)
