@@ -227,7 +227,8 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         if (a0 < 0 && !queue) {
             const int first = blockIdx.x * RPC;
             const int last = min(first + RPC, st.total_res) - 1;
-            // orders 0 and 1 sort by antigen: the first and last tell; order 2 mixes them
+            // the first and last residue's antigen (order 2: every residue's); a residue of
+            // another antigen reads its antigen from global memory all the same
             a0 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, first, st.total_res)]];
             a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, last, st.total_res)]];
             if (order_mode == 2)
