@@ -12,8 +12,9 @@
 // the weight-gradient GEMMs, split-K partials) fused on the tcgen05.ld path.
 //
 // Features of a residue (one warp per residue): a 20-way one-hot of its amino
-// acid, then for each of 8 radial shells of 1.25 A around its Calpha (0..10 A)
-// the number of antigen Calphas of each of the 20 amino acids, log1p-scaled.
+// acid (none for a mutation query, amino acid MLP_NO_AA), then for each of 8
+// radial shells of 1.25 A around its Calpha (0..10 A) the number of antigen
+// Calphas of each of the 20 amino acids, log1p-scaled.
 // Shell membership compares r^2 (the reference's f32 rounding) with the exact
 // f32 squares of the shell radii, and log1p comes from a table filled on the
 // host, so the features are bit-identical wherever they are computed.
