@@ -154,3 +154,27 @@ def test_block_io_ragged_antigens(ctx, pkg):
     e1, t1 = ctx.block_io(a, c, p, 10, k=16, n_res=pop.n_res, antigen_id=pop.antigen_id, n_segments=n_seg)
     assert np.array_equal(e0, e1) and np.array_equal(t0, t1)
     assert np.array_equal(a0, a) and np.array_equal(c0, c) and np.array_equal(p0, p)
+
+
+def test_block_io_edge_cases(ctx, oracle, pkg):
+    """binder_block_io without gradient steps scores the uploaded population as
+    binder_score_state does and writes it back unchanged; without top-k it returns
+    the energies only; bad step counts, k and amino acids are rejected."""
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, n_cand=64)
+    chi, pos = np.array(chi, np.float32), np.array(pos, np.float32)
+    a, c, p = aa.copy(), chi.copy(), pos.copy()
+    e, t = ctx.block_io(a, c, p, 0, k=8, uniform_n_res=n_res)
+    assert np.array_equal(a, aa) and np.array_equal(c, chi) and np.array_equal(p, pos)
+    assert np.array_equal(e, ctx.score_state())
+    assert np.array_equal(t[0], np.argsort(e, kind="stable")[:8])
+    e0, t0 = ctx.block_io(a, c, p, 5, k=0, uniform_n_res=n_res)
+    assert t0 is None and np.all(np.isfinite(e0))
+    for kw in ({"n_steps": -1, "k": 8}, {"n_steps": 5, "k": 2000}):
+        with pytest.raises(pkg.BinderError) as err:
+            ctx.block_io(aa.copy(), chi.copy(), pos.copy(), kw["n_steps"], k=kw["k"], uniform_n_res=n_res)
+        assert err.value.name == "BINDER_ERR_ARG"
+    bad = aa.copy()
+    bad[3] = 20
+    with pytest.raises(pkg.BinderError) as err:
+        ctx.block_io(bad, chi.copy(), pos.copy(), 5, k=8, uniform_n_res=n_res)
+    assert err.value.name == "BINDER_ERR_ARG"
