@@ -27,6 +27,7 @@
 // Accumulation: ACC = float reproduces the reference's f32 sums bit for bit; ACC =
 // double sums the same f32 pair terms in double and takes the Metropolis test on
 // the double energy difference.
+#include "cg_list.cuh"
 #include "geom.cuh"
 #include "kernels.h"
 #include "mlp_tile.cuh"
@@ -47,6 +48,7 @@ constexpr int AN_THREADS = AN_WARPS * 32;
 constexpr int CG_LANES = 8;                          // lanes per residue in the Langevin probe
 constexpr int CG_RES_PER_PASS = AN_THREADS / CG_LANES;
 constexpr int CG_SLOTS = 16;                         // in-cutoff terms a lane holds
+static_assert(CG_IN_MAX * (16 + 4) <= CG_LANES * CG_SLOTS * 16, "list scratch must fit a group's term slots");
 constexpr int STAGE_CAP = 64;                        // staged in-cutoff terms per warp
 constexpr int AG_STAGE_MAX = 1024;                   // antigen Calphas staged in shared memory
 constexpr int CELL_STAGE_MAX = 4096;                 // Calpha-grid cells staged in shared memory
@@ -79,7 +81,13 @@ struct AnSmem {
     int* iscal;
     uint8_t* agaa;                  // learned proposal: G staged antigen amino acids
     float* lg1p;                    // learned proposal: the log1p count table
+    int* cglist;                    // LR x CG_LIST_MAX: Verlet lists of the Langevin force
+    float4* cgcentre;               // LR: list centre, skin
+    int* cgnl;                      // LR: list length (-1: none yet)
 };
+// Residues with Verlet lists in shared memory: candidates of up to one Langevin
+// pass (CG_RES_PER_PASS residues); longer ones walk the 27 cells every step.
+__host__ __device__ inline int anneal_list_res(int R) { return R <= CG_RES_PER_PASS ? R : 0; }
 __host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
     const size_t t = (size_t)L * CG_SLOTS * 16;
@@ -91,7 +99,8 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
-           (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1) * 4 : 0);
+           (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1) * 4 : 0) +
+           15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4);  // 15: alignment of cgcentre
 }
 __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
     AnSmem s;
@@ -135,6 +144,11 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.iscal = (int*)take(32);
     s.agaa = learned ? (uint8_t*)take(((size_t)G + 15) / 16 * 16) : nullptr;
     s.lg1p = learned ? (float*)take((MLP_COUNT_CAP + 1) * 4) : nullptr;
+    const int LR = anneal_list_res(R);
+    b = (unsigned char*)(((uintptr_t)b + 15) & ~(uintptr_t)15);  // float4 alignment (the arrays before: ints)
+    s.cgcentre = (float4*)take((size_t)LR * 16);
+    s.cglist = (int*)take((size_t)LR * CG_LIST_MAX * 4);
+    s.cgnl = (int*)take((size_t)LR * 4);
     return s;
 }
 
@@ -447,6 +461,88 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
     fx = sx; fy = sy; fz = sz;
 }
 
+// compute_forces_with_grid for the residue of a group of CG_LANES lanes from its
+// Verlet list (cg_list.cuh), kept in shared memory across the steps of the launch
+// and rebuilt, with twice the skin up to CG_SKIN_MAX, when the Calpha leaves the
+// skin of the list centre (a backbone move or the steps' drift).  The list entries
+// passing the reference's tests, in list order, are the reference's pairs in its
+// order: the group compacts them (at most CG_IN_MAX a round), its lanes evaluate the
+// terms and lane 0 sums them in that order -- the sum of the 27-cell walk.  A list
+// that overflows, or cells near the i32 limits, fall back to the one-lane walk.
+// in / terms: the group's per-step scratch.  The force is in lane 0.
+__device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, unsigned gmask, int* list,
+                                    float4* centre, int* nlp, int* in, float4* terms, float& fx, float& fy,
+                                    float& fz) {
+    const GridView& g = A.ca_grid;
+    const F3 ca = {body.x, body.y, body.z};
+    float4 cc = *centre;
+    int nl = *nlp;
+    const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
+    if (nl < 0 || !(mx * mx + my * my + mz * mz <= (cc.w - 0.01f) * (cc.w - 0.01f))) {
+        const float skin = nl < 0 ? CG_SKIN : fminf(2.0f * cc.w, CG_SKIN_MAX);
+        nl = build_cg_list<CG_LANES>(g, A.ca_pq, ca, gl, gmask, list, skin);
+        cc = make_float4(ca.x, ca.y, ca.z, skin);
+        __syncwarp(gmask);
+        if (gl == 0) {
+            *centre = cc;
+            *nlp = nl;
+        }
+    }
+    const int cx = cell_coord(ca.x, g.inv), cy = cell_coord(ca.y, g.inv), cz = cell_coord(ca.z, g.inv);
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    if (nl > CG_LIST_MAX || cell_far(cx, cy, cz)) {
+        if (gl == 0) cg_force(A, body, sx, sy, sz);
+    } else {
+        const bool near_adjacent = g.cell >= 10.0f && fabsf(ca.x) < 1e4f && fabsf(ca.y) < 1e4f &&
+                                   fabsf(ca.z) < 1e4f;  // see k_langevin
+        const int gshift = (int)(threadIdx.x & 31) & ~(CG_LANES - 1);
+        const unsigned below = (1u << gl) - 1u;
+        int from = 0;
+        while (from < nl) {  // group-uniform
+            int n_in = 0;
+            while (from < nl && n_in + CG_LANES <= CG_IN_MAX) {
+                const int j = from + gl;
+                bool ok = false;
+                int i = 0;
+                if (j < nl) {
+                    i = list[j];
+                    const float4 a = A.ca_pq[i];
+                    const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
+                    ok = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                    if (ok && !(near_adjacent && r_sq <= CG_NEAR_SQ)) {  // the reference's cell test
+                        const int4 ce = A.ca_cell[i];
+                        ok = abs((long long)ce.x - cx) <= 1 && abs((long long)ce.y - cy) <= 1 &&
+                             abs((long long)ce.z - cz) <= 1;
+                    }
+                }
+                const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << CG_LANES) - 1u);
+                if (ok) in[n_in + __popc(m & below)] = i;
+                n_in += __popc(m);
+                from += CG_LANES;
+            }
+            __syncwarp(gmask);
+            for (int k = gl; k < n_in; k += CG_LANES) {
+                const int i = in[k];
+                float tx, ty, tz;
+                cg_term_parts(body, A.ca_pq[i], A.ca_prm[i], tx, ty, tz);
+                terms[k] = make_float4(tx, ty, tz, 0.f);
+            }
+            __syncwarp(gmask);
+            if (gl == 0)
+                for (int k = 0; k < n_in; ++k) {
+                    const float4 t = terms[k];
+                    sx = xadd(sx, t.x);
+                    sy = xadd(sy, t.y);
+                    sz = xadd(sz, t.z);
+                }
+            __syncwarp(gmask);  // the scratch is rewritten next round
+        }
+    }
+    fx = sx;
+    fy = sy;
+    fz = sz;
+}
+
 // The network's choice of every mutation and (known-rotamer) rotamer move drawn
 // this step and the moves' log Hastings ratios (all threads of the CTA call), one
 // network pass per tile of moves.  A move changes neither the residue's environment
@@ -559,6 +655,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             S.lhr[r] = 0.0;
         }
     }
+    const bool lists = anneal_list_res(R) > 0;  // Verlet lists of the Langevin force
+    for (int r = tid; lists && r < n; r += AN_THREADS) S.cgnl[r] = -1;
     long long n_mc = 0, n_mc_acc = 0, n_bb = 0, n_bb_acc = 0;
     __syncthreads();
 
@@ -577,8 +675,15 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
                 if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
                 const CgB body = cg_body(ca.x, ca.y, ca.z, S.aa[r]);
                 float fx, fy, fz;
-                group_cg_force(A, body, gl, gmask, S.terms + (size_t)tid * CG_SLOTS, S.tcount + tid, S.tcount + g0,
-                               S.terms + (size_t)g0 * CG_SLOTS, fx, fy, fz);
+                if (lists) {
+                    // the group's scratch: the CG_SLOTS term slots of its lanes
+                    unsigned char* scratch = (unsigned char*)(S.terms + (size_t)g0 * CG_SLOTS);
+                    group_cg_force_list(A, body, gl, gmask, S.cglist + (size_t)r * CG_LIST_MAX, S.cgcentre + r,
+                                        S.cgnl + r, (int*)(scratch + CG_IN_MAX * 16), (float4*)scratch, fx, fy, fz);
+                } else {
+                    group_cg_force(A, body, gl, gmask, S.terms + (size_t)tid * CG_SLOTS, S.tcount + tid,
+                                   S.tcount + g0, S.terms + (size_t)g0 * CG_SLOTS, fx, fy, fz);
+                }
                 if (gl == 0) {
                     const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
                     const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);

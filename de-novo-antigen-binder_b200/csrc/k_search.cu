@@ -12,6 +12,7 @@
 //    gradient-step and scoring kernels) and the slot packing kernels.
 #include <algorithm>
 
+#include "cg_list.cuh"
 #include "geom.cuh"
 #include "kernels.h"
 
@@ -83,10 +84,6 @@ __global__ void k_cg_forces(const AgView* __restrict__ ag, const float* __restri
 // walk (same sum).  The residue's atoms live in registers, atom k on lane k % G, and
 // take every step's translation as set_ca_pos does (allatom.rs:279-293).
 // COUNT: count the in-cutoff pairs of the same trajectory, leave the state as is.
-constexpr int CG_LIST_MAX = CG_LIST_CAP;
-constexpr float CG_SKIN = 2.0f;      // list radius = 10 A cutoff + skin; a residue's first skin
-constexpr float CG_SKIN_MAX = 5.0f;  // a residue that outruns its list gets twice the skin, up to this
-
 // The one-lane walk over all 27 cells, out of line: it is rarely taken and must
 // not take registers from the list path.
 template <bool COUNT>
@@ -97,75 +94,6 @@ __device__ __noinline__ void cg_force_walk(const AgView* __restrict__ ag, float 
     *out = make_float3(sx, sy, sz);
 }
 
-__device__ __forceinline__ bool cell_far(int cx, int cy, int cz) {
-    return abs(cx) > (1 << 29) || abs(cy) > (1 << 29) || abs(cz) > (1 << 29);
-}
-
-// Verlet list of the residue whose group of G lanes calls this (gl = lane in group):
-// positions (ascending) of the antigen Calphas within skin + 10 A (+ 10 mA for
-// rounding) of p, found by a walk over the (2K+1)^3 cells around p's cell, K =
-// ceil(radius / cell), culled by slab distance.  The lanes split the (2K+1)^2
-// (dx, dy) columns into contiguous runs (for fixed (dx, dy) the cells along z are
-// one contiguous range of the sorted array), count, take offsets by a prefix sum
-// and write.  Returns the list length (all lanes); a length above CG_LIST_MAX (or a
-// grid finer than radius / 8) leaves the list unusable.
-template <int G>
-__device__ __noinline__ int build_cg_list(const GridView& g, const float4* __restrict__ ca_pq, F3 p, int gl,
-                                          unsigned gmask, int* list, float skin) {
-    const float R = 10.0f + skin + 0.01f, R2 = R * R;
-    const int c[3] = {cell_coord(p.x, g.inv), cell_coord(p.y, g.inv), cell_coord(p.z, g.inv)};
-    if (cell_far(c[0], c[1], c[2]) || !(R <= 8.0f * g.cell)) return CG_LIST_MAX + 1;
-    const int K = (int)ceilf(R / g.cell), W = 2 * K + 1, ncol = W * W;
-    const float pp[3] = {p.x, p.y, p.z};
-    auto slab2 = [&](int d, int o) {  // squared distance from p to the cell slab c[d] + o along d
-        const float lo = (float)(c[d] + o) * g.cell, hi = lo + g.cell;
-        const float dd = fmaxf(fmaxf(lo - pp[d], pp[d] - hi), 0.0f);
-        return dd * dd;
-    };
-    const int col0 = (ncol * gl) / G, col1 = (ncol * (gl + 1)) / G;
-    int n_mine = 0, off = 0, total = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-        int w = off;
-        for (int col = col0; col < col1; ++col) {
-            const int ox = col / W - K, oy = col % W - K;
-            const float dxy = slab2(0, ox) + slab2(1, oy);
-            if (dxy > R2) continue;
-            const int X = c[0] + ox - g.ox, Y = c[1] + oy - g.oy;
-            if (X < 0 || Y < 0 || X >= g.nx || Y >= g.ny) continue;
-            int zl = -K, zh = K;
-            while (zl <= K && dxy + slab2(2, zl) > R2) ++zl;
-            while (zh >= zl && dxy + slab2(2, zh) > R2) --zh;
-            if (zl > zh) continue;
-            const int Z0 = max(c[2] + zl - g.oz, 0), Z1 = min(c[2] + zh - g.oz, g.nz - 1);
-            if (Z0 > Z1) continue;
-            const int base = (X * g.ny + Y) * g.nz;
-            const int a1 = g.cell_start[base + Z1 + 1];
-            for (int i = g.cell_start[base + Z0]; i < a1; ++i) {
-                const float4 a = ca_pq[i];
-                const float dx = p.x - a.x, dy = p.y - a.y, dz = p.z - a.z;
-                if (dx * dx + dy * dy + dz * dz > R2) continue;
-                if (pass == 0) ++n_mine;
-                else list[w++] = i;
-            }
-        }
-        if (pass == 0) {
-            int incl = n_mine;
-#pragma unroll
-            for (int d = 1; d < G; d <<= 1) {
-                const int v = __shfl_up_sync(gmask, incl, d, G);
-                if (gl >= d) incl += v;
-            }
-            total = __shfl_sync(gmask, incl, G - 1, G);
-            off = incl - n_mine;
-            if (total > CG_LIST_MAX) return total;
-        }
-    }
-    __syncwarp(gmask);
-    return total;
-}
-
-constexpr int CG_IN_MAX = 48;      // in-cutoff list entries a residue holds per step
-constexpr float CG_NEAR_SQ = 99.0f;  // r^2 below which a pair is in adjacent 10 A cells
 
 // Residue of a lane group's slot: the cell-sorted permutation (order_mode 0), the
 // state's own order (1: candidate after candidate), or a stride through it (2:
