@@ -1159,8 +1159,9 @@ static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_re
     }
     const int total = off[n_cand];
     if (total > 0 && (!aa || !chi || !pos)) return fail(ctx, BINDER_ERR_ARG, "NULL state array");
-    for (int r = 0; r < total; ++r)
-        if (aa[r] >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
+    uint8_t aa_max = 0;  // a branch-free scan (vectorised): this runs on every upload
+    for (int r = 0; r < total; ++r) aa_max = aa[r] > aa_max ? aa[r] : aa_max;
+    if (aa_max >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
     // a population of the same shape (candidates, residue counts, antigens, ids)
     // against the same antigen set keeps the device metadata; only the residues move
     const bool same_meta = S.n_cand == (int)n_cand && S.meta_epoch == ctx->ag_epoch && S.h_res_off == off &&
