@@ -73,6 +73,36 @@ def test_mc_steps_bit_exact(ctx, oracle, pkg, acc, sched):
     assert np.array_equal(g_pos, pos)
 
 
+@pytest.mark.parametrize("acc", [0, 1])
+@pytest.mark.parametrize("sched", ["hot", "cold"])
+def test_mc_long_candidates_bit_exact(ctx, oracle, pkg, acc, sched):
+    """40-residue candidates: more residues than one Langevin pass holds, so the
+    Langevin force walks the 27 neighbouring Calpha cells every step instead of
+    reading Verlet lists from shared memory."""
+    cfg = pkg.workloads.config1(n_cand=64)
+    ag_aa, ag_pos = _antigen(oracle, cfg)
+    ctx.clear_antigens()
+    gp, op = _params(pkg, oracle, cfg["shell"][0], acc, mutation_p=0.3, rotamer_move_p=0.5, backbone_move_p=0.2)
+    ctx.set_params(gp)
+    ctx.add_antigen(ag_aa, ag_pos)
+    A = oracle.Antigen(ag_aa, ag_pos)
+    pop = cfg["pop"]
+    n_res, n_cand = 40, 32
+    aa = pop.aa[:n_cand * n_res].copy()
+    pos, chi = oracle.build_residues(pop.ca[:n_cand * n_res], aa)
+    steps = HOT if sched == "hot" else COLD
+    temps = np.array([oracle.temperature(s, 600) for s in steps], np.float32)
+    cid = np.arange(n_cand, dtype=np.uint32) * 5 + 1
+    (g_aa, g_chi, g_pos), g_stats, o_stats = _run_pair(ctx, oracle, A, gp, op, aa, chi, pos, n_res, cid, steps,
+                                                       temps)
+    assert o_stats[:, 0].sum() > 2000 and o_stats[:, 2].sum() > 1000
+    assert (o_stats[:, 3] < o_stats[:, 2]).any()
+    assert np.array_equal(g_stats, o_stats)
+    assert np.array_equal(g_aa, aa)
+    assert np.array_equal(g_chi, chi)
+    assert np.array_equal(g_pos, pos)
+
+
 def _cys_chains(oracle, center, n_cand, n_res, rng):
     """Straight Calpha chains (3.8 A steps) half made of Cys: every residue of the
     ideal backbone has the same orientation, so neighbouring SG atoms sit 3.8 A
