@@ -517,24 +517,38 @@ def run_batched(pkg, ctx, torch, ext):
             "best_energy_per_antigen": [float(e_last[t[0]]) for t in top]}
 
 
-SCHEDULES = (150, 200, 300, 450, 600)  # annealed schedule lengths of the learned-proposal study
+SCHEDULES = (150, 200, 250, 300, 375, 450, 600)  # annealed schedule lengths of the learned-proposal study
+LEARNED_SEEDS = tuple(range(21, 33))
+# Proposal temperature floor Tp = max(T, T_PROP_MIN), chosen on the validation antigen
+# (held-out antigen 2 of the learned-proposal workload; `--learned-validation`), never
+# on the antigen the study reports.
+T_PROP_MIN = 0.5
+LEARNED_METHODS = (("uniform", {}),
+                   ("learned", {"learned": True, "t_prop_min": T_PROP_MIN}),
+                   ("learned_below_T1", {"learned": True, "t_prop_min": T_PROP_MIN, "t_max": 1.0}))
 
 
-def run_learned(pkg, ctx, seeds=(21, 22, 23, 24, 25), n_res=20):
+def _finite(x):
+    """x, or None (JSON null) when it is not finite: a run that never reaches the target."""
+    return float(x) if np.isfinite(x) else None
+
+
+def run_learned(pkg, ctx, seeds=LEARNED_SEEDS, n_res=20, eval_index=0, methods=LEARNED_METHODS,
+                schedules=SCHEDULES):
     """The learned proposal (configs of the learned-proposal workload): plain-MC
     tuples on 4 training antigens, GPU training, then annealed runs on a held-out
-    antigen, uniform vs learned proposal.  Time to target = first wall time at which
-    a run's champion is within 0.5 kcal/mol of the uniform proposal's median final
-    champion on the 600-step schedule; reported per schedule length (SCHEDULES, the
-    same grid for every method) and for each method at its best length (median over
-    the seeds)."""
+    antigen (eval_index 0: the reported one; 1: the validation one), uniform vs
+    learned proposal.  Time to target = first wall time at which a run's champion is
+    within 0.5 kcal/mol of the uniform proposal's median final champion on the
+    600-step schedule; reported per schedule length (the same grid for every method)
+    and for each method at its best length (median over the seeds)."""
     L = pkg.learned
-    cfg = pkg.workloads.config4(n_train=4, n_eval=1)
+    cfg = pkg.workloads.config4(n_train=4, n_eval=eval_index + 1)
     shell = float(cfg["train"][0][1])
     ctx.clear_antigens()
     ctx.set_params(pkg.Params.defaults(shell_radius=shell, seed=11))
     train_ids = L.add_antigens(ctx, [t[0] for t in cfg["train"]])
-    eval_ag, _, eval_pop = cfg["eval"][0]
+    eval_ag, _, eval_pop = cfg["eval"][eval_index]
     (eval_id,) = L.add_antigens(ctx, [eval_ag])
     t0 = time.perf_counter()
     n_tuples = L.generate_tuples(ctx, [t[2] for t in cfg["train"]], train_ids, n_res, gen_steps=300)
@@ -544,12 +558,10 @@ def run_learned(pkg, ctx, seeds=(21, 22, 23, 24, 25), n_res=20):
     agid = L.upload_populations(ctx, [eval_pop], [eval_id], n_res)
     ctx.diffuse(PHASE1_STEPS, 0)  # phase-1 gradient steps bring the population into contact
     s0 = ctx.state_download()
-    methods = (("uniform", {}), ("learned", {"learned": True, "t_prop_min": 1.0}),
-               ("learned_below_T0.5", {"learned": True, "t_prop_min": 1.0, "t_max": 0.5}))
     # every method on every schedule length; the 600-step schedule is the reference's
-    runs = {(name, n): [] for name, _ in methods for n in SCHEDULES}
+    runs = {(name, n): [] for name, _ in methods for n in schedules}
     acc = {k: [] for k in runs}
-    for n_steps in SCHEDULES:
+    for n_steps in schedules:
         for seed in seeds:
             ctx.set_params(pkg.Params.defaults(shell_radius=shell, seed=seed))
             for name, kw in methods:
@@ -557,8 +569,10 @@ def run_learned(pkg, ctx, seeds=(21, 22, 23, 24, 25), n_res=20):
                 runs[(name, n_steps)].append(traj)
                 acc[(name, n_steps)].append(st["mutation_rotamer_acceptance"])
     out = {"workload": "4 training antigens x 1024 antibodies (plain-MC tuples, 300 annealed steps), held-out "
-                       "300-residue antigen x 1024 antibodies x 20 residues, annealed Langevin + Metropolis "
-                       "runs of %s steps, %d seeds" % ("/".join(map(str, SCHEDULES)), len(seeds)),
+                       "300-residue antigen %d x 1024 antibodies x 20 residues, annealed Langevin + Metropolis "
+                       "runs of %s steps, %d seeds" % (eval_index + 1, "/".join(map(str, schedules)), len(seeds)),
+           "methods": {name: {k: _finite(v) if isinstance(v, float) else v for k, v in kw.items()}
+                       for name, kw in methods},
            "tuples": int(n_tuples), "tuple_gen_s": gen_s, "train_steps": train_steps,
            "train_batch": 8192, "train_s": train_s, "loss_first": float(np.mean(losses[:10])),
            "loss_last": float(np.mean(losses[-50:])), "time_unit": "ms of Metropolis steps (wall clock)"}
@@ -570,15 +584,37 @@ def run_learned(pkg, ctx, seeds=(21, 22, 23, 24, 25), n_res=20):
         _, _, tt = L.time_to_target(runs[("uniform", PHASE2_STEPS)], rs)
         med[(name, n)] = float(np.median(tt))
         out.setdefault(name, {})["steps_%d" % n] = {
-            "time_to_target_ms": tt, "median_ms": med[(name, n)], "final_champions": [r[-1][1] for r in rs],
+            "time_to_target_ms": [_finite(x) for x in tt], "median_ms": _finite(med[(name, n)]),
+            "final_champions": [r[-1][1] for r in rs],
             "ms_per_run": float(np.mean([r[-1][0] for r in rs])), "acceptance": float(np.mean(acc[(name, n)]))}
-    best = {name: min((med[(name, n)], n) for n in SCHEDULES) for name, _ in methods}
+    best = {name: min((med[(name, n)], n) for n in schedules) for name, _ in methods}
     for name, _ in methods:
-        out[name]["best"] = {"median_ms": best[name][0], "schedule_steps": best[name][1]}
+        out[name]["best"] = {"median_ms": _finite(best[name][0]), "schedule_steps": best[name][1]}
         if name != "uniform":
-            out[name]["speedup_vs_uniform_600"] = float(med[("uniform", PHASE2_STEPS)] / med[(name, PHASE2_STEPS)])
-            out[name]["speedup_vs_uniform_best_schedules"] = float(best["uniform"][0] / best[name][0])
+            out[name]["speedup_vs_uniform_600"] = _finite(med[("uniform", PHASE2_STEPS)] / med[(name, PHASE2_STEPS)])
+            out[name]["speedup_vs_uniform_best_schedules"] = _finite(best["uniform"][0] / best[name][0])
     return out
+
+
+def run_learned_validation(args):
+    """The proposal temperature floor and the learned-below-T cutoff on the
+    validation antigen: the study's time to target for t_prop_min 0.1 / 0.3 / 0.5 /
+    1.0 x learned on every step / below T = 1 / below T = 0.5.  Prints one JSON line
+    of speedups (best schedules) per setting."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(0)
+    methods = (("uniform", {}),) + tuple(
+        ("tp%g_%s" % (tp, "every_step" if tm == float("inf") else "below_T%g" % tm),
+         {"learned": True, "t_prop_min": tp, "t_max": tm})
+        for tp in (0.1, 0.3, 0.5, 1.0) for tm in (float("inf"), 1.0, 0.5))
+    out = run_learned(pkg, ctx, eval_index=1, methods=methods)
+    print(json.dumps({"learned_validation": {
+        name: {"speedup_vs_uniform_best_schedules": out[name].get("speedup_vs_uniform_best_schedules", 1.0),
+               "best": out[name]["best"]} for name, _ in methods},
+        "target_champion": out["target_champion"], "workload": out["workload"]}), flush=True)
+    ctx.close()
+    return 0
 
 
 def run_block_only(args):
@@ -655,6 +691,8 @@ def main():
                     help="profiling case: 3 search blocks at this gradient-step launch shape")
     ap.add_argument("--mlp-only", type=int, default=0, metavar="ROWS",
                     help="profiling case: 3 loss + gradient passes of the proposal network on ROWS rows")
+    ap.add_argument("--learned-validation", action="store_true",
+                    help="proposal temperature settings of the learned proposal on the validation antigen")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -669,6 +707,8 @@ def main():
         return run_block_only(args)
     if args.mlp_only:
         return run_mlp_only(args)
+    if args.learned_validation:
+        return run_learned_validation(args)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -727,7 +727,7 @@ class GpuContext:
         self._check(lib().binder_mlp_get_tuples(self._h, _ptr(out), len(out), C.byref(n)))
         return out
 
-    def set_proposal(self, learned, t_prop_min=0.3, t_max=float("inf")):
+    def set_proposal(self, learned, t_prop_min=0.5, t_max=float("inf")):
         """Mutation / rotamer proposal of diffuse(): uniform (the reference) or the
         network (at steps with temperature <= t_max)."""
         self._check(lib().binder_set_proposal(self._h, PROPOSAL_LEARNED if learned else PROPOSAL_UNIFORM,

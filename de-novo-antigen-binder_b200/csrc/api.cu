@@ -178,7 +178,7 @@ struct MlpState {
     size_t n_tuples = 0;
     // proposal of binder_diffuse's mutation / rotamer moves, and the proposal log
     bool learned = false;
-    float t_prop_min = 0.3f, t_max = INFINITY;
+    float t_prop_min = 0.5f, t_max = INFINITY;
     DBuf<MlpTuple> log;
     DBuf<unsigned long long> log_n;
     size_t log_cap = 0;

@@ -81,6 +81,7 @@ struct AnSmem {
     int* iscal;
     uint8_t* agaa;                  // learned proposal: G staged antigen amino acids
     float* lg1p;                    // learned proposal: the log1p count table
+    float* mbias;                   // learned proposal: the network's biases b1 | b2 | b3
     int* cglist;                    // LR x CG_LIST_MAX: Verlet lists of the Langevin force
     float4* cgcentre;               // LR: list centre, skin
     int* cgnl;                      // LR: list length (-1: none yet)
@@ -99,7 +100,7 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
-           (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1) * 4 : 0) +
+           (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1 + MLP_BIASES) * 4 : 0) +
            15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4);  // 15: alignment of cgcentre
 }
 __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
@@ -144,6 +145,7 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.iscal = (int*)take(32);
     s.agaa = learned ? (uint8_t*)take(((size_t)G + 15) / 16 * 16) : nullptr;
     s.lg1p = learned ? (float*)take((MLP_COUNT_CAP + 1) * 4) : nullptr;
+    s.mbias = learned ? (float*)take(MLP_BIASES * 4) : nullptr;
     const int LR = anneal_list_res(R);
     b = (unsigned char*)(((uintptr_t)b + 15) & ~(uintptr_t)15);  // float4 alignment (the arrays before: ints)
     s.cgcentre = (float4*)take((size_t)LR * 16);
@@ -311,18 +313,18 @@ __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* r
 }
 
 // Choice among n options (n <= 32) with probabilities softmax(-y / tp), by one
-// warp, lane k holding option k: weights w_k = exp(l_k - m), l_k = -y[k] / tp,
-// m = max l, and the inverse CDF on u = dz / 2^32 over their prefix sums (for equal
-// logits exactly urange(dz, n): the prefix sums are then exact integers).  Returns
-// the option (all lanes).  Its log probability is never needed: a move's Hastings
-// ratio is a difference of two logits of the same softmax.
-__device__ int warp_sample(const float* y, int n, float tp, uint32_t dz) {
+// warp, lane k holding option k: FP64 weights w_k = exp((min y - y[k]) / tp) (the
+// largest is 1) and the inverse CDF on u = dz / 2^32 over their prefix sums (for
+// equal outputs exactly urange(dz, n): the prefix sums are then exact integers).
+// inv_tp = 1 / tp.  Returns the option (all lanes).  Its log probability is never
+// needed: a move's Hastings ratio is a difference of two logits of the same softmax.
+__device__ int warp_sample(const float* y, int n, double inv_tp, uint32_t dz) {
     const int lane = threadIdx.x & 31;
-    const double l = lane < n ? -(double)y[lane] / (double)tp : -INFINITY;
-    double m = l;
+    const float yl = lane < n ? y[lane] : INFINITY;
+    float ymin = yl;
 #pragma unroll
-    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    double cum = lane < n ? exp(l - m) : 0.0;  // inclusive prefix sum in lane order
+    for (int o = 16; o; o >>= 1) ymin = fminf(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+    double cum = lane < n ? exp(((double)ymin - (double)yl) * inv_tp) : 0.0;  // inclusive prefix sum in lane order
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const double v = __shfl_up_sync(0xffffffffu, cum, o);
@@ -548,19 +550,32 @@ __device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, un
 // network pass per tile of moves.  A move changes neither the residue's environment
 // nor its query (mutation: no amino-acid input; rotamer: the unchanged amino acid),
 // so the reverse move's proposal is the same softmax: log q(reverse) - log q(move)
-// = (y[move] - y[back]) / Tp, the normalisers cancelling.
-__device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const float4* agq, const uint8_t* ag_aa,
-                                                int nag, const MlpDev& mlp, float temp) {
+// = (y[move] - y[back]) / Tp, the normalisers cancelling.  The shared-memory
+// layout is carved again from its base (smem, R, G, C) and the network comes by
+// value: a reference to the kernel's copies would put them in local memory.  The
+// biases are read from their shared-memory copies (staged by the kernel).
+__device__ __noinline__ void an_learned_choices(unsigned char* smem, int R, int G, int C, int n, const float4* agq,
+                                                const uint8_t* ag_aa, int nag, MlpDev mlp, float temp) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const AnSmem S = carve(smem, R, G, C, 1);
+    mlp.b1 = S.mbias;  // the biases' shared-memory copies
+    mlp.b2 = S.mbias + MLP_H;
+    mlp.b3 = S.mbias + 2 * MLP_H;
     const MlpTile T = mlp_tile_carve((unsigned char*)S.terms);
-    const float tp = fmaxf(temp, mlp.t_prop_min);
+    const double inv_tp = 1.0 / (double)fmaxf(temp, mlp.t_prop_min);
     uint4 w[MT_WREGS];
     mlp_tile_prefetch(mlp, w);  // the first weights are on their way during the features
-    if (tid == 0) {  // mutations, and rotamer moves from a known library rotamer
+    if (warp == 0) {  // mutations, and rotamer moves from a known library rotamer, in residue order
         int k = 0;
-        for (int r = 0; r < n; ++r)
-            if (S.kind[r] == MV_MUT || (S.kind[r] == MV_ROT && S.rot[r] >= 0)) S.mvl[k++] = r;
-        S.iscal[IS_NMV] = k;
+        for (int b = 0; b < n; b += 32) {
+            const int r = b + lane;
+            const int kind = r < n ? S.kind[r] : MV_NONE;
+            const bool m = kind == MV_MUT || (kind == MV_ROT && S.rot[r] >= 0);
+            const unsigned bal = __ballot_sync(0xffffffffu, m);
+            if (m) S.mvl[k + __popc(bal & ((1u << lane) - 1u))] = r;
+            k += __popc(bal);
+        }
+        if (lane == 0) S.iscal[IS_NMV] = k;
     }
     __syncthreads();
     const int n_mv = S.iscal[IS_NMV];
@@ -572,19 +587,15 @@ __device__ __noinline__ void an_learned_choices(const AnSmem& S, int n, const fl
         mlp_tile_forward(mlp, T, w, rows);
         for (int i = warp; i < rows; i += AN_WARPS) {  // one warp per row
             const int r = S.mvl[base + i];
-            const float* y = T.y + i * MT_YS;
-            if (S.kind[r] == MV_ROT) {
-                const int k = warp_sample(y + N_AA, s_rot_n[S.aa[r]], tp, S.dz[r]);
-                if (lane == 0) {
-                    S.new_rot[r] = k;
-                    S.lhr[r] = -(double)y[N_AA + S.rot[r]] / (double)tp + (double)y[N_AA + k] / (double)tp;
-                }
-            } else {
-                const int a = warp_sample(y, N_AA, tp, S.dz[r]);
-                if (lane == 0) {
-                    S.new_aa[r] = a;
-                    S.lhr[r] = -(double)y[S.aa[r]] / (double)tp + (double)y[a] / (double)tp;
-                }
+            const bool rot = S.kind[r] == MV_ROT;
+            // rotamer query: outputs 20 + j over the residue's rotamers; mutation: outputs 0..19
+            const float* y = T.y + i * MT_YS + (rot ? N_AA : 0);
+            const int k = warp_sample(y, rot ? s_rot_n[S.aa[r]] : N_AA, inv_tp, S.dz[r]);
+            if (lane == 0) {
+                const int back = rot ? S.rot[r] : S.aa[r];  // the reverse move's option
+                if (rot) S.new_rot[r] = k;
+                else S.new_aa[r] = k;
+                S.lhr[r] = ((double)y[k] - (double)y[back]) * inv_tp;
             }
         }
         __syncthreads();
@@ -622,9 +633,11 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         S.cgp[i] = A.ca_prm[i];
     }
     for (int i = tid; cells_staged && i < ncell; i += AN_THREADS) S.cgcell[i] = A.ca_grid.cell_start[i];
-    if (EXT && learned) {  // the network's features read these every step
+    if (EXT && learned) {  // the network's features and epilogues read these every step
         for (int i = tid; staged && i < nag; i += AN_THREADS) S.agaa[i] = A.res_aa[i];
         for (int i = tid; i <= MLP_COUNT_CAP; i += AN_THREADS) S.lg1p[i] = g_an_log1p[i];
+        for (int i = tid; i < MLP_BIASES; i += AN_THREADS)
+            S.mbias[i] = i < MLP_H ? mlp.b1[i] : i < 2 * MLP_H ? mlp.b2[i - MLP_H] : mlp.b3[i - 2 * MLP_H];
     }
     __syncthreads();
     if (tid == 0 && cells_staged) {  // the CG probe reads the staged copies through the view
@@ -792,7 +805,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         // learned proposal: the choice of each drawn move comes from the network
         // (same draw d.z, inverse CDF) and the move carries its Hastings ratio
         if (EXT && learned && temp <= mlp.t_max)
-            an_learned_choices(S, n, agq, staged ? S.agaa : A.res_aa, nag, mlp, temp);
+            an_learned_choices(an_smem, R, G, C, n, agq, staged ? S.agaa : A.res_aa, nag, mlp, temp);
         // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
         // the Calpha energies before / after each move on warps 0..3 (one warp each)
         if (warp >= AN_WARPS / 2) {

@@ -27,6 +27,7 @@ constexpr int MLP_OFF_B2 = MLP_OFF_W2 + MLP_H * MLP_H;
 constexpr int MLP_OFF_W3 = MLP_OFF_B2 + MLP_H;
 constexpr int MLP_OFF_B3 = MLP_OFF_W3 + MLP_OUT_PAD * MLP_H;
 constexpr int MLP_N_PARAMS = MLP_OFF_B3 + MLP_OUT_PAD;
+constexpr int MLP_BIASES = 2 * MLP_H + MLP_OUT_PAD;  // b1, b2, b3
 
 // Shell of a squared distance r2 < 100: the number of squared shell radii
 // (1.25 k)^2, k = 1..7, that r2 reaches.  Every radius square is exact in f32.
@@ -37,13 +38,28 @@ __host__ __device__ __forceinline__ int mlp_shell(float r2) {
 
 // Counts of antigen Calphas by (shell, amino acid) around (x, y, z), by one warp:
 // cnt[shell * 20 + aa] += 1 for every antigen Calpha with r^2 < 100 (the
-// reference's f32 rounding of r^2).  cnt is zeroed by the caller.
+// reference's f32 rounding of r^2).  cnt is zeroed by the caller.  Each lane reads
+// and tests four Calphas before its first count, so that their loads overlap.
 __device__ __forceinline__ void mlp_count_env(const float4* __restrict__ ag_ca, const uint8_t* __restrict__ ag_aa,
                                               int n, float x, float y, float z, int* cnt) {
-    for (int i = (threadIdx.x & 31); i < n; i += 32) {
-        const float4 a = ag_ca[i];
-        const float r2 = xdist2(xsub(x, a.x), xsub(y, a.y), xsub(z, a.z));
-        if (r2 < 100.0f) atomicAdd(&cnt[mlp_shell(r2) * N_AA + ag_aa[i]], 1);
+    constexpr int U = 4;
+    for (int i0 = (threadIdx.x & 31); i0 < n; i0 += 32 * U) {
+        float r2[U];
+        int a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + 32 * u;
+            r2[u] = 1e30f;
+            a[u] = 0;
+            if (i < n) {
+                const float4 q = ag_ca[i];
+                r2[u] = xdist2(xsub(x, q.x), xsub(y, q.y), xsub(z, q.z));
+                a[u] = ag_aa[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (r2[u] < 100.0f) atomicAdd(&cnt[mlp_shell(r2[u]) * N_AA + a[u]], 1);
     }
 }
 

@@ -69,7 +69,7 @@ def train(ctx, n_steps=1500, batch=8192, lr=1e-3, huber_delta=1.0, seed=3, init_
     return losses, time.perf_counter() - t0
 
 
-def anneal_champions(ctx, state, agid, n_res, n_steps=600, chunk=25, learned=False, t_prop_min=1.0,
+def anneal_champions(ctx, state, agid, n_res, n_steps=600, chunk=25, learned=False, t_prop_min=0.5,
                      t_max=float("inf"), step0=200000):
     """One annealed run from `state`; [(cumulative Metropolis wall ms, champion,
     median energy)] after each chunk, and the run's move statistics."""
