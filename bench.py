@@ -617,6 +617,33 @@ def run_learned_validation(args):
     return 0
 
 
+def run_learned_anneal_only(args):
+    """Small profiling case for the Metropolis kernel with the learned proposal: on
+    the held-out antigen of the learned-proposal workload (1024 x 20 residues), one
+    25-step launch with the uniform proposal and one with a network of zero weights
+    (constant outputs: the same trajectory, every network call made)."""
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    ctx = pkg.GpuContext.create(0)
+    L = pkg.learned
+    cfg = pkg.workloads.config4(n_train=1, n_eval=1)
+    shell = float(cfg["train"][0][1])
+    ctx.set_params(pkg.Params.defaults(shell_radius=shell, seed=11))
+    eval_ag, _, eval_pop = cfg["eval"][0]
+    (eval_id,) = L.add_antigens(ctx, [eval_ag])
+    agid = L.upload_populations(ctx, [eval_pop], [eval_id], 20)
+    ctx.diffuse(PHASE1_STEPS, 0)
+    s0 = ctx.state_download()
+    ctx.mlp_set_params(np.zeros(pkg.MLP_N_PARAMS, np.float32))
+    ms = {}
+    for learned in (False, True):
+        traj, _ = L.anneal_champions(ctx, s0, agid, 20, n_steps=25, chunk=25, learned=learned)
+        ms["learned" if learned else "uniform"] = traj[-1][0]
+    print(json.dumps({"learned_anneal_only": {"steps": 25, "candidates": 1024, "ms": ms}}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_block_only(args):
     """Small profiling case for the search block: 3 eagerly issued blocks of the
     bench workload at launch shape (cg_warps, cg_lanes[, cg_order])."""
@@ -691,6 +718,8 @@ def main():
                     help="profiling case: 3 search blocks at this gradient-step launch shape")
     ap.add_argument("--mlp-only", type=int, default=0, metavar="ROWS",
                     help="profiling case: 3 loss + gradient passes of the proposal network on ROWS rows")
+    ap.add_argument("--learned-anneal-only", action="store_true",
+                    help="profiling case: one uniform and one learned-proposal Metropolis launch of 25 steps")
     ap.add_argument("--learned-validation", action="store_true",
                     help="proposal temperature settings of the learned proposal on the validation antigen")
     args = ap.parse_args()
@@ -709,6 +738,8 @@ def main():
         return run_mlp_only(args)
     if args.learned_validation:
         return run_learned_validation(args)
+    if args.learned_anneal_only:
+        return run_learned_anneal_only(args)
     return run_ours(args, rank, world, local_rank)
 
 
