@@ -211,6 +211,12 @@ struct GroupSmem {
     __align__(8) float sx[GMAX];
     __align__(8) float sy[GMAX];
     __align__(8) float sz[GMAX];
+    // charge * sqrt(332), r_min_half, sqrt(epsilon), hydrophobic as separate arrays too,
+    // so that the pair terms read two atoms' parameters as one 8-byte word
+    __align__(8) float sqs[GMAX];
+    __align__(8) float srm[GMAX];
+    __align__(8) float sse[GMAX];
+    __align__(8) float shy[GMAX];
     int q[64];         // queued antigen atom indices
 };
 
@@ -221,6 +227,17 @@ __device__ __forceinline__ void group_xyz(GroupSmem& s, int lane, int n, float x
         s.sz[lane] = z;
     } else if (lane < GMAX) {
         s.sx[lane] = s.sy[lane] = s.sz[lane] = GROUP_PAD;
+    }
+}
+// the parameter arrays of group atom `lane` (pads: zeros, finite terms never added)
+__device__ __forceinline__ void group_prm(GroupSmem& s, int lane, int n, float qs, float rmh, float se, float hy) {
+    if (lane < n) {
+        s.sqs[lane] = qs;
+        s.srm[lane] = rmh;
+        s.sse[lane] = se;
+        s.shy[lane] = hy;
+    } else if (lane < GMAX) {
+        s.sqs[lane] = s.srm[lane] = s.sse[lane] = s.shy[lane] = 0.0f;
     }
 }
 
@@ -262,8 +279,10 @@ struct SrcStateG {
             s.pos[lane] = make_float4(p.x, p.y, p.z, m.x);
             s.prm[lane] = make_float4(m.y, m.z, m.w, (float)c_slot_type[aa][lane]);
             group_xyz(s, lane, n, p.x, p.y, p.z);
+            group_prm(s, lane, n, m.x, m.y, m.z, m.w);
         } else {
             group_xyz(s, lane, n, 0.f, 0.f, 0.f);
+            group_prm(s, lane, n, 0.f, 0.f, 0.f, 0.f);
         }
         return n;
     }
@@ -287,8 +306,10 @@ struct SrcFlatG {
             s.pos[lane] = make_float4(p0.x, p0.y, p0.z, p0.w * SQRT_COULOMB_K);
             s.prm[lane] = make_float4(p1.x, sqrtf(p1.y), p1.z > 0.5f ? 1.0f : 0.0f, 0.0f);
             group_xyz(s, lane, n, p0.x, p0.y, p0.z);
+            group_prm(s, lane, n, s.pos[lane].w, s.prm[lane].x, s.prm[lane].y, s.prm[lane].z);
         } else {
             group_xyz(s, lane, n, 0.f, 0.f, 0.f);
+            group_prm(s, lane, n, 0.f, 0.f, 0.f, 0.f);
         }
         return n;
     }
@@ -337,14 +358,42 @@ __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const
         if (COUNT) ++np;
     };
     const uint64_t ax = f2_pack(a.x, a.x), ay = f2_pack(a.y, a.y), az = f2_pack(a.z, a.z);
+    const uint64_t aq = f2_pack(a.w, a.w), arm = f2_pack(ap.x, ap.x), ase = f2_pack(ap.y, ap.y);
+    const uint64_t ahy = f2_pack(HYDRO_BONUS * ap.z, HYDRO_BONUS * ap.z), two = f2_pack(2.0f, 2.0f);
+#pragma unroll 1
     for (int j = 0; j < n; j += 2) {
         const uint64_t dx = f2_sub(*(const uint64_t*)&s.sx[j], ax);
         const uint64_t dy = f2_sub(*(const uint64_t*)&s.sy[j], ay);
         const uint64_t dz = f2_sub(*(const uint64_t*)&s.sz[j], az);
         const uint64_t r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
         const float r2a = f2_lo(r2), r2b = f2_hi(r2);
-        if (r2a <= CUTOFF_SQ && r2a >= MIN_R_SQ) term(j, r2a);
-        if (r2b <= CUTOFF_SQ && r2b >= MIN_R_SQ) term(j + 1, r2b);  // j + 1 = n: a pad, +inf
+        const bool ina = r2a <= CUTOFF_SQ && r2a >= MIN_R_SQ;
+        const bool inb = r2b <= CUTOFF_SQ && r2b >= MIN_R_SQ;  // j + 1 = n: a pad, +inf
+        if (FULL) {
+            if (ina) term(j, r2a);
+            if (inb) term(j + 1, r2b);
+        } else if (ina || inb) {
+            // both pairs' terms in packed f32x2 arithmetic; an out-of-range element is
+            // computed but never added
+            const uint64_t ir = f2_pack(rsqrtf(r2a), rsqrtf(r2b));
+            const uint64_t ir2 = f2_mul(ir, ir);
+            const uint64_t R = f2_add(*(const uint64_t*)&s.srm[j], arm);
+            const uint64_t s2 = f2_mul(f2_mul(R, R), ir2);
+            const uint64_t s6 = f2_mul(f2_mul(s2, s2), s2);
+            const uint64_t lj = f2_mul(f2_mul(*(const uint64_t*)&s.sse[j], ase), f2_mul(s6, f2_sub(s6, two)));
+            const uint64_t coul = f2_mul(f2_mul(*(const uint64_t*)&s.sqs[j], aq), ir);
+            const uint64_t hy = f2_mul(*(const uint64_t*)&s.shy[j], ahy);
+            const float hya = r2a < HYDRO_CUTOFF_SQ ? f2_lo(hy) : 0.0f;
+            const float hyb = r2b < HYDRO_CUTOFF_SQ ? f2_hi(hy) : 0.0f;
+            const uint64_t e = f2_add(f2_add(lj, coul), f2_pack(hya, hyb));
+            if (ina) part += f2_lo(e);
+            if (inb) part += f2_hi(e);
+            if (ABS) {
+                if (ina) pabs += fabsf(f2_lo(lj)) + fabsf(f2_lo(coul)) + fabsf(hya);
+                if (inb) pabs += fabsf(f2_hi(lj)) + fabsf(f2_hi(coul)) + fabsf(hyb);
+            }
+            if (COUNT) np += (int)ina + (int)inb;
+        }
     }
     acc_add<KAHAN>(acc, part);
     if (ABS) acc.abs_s += pabs;
