@@ -58,6 +58,29 @@ __device__ __forceinline__ float xdist2(float dx, float dy, float dz) {
     return xadd(xadd(xmul(dx, dx), xmul(dy, dy)), xmul(dz, dz));
 }
 
+// Packed pairs of f32 (element 0 in the low word) and the sm_100 two-wide FP32
+// instructions; each element is rounded exactly as the scalar instruction rounds it.
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+    return (uint64_t)__float_as_uint(lo) | ((uint64_t)__float_as_uint(hi) << 32);
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float f2_lo(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float f2_hi(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+
 // Transcendentals of the Metropolis path (acceptance exp, H-bond and disulfide
 // Gaussians, rotation by a random torsion): evaluated in double and rounded once
 // to f32, on the device and in the CPU restatement alike.  Both double functions

@@ -69,6 +69,7 @@ struct AnSmem {
     float4* stage;             // AN_WARPS * STAGE_CAP: in-cutoff Calpha-energy terms
     float4 *agq, *agp;         // G staged antigen Calphas: x, y, z, q | r_min_half, eps, hyd, type
     float4 *cgq, *cgp;         // G staged Calphas in CG-grid order (AgView::ca_pq, ca_prm)
+    float *agx, *agy, *agz;    // anneal_xyz_len(G) each: the staged Calphas' x, y, z (pad +1e30)
     int* cgcell;               // C staged CG-grid cell starts
     AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
@@ -86,6 +87,9 @@ struct AnSmem {
     float4* cgcentre;               // LR: list centre, skin
     int* cgnl;                      // LR: list length (-1: none yet)
 };
+// Entries of each staged x / y / z array: room for the pad, a multiple of 4 (the
+// arrays after them keep their 16-byte alignment).
+__host__ __device__ inline int anneal_xyz_len(int G) { return G > 0 ? (G + 4) & ~3 : 0; }
 // Residues with Verlet lists in shared memory: candidates of up to one Langevin
 // pass (CG_RES_PER_PASS residues); longer ones walk the 27 cells every step.
 __host__ __device__ inline int anneal_list_res(int R) { return R <= CG_RES_PER_PASS ? R : 0; }
@@ -97,7 +101,8 @@ __host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
 __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
     return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + anneal_terms_bytes(R, learned) +
-           (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + ((size_t)C * 4 + 15) / 16 * 16 +
+           (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + (size_t)anneal_xyz_len(G) * 12 +
+           ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
            (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1 + MLP_BIASES) * 4 : 0) +
@@ -120,6 +125,9 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.agp = (float4*)take((size_t)G * 16);
     s.cgq = (float4*)take((size_t)G * 16);
     s.cgp = (float4*)take((size_t)G * 16);
+    s.agx = (float*)take((size_t)anneal_xyz_len(G) * 4);
+    s.agy = (float*)take((size_t)anneal_xyz_len(G) * 4);
+    s.agz = (float*)take((size_t)anneal_xyz_len(G) * 4);
     s.cgcell = (int*)take(((size_t)C * 4 + 15) / 16 * 16);
     s.ag = (AgView*)take(((sizeof(AgView) + 15) / 16) * 16);
     s.c_cur = (double*)take((size_t)R * 8);
@@ -175,6 +183,33 @@ __device__ __forceinline__ void fold_terms(const float4* stage, int cnt, ACC& e)
     }
 }
 
+// The staged terms of one in-cutoff pair (r_sq passed the reference's cutoff test):
+// lj; coulomb (flag 1); hydrophobic (flag 2); hbond (flag 4) -- residue_contribution_
+// allatom's per-pair arithmetic (diffusion.rs:425-463).  b = the residue's Calpha
+// (q, r_min_half, epsilon, hydrophobic), bhb its H-bond role.
+__device__ __forceinline__ float4 ca_pair_terms(const float4& b, int bhb, const float4& a, const float4& ap,
+                                                float r_sq) {
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned fl = 0;
+    const float r_ij = xadd(b.y, ap.x);
+    const float eps = xsqrt(xmul(b.z, ap.y));
+    const float r2 = xdiv(xmul(r_ij, r_ij), r_sq);
+    const float r6 = xmul(xmul(r2, r2), r2);
+    t.x = xmul(eps, xsub(xmul(r6, r6), xmul(2.0f, r6)));
+    if (b.x != 0.0f && a.w != 0.0f) {
+        t.y = xdiv(xmul(xmul(COULOMB_K, b.x), a.w), xsqrt(r_sq));
+        fl |= 1u;
+    }
+    if (b.w == 1.0f && ap.z == 1.0f && r_sq < HYDRO_CUTOFF_SQ) fl |= 2u;
+    const int ahb = s_hb_role[(int)ap.w];
+    if (((bhb & 1) && (ahb & 2)) || ((bhb & 2) && (ahb & 1))) {
+        t.z = hbond_mc(r_sq);
+        fl |= 4u;
+    }
+    t.w = __uint_as_float(fl);
+    return t;
+}
+
 // residue_contribution_allatom (diffusion.rs:425-463) of a Calpha at `ca` of amino
 // acid `aa`, by one warp: lanes evaluate 32 antigen Calphas at a time (index
 // order), in-cutoff terms are compacted into the warp's stage in that order and
@@ -195,26 +230,7 @@ __device__ ACC warp_contribution(const float4* __restrict__ agq, const float4* _
             const float4 a = agq[i];
             const float r_sq = xdist2(xsub(ca.x, a.x), xsub(ca.y, a.y), xsub(ca.z, a.z));
             in = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
-            if (in) {
-                const float4 ap = agp[i];
-                unsigned fl = 0;
-                const float r_ij = xadd(b.y, ap.x);
-                const float eps = xsqrt(xmul(b.z, ap.y));
-                const float r2 = xdiv(xmul(r_ij, r_ij), r_sq);
-                const float r6 = xmul(xmul(r2, r2), r2);
-                t.x = xmul(eps, xsub(xmul(r6, r6), xmul(2.0f, r6)));
-                if (b.x != 0.0f && a.w != 0.0f) {
-                    t.y = xdiv(xmul(xmul(COULOMB_K, b.x), a.w), xsqrt(r_sq));
-                    fl |= 1u;
-                }
-                if (b.w == 1.0f && ap.z == 1.0f && r_sq < HYDRO_CUTOFF_SQ) fl |= 2u;
-                const int ahb = s_hb_role[(int)ap.w];
-                if (((bhb & 1) && (ahb & 2)) || ((bhb & 2) && (ahb & 1))) {
-                    t.z = hbond_mc(r_sq);
-                    fl |= 4u;
-                }
-                t.w = __uint_as_float(fl);
-            }
+            if (in) t = ca_pair_terms(b, bhb, a, agp[i], r_sq);
         }
         const unsigned m = __ballot_sync(0xffffffffu, in);
         if (in) stage[cnt + __popc(m & ((1u << lane) - 1u))] = t;
@@ -229,6 +245,63 @@ __device__ ACC warp_contribution(const float4* __restrict__ agq, const float4* _
     __syncwarp();
     if (lane == 0) fold_terms(stage, cnt, e);
     __syncwarp();
+    return e;
+}
+
+// The same for a staged antigen whose Calpha coordinates are also kept as x / y / z
+// arrays (ax, ay, az; 8-byte aligned, entry nag a +1e30 pad when nag is odd).  Lane
+// l tests Calphas base + 2l and base + 2l + 1 with one packed f32x2 computation (the
+// same roundings as xdist2), 64 Calphas per warp step, and stages each in-cutoff
+// Calpha's (r^2, index) in index order; the pair terms of everything staged are then
+// computed one entry per lane (in place) and lane 0 adds them in order -- so the
+// term code runs once per 32 in-cutoff Calphas instead of once per scan step.
+template <class ACC>
+__device__ ACC warp_contribution_pairs(const float* __restrict__ ax, const float* __restrict__ ay,
+                                       const float* __restrict__ az, const float4* __restrict__ agq,
+                                       const float4* __restrict__ agp, int nag, F3 ca, int aa, float4* stage) {
+    static_assert(STAGE_CAP >= 64, "one step stages up to 64 entries");
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const float4 b = s_ca_atom[aa];
+    const int bhb = s_hb_role[s_ca_type[aa]];
+    const uint64_t cx = f2_pack(ca.x, ca.x), cy = f2_pack(ca.y, ca.y), cz = f2_pack(ca.z, ca.z);
+    ACC e = 0;
+    int cnt = 0;
+    auto terms_and_fold = [&]() {  // the staged entries' terms, in place, then their sum in order
+        __syncwarp();
+        for (int k = lane; k < cnt; k += 32) {
+            const float4 v = stage[k];
+            const int i = __float_as_int(v.y);
+            stage[k] = ca_pair_terms(b, bhb, agq[i], agp[i], v.x);
+        }
+        __syncwarp();
+        if (lane == 0) fold_terms(stage, cnt, e);
+        __syncwarp();
+        cnt = 0;
+    };
+    for (int base = 0; base < nag; base += 64) {
+        const int i = base + 2 * lane;
+        bool in0 = false, in1 = false;
+        float r0 = 0.0f, r1 = 0.0f;
+        if (i < nag) {
+            const uint64_t dx = f2_sub(cx, *(const uint64_t*)&ax[i]);
+            const uint64_t dy = f2_sub(cy, *(const uint64_t*)&ay[i]);
+            const uint64_t dz = f2_sub(cz, *(const uint64_t*)&az[i]);
+            const uint64_t r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
+            r0 = f2_lo(r2);
+            r1 = f2_hi(r2);
+            in0 = !(r0 > CUTOFF_SQ || r0 < MIN_R_SQ);
+            in1 = i + 1 < nag && !(r1 > CUTOFF_SQ || r1 < MIN_R_SQ);
+        }
+        const unsigned m0 = __ballot_sync(0xffffffffu, in0), m1 = __ballot_sync(0xffffffffu, in1);
+        const int n_step = __popc(m0) + __popc(m1);
+        if (cnt + n_step > STAGE_CAP) terms_and_fold();
+        const int at = cnt + __popc(m0 & lt) + __popc(m1 & lt);  // Calphas before base + 2 * lane
+        if (in0) stage[at] = make_float4(r0, __int_as_float(i), 0.f, 0.f);
+        if (in1) stage[at + (in0 ? 1 : 0)] = make_float4(r1, __int_as_float(i + 1), 0.f, 0.f);
+        cnt += n_step;
+    }
+    terms_and_fold();
     return e;
 }
 
@@ -627,11 +700,16 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     const int ncell = A.ca_grid.nx * A.ca_grid.ny * A.ca_grid.nz + 1;
     const bool cells_staged = staged && ncell <= C;
     for (int i = tid; staged && i < nag; i += AN_THREADS) {
-        S.agq[i] = A.ca_atom[i];
+        const float4 q = A.ca_atom[i];
+        S.agq[i] = q;
         S.agp[i] = A.ca_atom_prm[i];
         S.cgq[i] = A.ca_pq[i];
         S.cgp[i] = A.ca_prm[i];
+        S.agx[i] = q.x;
+        S.agy[i] = q.y;
+        S.agz[i] = q.z;
     }
+    if (tid == 0 && staged && (nag & 1)) S.agx[nag] = S.agy[nag] = S.agz[nag] = 1e30f;
     for (int i = tid; cells_staged && i < ncell; i += AN_THREADS) S.cgcell[i] = A.ca_grid.cell_start[i];
     if (EXT && learned) {  // the network's features and epilogues read these every step
         for (int i = tid; staged && i < nag; i += AN_THREADS) S.agaa[i] = A.res_aa[i];
@@ -648,6 +726,11 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     const float4* agq = staged ? S.agq : A.ca_atom;
     const float4* agp = staged ? S.agp : A.ca_atom_prm;
     float4* stage = S.stage + warp * STAGE_CAP;
+    // residue_contribution_allatom of a Calpha at q with amino acid a, by the warp
+    auto ca_energy = [&](F3 q, int a) -> ACC {
+        return staged ? warp_contribution_pairs<ACC>(S.agx, S.agy, S.agz, agq, agp, nag, q, a, stage)
+                      : warp_contribution<ACC>(agq, agp, nag, q, a, stage);
+    };
 
     for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
     for (int r = tid; r < n; r += AN_THREADS) {
@@ -821,7 +904,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
                 const bool same = kind == MV_ROT || S.new_aa[r] == S.aa[r];
                 if (which == 1 && same) continue;  // same Calpha, same amino acid: same energy
                 const int a = which ? S.new_aa[r] : S.aa[r];
-                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[r * SLOT_STRIDE + 1]), a, stage);
+                const ACC e = ca_energy(f3(S.pos[r * SLOT_STRIDE + 1]), a);
                 if (lane == 0) {
                     if (which == 0) {
                         S.c_old[r] = (double)e;
@@ -927,7 +1010,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             }
             for (int i = r + warp; i < n; i += AN_WARPS) {
                 if (S.valid[i]) continue;
-                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
+                const ACC e = ca_energy(f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i]);
                 if (lane == 0) {
                     S.c_cur[i] = (double)e;
                     S.valid[i] = 1;
@@ -943,7 +1026,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             rotate_downstream(S, n, r, phi, bt.x, bt.y);
             __syncthreads();
             for (int i = r + 1 + warp; i < n; i += AN_WARPS) {
-                const ACC e = warp_contribution<ACC>(agq, agp, nag, f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i], stage);
+                const ACC e = ca_energy(f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i]);
                 if (lane == 0) S.c_new[i] = (double)e;
             }
             __syncthreads();

@@ -103,6 +103,32 @@ def test_mc_long_candidates_bit_exact(ctx, oracle, pkg, acc, sched):
     assert np.array_equal(g_pos, pos)
 
 
+@pytest.mark.parametrize("acc", [0, 1])
+def test_mc_odd_antigen_bit_exact(ctx, oracle, pkg, acc):
+    """An antigen of 299 residues: the Calpha-energy scan tests two antigen Calphas
+    per lane and step, so an odd count leaves a padded entry in the last step."""
+    cfg = pkg.workloads.config1(n_cand=64)
+    ag_aa, ag_ca = cfg["antigens"][0]
+    ag_aa, ag_ca = ag_aa[:299].copy(), ag_ca[:299].copy()
+    ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    gp, op = _params(pkg, oracle, cfg["shell"][0], acc, mutation_p=0.3, rotamer_move_p=0.5, backbone_move_p=0.2)
+    ctx.set_params(gp)
+    ctx.add_antigen(ag_aa, ag_pos)
+    A = oracle.Antigen(ag_aa, ag_pos)
+    pop = cfg["pop"]
+    n_res, n_cand = 20, 32
+    aa = pop.aa[:n_cand * n_res].copy()
+    pos, chi = oracle.build_residues(pop.ca[:n_cand * n_res], aa)
+    temps = np.array([oracle.temperature(s, 600) for s in COLD], np.float32)
+    cid = np.arange(n_cand, dtype=np.uint32) * 3 + 2
+    (g_aa, g_chi, g_pos), g_stats, o_stats = _run_pair(ctx, oracle, A, gp, op, aa, chi, pos, n_res, cid, COLD,
+                                                       temps)
+    assert o_stats[:, 0].sum() > 500
+    assert np.array_equal(g_stats, o_stats)
+    assert np.array_equal(g_aa, aa) and np.array_equal(g_chi, chi) and np.array_equal(g_pos, pos)
+
+
 def _cys_chains(oracle, center, n_cand, n_res, rng):
     """Straight Calpha chains (3.8 A steps) half made of Cys: every residue of the
     ideal backbone has the same orientation, so neighbouring SG atoms sit 3.8 A
