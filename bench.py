@@ -404,7 +404,7 @@ def run_ours(args, rank, world, local_rank):
     run_cfg = pkg.RunCfg.defaults(phase1_steps=PHASE1_STEPS, score_every=N_STEPS_PER_BLOCK, survivors=TOP_K,
                                   phase2_steps=PHASE2_STEPS, top_n=TOP_K)
     run_times = []
-    for rep in range(4):  # the first call (untimed) pays the one-time kernel loading and buffer growth
+    for rep in range(8):  # the first call (untimed) pays the one-time kernel loading and buffer growth
         ctx.state_upload(pop.aa, chi, pos, uniform_n_res=n_res)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -412,9 +412,10 @@ def run_ours(args, rank, world, local_rank):
         if rep:
             run_times.append(1e3 * (time.perf_counter() - t0))
     run_ms = statistics.median(run_times)
-    run_allatom = {"ms": run_ms, "phase1_steps": PHASE1_STEPS, "phase2_steps": PHASE2_STEPS, "candidates": n_cand,
-                   "survivors": TOP_K, "best_energy": float(run_e[0][0]), "best_index": int(run_cand[0][0]),
-                   "api": "binder_run_allatom (wall clock, host call to results; median of 3 calls after one untimed)"}
+    run_allatom = {"ms": run_ms, "ms_all": [round(t, 3) for t in run_times], "phase1_steps": PHASE1_STEPS,
+                   "phase2_steps": PHASE2_STEPS, "candidates": n_cand, "survivors": TOP_K,
+                   "best_energy": float(run_e[0][0]), "best_index": int(run_cand[0][0]),
+                   "api": "binder_run_allatom (wall clock, host call to results; median of 7 calls after one untimed)"}
 
     peaks, peaks_kind = load_peaks()
     fp32_scalar, fp32_packed = ctx.fp32_peak()
