@@ -129,6 +129,45 @@ def test_mc_odd_antigen_bit_exact(ctx, oracle, pkg, acc):
     assert np.array_equal(g_aa, aa) and np.array_equal(g_chi, chi) and np.array_equal(g_pos, pos)
 
 
+_LARGE = {}
+
+
+def _large_antigen(W):
+    """A seeded 1101-residue globule (built once: the self-avoiding walk takes seconds)."""
+    if not _LARGE:
+        rng = W.rng_for(7)
+        _LARGE["ag"] = W._globule_antigen(1101, rng)
+        _LARGE["rng_state"] = rng.bit_generator.state
+    rng = np.random.default_rng()
+    rng.bit_generator.state = _LARGE["rng_state"]
+    return _LARGE["ag"], rng
+
+
+@pytest.mark.parametrize("acc", [0, 1])
+def test_mc_large_antigen_bit_exact(ctx, oracle, pkg, acc):
+    """An antigen of 1101 residues, more than the Metropolis kernel stages in shared
+    memory: its Calphas, CG grid and parameters are read from global memory."""
+    W = pkg.workloads
+    (ag_aa, ag_ca, radius), rng = _large_antigen(W)
+    ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    gp, op = _params(pkg, oracle, radius + 4.0, acc, mutation_p=0.3, rotamer_move_p=0.5, backbone_move_p=0.2)
+    ctx.set_params(gp)
+    ctx.add_antigen(ag_aa, ag_pos)
+    A = oracle.Antigen(ag_aa, ag_pos)
+    n_res, n_cand = 20, 16
+    ca = W.sphere_points(n_cand * n_res, radius + 4.0, W.ca_center(ag_ca), rng)
+    aa = W.random_sequence(n_cand * n_res, rng)
+    pos, chi = oracle.build_residues(ca, aa)
+    temps = np.array([oracle.temperature(s, 600) for s in HOT], np.float32)
+    cid = np.arange(n_cand, dtype=np.uint32) * 11 + 5
+    (g_aa, g_chi, g_pos), g_stats, o_stats = _run_pair(ctx, oracle, A, gp, op, aa, chi, pos, n_res, cid, HOT,
+                                                       temps)
+    assert o_stats[:, 0].sum() > 100
+    assert np.array_equal(g_stats, o_stats)
+    assert np.array_equal(g_aa, aa) and np.array_equal(g_chi, chi) and np.array_equal(g_pos, pos)
+
+
 def _cys_chains(oracle, center, n_cand, n_res, rng):
     """Straight Calpha chains (3.8 A steps) half made of Cys: every residue of the
     ideal backbone has the same orientation, so neighbouring SG atoms sit 3.8 A
