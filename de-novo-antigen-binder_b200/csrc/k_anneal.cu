@@ -215,7 +215,7 @@ __device__ __forceinline__ float4 ca_pair_terms(const float4& b, int bhb, const 
 // order), in-cutoff terms are compacted into the warp's stage in that order and
 // lane 0 adds them in the reference's order.  Result valid in lane 0.
 template <class ACC>
-__device__ ACC warp_contribution(const float4* __restrict__ agq, const float4* __restrict__ agp, int nag, F3 ca,
+__device__ __noinline__ ACC warp_contribution(const float4* __restrict__ agq, const float4* __restrict__ agp, int nag, F3 ca,
                                  int aa, float4* stage) {
     const int lane = threadIdx.x & 31;
     const float4 b = s_ca_atom[aa];  // q, r_min_half, epsilon, hydrophobic
@@ -256,7 +256,7 @@ __device__ ACC warp_contribution(const float4* __restrict__ agq, const float4* _
 // computed one entry per lane (in place) and lane 0 adds them in order -- so the
 // term code runs once per 32 in-cutoff Calphas instead of once per scan step.
 template <class ACC>
-__device__ ACC warp_contribution_pairs(const float* __restrict__ ax, const float* __restrict__ ay,
+__device__ __noinline__ ACC warp_contribution_pairs(const float* __restrict__ ax, const float* __restrict__ ay,
                                        const float* __restrict__ az, const float4* __restrict__ agq,
                                        const float4* __restrict__ agp, int nag, F3 ca, int aa, float4* stage) {
     static_assert(STAGE_CAP >= 64, "one step stages up to 64 entries");
@@ -726,7 +726,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     const float4* agq = staged ? S.agq : A.ca_atom;
     const float4* agp = staged ? S.agp : A.ca_atom_prm;
     float4* stage = S.stage + warp * STAGE_CAP;
-    // residue_contribution_allatom of a Calpha at q with amino acid a, by the warp
+    // residue_contribution_allatom of a Calpha at q with amino acid a, by the warp (the
+    // scans are noinline: one copy each instead of one per call site, less code to fetch)
     auto ca_energy = [&](F3 q, int a) -> ACC {
         return staged ? warp_contribution_pairs<ACC>(S.agx, S.agy, S.agz, agq, agp, nag, q, a, stage)
                       : warp_contribution<ACC>(agq, agp, nag, q, a, stage);
