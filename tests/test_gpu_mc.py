@@ -168,6 +168,42 @@ def test_mc_large_antigen_bit_exact(ctx, oracle, pkg, acc):
     assert np.array_equal(g_aa, aa) and np.array_equal(g_chi, chi) and np.array_equal(g_pos, pos)
 
 
+def _ball(rng, n, r_lo, r_hi):
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return (v * (r_lo + (r_hi - r_lo) * rng.random((n, 1)))).astype(np.float32)
+
+
+@pytest.mark.parametrize("acc", [0, 1])
+def test_mc_dense_antigen_bit_exact(ctx, oracle, pkg, acc):
+    """120 antigen Calphas packed into a 9 A ball, candidates around it: up to ~90
+    antigen Calphas within the cutoff of one residue, more than the Calpha-energy
+    stage holds, so the scan computes and adds its staged terms mid-way."""
+    W = pkg.workloads
+    rng = np.random.default_rng(123)
+    ag_ca = _ball(rng, 120, 0.0, 9.0)
+    ag_aa = W.random_sequence(120, rng)
+    ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    gp, op = _params(pkg, oracle, 10.0, acc, mutation_p=0.3, rotamer_move_p=0.5, backbone_move_p=0.2)
+    ctx.set_params(gp)
+    ctx.add_antigen(ag_aa, ag_pos)
+    A = oracle.Antigen(ag_aa, ag_pos)
+    n_res, n_cand = 8, 16
+    ca = _ball(rng, n_cand * n_res, 4.0, 12.0)
+    aa = W.random_sequence(n_cand * n_res, rng)
+    pos, chi = oracle.build_residues(ca, aa)
+    d2 = ((ca[:, None, :] - ag_ca[None, :, :]) ** 2).sum(-1)
+    assert (d2 <= 100.0).sum(1).max() > 64
+    temps = np.array([oracle.temperature(s, 600) for s in HOT], np.float32)
+    cid = np.arange(n_cand, dtype=np.uint32)
+    (g_aa, g_chi, g_pos), g_stats, o_stats = _run_pair(ctx, oracle, A, gp, op, aa, chi, pos, n_res, cid, HOT,
+                                                       temps)
+    assert o_stats[:, 0].sum() > 300
+    assert np.array_equal(g_stats, o_stats)
+    assert np.array_equal(g_aa, aa) and np.array_equal(g_chi, chi) and np.array_equal(g_pos, pos)
+
+
 def _cys_chains(oracle, center, n_cand, n_res, rng):
     """Straight Calpha chains (3.8 A steps) half made of Cys: every residue of the
     ideal backbone has the same orientation, so neighbouring SG atoms sit 3.8 A
