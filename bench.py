@@ -436,7 +436,8 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(workload_config(), launch=tuned, cuda_graph=True),
         "pair_evals_per_s": total_cand / n_cand * score_pairs / (ph[1] * 1e-3),
         "roofline": {"kernel": dom, "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak, "traffic": None,
+                     "frac": achieved / fp32_peak, "traffic": NCU_DRAM_BYTES.get(dom),
+                     "traffic_unit": "bytes per launch", "traffic_source": NCU_DRAM_SOURCE,
                      "peak_source": "FP32 FMA microbenchmark on this GPU (max of scalar/f32x2), "
                                     f"scalar {fp32_scalar:.1f}, packed {fp32_packed:.1f}; "
                                     f"nominal {148 * 128 * 2 * 1.965e-3:.1f} at 1965 MHz",
@@ -517,6 +518,13 @@ def run_batched(pkg, ctx, torch, ext):
             "launch": tuned, "survivors_per_antigen": [int((t >= 0).sum()) for t in top],
             "best_energy_per_antigen": [float(e_last[t[0]]) for t in top]}
 
+
+# DRAM bytes (read + write) of one launch of each block kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --block-only 8,8,1`,
+# the same per-launch work as the timed blocks
+NCU_DRAM_BYTES = {"langevin_cg": 7_612_928 + 321_792, "score_allatom": 3_970_560}
+NCU_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of "
+                   "bench.py --block-only 8,8,1 (cold cache, serialised)")
 
 SCHEDULES = (150, 200, 250, 300, 375, 450, 600)  # annealed schedule lengths of the learned-proposal study
 LEARNED_SEEDS = tuple(range(21, 33))
