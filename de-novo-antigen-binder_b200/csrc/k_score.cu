@@ -129,7 +129,7 @@ __device__ __forceinline__ void atom_vs_antigen(const AgView& A, const AtomIn& b
                             if (r2 <= HB_CUTOFF_SQ) {
                                 const float r = r2 * ir;
                                 const float z = (r - HB_R0) / HB_SIGMA;
-                                e += -HB_DEPTH * __expf(-0.5f * z * z);
+                                e += -HB_DEPTH * expf(-0.5f * z * z);
                             }
                         }
                         const float4 ej = c_eef1[b.type];
@@ -137,8 +137,8 @@ __device__ __forceinline__ void atom_vs_antigen(const AgView& A, const AtomIn& b
                             const float4 ei = c_eef1[at];
                             const float r = r2 * ir;
                             const float xi = r / ei.z, xj = r / ej.z;
-                            const float fi = __expf(-(xi * xi)) * ei.w;
-                            const float fj = __expf(-(xj * xj)) * ej.w;
+                            const float fi = expf(-(xi * xi)) * ei.w;
+                            const float fj = expf(-(xj * xj)) * ej.w;
                             e += -(ei.x * ej.y * fi + ej.x * ei.y * fj);
                         }
                     }
@@ -320,14 +320,14 @@ __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const
             if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) &&
                 r2 <= HB_CUTOFF_SQ) {
                 const float z = (r2 * ir - HB_R0) / HB_SIGMA;
-                e += -HB_DEPTH * __expf(-0.5f * z * z);
+                e += -HB_DEPTH * expf(-0.5f * z * z);
             }
             const float4 ej = c_eef1[bt];
             if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
                 const float4 ei = c_eef1[at];
                 const float r = r2 * ir;
                 const float xi = r / ei.z, xj = r / ej.z;
-                e += -(ei.x * ej.y * __expf(-(xi * xi)) * ei.w + ej.x * ei.y * __expf(-(xj * xj)) * ej.w);
+                e += -(ei.x * ej.y * expf(-(xi * xi)) * ei.w + ej.x * ei.y * expf(-(xj * xj)) * ej.w);
             }
         }
         part += e;

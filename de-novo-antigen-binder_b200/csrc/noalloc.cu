@@ -15,7 +15,12 @@
 // two calls whose work overlaps on the GPU (different streams, or different host
 // threads) race on it.  The device address of the array is looked up once per
 // device, on that device's first call (cudaGetSymbolAddress with the device
-// current); make that first call before any stream capture.
+// current); make that first call before any stream capture.  The work goes to the
+// current device: the caller's stream must belong to it.  The looked-up address
+// is kept for the life of the process, so after cudaDeviceReset on a device (which
+// unloads the library's module there) this entry point must not be called on that
+// device again.  Each call waits on the caller's stream twice (to read the
+// occupied cell box and the neighbour count back to the host).
 #include <cstring>
 #include <mutex>
 
@@ -126,6 +131,9 @@ extern "C" int binder_grid_neighbors_noalloc(float cell, const float* ax, const 
     if (n_q > (size_t)INT32_MAX / 2) return BINDER_ERR_ARG;
     if (!d_offsets || !out_total || (n_ag && (!ax || !ay || !az)) || (n_q && (!px || !py || !pz)))
         return BINDER_ERR_ARG;
+    // an error left pending by earlier work of the process is not this call's: report
+    // it without consuming it, so that the launch checks below see only this call's
+    if (cudaPeekAtLastError() != cudaSuccess) return BINDER_ERR_CUDA;
     unsigned char* base = nullptr;
     int s = scratch_base(&base);
     if (s) return s;

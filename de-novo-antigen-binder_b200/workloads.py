@@ -208,3 +208,18 @@ def config4(n_train=4, n_eval=2, n_cand=1024, n_res=20):
     train = [_config1_like(rng_for(4, salt=s), n_cand, n_res) for s in range(1, n_train + 1)]
     held = [_config1_like(rng_for(4, salt=1000 + s), n_cand, n_res) for s in range(1, n_eval + 1)]
     return dict(name="config4", train=train, eval=held)
+
+
+def config3_slots(ag_cloud_xyz, tables, n_cand=1024, n_res=20, charged_frac=0.3):
+    """The frozen contact-skewed poses of config3_poses in the slot layout of the
+    resident state: returns (aa [n_cand * n_res], pos [n_cand * n_res, 14, 3]), the
+    used slots of every residue holding the pose's atoms, the others zero."""
+    g, _, aa = config3_poses(ag_cloud_xyz, tables, n_cand, n_res, charged_frac)
+    n_at = tables.n_atoms[aa]
+    res_of_atom = np.repeat(np.arange(len(aa)), n_at)
+    slot = np.concatenate([np.arange(k) for k in n_at])
+    pos = np.zeros((len(aa), 14, 3), np.float32)
+    pos[res_of_atom, slot, 0] = g["x"]
+    pos[res_of_atom, slot, 1] = g["y"]
+    pos[res_of_atom, slot, 2] = g["z"]
+    return aa, pos

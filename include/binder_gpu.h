@@ -192,8 +192,13 @@ int binder_grid_neighbors(binder_ctx* ctx, float cell, const float* ax, const fl
    occupied cells <= BINDER_NOALLOC_MAX_CELLS (else BINDER_ERR_GRID);
    BINDER_ERR_CAPACITY with *out_total set when cap is too small.  Every call
    shares the scratch array: calls whose GPU work overlaps (different streams or
-   threads) race.  The first call on a device looks the array up on that device
-   (make it before any stream capture).  */
+   threads) race.  The work runs on the current device, so `stream` must belong
+   to it.  The first call on a device looks the array up on that device (make it
+   before any stream capture) and keeps the address for the life of the process:
+   after cudaDeviceReset on a device, do not call this entry point on it again.
+   Each call waits on `stream` twice, to read back the occupied cell box and the
+   neighbour count.  A CUDA error left pending by earlier work of the process is
+   reported as BINDER_ERR_CUDA before anything is enqueued, and left pending.  */
 #define BINDER_NOALLOC_MAX_ATOMS 65536
 #define BINDER_NOALLOC_MAX_CELLS 262144
 int binder_grid_neighbors_noalloc(float cell, const float* d_ax, const float* d_ay, const float* d_az,

@@ -1003,7 +1003,7 @@ void orc_step(const orc_antigen* A, const orc_params* prm, int n_cand, int n_res
 
 // allatom_energy (diffusion.rs:281-283) when full, else the score_batch terms
 void orc_score_slots64(const orc_antigen* A, int n_cand, int n_res, const uint8_t* aa, const float* pos, int full,
-                       double* out, int n_threads) {
+                       double* out, double* out_abs, int n_threads) {
     orc_cloud ag{A->x.data(), A->y.data(), A->z.data(), A->q.data(), A->rmh.data(), A->eps.data(), A->hyd.data(),
                  A->type.data(), (int64_t)A->x.size()};
     parallel_for(n_cand, n_threads, [&](int64_t c) {
@@ -1019,13 +1019,17 @@ void orc_score_slots64(const orc_antigen* A, int n_cand, int n_res, const uint8_
         double e[5], ea[5];
         orc_energy_atoms64(&ag, &ab, e, ea);
         double tot = e[0] + e[1] + e[2];
+        double tot_abs = ea[0] + ea[1] + ea[2];
         if (full) {
             std::vector<uint8_t> a2(caa, caa + n_res);
             std::vector<float> chi((size_t)n_res * 4, 0.f);
             Prot P{n_res, a2.data(), chi.data(), const_cast<float*>(cpos)};
-            tot += e[3] + e[4] + (double)disulfide(P);
+            const double ds = (double)disulfide(P);
+            tot += e[3] + e[4] + ds;
+            tot_abs += ea[3] + ea[4] + std::fabs(ds);
         }
         out[c] = tot;
+        if (out_abs) out_abs[c] = tot_abs;
     });
 }
 

@@ -151,9 +151,10 @@ void orc_step(const orc_antigen*, const orc_params*, int n_cand, int n_res,
               float temp, int with_noise, int with_mc, int64_t* stats, int n_threads);
 
 /* score every candidate (slot layout) against the antigen with the all-atom
-   LJ+Coulomb+hydrophobic (+ hbond + EEF1 if full) energy, f64 accumulation */
+   LJ+Coulomb+hydrophobic (+ hbond + EEF1 + disulfide if full) energy, f64
+   accumulation; out_abs (may be NULL) = the sum of |pair term| of the same terms */
 void orc_score_slots64(const orc_antigen*, int n_cand, int n_res, const uint8_t* aa, const float* pos,
-                       int full, double* out, int n_threads);
+                       int full, double* out, double* out_abs, int n_threads);
 
 /* stable ascending sort of energies, NaN last; first k indices (diffusion.rs:1045-1047) */
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx);

@@ -45,7 +45,7 @@ def lib():
         _L.orc_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_uint32, C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_int]
         _L.orc_score_slots64.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
-                                         C.c_int]
+                                         C.c_void_p, C.c_int]
         _L.orc_place_atom.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_void_p]
         _L.orc_grid_cell.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p]
     return _L
@@ -322,12 +322,15 @@ class Antigen:
         lib().orc_step(self.h, C.byref(params), n_cand, n_res, P(aa), P(chi), P(pos), P(cid), step_id, temp,
                        int(with_noise), int(with_mc), P(stats), threads)
 
-    def score_slots64(self, aa, pos, n_res, full=False, threads=8):
+    def score_slots64(self, aa, pos, n_res, full=False, threads=8, with_abs=False):
+        """f64 energy per candidate; with_abs also the sum of |pair term| (the
+        denominator of the norm-wise error of ill-conditioned candidates)"""
         aa, pos = u8(aa), f32(pos)
         n_cand = len(aa) // n_res
         out = np.zeros(n_cand, np.float64)
-        lib().orc_score_slots64(self.h, n_cand, n_res, P(aa), P(pos), int(full), P(out), threads)
-        return out
+        ab = np.zeros(n_cand, np.float64) if with_abs else None
+        lib().orc_score_slots64(self.h, n_cand, n_res, P(aa), P(pos), int(full), P(out), P(ab), threads)
+        return (out, ab) if with_abs else out
 
 
 def disulfide(aa, pos):

@@ -28,11 +28,12 @@ def _call(pkg, torch, cell, ag, q, cap):
     d_ag = [torch.from_numpy(np.ascontiguousarray(ag[:, k])).to(dev) for k in range(3)]
     d_q = [torch.from_numpy(np.ascontiguousarray(q[:, k])).to(dev) for k in range(3)]
     d_off = torch.full((len(q) + 1,), -7, dtype=torch.int64, device=dev)
-    d_idx = torch.full((cap,), -7, dtype=torch.int32, device=dev)
+    d_idx = torch.full((max(cap, 1),), -7, dtype=torch.int32, device=dev)
     total = C.c_size_t(0)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    st = _fn(pkg)(cell, *(t.data_ptr() for t in d_ag), len(ag), *(t.data_ptr() for t in d_q), len(q),
-                  d_off.data_ptr(), d_idx.data_ptr(), cap, C.byref(total), stream)
+    ptr = lambda t: t.data_ptr() if t.numel() else None  # noqa: E731 (empty inputs: NULL)
+    st = _fn(pkg)(cell, *(ptr(t) for t in d_ag), len(ag), *(ptr(t) for t in d_q), len(q),
+                  d_off.data_ptr(), d_idx.data_ptr() if cap else None, cap, C.byref(total), stream)
     torch.cuda.synchronize(dev)
     return st, total.value, d_off.cpu().numpy(), d_idx.cpu().numpy().view(np.uint32)
 
@@ -64,3 +65,32 @@ def test_noalloc_limits(pkg):
     ag = np.float32([[0, 0, 0], [1, 0, 0]])
     st, total, *_ = _call(pkg, torch, 10.0, ag, q, cap=1)
     assert st == 9 and total == 8  # BINDER_ERR_CAPACITY reports the size needed
+
+
+def test_noalloc_edge_cases_match_allocating_entry_point(pkg, ctx):
+    """Empty antigen, empty probes, no neighbours with a NULL index buffer, and a
+    NaN antigen coordinate (BINDER_ERR_NAN) followed by a good call: the scratch is
+    re-initialised by every call, so nothing of a failed call leaks into the next."""
+    import torch
+    rng = np.random.default_rng(7)
+    ag = rng.uniform(-20, 20, size=(400, 3)).astype(np.float32)
+    q = rng.uniform(-30, 30, size=(300, 3)).astype(np.float32)
+    far = np.float32([[500, 500, 500], [-500, 0, 0]])
+    cases = [(ag[:0], q, 64), (ag, q[:0], 64), (ag, far, 0)]
+    for a, p, cap in cases:
+        ref_off, ref_idx = ctx.grid_neighbors(8.0, a[:, 0], a[:, 1], a[:, 2], p[:, 0], p[:, 1], p[:, 2])
+        st, total, off, idx = _call(pkg, torch, 8.0, a, p, cap=cap)
+        assert st == 0 and total == len(ref_idx) == 0, (len(a), len(p), st, total)
+        assert np.array_equal(off, ref_off)
+    bad = ag.copy()
+    bad[17, 1] = np.nan
+    with pytest.raises(pkg.BinderError) as e:
+        ctx.grid_neighbors(8.0, bad[:, 0], bad[:, 1], bad[:, 2], q[:, 0], q[:, 1], q[:, 2])
+    assert e.value.status == 5
+    st, *_ = _call(pkg, torch, 8.0, bad, q, cap=1 << 16)
+    assert st == 5  # BINDER_ERR_NAN, as the allocating entry point reports
+    ref_off, ref_idx = ctx.grid_neighbors(8.0, ag[:, 0], ag[:, 1], ag[:, 2], q[:, 0], q[:, 1], q[:, 2])
+    for _ in range(2):
+        st, total, off, idx = _call(pkg, torch, 8.0, ag, q, cap=len(ref_idx))
+        assert st == 0 and total == len(ref_idx)
+        assert np.array_equal(off, ref_off) and np.array_equal(idx[:total], ref_idx)
