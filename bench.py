@@ -712,6 +712,53 @@ def run_phase2_only(args):
     return 0
 
 
+def launch_ranks(n, argv, timeout_s=3600):
+    """`bench.py --gpus N` started as one process (no WORLD_SIZE in the environment):
+    start N ranks, one per GPU, under torch.distributed.run on 127.0.0.1 and return
+    its exit status.  Rank 0 prints the one JSON line; the others print nothing."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve())] + list(argv)
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "1"))
+    try:
+        return subprocess.run(cmd, env=env, timeout=timeout_s).returncode
+    except subprocess.TimeoutExpired:
+        sys.stderr.write(f"bench.py: {n} ranks did not finish within {timeout_s} s\n")
+        return 124
+
+
+def run_rank_check(args, rank, world):
+    """The multi-rank plumbing of the timed run without a GPU (CPU `gloo`): every rank
+    holds a seeded local population's energies and times, the ranks meet at the
+    barrier, the timed region is the max over ranks, the candidate total the sum, and
+    the survivors are merged by the one all-gather -- the calls run_ours makes on N
+    GPUs.  Rank 0 prints one JSON line."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        dist.init_process_group(backend="gloo", timeout=timedelta(seconds=60))
+    cpu = torch.device("cpu")
+    rng = np.random.default_rng(1000 + rank)
+    n_cand = 1024
+    e = rng.normal(-20.0, 5.0, size=n_cand)
+    local = np.lexsort((np.arange(n_cand), e))[:TOP_K]
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks(torch, dist, world, 0.2 + 0.01 * rank, cpu)
+    total = sum_over_ranks(torch, dist, world, float(n_cand), cpu)
+    idx, ev = merge_survivors(torch, dist, world, e, local, rank, n_cand)
+    if rank == 0:
+        print(json.dumps({"rank_check": True, "n_gpus": world, "ms_per_step": ms, "candidates": int(total),
+                          "survivors": idx.tolist(), "survivor_energies": ev.tolist()}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -731,12 +778,18 @@ def main():
                     help="profiling case: one uniform and one learned-proposal Metropolis launch of 25 steps")
     ap.add_argument("--learned-validation", action="store_true",
                     help="proposal temperature settings of the learned proposal on the validation antigen")
+    ap.add_argument("--rank-check", action="store_true",
+                    help="the multi-rank plumbing (barrier, max/sum over ranks, survivor all-gather) on CPU gloo")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus, sys.argv[1:])
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.rank_check:
+        return run_rank_check(args, rank, world)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.phase2_only:

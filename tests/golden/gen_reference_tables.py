@@ -18,14 +18,18 @@ Sources parsed (paths inside the reference project):
   src/diffusion.rs scalar hyper-parameters (:30-83)
   src/allatom.rs   ideal-backbone bond lengths (:494-497)
 
-Usage:  python tests/golden/gen_reference_tables.py [reference_root]
+Usage:  python tests/golden/gen_reference_tables.py <reference_root>
+
+reference_root is the directory of the reference crate (the one holding src/).
 """
 import json
 import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: gen_reference_tables.py <reference_root>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).with_name("reference_tables.json")
 
 AA_NAMES = ["Ala", "Arg", "Asn", "Asp", "Cys", "Gln", "Glu", "Gly", "His", "Ile",

@@ -95,3 +95,23 @@ def test_merge_single_rank_is_local_top_k():
     local = _order(e, np.arange(N_CAND))[:K]
     idx, ev = bench.merge_survivors(None, None, 1, e, local, 0, N_CAND, k=K)
     assert np.array_equal(idx, local) and np.array_equal(ev, e[local], equal_nan=True)
+
+
+def test_bench_gpus_2_starts_two_ranks():
+    """`bench.py --gpus 2` run as one process starts two ranks (torch.distributed.run
+    on 127.0.0.1) that meet in a world-size-2 group; with --rank-check they run the
+    timed run's collective calls on CPU gloo and rank 0 alone prints one line."""
+    import json
+    import subprocess
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--rank-check"], capture_output=True,
+                       text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    out = json.loads(lines[0])
+    assert out["n_gpus"] == 2 and out["candidates"] == 2048
+    # the merged survivors = the global top-64 of both ranks' seeded energies
+    e = np.concatenate([np.random.default_rng(1000 + rank).normal(-20.0, 5.0, size=1024) for rank in range(2)])
+    exp = _order(e, np.arange(2048))[:64]
+    assert out["survivors"] == exp.tolist()
+    assert out["ms_per_step"] == pytest.approx(0.21)
