@@ -79,12 +79,12 @@ class LaunchCfg(C.Structure):
     """binder_launch_cfg (include/binder_gpu.h): launch shapes of the search block."""
     _fields_ = [("score_warps", C.c_int32), ("score_ctas_per_sm", C.c_int32), ("cg_warps", C.c_int32),
                 ("cg_lanes", C.c_int32), ("cg_order", C.c_int32), ("score_order", C.c_int32),
-                ("cg_queue", C.c_int32)]
+                ("cg_queue", C.c_int32), ("cg_flat", C.c_int32)]
 
     def as_dict(self):
         return {"score_warps": self.score_warps, "score_ctas_per_sm": self.score_ctas_per_sm,
                 "cg_warps": self.cg_warps, "cg_lanes": self.cg_lanes, "cg_order": self.cg_order,
-                "score_order": self.score_order, "cg_queue": self.cg_queue}
+                "score_order": self.score_order, "cg_queue": self.cg_queue, "cg_flat": self.cg_flat}
 
 
 FLAG_GRAPH = 1
@@ -183,6 +183,8 @@ _SIGS = {
     "binder_set_proposal": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float]),
     "binder_selftest_wait": (C.c_int, [C.c_void_p, C.c_uint32]),
     "binder_debug_fail_alloc": (C.c_int, [C.c_int64]),
+    "binder_minimize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "binder_affinity_maturation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 
@@ -589,14 +591,30 @@ class GpuContext:
         self._sync_state_info()
         return cand.reshape(n_segments, -1), e.reshape(n_segments, -1)
 
+    def minimize(self, steps=60):
+        """minimize (diffusion.rs:854-916) of every resident candidate against its
+        antigen, in place; returns the final energies."""
+        out = np.zeros(self._state_cand, np.float64)
+        self._check(lib().binder_minimize(self._h, int(steps), _ptr(out)))
+        return out
+
+    def affinity_maturation(self):
+        """affinity_maturation_allatom (diffusion.rs:924-961) over every resident
+        candidate's interface residues, in place; returns (final scores, mutations
+        kept)."""
+        out = np.zeros(self._state_cand, np.float64)
+        kept = np.zeros(self._state_cand, np.int32)
+        self._check(lib().binder_affinity_maturation(self._h, _ptr(out), _ptr(kept)))
+        return out, kept
+
     def launch_cfg(self):
         c = LaunchCfg()
         self._check(lib().binder_get_launch_cfg(self._h, C.byref(c)))
         return c
 
     def set_launch_cfg(self, score_warps=8, score_ctas_per_sm=4, cg_warps=8, cg_lanes=8, cg_order=1, score_order=0,
-                       cg_queue=1):
-        c = LaunchCfg(score_warps, score_ctas_per_sm, cg_warps, cg_lanes, cg_order, score_order, cg_queue)
+                       cg_queue=1, cg_flat=0):
+        c = LaunchCfg(score_warps, score_ctas_per_sm, cg_warps, cg_lanes, cg_order, score_order, cg_queue, cg_flat)
         self._check(lib().binder_set_launch_cfg(self._h, C.byref(c)))
 
     def autotune(self, reps=5):

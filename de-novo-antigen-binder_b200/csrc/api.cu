@@ -647,7 +647,7 @@ binder_ctx* binder_create(int device, const binder_params* params, int* status) 
     else binder_default_params(&ctx->params);
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         score_init_tables() != cudaSuccess || search_init_tables() != cudaSuccess ||
-        anneal_init_tables() != cudaSuccess || init_mlp_tables() != cudaSuccess) {
+        anneal_init_tables() != cudaSuccess || init_mlp_tables() != cudaSuccess || post_init_tables() != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
         *status = BINDER_ERR_CUDA;
@@ -1374,7 +1374,8 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
         }
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
                    temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
-                   ctx->cfg.cg_order, max_ag, max_cells, stage_ag, ctx->cfg.cg_queue ? S.queue.p + 1 : nullptr);
+                   ctx->cfg.cg_order, max_ag, max_cells, stage_ag, ctx->cfg.cg_queue ? S.queue.p + 1 : nullptr,
+                   ctx->cfg.cg_flat);
     LAUNCHED("diffuse");
     return BINDER_OK;
 }
@@ -1462,7 +1463,8 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
         (uint64_t)n_steps, (uint64_t)k, (uint64_t)S.n_cand, (uint64_t)S.total_res, (uint64_t)S.n_segments,
         (uint64_t)S.n_keys, (uint64_t)ctx->cfg.score_warps, (uint64_t)ctx->cfg.score_ctas_per_sm,
         (uint64_t)ctx->cfg.cg_warps, (uint64_t)ctx->cfg.cg_lanes, (uint64_t)ctx->cfg.cg_order,
-        (uint64_t)ctx->cfg.score_order, (uint64_t)ctx->cfg.cg_queue, (uint64_t)ctx->ags.size()};
+        (uint64_t)ctx->cfg.score_order, (uint64_t)ctx->cfg.cg_queue, (uint64_t)ctx->cfg.cg_flat,
+        (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
                           S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
@@ -1522,8 +1524,8 @@ void tune_cache_load(binder_ctx* ctx) {
     if (!f) return;
     char key[1024];
     LaunchCfg c;
-    while (std::fscanf(f, "%1023s %d %d %d %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
-                       &c.cg_lanes, &c.cg_order, &c.score_order, &c.cg_queue) == 8)
+    while (std::fscanf(f, "%1023s %d %d %d %d %d %d %d %d", key, &c.score_warps, &c.score_ctas_per_sm, &c.cg_warps,
+                       &c.cg_lanes, &c.cg_order, &c.score_order, &c.cg_queue, &c.cg_flat) == 9)
         ctx->tune_cache.emplace_back(key, c);
     std::fclose(f);
 }
@@ -1534,8 +1536,8 @@ void tune_cache_store(binder_ctx* ctx, const std::string& key, const LaunchCfg& 
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps,
-                 c.cg_lanes, c.cg_order, c.score_order, c.cg_queue);
+    std::fprintf(f, "%s %d %d %d %d %d %d %d %d\n", key.c_str(), c.score_warps, c.score_ctas_per_sm, c.cg_warps,
+                 c.cg_lanes, c.cg_order, c.score_order, c.cg_queue, c.cg_flat);
     std::fclose(f);
 }
 
@@ -1577,6 +1579,7 @@ int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out) {
     out->cg_order = ctx->cfg.cg_order;
     out->score_order = ctx->cfg.score_order;
     out->cg_queue = ctx->cfg.cg_queue;
+    out->cg_flat = ctx->cfg.cg_flat;
     return BINDER_OK;
 }
 
@@ -1586,7 +1589,9 @@ int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
         c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8) ||
         (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8) || c->cg_order < 0 ||
         c->cg_order > 2 || c->score_order < 0 || c->score_order > 1 ||
-        c->cg_queue < 0 || c->cg_queue > 1)
+        c->cg_queue < 0 || c->cg_queue > 1 ||
+        (c->cg_flat != 0 && c->cg_flat != 8 && c->cg_flat != 16 && c->cg_flat != 32) ||
+        (c->cg_flat == 32 && c->cg_warps != 4) || (c->cg_flat && c->cg_warps != 4 && c->cg_warps != 8))
         return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
     ctx->cfg.score_warps = c->score_warps;
     ctx->cfg.score_ctas_per_sm = c->score_ctas_per_sm;
@@ -1595,6 +1600,7 @@ int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
     ctx->cfg.cg_order = c->cg_order;
     ctx->cfg.score_order = c->score_order;
     ctx->cfg.cg_queue = c->cg_queue;
+    ctx->cfg.cg_flat = c->cg_flat;
     return BINDER_OK;
 }
 
@@ -1620,22 +1626,25 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
     CK(cudaMemcpyAsync(saved.p, S.res_pos.p, n_slots * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     LaunchCfg best = ctx->cfg;
     float best_ms = 1e30f;
+    // lane-group shapes (flat 0: lanes x warps) and flat shapes (residues per warp x warps)
+    const int shapes[][3] = {{0, 4, 2}, {0, 4, 4}, {0, 8, 2}, {0, 8, 4}, {0, 8, 8},
+                             {32, 8, 4}, {16, 8, 4}, {16, 8, 8}, {8, 8, 4}, {8, 8, 8}};
     for (int queue : {0, 1})
     for (int order : {0, 1, 2})
-    for (int lanes : {4, 8})
-        for (int w : {2, 4, 8}) {
+        for (const auto& sh : shapes) {
             if (s) break;
-            if (lanes == 4 && w == 8) continue;  // not a supported shape
-            ctx->cfg.cg_warps = w;
-            ctx->cfg.cg_lanes = lanes;
+            ctx->cfg.cg_flat = sh[0];
+            ctx->cfg.cg_lanes = sh[1];
+            ctx->cfg.cg_warps = sh[2];
             ctx->cfg.cg_order = order;
             ctx->cfg.cg_queue = queue;
             float ms = 0.f;
             if ((s = time_ms(ctx, reps, [&] { return enqueue_diffuse(ctx, 10, 0, 0, 0, nullptr); }, &ms))) break;
             if (ms < best_ms) {
                 best_ms = ms;
-                best.cg_warps = w;
-                best.cg_lanes = lanes;
+                best.cg_flat = sh[0];
+                best.cg_warps = sh[2];
+                best.cg_lanes = sh[1];
                 best.cg_order = order;
                 best.cg_queue = queue;
             }
@@ -1857,6 +1866,74 @@ int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* o
     }
     // the resident state becomes the results in rank order
     return binder_state_select(ctx, keep.data(), keep.size());
+}
+
+int binder_minimize(binder_ctx* ctx, int steps, double* out_energy) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (steps < 0) return fail(ctx, BINDER_ERR_ARG, "negative step count");
+    if ((s = ensure_trig(ctx))) return s;
+    if ((s = clear_err(ctx))) return s;
+    DBuf<float4> trial;
+    DBuf<double> best, e_trial;
+    CK(trial.ensure((size_t)S.total_res * SLOT_STRIDE), "alloc");
+    CK(best.ensure(S.n_cand), "alloc");
+    CK(e_trial.ensure(S.n_cand), "alloc");
+    // the energy minimize starts from (partners_energy, diffusion.rs:859)
+    if ((s = enqueue_score_state(ctx, 1))) return s;
+    CK(cudaMemcpyAsync(best.p, ctx->energy.p, S.n_cand * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream),
+       "copy");
+    StateView tv = S.view();
+    tv.res_pos = trial.p;
+    const StateScoreScratch scr{nullptr, S.queue.p, S.res_e.p, S.res_abs.p};
+    const ScoreOut o{e_trial.p, nullptr, nullptr, nullptr, ctx->errf.p};
+    for (int step = 0; step < steps; ++step) {
+        // step size decaying linearly to zero (diffusion.rs:880-881), f32 as the reference
+        const float frac = 1.0f - (float)step / (float)steps;
+        const float step_size = 0.04f * frac;
+        launch_min_move(ctx->stream, S.view(), ctx->d_views.p, S.res_pos.p, trial.p, step_size);
+        LAUNCHED("min_move");
+        ctx->launches += launch_score_state(ctx->stream, tv, ctx->d_views.p, ctx->params.accumulate, 1, o, scr,
+                                            persistent_ctas(ctx), ctx->cfg.score_warps) - 1;
+        LAUNCHED("score_state");
+        launch_min_accept(ctx->stream, S.view(), trial.p, e_trial.p, best.p, nullptr);
+        LAUNCHED("min_accept");
+    }
+    S.order_valid = false;  // residues moved
+    if ((s = check_err(ctx))) return s;
+    if (out_energy)
+        CK(cudaMemcpyAsync(out_energy, best.p, S.n_cand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_affinity_maturation(binder_ctx* ctx, double* out_energy, int32_t* out_mutated) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if (S.max_res > ANNEAL_MAX_RES)
+        return fail(ctx, BINDER_ERR_ARG, "affinity maturation holds at most %d residues per candidate", ANNEAL_MAX_RES);
+    if ((s = ensure_trig(ctx))) return s;
+    if ((s = clear_err(ctx))) return s;
+    DBuf<double> best;
+    DBuf<int> kept;
+    CK(best.ensure(S.n_cand), "alloc");
+    CK(kept.ensure(S.n_cand), "alloc");
+    // per-residue full energies of the state (the scan changes one residue at a time)
+    if ((s = enqueue_score_state(ctx, 1))) return s;
+    launch_mature(ctx->stream, S.view(), ctx->d_views.p, S.res_e.p, best.p, kept.p, ctx->errf.p);
+    LAUNCHED("mature");
+    S.order_valid = false;
+    if ((s = check_err(ctx))) return s;
+    if (out_energy)
+        CK(cudaMemcpyAsync(out_energy, best.p, S.n_cand * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if (out_mutated)
+        CK(cudaMemcpyAsync(out_mutated, kept.p, S.n_cand * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
 }
 
 void* binder_stream(binder_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

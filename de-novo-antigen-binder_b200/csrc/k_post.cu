@@ -1,0 +1,276 @@
+// k_post.cu — the post-search refinement of the reference's all-atom results on
+// the GPU, batched over every resident candidate (main.rs:336-346).
+//
+//  * minimize (diffusion.rs:854-916) against the candidate's antigen: steepest
+//    descent on the Calpha-level grid force (compute_forces_with_grid,
+//    energy.rs:322-398) with a step decaying linearly to zero (MIN_STEP 0.04,
+//    every component clamped to MIN_MAX_DISP 0.5, diffusion.rs:63-64), the side
+//    chains rebuilt from the moved backbone (allatom.rs:244-270), and a step kept
+//    only when the all-atom energy (allatom_energy: interaction_energy_atoms +
+//    disulfide_energy, diffusion.rs:281-283, 835-840) drops.  Three launches per
+//    step: the move of every residue into a trial copy of the positions, the full
+//    score of the trial copy, the per-candidate keep-or-restore.
+//  * affinity_maturation_allatom (diffusion.rs:924-961) over the interface
+//    residues (filters.rs:96-105, main.rs:342-344): one CTA per candidate walks its
+//    mutable positions in order; at a position the 19 other amino acids (ALL_AA
+//    order, atom.rs:29, each at its top rotamer) and the mutation back to the old
+//    amino acid and chi are built at once (mutate_residue, allatom.rs:299-384),
+//    their residue energies computed by the warps of the CTA, and the first
+//    amino acid whose total is strictly below the best is kept -- the reference's
+//    scan, whose candidates differ only in the one residue.
+//
+// Residue geometry keeps the reference's f32 operation order (bit-identical to
+// the CPU restatement); energies are f32 pair terms with compensated sums and
+// FP64 totals, so every keep / reject decision is the f64 energy's.
+#include "geom.cuh"
+#include "score.cuh"
+
+namespace binder {
+
+cudaError_t post_init_tables() {
+    cudaError_t e = geom_init_tables();
+    if (e != cudaSuccess) return e;
+    return score_tables_init();
+}
+
+// ---- minimize -----------------------------------------------------------------------
+// One thread per residue: the grid force on the pre-step Calpha (pos_in), the
+// clamped move, the translated residue and its rebuilt side chain (pos_out).
+__global__ void k_min_move(StateView st, const AgView* __restrict__ ags, const float4* __restrict__ pos_in,
+                           float4* __restrict__ pos_out, float step_size) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= st.total_res) return;
+    const int aa = st.res_aa[r];
+    const AgView& A = ags[st.cand_ag[st.res_cand[r]]];
+    const float4* in = pos_in + (size_t)r * SLOT_STRIDE;
+    const int n_at = s_topo_n[aa];
+    const float4 c4 = in[1];  // Calpha = topology atom 1
+    const F3 ca = {c4.x, c4.y, c4.z};
+    float fx, fy, fz;
+    cg_force(A, cg_body(ca.x, ca.y, ca.z, aa), fx, fy, fz);
+    // fx_buf (zeroed) += the one partner's force, then the clamped step (f32 clamp)
+    constexpr float MAXD = 0.5f;
+    auto clampf = [](float v) { return v < -MAXD ? -MAXD : (v > MAXD ? MAXD : v); };
+    const float dx = clampf(xmul(step_size, xadd(0.0f, fx)));
+    const float dy = clampf(xmul(step_size, xadd(0.0f, fy)));
+    const float dz = clampf(xmul(step_size, xadd(0.0f, fz)));
+    const F3 new_ca = {xadd(ca.x, dx), xadd(ca.y, dy), xadd(ca.z, dz)};
+    const F3 dl = sub3(new_ca, ca);  // set_ca_pos: every atom += new - old
+    F3 atoms[SLOTS];
+#pragma unroll
+    for (int k = 0; k < SLOTS; ++k) {
+        const float4 v = in[k];
+        atoms[k] = k < n_at ? F3{xadd(v.x, dl.x), xadd(v.y, dl.y), xadd(v.z, dl.z)} : F3{v.x, v.y, v.z};
+    }
+    // rebuild_side_chain: the side chain from the moved backbone at the residue's chi
+    const int n_bb = aa == GLY ? 4 : 5;
+    const ChiTrig ct = unpack_trig(st.res_trig[2 * r], st.res_trig[2 * r + 1]);
+    build_side_chain(aa, atoms, n_bb, ct);
+    float4* out = pos_out + (size_t)r * SLOT_STRIDE;
+#pragma unroll
+    for (int k = 0; k < SLOT_STRIDE; ++k)
+        out[k] = k < n_at ? make_float4(atoms[k].x, atoms[k].y, atoms[k].z, 0.f) : in[k];
+}
+
+// Keep the trial positions of candidate c when its energy is strictly lower.
+__global__ void k_min_accept(StateView st, const float4* __restrict__ trial, const double* __restrict__ e_trial,
+                             double* __restrict__ best, int* __restrict__ kept) {
+    const int c = blockIdx.x;
+    __shared__ int s_take;
+    if (threadIdx.x == 0) {
+        const double e = e_trial[c];
+        s_take = e < best[c];
+        if (s_take) {
+            best[c] = e;
+            if (kept) kept[c] += 1;
+        }
+    }
+    __syncthreads();
+    if (!s_take) return;
+    const size_t s0 = (size_t)st.cand_res_off[c] * SLOT_STRIDE, s1 = (size_t)st.cand_res_off[c + 1] * SLOT_STRIDE;
+    for (size_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) st.res_pos[i] = trial[i];
+}
+
+void launch_min_move(cudaStream_t s, const StateView& st, const AgView* ags, const float4* pos_in, float4* pos_out,
+                     float step_size) {
+    if (st.total_res > 0) k_min_move<<<(st.total_res + 127) / 128, 128, 0, s>>>(st, ags, pos_in, pos_out, step_size);
+}
+void launch_min_accept(cudaStream_t s, const StateView& st, const float4* trial, const double* e_trial, double* best,
+                       int* kept) {
+    if (st.n_cand > 0) k_min_accept<<<st.n_cand, 128, 0, s>>>(st, trial, e_trial, best, kept);
+}
+
+// ---- affinity maturation ------------------------------------------------------------
+constexpr int MAT_TRIALS = 20;  // 19 other amino acids + the mutation back
+constexpr int MAT_WARPS = 10;
+
+// disulfide_energy (allatom.rs:155-180) of candidate c with residue `rr` replaced by
+// (aa_r, sg_r): Gaussian well between every pair of Cys SG atoms (topology atom 5),
+// pairs in the reference's order, f32.
+__device__ float disulfide_with(const StateView& st, int c, int rr, int aa_r, float4 sg_r) {
+    const int r0 = st.cand_res_off[c], r1 = st.cand_res_off[c + 1];
+    float ds = 0.0f;
+    for (int ri = r0; ri < r1; ++ri) {
+        const int ai = ri == rr ? aa_r : st.res_aa[ri];
+        if (ai != CYS) continue;
+        const float4 pi = ri == rr ? sg_r : st.res_pos[(size_t)ri * SLOT_STRIDE + 5];
+        for (int rj = ri + 1; rj < r1; ++rj) {
+            const int aj = rj == rr ? aa_r : st.res_aa[rj];
+            if (aj != CYS) continue;
+            const float4 pj = rj == rr ? sg_r : st.res_pos[(size_t)rj * SLOT_STRIDE + 5];
+            const float d = xsqrt(xdist2(xsub(pi.x, pj.x), xsub(pi.y, pj.y), xsub(pi.z, pj.z)));
+            if (d > 4.0f) continue;
+            const float z = xdiv(xsub(d, 2.05f), 0.4f);
+            ds = xsub(ds, xmul(4.0f, mc_exp(xmul(xmul(-0.5f, z), z))));
+        }
+    }
+    return ds;
+}
+
+// One CTA per candidate.  res_e: the per-residue full energies of the state (kept
+// current); out_best: the final score (the reference's `best`); out_kept:
+// mutations kept.
+__global__ void __launch_bounds__(MAT_WARPS * 32) k_mature(StateView st, const AgView* __restrict__ ags,
+                                                            double* __restrict__ res_e, double* __restrict__ out_best,
+                                                            int* __restrict__ out_kept, uint32_t* __restrict__ err) {
+    const int c = blockIdx.x;
+    const int r0 = st.cand_res_off[c], r1 = st.cand_res_off[c + 1], n = r1 - r0;
+    const AgView& A = ags[st.cand_ag[c]];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    __shared__ GroupSmem gs[MAT_WARPS];
+    __shared__ float4 s_pos[MAT_TRIALS][SLOTS];
+    __shared__ int s_aa[MAT_TRIALS];
+    __shared__ float4 s_chi[MAT_TRIALS], s_trig[MAT_TRIALS][2];
+    __shared__ double s_e[MAT_TRIALS];
+    __shared__ float s_ds[MAT_TRIALS];
+    __shared__ unsigned char s_mut[ANNEAL_MAX_RES];
+    __shared__ double s_best;
+    __shared__ int s_pick, s_kept;
+    if (n > ANNEAL_MAX_RES) {
+        if (threadIdx.x == 0) atomicOr(err, ERRF_RANGE);
+        return;
+    }
+    // mutable = interface residues (filters.rs:96-105): an antigen Calpha closer than 8 A
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 p = st.res_pos[(size_t)(r0 + i) * SLOT_STRIDE + 1];
+        bool any = false;
+        for (int j = 0; j < A.n_res && !any; ++j) {
+            const float4 q = A.ca_atom[j];
+            any = xdist2(xsub(p.x, q.x), xsub(p.y, q.y), xsub(p.z, q.z)) < 64.0f;
+        }
+        s_mut[i] = any;
+    }
+    if (threadIdx.x == 0) {
+        double e = 0.0;
+        for (int r = r0; r < r1; ++r) e += res_e[r];
+        s_best = e + (double)disulfide_with(st, c, -1, 0, make_float4(0.f, 0.f, 0.f, 0.f));
+        s_kept = 0;
+    }
+    __syncthreads();
+    for (int i = 0; i < n; ++i) {
+        if (!s_mut[i]) continue;  // CTA-uniform
+        const int r = r0 + i;
+        const int old_aa = st.res_aa[r];
+        // build the trials: t < 19 the t-th other amino acid at its top rotamer, 19 the old one at its chi
+        if (threadIdx.x < MAT_TRIALS) {
+            const int t = threadIdx.x;
+            const float4 c4 = st.res_pos[(size_t)r * SLOT_STRIDE + 1];
+            int aa;
+            ChiTrig ct;
+            float4 chi, tr0, tr1;
+            if (t < MAT_TRIALS - 1) {
+                aa = t < old_aa ? t : t + 1;
+                if (s_rot_n[aa] > 0) {
+                    ct = rot_trig(aa, 0);
+                    chi = s_rot_chi[aa][0];
+                } else {
+                    ct = zero_trig();
+                    chi = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                tr0 = make_float4(ct.t[0].x, ct.t[0].y, ct.t[1].x, ct.t[1].y);
+                tr1 = make_float4(ct.t[2].x, ct.t[2].y, ct.t[3].x, ct.t[3].y);
+            } else {
+                aa = old_aa;
+                tr0 = st.res_trig[2 * r];
+                tr1 = st.res_trig[2 * r + 1];
+                ct = unpack_trig(tr0, tr1);
+                chi = st.res_chi[r];
+            }
+            F3 atoms[SLOTS];
+            const int n_bb = ideal_backbone(F3{c4.x, c4.y, c4.z}, aa, atoms);
+            build_side_chain(aa, atoms, n_bb, ct);
+            const int n_at = s_topo_n[aa];
+            for (int k = 0; k < SLOTS; ++k)
+                s_pos[t][k] = k < n_at ? make_float4(atoms[k].x, atoms[k].y, atoms[k].z, 0.f)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+            s_aa[t] = aa;
+            s_chi[t] = chi;
+            s_trig[t][0] = tr0;
+            s_trig[t][1] = tr1;
+            s_ds[t] = disulfide_with(st, c, r, aa, s_pos[t][5]);
+        }
+        __syncthreads();
+        // residue energy of every trial: one warp per trial
+        GroupSmem& g = gs[warp];
+        for (int t = warp; t < MAT_TRIALS; t += MAT_WARPS) {
+            const int aa = s_aa[t];
+            const int na = c_topo_n[aa];
+            if (lane < na) {
+                const float4 p = s_pos[t][lane];
+                const float4 m = c_slot_prm[aa][lane];
+                g.pos[lane] = make_float4(p.x, p.y, p.z, m.x);
+                g.prm[lane] = make_float4(m.y, m.z, m.w, (float)c_slot_type[aa][lane]);
+                group_xyz(g, lane, na, p.x, p.y, p.z);
+                group_prm(g, lane, na, m.x, m.y, m.z, m.w);
+            } else {
+                group_xyz(g, lane, na, 0.f, 0.f, 0.f);
+                group_prm(g, lane, na, 0.f, 0.f, 0.f, 0.f);
+            }
+            __syncwarp();
+            Acc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0};
+            score_group<true, true, false, false>(&A, g, na, lane, lt, acc);
+            const double e = warp_sum_d((double)acc.s - (double)acc.c);
+            if (lane == 0) s_e[t] = e;
+            __syncwarp();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double others = 0.0;
+            for (int q = r0; q < r1; ++q)
+                if (q != r) others += res_e[q];
+            int pick = MAT_TRIALS - 1;
+            for (int t = 0; t < MAT_TRIALS - 1; ++t) {
+                const double tot = (others + s_e[t]) + (double)s_ds[t];
+                if (tot < s_best) {
+                    s_best = tot;
+                    pick = t;
+                    ++s_kept;
+                    break;
+                }
+            }
+            s_pick = pick;
+            res_e[r] = s_e[pick];
+            st.res_aa[r] = (uint8_t)s_aa[pick];
+            st.res_chi[r] = s_chi[pick];
+            st.res_trig[2 * r] = s_trig[pick][0];
+            st.res_trig[2 * r + 1] = s_trig[pick][1];
+        }
+        __syncthreads();
+        if (threadIdx.x < SLOT_STRIDE)
+            st.res_pos[(size_t)r * SLOT_STRIDE + threadIdx.x] =
+                threadIdx.x < SLOTS ? s_pos[s_pick][threadIdx.x] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out_best[c] = s_best;
+        if (out_kept) out_kept[c] = s_kept;
+    }
+}
+
+void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, double* res_e, double* out_best,
+                   int* out_kept, uint32_t* err) {
+    if (st.n_cand > 0) k_mature<<<st.n_cand, MAT_WARPS * 32, 0, s>>>(st, ags, res_e, out_best, out_kept, err);
+}
+
+}  // namespace binder

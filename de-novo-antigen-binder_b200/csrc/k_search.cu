@@ -430,6 +430,349 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
     }
 }
 
+// ---- gradient steps, flat form -------------------------------------------------------
+// The same steps and sums as k_langevin with the work laid out differently.  A warp
+// takes R residues (lane q < R owns residue q: its Calpha, list, force sum and
+// update).  Each step the warp scans the concatenation of its R residues' Verlet
+// lists 32 entries at a time, one entry per lane, whatever list an entry belongs
+// to, and compacts the entries that pass the reference's tests into a hit buffer
+// in concatenation order -- residue after residue, list order within a residue;
+// the hits are then evaluated one pair per lane, and lane q adds its residue's
+// terms in that order: the reference's pair set in the reference's order.  Long
+// and short lists thereby share the warp's lanes instead of leaving them idle.
+// The residue's atoms are not carried through the steps: each step's translation
+// (set_ca_pos, allatom.rs:289-293) is recorded and the atoms take the recorded
+// translations one after another, in step order, when the record is full and at
+// the end -- the same additions in the same order as translating them every step.
+// Lists live in the state's list storage (global memory); a residue that leaves
+// its skin gets a new list built by the whole warp.  A list that overflows, or a
+// cell index near the i32 limits, sends the residue to the one-lane 27-cell walk.
+constexpr int FLAT_HCAP = 128;   // hits a warp holds per round
+constexpr int FLAT_DSTEPS = 10;  // step translations recorded before the atoms take them
+template <int R>
+struct FlatWarp {
+    float4 body[R];             // Calpha x, y, z of the current step
+    float4 prm[R];              // residue-level charge, epsilon, sigma, hydrophobic
+    int4 cell[R];               // CG cell of the Calpha, w = cell test needed only beyond CG_NEAR_SQ
+    const float4* pq[R];        // the residue's antigen Calphas (shared memory when staged)
+    const float4* aprm[R];
+    const int4* acell[R];
+    const int* list[R];         // the residue's Verlet list in the state's list storage
+    int pref[R + 1];            // exclusive prefix of the list lengths scanned this step
+    int rid[R];                 // residue index (-1: no residue)
+    int nat[R];                 // atoms of the residue
+    int hit[FLAT_HCAP];         // residue slot << 26 | antigen Calpha position
+    float3 term[FLAT_HCAP];
+    float3 dl[FLAT_DSTEPS][R];  // recorded translations
+};
+
+// Apply the recorded translations 0..nd-1 to every atom of the warp's residues.
+template <int R>
+__device__ __forceinline__ void flat_flush(const StateView& st, FlatWarp<R>& fw, int nd, int lane) {
+    __syncwarp();
+    for (int t = lane; t < R * SLOTS; t += 32) {
+        const int q = t / SLOTS, k = t - q * SLOTS;
+        const int r = fw.rid[q];
+        if (r < 0 || k >= fw.nat[q]) continue;
+        float4* at = st.res_pos + (size_t)r * SLOT_STRIDE + k;
+        float4 v = *at;
+        for (int d = 0; d < nd; ++d) {
+            const float3 u = fw.dl[d][q];
+            v.x = xadd(v.x, u.x);
+            v.y = xadd(v.y, u.y);
+            v.z = xadd(v.z, u.z);
+        }
+        *at = v;
+    }
+    __syncwarp();
+}
+
+template <int W, int R>
+__global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, const AgView* __restrict__ ags, StepParams p,
+                                                           int n_steps, uint32_t step0, int with_noise,
+                                                           const float* __restrict__ temps, uint32_t* __restrict__ err,
+                                                           const int* __restrict__ order, int order_mode,
+                                                           int stage_cap, int stage_ag, int* __restrict__ queue) {
+    static_assert(R == 8 || R == 16 || R == 32, "residues per warp");
+    constexpr int RPC = W * R;  // residues per CTA
+    __shared__ FlatWarp<R> s_fw[W];
+    __shared__ int s_stage_ag;
+    extern __shared__ __align__(16) unsigned char cg_dyn[];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    FlatWarp<R>& fw = s_fw[threadIdx.x >> 5];
+    // antigen staging, as k_langevin does it
+    if (threadIdx.x == 0) {
+        int a0 = stage_ag, a1 = stage_ag;
+        if (a0 < 0 && !queue) {
+            const int first = blockIdx.x * RPC;
+            const int last = min(first + RPC, st.total_res) - 1;
+            a0 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, first, st.total_res)]];
+            a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, last, st.total_res)]];
+            if (order_mode == 2)
+                for (int q = first; q <= last && a1 == a0; ++q)
+                    a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, q, st.total_res)]];
+        }
+        bool fits = a0 >= 0 && a0 == a1;
+        if (fits) {
+            const GridView& gv = ags[a0].ca_grid;
+            fits = cg_stage_bytes(ags[a0].n_res, gv.nx * gv.ny * gv.nz) <= (size_t)stage_cap;
+        }
+        s_stage_ag = fits ? a0 : -1;
+    }
+    __syncthreads();
+    const int sa = s_stage_ag;
+    float4* spq = (float4*)cg_dyn;
+    float4* sprm = spq;
+    int4* scell = (int4*)cg_dyn;
+    int* sstart = (int*)cg_dyn;
+    if (sa >= 0) {
+        const AgView& S = ags[sa];
+        const int n = S.n_res, ncell = S.ca_grid.nx * S.ca_grid.ny * S.ca_grid.nz;
+        sprm = spq + n;
+        scell = (int4*)(sprm + n);
+        sstart = (int*)(scell + n);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            spq[i] = S.ca_pq[i];
+            sprm[i] = S.ca_prm[i];
+            scell[i] = S.ca_cell[i];
+        }
+        for (int i = threadIdx.x; i <= ncell; i += blockDim.x) sstart[i] = S.ca_grid.cell_start[i];
+        __syncthreads();
+    }
+    const int epoch = st.ag_epoch ? *st.ag_epoch : -2;
+
+    // Build residue q's list with the whole warp (all lanes call; q's antigen, centre
+    // and skin are taken from lane q).  Returns the length on every lane.
+    auto warp_build = [&](int q, int a, F3 centre, float skin) -> int {
+        a = __shfl_sync(0xffffffffu, a, q);
+        centre.x = __shfl_sync(0xffffffffu, centre.x, q);
+        centre.y = __shfl_sync(0xffffffffu, centre.y, q);
+        centre.z = __shfl_sync(0xffffffffu, centre.z, q);
+        skin = __shfl_sync(0xffffffffu, skin, q);
+        GridView g = ags[a].ca_grid;
+        const float4* pq = ags[a].ca_pq;
+        if (a == sa) {
+            g.cell_start = sstart;
+            pq = spq;
+        }
+        int* list = st.cg_list + (size_t)fw.rid[q] * CG_LIST_MAX;
+        return build_cg_list<32>(g, pq, centre, lane, 0xffffffffu, list, skin);
+    };
+
+    int task = blockIdx.x * W + (int)(threadIdx.x >> 5);
+    for (;;) {
+        if (queue) {
+            __syncwarp();
+            int t = 0;
+            if (lane == 0) t = atomicAdd(queue, 1);
+            task = __shfl_sync(0xffffffffu, t, 0);
+        }
+        if ((long long)task * R >= st.total_res) break;
+        // ---- this lane's residue (lanes >= R own none) ----
+        const int slot_id = task * R + lane;
+        const bool valid = lane < R && slot_id < st.total_res;
+        const int r = valid ? res_of_slot(order, order_mode, slot_id, st.total_res) : 0;
+        const int c = valid ? st.res_cand[r] : 0;
+        const int r_local = valid ? r - st.cand_res_off[c] : 0;
+        const uint32_t cid = valid ? st.cand_id[c] : 0u;
+        const int a = valid ? st.cand_ag[c] : 0;
+        const AgView* __restrict__ Ap = ags + a;
+        const float ginv = Ap->ca_grid.inv, gcell = Ap->ca_grid.cell;
+        const float ag_cx = Ap->cx, ag_cy = Ap->cy, ag_cz = Ap->cz;
+        const int aa = valid ? st.res_aa[r] : 0;
+        F3 ca = {0.f, 0.f, 0.f};
+        if (valid) {
+            const float4 v1 = st.res_pos[(size_t)r * SLOT_STRIDE + 1];
+            ca = {v1.x, v1.y, v1.z};
+            if (err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);
+        }
+        if (lane < R) {
+            fw.rid[lane] = valid ? r : -1;
+            fw.nat[lane] = valid ? s_topo_n[aa] : 0;
+            fw.prm[lane] = s_res[aa];
+            const bool staged = valid && a == sa;
+            fw.pq[lane] = staged ? spq : Ap->ca_pq;
+            fw.aprm[lane] = staged ? sprm : Ap->ca_prm;
+            fw.acell[lane] = staged ? scell : Ap->ca_cell;
+            fw.list[lane] = st.cg_list + (size_t)(valid ? r : 0) * CG_LIST_MAX;
+        }
+        // the list of the previous launch when it was built for this antigen set and
+        // antigen and still covers the Calpha, else a new one
+        F3 centre = ca;
+        int nl = 0;
+        bool dirty = false;
+        float skin = CG_SKIN;
+        bool need = false;
+        if (valid) {
+            const int4 meta = st.cg_meta[r];
+            bool reuse = false;
+            if (epoch >= 0 && meta.z == epoch && meta.y == a && meta.x >= 0 && meta.x <= CG_LIST_MAX) {
+                const float4 cc = st.cg_centre[r];
+                skin = fminf(fmaxf(cc.w, CG_SKIN), CG_SKIN_MAX);
+                const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
+                reuse = mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f);
+                if (reuse) {
+                    centre = {cc.x, cc.y, cc.z};
+                    nl = meta.x;
+                } else {
+                    skin = fminf(2.0f * skin, CG_SKIN_MAX);  // it outran the list
+                }
+            }
+            need = !reuse;
+        }
+        __syncwarp();
+        for (unsigned m = __ballot_sync(0xffffffffu, need); m; m &= m - 1) {
+            const int q = __ffs(m) - 1;
+            const int n = warp_build(q, a, centre, skin);
+            if (lane == q) {
+                nl = n;
+                dirty = true;
+            }
+        }
+        int nd = 0;  // recorded translations
+        for (int s = 0; s < n_steps; ++s) {
+            const int cx = cell_coord(ca.x, ginv), cy = cell_coord(ca.y, ginv), cz = cell_coord(ca.z, ginv);
+            const bool use_list = valid && nl <= CG_LIST_MAX && !cell_far(cx, cy, cz);
+            // cells at least as wide as the cutoff and coordinates below 1e4 A: pairs with
+            // r^2 <= CG_NEAR_SQ are in adjacent cells (see k_langevin)
+            const bool near_adjacent = gcell >= 10.0f && fabsf(ca.x) < 1e4f && fabsf(ca.y) < 1e4f && fabsf(ca.z) < 1e4f;
+            const int nle = use_list ? nl : 0;
+            int incl = nle;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int my_lo = incl - nle;  // this residue's entries: [my_lo, incl)
+            if (lane < R) {
+                fw.body[lane] = make_float4(ca.x, ca.y, ca.z, 0.f);
+                fw.cell[lane] = make_int4(cx, cy, cz, near_adjacent ? 1 : 0);
+                fw.pref[lane + 1] = incl;
+                if (lane == 0) fw.pref[0] = 0;
+            }
+            __syncwarp();
+            float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+            int f0 = 0, rq = 0;
+            while (f0 < total) {  // rounds: scan until the hit buffer could overflow
+                int nh = 0, my_cnt = 0, my_first = -1;
+                while (f0 < total && nh + 32 <= FLAT_HCAP) {
+                    const int f = f0 + lane;
+                    bool hit = false;
+                    int code = 0;
+                    if (f < total) {
+                        while (fw.pref[rq + 1] <= f) ++rq;
+                        const int i = fw.list[rq][f - fw.pref[rq]];
+                        const float4 b = fw.body[rq];
+                        const float4 ap = fw.pq[rq][i];
+                        const float r_sq = xdist2(xsub(b.x, ap.x), xsub(b.y, ap.y), xsub(b.z, ap.z));
+                        hit = !(r_sq > CUTOFF_SQ || r_sq < MIN_R_SQ);
+                        const int4 cc = fw.cell[rq];
+                        if (hit && !(cc.w && r_sq <= CG_NEAR_SQ)) {  // the reference's cell test
+                            const int4 ce = fw.acell[rq][i];
+                            hit = abs((long long)ce.x - cc.x) <= 1 && abs((long long)ce.y - cc.y) <= 1 &&
+                                  abs((long long)ce.z - cc.z) <= 1;
+                        }
+                        code = (rq << 26) | i;
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) fw.hit[nh + __popc(m & lt)] = code;
+                    // this lane's residue: its hits of the chunk are the ballot bits of its entries
+                    const int lo = max(my_lo - f0, 0), hi = min(incl - f0, 32);
+                    if (lane < R && hi > lo) {
+                        const unsigned mask = (hi == 32 ? 0xffffffffu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+                        const unsigned mine = m & mask;
+                        if (mine && my_first < 0) my_first = nh + __popc(m & ((1u << lo) - 1u));
+                        my_cnt += __popc(mine);
+                    }
+                    nh += __popc(m);
+                    f0 += 32;
+                }
+                __syncwarp();
+                for (int h = lane; h < nh; h += 32) {  // the round's pair terms, one pair per lane
+                    const int code = fw.hit[h];
+                    const int q = code >> 26, i = code & ((1 << 26) - 1);
+                    const float4 b = fw.body[q], bp = fw.prm[q];
+                    const CgB body{b.x, b.y, b.z, bp.x, bp.y, bp.z, bp.w};
+                    float tx, ty, tz;
+                    cg_term_parts(body, fw.pq[q][i], fw.aprm[q][i], tx, ty, tz);
+                    fw.term[h] = make_float3(tx, ty, tz);
+                }
+                __syncwarp();
+                for (int k = 0; k < my_cnt; ++k) {  // this residue's terms, in order
+                    const float3 t = fw.term[my_first + k];
+                    sx = xadd(sx, t.x);
+                    sy = xadd(sy, t.y);
+                    sz = xadd(sz, t.z);
+                }
+                __syncwarp();  // hit and term slots are rewritten next round
+            }
+            if (valid && !use_list) {  // list overflow or cells near the i32 limits
+                int np = 0;
+                float3 f;
+                cg_force_walk<false>(Ap, ca.x, ca.y, ca.z, aa, &f, &np);
+                sx = f.x; sy = f.y; sz = f.z;
+            }
+            bool rebuild = false;
+            if (valid) {
+                float fx = sx, fy = sy, fz = sz;
+                // harmonic restraint toward the shell (diffusion.rs:317-327)
+                const float dx_c = xsub(ca.x, ag_cx), dy_c = xsub(ca.y, ag_cy), dz_c = xsub(ca.z, ag_cz);
+                const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
+                const float excess = xsub(d, p.shell_radius);
+                const float f_r = xdiv(xmul(-p.restraint_k, excess), d);
+                fx = xadd(fx, xmul(f_r, dx_c));
+                fy = xadd(fy, xmul(f_r, dy_c));
+                fz = xadd(fz, xmul(f_r, dz_c));
+                float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+                if (with_noise) {
+                    const float temp = temps ? temps[s] : p.t_hot;
+                    const float sigma = xmul(p.noise_base, xsqrt(temp));
+                    const U4 u = rng_draw(p.seed, cid, step0 + (uint32_t)s, STREAM_NOISE, (uint32_t)r_local);
+                    nx = frange(u.x, -sigma, sigma);
+                    ny = frange(u.y, -sigma, sigma);
+                    nz = frange(u.z, -sigma, sigma);
+                }
+                const float md = p.max_disp;
+                const F3 new_ca = {xadd(xadd(ca.x, fminf(fmaxf(xmul(p.step, fx), -md), md)), nx),
+                                   xadd(xadd(ca.y, fminf(fmaxf(xmul(p.step, fy), -md), md)), ny),
+                                   xadd(xadd(ca.z, fminf(fmaxf(xmul(p.step, fz), -md), md)), nz)};
+                // set_ca_pos: delta = new - old; every atom (the Calpha included) += delta
+                const F3 dl = sub3(new_ca, ca);
+                fw.dl[nd][lane] = make_float3(dl.x, dl.y, dl.z);
+                ca = {xadd(ca.x, dl.x), xadd(ca.y, dl.y), xadd(ca.z, dl.z)};
+                if (s + 1 < n_steps) {
+                    const float mx = ca.x - centre.x, my = ca.y - centre.y, mz = ca.z - centre.z;
+                    if (!(mx * mx + my * my + mz * mz <= (skin - 0.01f) * (skin - 0.01f))) {
+                        // left the skin (or NaN): a new list with twice the skin
+                        skin = fminf(2.0f * skin, CG_SKIN_MAX);
+                        centre = ca;
+                        rebuild = true;
+                    }
+                }
+            }
+            if (++nd == FLAT_DSTEPS || s + 1 == n_steps) {
+                flat_flush<R>(st, fw, nd, lane);
+                nd = 0;
+            }
+            for (unsigned m = __ballot_sync(0xffffffffu, rebuild); m; m &= m - 1) {
+                const int q = __ffs(m) - 1;
+                const int n = warp_build(q, a, centre, skin);
+                if (lane == q) {
+                    nl = n;
+                    dirty = true;
+                }
+            }
+        }
+        if (valid && dirty) {  // keep the list for the next launch
+            st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
+            st.cg_meta[r] = make_int4(nl, a, epoch, 0);
+        }
+        if (!queue) break;
+    }
+}
+
 // ---- launchers ----------------------------------------------------------------------
 void launch_build_residues(cudaStream_t s, int n, const float* ca_xyz, const uint8_t* aa, const float4* chi_trig,
                            const float* chi_deg, float4* out_pos, float4* out_chi) {
@@ -503,15 +846,51 @@ static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, co
                                                  order_mode, stage_bytes, stage_ag, queue);
 }
 
+template <int W, int R>
+static void diffuse_flat(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
+                         uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
+                         int order_mode, int stage_bytes, int stage_ag, int* queue) {
+    const int threads = W * 32;
+    const long long tasks = ((long long)st.total_res + R - 1) / R;
+    long long ctas = (tasks + W - 1) / W;
+    auto kern = k_langevin_flat<W, R>;
+    if (stage_bytes > 0) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
+    if (queue) {  // persistent: the CTAs that are resident at once
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, stage_bytes);
+        ctas = std::min(ctas, (long long)std::max(1, sms * std::max(per_sm, 1)));
+        cudaMemsetAsync(queue, 0, sizeof(int), s);
+    }
+    kern<<<(int)ctas, threads, stage_bytes, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode,
+                                                 stage_bytes, stage_ag, queue);
+}
+
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
                     int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
-                    int stage_ag, int* queue) {
+                    int stage_ag, int* queue, int flat_res) {
     if (st.total_res <= 0 || n_steps <= 0) return;
     if (order_mode == 2 && st.total_res % CG_STRIDE == 0) order_mode = 1;  // stride not a bijection
     // antigen staging: up to 96 KB of dynamic shared memory per CTA
     const size_t sb = cg_stage_bytes(max_ag_res, max_ag_cells);
     const int stage = sb <= 96 * 1024 ? (int)sb : 0;
+    if (flat_res && st.cg_list && st.cg_meta && st.cg_centre) {
+#define BINDER_FLAT(W, R)                                                                                    \
+    diffuse_flat<W, R>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage,          \
+                       stage ? stage_ag : -1, queue)
+        if (flat_res == 32) BINDER_FLAT(4, 32);
+        else if (flat_res == 16) {
+            if (warps_per_cta <= 4) BINDER_FLAT(4, 16);
+            else BINDER_FLAT(8, 16);
+        } else {
+            if (warps_per_cta <= 4) BINDER_FLAT(4, 8);
+            else BINDER_FLAT(8, 8);
+        }
+#undef BINDER_FLAT
+        return;
+    }
 #define BINDER_DIFFUSE(W, G)                                                                                 \
     diffuse_w<W, G>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage,               \
                     stage ? stage_ag : -1, queue)

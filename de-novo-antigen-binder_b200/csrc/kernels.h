@@ -18,6 +18,8 @@ struct LaunchCfg {
     int cg_order = 1;            // residue order of the gradient-step kernel: 0 cell, 1 candidate, 2 strided
     int score_order = 0;         // work-queue order of the scoring kernel: 0 cell, 1 residue index
     int cg_queue = 1;            // gradient-step kernel: 0 static grid, 1 persistent CTAs on a work queue
+    int cg_flat = 0;             // gradient-step kernel: 0 lane groups (cg_lanes per residue), 8 / 16 / 32 the
+                                 // flat form with that many residues per warp
 };
 
 // ---- k_grid.cu: SpatialHashGrid ----
@@ -76,7 +78,7 @@ void launch_cg_forces(cudaStream_t s, const AgView* ag, const float* bx, const f
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                     uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
                     int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
-                    int stage_ag, int* queue);
+                    int stage_ag, int* queue, int flat_res);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);
@@ -135,6 +137,19 @@ void launch_pack_weights(cudaStream_t s, const float* p, const MlpBf16& o);
 void launch_gather_tuples(cudaStream_t s, int m, const int* idx, const MlpTuple* tup, float* ca, uint8_t* aa, int* ag,
                           int* action, int* ref, float* target);
 void launch_draw_batch(cudaStream_t s, int m, int n_tuples, uint64_t seed, uint32_t step, int* idx);
+
+// ---- k_post.cu: minimize and affinity maturation of the resident candidates ----
+cudaError_t post_init_tables();
+// every residue: the clamped grid-force step from pos_in, side chain rebuilt, into pos_out
+void launch_min_move(cudaStream_t s, const StateView& st, const AgView* ags, const float4* pos_in, float4* pos_out,
+                     float step_size);
+// per candidate: keep the trial positions when e_trial < best (best updated, kept[c]++)
+void launch_min_accept(cudaStream_t s, const StateView& st, const float4* trial, const double* e_trial, double* best,
+                       int* kept);
+// affinity_maturation_allatom of every candidate over its interface residues; res_e
+// (per-residue full energies of the state) kept current
+void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, double* res_e, double* out_best,
+                   int* out_kept, uint32_t* err);
 
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
 double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);

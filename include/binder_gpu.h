@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define BINDER_ABI_VERSION 1
+#define BINDER_ABI_VERSION 2
 #define BINDER_MAX_SLOTS 14
 
 enum binder_status {
@@ -310,6 +310,10 @@ typedef struct binder_launch_cfg {
                                    sorting launches after every move), 1 residue index */
     int32_t cg_queue;           /* gradient-step kernel: 0 one CTA per residue batch, 1 persistent
                                    CTAs whose warps take residue batches from a work queue */
+    int32_t cg_flat;            /* gradient-step kernel: 0 the lane-group form (cg_lanes lanes per
+                                   residue); 8, 16 or 32 the flat form with that many residues per
+                                   warp (the warp scans their concatenated lists together; 32 with
+                                   4 warps per CTA, 8 and 16 with 4 or 8) */
 } binder_launch_cfg;
 int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
@@ -340,6 +344,25 @@ typedef struct binder_run_cfg {
 } binder_run_cfg;
 void binder_default_run_cfg(binder_run_cfg* cfg);
 int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg, int32_t* out_cand, double* out_energy);
+
+/* ---- post-search refinement of the results (main.rs:336-346) ------------------------
+   minimize (diffusion.rs:854-916) of every resident candidate against its antigen
+   (the one partner, main.rs:338): `steps` steps of steepest descent on the
+   Calpha-level grid force (compute_forces_with_grid, energy.rs:322-398) with the
+   step size 0.04 * (1 - step / steps), each component clamped to 0.5 A, every
+   residue translated and its side chain rebuilt at its chi (allatom.rs:244-293),
+   a step kept only when allatom_energy (diffusion.rs:281-283) drops.  In place;
+   out_energy double[n_cand] (may be NULL) = each candidate's final energy. */
+int binder_minimize(binder_ctx* ctx, int steps, double* out_energy);
+/* affinity_maturation_allatom (diffusion.rs:924-961) of every resident candidate
+   over its interface residues (Calpha within 8 A of an antigen Calpha,
+   filters.rs:96-105, main.rs:342-344): at each such position, in order, the other
+   amino acids in AminoAcid order are tried at their top rotamer and the first that
+   lowers allatom_energy is kept; otherwise the residue is rebuilt with its old
+   amino acid and chi (mutate_residue, allatom.rs:299-384).  In place (at most 128
+   residues per candidate); out_energy (may be NULL) = the final score as the
+   reference returns it, out_mutated int32[n_cand] (may be NULL) = mutations kept. */
+int binder_affinity_maturation(binder_ctx* ctx, double* out_energy, int32_t* out_mutated);
 
 /* ---- learned mutation / rotamer proposal (no reference counterpart) ------------------
    A BF16 MLP, 180 -> 256 (SiLU) -> 256 (SiLU) -> 25, FP32 accumulation, trained on

@@ -1033,6 +1033,128 @@ void orc_score_slots64(const orc_antigen* A, int n_cand, int n_res, const uint8_
     });
 }
 
+// partners_energy (diffusion.rs:835-840) with the antigen as the one partner =
+// allatom_energy (diffusion.rs:281-283): interaction_energy_atoms (the five terms of
+// energy.rs:261-314 + solvation.rs:52-84, added as AtomEnergyBreakdown::total does)
+// plus disulfide_energy.  acc64: the same terms re-evaluated in f64.
+static double partner_energy(const orc_antigen* A, const Prot& P, int acc64) {
+    int m = 0;
+    for (int r = 0; r < P.n; ++r) m += T_TOPO_N[P.aa[r]];
+    std::vector<float> x(m), y(m), z(m), q(m), rmh(m), eps(m);
+    std::vector<uint8_t> hyd(m), type(m);
+    orc_flatten(P.n, P.aa, P.pos, x.data(), y.data(), z.data(), q.data(), rmh.data(), eps.data(), hyd.data(),
+                type.data(), nullptr);
+    orc_cloud ag{A->x.data(), A->y.data(), A->z.data(), A->q.data(), A->rmh.data(), A->eps.data(), A->hyd.data(),
+                 A->type.data(), (int64_t)A->x.size()};
+    orc_cloud ab{x.data(), y.data(), z.data(), q.data(), rmh.data(), eps.data(), hyd.data(), type.data(), m};
+    if (acc64) {
+        double e[5];
+        orc_energy_atoms64(&ag, &ab, e, nullptr);
+        return (((e[0] + e[1]) + e[2]) + e[3]) + e[4] + (double)disulfide(P);
+    }
+    float e[5];
+    orc_energy_atoms32(&ag, &ab, e);
+    return (double)((((e[0] + e[1]) + e[2]) + e[3]) + e[4] + disulfide(P));
+}
+
+// minimize (diffusion.rs:854-916) with the antigen as the one partner
+// (main.rs:338): steepest descent on the Calpha-level grid force with the step
+// decaying linearly (MIN_STEP 0.04, MIN_MAX_DISP 0.5, diffusion.rs:63-64), side
+// chains rebuilt after every move, a step kept only when the all-atom energy
+// drops.  out_energy = the final best energy.
+void orc_minimize(const orc_antigen* A, int n_cand, int n_res, uint8_t* aa, float* chi, float* pos, int steps,
+                  int acc64, double* out_energy, double* out_margin, int n_threads) {
+    const float MIN_STEP = 0.04f, MIN_MAX_DISP = 0.5f;
+    parallel_for(n_cand, n_threads, [&](int64_t c) {
+        Prot P{n_res, aa + (size_t)c * n_res, chi + (size_t)c * n_res * 4, pos + (size_t)c * n_res * SLOTS * 3};
+        double best = partner_energy(A, P, acc64);
+        double margin = INFINITY;  // smallest |e - best| / max(|best|, 1) of any keep / restore decision
+        if (n_res > 0 && steps > 0) {
+            std::vector<float> fx(n_res), fy(n_res), fz(n_res);
+            std::vector<float> keep_pos((size_t)n_res * SLOTS * 3);
+            for (int step = 0; step < steps; ++step) {
+                const float frac = 1.0f - (float)step / (float)steps;
+                const float step_size = MIN_STEP * frac;
+                std::copy(P.pos, P.pos + keep_pos.size(), keep_pos.begin());
+                for (int r = 0; r < n_res; ++r) {  // compute_forces_with_grid on the pre-step Calphas
+                    V3 ca = P.at(r, T_TOPO_CA[P.aa[r]]);
+                    CgAtom b = cg_atom(ca[0], ca[1], ca[2], P.aa[r]);
+                    float sx = 0.f, sy = 0.f, sz = 0.f;
+                    A->grid.query(b.x, b.y, b.z, [&](uint32_t i) { cg_pair(b, A->cg[i], sx, sy, sz); });
+                    // fx_buf (zeroed) += the one partner's force
+                    fx[r] = 0.0f + sx; fy[r] = 0.0f + sy; fz[r] = 0.0f + sz;
+                }
+                auto clampf = [&](float v) { return v < -MIN_MAX_DISP ? -MIN_MAX_DISP : (v > MIN_MAX_DISP ? MIN_MAX_DISP : v); };
+                for (int r = 0; r < n_res; ++r) {
+                    V3 ca = P.at(r, T_TOPO_CA[P.aa[r]]);
+                    V3 disp = {clampf(step_size * fx[r]), clampf(step_size * fy[r]), clampf(step_size * fz[r])};
+                    set_ca_pos(P, r, V3{ca[0] + disp[0], ca[1] + disp[1], ca[2] + disp[2]});
+                    rebuild_side_chain(P, r);
+                }
+                const double e = partner_energy(A, P, acc64);
+                margin = std::min(margin, std::fabs(e - best) / std::max(std::fabs(best), 1.0));
+                if (e < best) best = e;
+                else std::copy(keep_pos.begin(), keep_pos.end(), P.pos);
+            }
+        }
+        out_energy[c] = best;
+        if (out_margin) out_margin[c] = margin;
+    });
+}
+
+// is_interface (filters.rs:96-105): some antigen Calpha closer than IFACE_SQ (64)
+static bool is_interface(const orc_antigen* A, const Prot& P, int r) {
+    V3 p = P.at(r, T_TOPO_CA[P.aa[r]]);
+    for (int i = 0; i < A->n_res; ++i) {
+        float dx = p[0] - A->cx[i], dy = p[1] - A->cy[i], dz = p[2] - A->cz[i];
+        if (dx * dx + dy * dy + dz * dz < 64.0f) return true;
+    }
+    return false;
+}
+
+// affinity_maturation_allatom (diffusion.rs:924-961) over the interface residues
+// (main.rs:342-345): for each mutable position in order, the amino acids in
+// ALL_AA order (atom.rs:29) other than the current one, each built at its top
+// rotamer (chi 0 without rotamers); the first strictly lower allatom_energy is
+// kept, otherwise the residue is mutated back to its old amino acid and chi.
+// out_energy = the final best score, out_mutated[c] = mutations kept.
+void orc_affinity_maturation(const orc_antigen* A, int n_cand, int n_res, uint8_t* aa, float* chi, float* pos,
+                             int acc64, double* out_energy, int32_t* out_mutated, double* out_margin,
+                             int n_threads) {
+    parallel_for(n_cand, n_threads, [&](int64_t c) {
+        Prot P{n_res, aa + (size_t)c * n_res, chi + (size_t)c * n_res * 4, pos + (size_t)c * n_res * SLOTS * 3};
+        std::vector<int> mutable_pos;
+        for (int r = 0; r < n_res; ++r)
+            if (is_interface(A, P, r)) mutable_pos.push_back(r);
+        double best = partner_energy(A, P, acc64);
+        double margin = INFINITY;
+        int kept = 0;
+        for (int r : mutable_pos) {
+            const int old_aa = P.aa[r];
+            float old_chi[4];
+            for (int k = 0; k < 4; ++k) old_chi[k] = P.chi[r * 4 + k];
+            for (int cand_aa = 0; cand_aa < 20; ++cand_aa) {
+                if (cand_aa == old_aa) continue;
+                float new_chi[4] = {0.f, 0.f, 0.f, 0.f};
+                if (T_ROT_N[cand_aa] > 0)
+                    for (int k = 0; k < 4; ++k) new_chi[k] = T_ROT[cand_aa][0][k];
+                mutate_residue(P, r, cand_aa, new_chi);
+                const double e = partner_energy(A, P, acc64);
+                margin = std::min(margin, std::fabs(e - best) / std::max(std::fabs(best), 1.0));
+                if (e < best) {
+                    best = e;
+                    ++kept;
+                    break;
+                }
+                mutate_residue(P, r, old_aa, old_chi);
+            }
+        }
+        out_energy[c] = best;
+        if (out_mutated) out_mutated[c] = kept;
+        if (out_margin) out_margin[c] = margin;
+    });
+}
+
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx) {
     std::vector<int32_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0);

@@ -156,6 +156,21 @@ void orc_step(const orc_antigen*, const orc_params*, int n_cand, int n_res,
 void orc_score_slots64(const orc_antigen*, int n_cand, int n_res, const uint8_t* aa, const float* pos,
                        int full, double* out, double* out_abs, int n_threads);
 
+/* minimize (diffusion.rs:854-916) of every candidate against the antigen: steps of
+   Calpha-grid steepest descent with side-chain rebuilds, each kept only when
+   allatom_energy drops (acc64 = 0: the reference's f32 energy; 1: its f64
+   re-evaluation).  In place; out_energy = final energies; out_margin (may be
+   NULL) = the smallest |e - best| / max(|best|, 1) met by a keep / restore decision. */
+void orc_minimize(const orc_antigen*, int n_cand, int n_res, uint8_t* aa, float* chi, float* pos, int steps,
+                  int acc64, double* out_energy, double* out_margin, int n_threads);
+/* affinity_maturation_allatom (diffusion.rs:924-961) over each candidate's
+   interface residues (filters.rs:96-105).  In place; out_energy = final scores,
+   out_mutated (may be NULL) = mutations kept per candidate, out_margin (may be NULL)
+   as for orc_minimize. */
+void orc_affinity_maturation(const orc_antigen*, int n_cand, int n_res, uint8_t* aa, float* chi, float* pos,
+                             int acc64, double* out_energy, int32_t* out_mutated, double* out_margin,
+                             int n_threads);
+
 /* stable ascending sort of energies, NaN last; first k indices (diffusion.rs:1045-1047) */
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx);
 

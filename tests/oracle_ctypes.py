@@ -322,6 +322,27 @@ class Antigen:
         lib().orc_step(self.h, C.byref(params), n_cand, n_res, P(aa), P(chi), P(pos), P(cid), step_id, temp,
                        int(with_noise), int(with_mc), P(stats), threads)
 
+    def minimize(self, aa, chi, pos, n_res, steps, acc64=True, threads=8, with_margin=False):
+        """minimize (diffusion.rs:854-916) against this antigen, in place; final
+        energies (and the smallest relative keep / restore margin per candidate)"""
+        n_cand = len(aa) // n_res
+        out = np.zeros(n_cand, np.float64)
+        margin = np.zeros(n_cand, np.float64)
+        lib().orc_minimize(C.c_void_p(self.h), n_cand, n_res, P(aa), P(chi), P(pos), steps, int(acc64), P(out),
+                           P(margin), threads)
+        return (out, margin) if with_margin else out
+
+    def affinity_maturation(self, aa, chi, pos, n_res, acc64=True, threads=8, with_margin=False):
+        """affinity_maturation_allatom over the interface residues, in place; (final
+        scores, mutations kept[, smallest relative decision margin]) per candidate"""
+        n_cand = len(aa) // n_res
+        out = np.zeros(n_cand, np.float64)
+        kept = np.zeros(n_cand, np.int32)
+        margin = np.zeros(n_cand, np.float64)
+        lib().orc_affinity_maturation(C.c_void_p(self.h), n_cand, n_res, P(aa), P(chi), P(pos), int(acc64), P(out),
+                                      P(kept), P(margin), threads)
+        return (out, kept, margin) if with_margin else (out, kept)
+
     def score_slots64(self, aa, pos, n_res, full=False, threads=8, with_abs=False):
         """f64 energy per candidate; with_abs also the sum of |pair term| (the
         denominator of the norm-wise error of ill-conditioned candidates)"""

@@ -45,7 +45,7 @@ def test_header_compiles_as_c(tmp_path):
 
 def test_status_strings_and_abi_version(pkg):
     L = pkg.lib()
-    assert L.binder_abi_version() == 1
+    assert L.binder_abi_version() == 2
     assert L.binder_status_string(0) == b"ok"
     assert b"sm_100" in L.binder_status_string(8)
 

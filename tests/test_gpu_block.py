@@ -51,7 +51,8 @@ def test_graph_block_matches_eager(ctx, oracle, pkg):
 
 @pytest.mark.parametrize("shape", [(4, 1, 2, 4, 0, 1, 0), (16, 8, 4, 8, 1, 0, 1), (8, 2, 4, 4, 2, 1, 1),
                                    (8, 4, 2, 8, 0, 0, 0), (8, 4, 8, 8, 2, 1, 0), (8, 4, 8, 8, 1, 1, 1),
-                                   (8, 4, 2, 4, 0, 0, 1)])
+                                   (8, 4, 2, 4, 0, 0, 1), (8, 4, 4, 8, 1, 0, 1, 32), (8, 4, 8, 8, 0, 1, 1, 16),
+                                   (8, 4, 8, 8, 2, 0, 0, 8), (8, 4, 4, 8, 1, 1, 0, 16)])
 def test_launch_shapes_bit_identical(ctx, oracle, pkg, shape):
     aa, chi, pos, n_res = _setup(ctx, oracle, pkg)
     ctx.set_launch_cfg(8, 4, 8, 8, 0, 0, 0)
@@ -69,6 +70,7 @@ def test_autotune_restores_state_and_caches(ctx, oracle, pkg, tmp_path, monkeypa
     cfg = ctx.autotune(reps=2)
     assert cfg.score_warps in (4, 8, 16) and cfg.cg_warps in (2, 4, 8) and 1 <= cfg.score_ctas_per_sm <= 8
     assert cfg.cg_lanes in (4, 8) and cfg.cg_order in (0, 1, 2) and cfg.score_order in (0, 1) and cfg.cg_queue in (0, 1)
+    assert cfg.cg_flat in (0, 8, 16, 32)
     _, _, p_after = ctx.state_download()
     assert np.array_equal(p_after, pos)  # the timing runs worked on a copy
     got = [ctx.block(10, 10 * b, k=64) for b in range(3)], ctx.state_download()

@@ -236,12 +236,19 @@ def _setup_search(ctx, oracle, pkg, cfg, n_cand):
 
 
 @pytest.mark.parametrize("with_noise", [False, True])
-def test_langevin_steps_bit_exact(ctx, oracle, pkg, with_noise):
+@pytest.mark.parametrize("flat,warps,n_steps", [(0, 8, 10), (8, 8, 10), (16, 4, 25), (32, 4, 10)])
+def test_langevin_steps_bit_exact(ctx, oracle, pkg, with_noise, flat, warps, n_steps):
+    """Gradient steps in the lane-group form (flat 0) and the flat form with 8, 16,
+    32 residues per warp (25 steps: the recorded translations are applied twice
+    mid-launch and once at the end)."""
     cfg = pkg.workloads.config1(n_cand=64)
     A, aa, chi, pos, n_res = _setup_search(ctx, oracle, pkg, cfg, 64)
-    n_steps = 10
     temps = np.array([oracle.temperature(i, 600) for i in range(n_steps)], np.float32)
-    ctx.diffuse(n_steps, step0=0, with_noise=with_noise, temps=temps)
+    ctx.set_launch_cfg(cg_warps=warps, cg_flat=flat)
+    try:
+        ctx.diffuse(n_steps, step0=0, with_noise=with_noise, temps=temps)
+    finally:
+        ctx.set_launch_cfg()
     g_aa, g_chi, g_pos = ctx.state_download()
     prm = oracle.OrcParams.defaults(shell_radius=cfg["shell"][0], seed=1234)
     for s in range(n_steps):
@@ -275,7 +282,8 @@ def test_langevin_steps_bit_exact_mixed_antigens(ctx, oracle, pkg, with_noise):
             o0, o1 = off[c], off[c + 1]
             As[pop.antigen_id[c]].step(prm, aa[o0:o1], chi[o0:o1], pos[o0:o1], int(pop.n_res[c]), [c], s,
                                        temps[s], with_noise, False)
-    for shape in ((8, 4, 8, 8, 1, 1, 1), (8, 4, 8, 8, 0, 0, 0)):
+    for shape in ((8, 4, 8, 8, 1, 1, 1), (8, 4, 8, 8, 0, 0, 0), (8, 4, 8, 8, 1, 1, 1, 16), (8, 4, 4, 8, 0, 0, 0, 32),
+                  (8, 4, 8, 8, 2, 1, 0, 8)):
         ctx.set_launch_cfg(*shape)
         ctx.state_upload(pop.aa, chi0, pos0, n_res=pop.n_res, antigen_id=pop.antigen_id)
         ctx.diffuse(n_steps, step0=0, with_noise=with_noise, temps=temps)

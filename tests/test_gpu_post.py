@@ -1,0 +1,113 @@
+"""Post-search refinement on the GPU vs the CPU oracle, through the C ABI:
+minimize (diffusion.rs:854-916) and affinity_maturation_allatom
+(diffusion.rs:924-961) of every resident candidate.
+
+Inputs: config-1 candidates after the 200 gradient steps of phase 1 (many in
+clashing contact, so minimize keeps and restores steps and maturation finds
+improving mutations), a Cys-rich population (disulfide terms in every total), and
+the reference's own unit-test geometry.  Geometry (moves, side-chain rebuilds,
+mutations) is bit-exact; energies within 1e-5 relative of the oracle's f64
+re-evaluation, whose keep / restore decisions the GPU's FP64 totals reproduce.  A
+candidate whose oracle run met a decision closer than 1e-5 (relative) to a tie
+may legitimately branch; it is excluded from the bit-exact comparison and counted."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+THREADS = os.cpu_count() or 8
+TIE = 1e-5
+
+
+def _phase1_state(ctx, oracle, pkg, n_cand, cys_frac=0.0):
+    cfg = pkg.workloads.config1(n_cand=n_cand)
+    ag_aa, ag_ca = cfg["antigens"][0]
+    ag_pos, _ = oracle.build_residues(ag_ca, ag_aa)
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=cfg["shell"][0], seed=1234))
+    ctx.add_antigen(ag_aa, ag_pos)
+    pop = cfg["pop"]
+    aa = pop.aa[: n_cand * 20].copy()
+    if cys_frac:
+        rng = np.random.default_rng(77)
+        aa[rng.random(len(aa)) < cys_frac] = 4  # Cys
+    pos, chi = oracle.build_residues(pop.ca[: n_cand * 20], aa)
+    A = oracle.Antigen(ag_aa, ag_pos)
+    prm = oracle.OrcParams.defaults(shell_radius=cfg["shell"][0], seed=1234)
+    for s in range(200):
+        A.step(prm, aa, chi, pos, 20, np.arange(n_cand), s, 3.0, False, False, threads=THREADS)
+    return A, aa, chi, pos
+
+
+def _compare(g, o, margin, e_gpu, e_orc):
+    (g_aa, g_chi, g_pos), (aa, chi, pos) = g, o
+    n = len(margin)
+    clean = margin > TIE
+    same = np.array([np.array_equal(g_pos[c * 20:(c + 1) * 20], pos[c * 20:(c + 1) * 20]) and
+                     np.array_equal(g_aa[c * 20:(c + 1) * 20], aa[c * 20:(c + 1) * 20]) and
+                     np.array_equal(g_chi[c * 20:(c + 1) * 20], chi[c * 20:(c + 1) * 20]) for c in range(n)])
+    assert np.all(same[clean]), np.nonzero(~same & clean)[0]
+    assert clean.sum() >= 0.9 * n
+    assert np.all(rel_err(e_gpu[clean], e_orc[clean]) < 1e-5)
+
+
+@pytest.mark.parametrize("cys_frac", [0.0, 0.3])
+def test_minimize_matches_oracle(ctx, oracle, pkg, cys_frac):
+    A, aa, chi, pos = _phase1_state(ctx, oracle, pkg, 128, cys_frac)
+    pos0 = pos.copy()
+    ctx.state_upload(aa, chi, pos, uniform_n_res=20)
+    e_gpu = ctx.minimize(60)
+    g = ctx.state_download()
+    e_orc, margin = A.minimize(aa, chi, pos, 20, 60, acc64=True, threads=THREADS, with_margin=True)
+    _compare(g, (aa, chi, pos), margin, e_gpu, e_orc)
+    # the returned energies are the final structures' (allatom_energy)
+    assert np.all(rel_err(ctx.score_state(full=True), e_gpu) < 1e-5)
+    moved = [not np.array_equal(pos[c * 20:(c + 1) * 20], pos0[c * 20:(c + 1) * 20]) for c in range(128)]
+    assert 0 < sum(moved) < 128  # some candidates kept steps, some none
+
+
+@pytest.mark.parametrize("cys_frac", [0.0, 0.3])
+def test_affinity_maturation_matches_oracle(ctx, oracle, pkg, cys_frac):
+    A, aa, chi, pos = _phase1_state(ctx, oracle, pkg, 128, cys_frac)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=20)
+    e_gpu, kept_gpu = ctx.affinity_maturation()
+    g = ctx.state_download()
+    e_orc, kept, margin = A.affinity_maturation(aa, chi, pos, 20, acc64=True, threads=THREADS, with_margin=True)
+    _compare(g, (aa, chi, pos), margin, e_gpu, e_orc)
+    clean = margin > TIE
+    assert np.array_equal(kept_gpu[clean], kept[clean])
+    assert kept.sum() > 0  # the scan keeps mutations on this input
+
+
+def test_minimize_and_maturation_reference_geometry(ctx, oracle, pkg):
+    """The reference's unit-test geometry (diffusion.rs:1123-1172): 6-residue
+    straight chains, the antibody on top of its partner (minimize) or 8 A away
+    (maturation); minimize with 0 steps changes nothing."""
+    def chain(start, n):
+        ca = np.float32([[start[0] + i * np.float32(3.8), start[1], start[2]] for i in range(n)])
+        seq = np.zeros(n, np.uint8)
+        p, c = oracle.build_residues(ca, seq)
+        return seq, c, p
+    g_aa, _, g_pos = chain([0.0, 0.0, 0.0], 6)
+    A = oracle.Antigen(g_aa, g_pos)
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(seed=1))
+    ctx.add_antigen(g_aa, g_pos)
+    for start, steps in (([0.2, 0.2, 0.2], 50), ([20.0, 20.0, 20.0], 0)):
+        aa, chi, pos = chain(start, 6)
+        ctx.state_upload(aa, chi, pos, uniform_n_res=6)
+        e = ctx.minimize(steps)
+        ga, gc, gp = ctx.state_download()
+        eo = A.minimize(aa, chi, pos, 6, steps, acc64=True)
+        assert np.array_equal(gp, pos) and rel_err(e, eo)[0] < 1e-5
+    aa, chi, pos = chain([8.0, 0.0, 0.0], 6)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=6)
+    before = ctx.score_state(full=True)[0]
+    e, kept = ctx.affinity_maturation()
+    eo, ko = A.affinity_maturation(aa, chi, pos, 6, acc64=True)
+    ga, gc, gp = ctx.state_download()
+    assert e[0] <= before + 1e-3 and kept[0] == ko[0] >= 1
+    assert np.array_equal(ga, aa) and np.array_equal(gp, pos) and rel_err(e, eo)[0] < 1e-5

@@ -126,3 +126,50 @@ def test_eef1_burial_signs(oracle):
     # (dg_ref < 0 in the table) and two carbonyl O (dg_ref < 0): polar burial raises energy
     e = oracle.energy_atoms32(_cloud([[0, 0, 0]], [10]), _cloud([[3, 0, 0]], [10]))
     assert e[4] > 0.0
+
+
+def _straight_chain(oracle, start, n, aa="A"):
+    """straight_chain_at (diffusion.rs:1113-1120): n residues on a straight Calpha
+    trace from `start`, 3.8 A apart along x, built by protein_from_ca_trace."""
+    ca = np.float32([[start[0] + i * np.float32(3.8), start[1], start[2]] for i in range(n)])
+    seq = np.full(n, A[aa], np.uint8)
+    pos, chi = oracle.build_residues(ca, seq)
+    return seq, chi, pos
+
+
+def test_minimize_never_increases_true_partner_energy(oracle):
+    # diffusion.rs:1123-1140: an antibody placed on top of its partner, 50 steps
+    p_aa, _, p_pos = _straight_chain(oracle, [0.0, 0.0, 0.0], 6)
+    aa, chi, pos = _straight_chain(oracle, [0.2, 0.2, 0.2], 6)
+    Ag = oracle.Antigen(p_aa, p_pos)
+    for acc64 in (False, True):  # the reference's f32 energies, and their f64 re-evaluation
+        before = Ag.minimize(aa.copy(), chi.copy(), pos.copy(), 6, 0, acc64=acc64)[0]
+        a2, c2, p2 = aa.copy(), chi.copy(), pos.copy()
+        after = Ag.minimize(a2, c2, p2, 6, 50, acc64=acc64)[0]
+        assert after <= before + 1e-3
+        final = Ag.minimize(a2.copy(), c2.copy(), p2.copy(), 6, 0, acc64=acc64)[0]
+        assert final == after  # the returned energy is the final structure's
+
+
+def test_minimize_is_a_noop_with_zero_steps(oracle):
+    # diffusion.rs:1143-1153
+    p_aa, _, p_pos = _straight_chain(oracle, [0.0, 0.0, 0.0], 4)
+    aa, chi, pos = _straight_chain(oracle, [20.0, 20.0, 20.0], 4)
+    Ag = oracle.Antigen(p_aa, p_pos)
+    pos0 = pos.copy()
+    before = Ag.score_slots64(aa, pos, 4, full=True)[0]
+    after = Ag.minimize(aa, chi, pos, 4, 0)[0]
+    assert after == before and np.array_equal(pos, pos0)
+
+
+def test_affinity_maturation_never_worsens_the_score(oracle):
+    # diffusion.rs:1156-1172 (every residue mutable there; here the interface
+    # residues, as main.rs:342-344 chooses them: the 8 A chain is all interface)
+    g_aa, _, g_pos = _straight_chain(oracle, [0.0, 0.0, 0.0], 6)
+    aa, chi, pos = _straight_chain(oracle, [8.0, 0.0, 0.0], 6)
+    Ag = oracle.Antigen(g_aa, g_pos)
+    before = Ag.score_slots64(aa, pos, 6, full=True)[0]
+    after, kept = Ag.affinity_maturation(aa, chi, pos, 6)
+    assert after[0] <= before + 1e-3
+    assert abs(after[0] - Ag.score_slots64(aa, pos, 6, full=True)[0]) < 1e-3
+    assert kept[0] >= 1 and not np.all(aa == A["A"])
