@@ -135,6 +135,12 @@ struct State {
     // scoring work queue and per-residue energies
     DBuf<int> queue;
     DBuf<double> res_e, res_abs;
+    // survivor selection gathers into these and swaps them in (the replaced buffers
+    // become the next selection's), so that selections allocate nothing once grown
+    DBuf<uint8_t> alt_aa;
+    DBuf<float4> alt_chi, alt_trig, alt_pos;
+    DBuf<long long> alt_stats;
+    DBuf<int> sel_map, sel_cidx;
     StateView view() {
         StateView v;
         v.n_cand = n_cand;
@@ -1212,29 +1218,27 @@ int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n) {
         for (int r = S.h_res_off[c]; r < S.h_res_off[c + 1]; ++r) map.push_back(r);
     }
     const int total = off[n];
-    if ((s = ensure_trig(ctx))) return s;
-    // gather residues (and statistics) into fresh buffers, then swap them in
-    DBuf<int> d_map, d_cidx;
-    DBuf<uint8_t> aa;
-    DBuf<float4> chi, trig, pos;
-    DBuf<long long> stats;
-    if ((s = upload(ctx, d_map, map.data(), map.size(), "select")) ||
-        (s = upload(ctx, d_cidx, idx, n, "select")))
+    // gather residues (and statistics) into the alternate buffers, then swap them in;
+    // chi sin/cos are gathered when current, else derived later for the selection only
+    const bool trig = S.trig_valid && S.res_trig.p;
+    if ((s = upload(ctx, S.sel_map, map.data(), map.size(), "select")) ||
+        (s = upload(ctx, S.sel_cidx, idx, n, "select")))
         return s;
-    CK(aa.ensure(std::max(total, 1)), "alloc");
-    CK(chi.ensure(std::max(total, 1)), "alloc");
-    CK(trig.ensure(2 * std::max(total, 1)), "alloc");
-    CK(pos.ensure((size_t)std::max(total, 1) * SLOT_STRIDE), "alloc");
-    CK(stats.ensure(4 * n), "alloc");
-    launch_gather_state(ctx->stream, total, d_map.p, S.res_aa.p, S.res_chi.p, S.res_trig.p, S.res_pos.p, aa.p, chi.p,
-                        trig.p, pos.p, (int)n, d_cidx.p, S.mc_stats.p, stats.p);
+    CK(S.alt_aa.ensure(std::max(total, 1)), "alloc");
+    CK(S.alt_chi.ensure(std::max(total, 1)), "alloc");
+    CK(S.alt_trig.ensure(2 * std::max(total, 1)), "alloc");
+    CK(S.alt_pos.ensure((size_t)std::max(total, 1) * SLOT_STRIDE), "alloc");
+    CK(S.alt_stats.ensure(4 * n), "alloc");
+    launch_gather_state(ctx->stream, total, S.sel_map.p, S.res_aa.p, S.res_chi.p, trig ? S.res_trig.p : nullptr,
+                        S.res_pos.p, S.alt_aa.p, S.alt_chi.p, S.alt_trig.p, S.alt_pos.p, (int)n, S.sel_cidx.p,
+                        S.mc_stats.p, S.alt_stats.p);
     LAUNCHED("gather_state");
-    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
-    S.res_aa.swap(aa);
-    S.res_chi.swap(chi);
-    S.res_trig.swap(trig);
-    S.res_pos.swap(pos);
-    S.mc_stats.swap(stats);
+    S.res_aa.swap(S.alt_aa);
+    S.res_chi.swap(S.alt_chi);
+    S.res_trig.swap(S.alt_trig);
+    S.res_pos.swap(S.alt_pos);
+    S.mc_stats.swap(S.alt_stats);
+    S.trig_valid = trig;
     if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
     return BINDER_OK;
@@ -1823,14 +1827,25 @@ int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* o
     if ((s = clear_err(ctx))) return s;
     // ---- phase 1: blocks of score_every steps, each scored with its survivors ----
     const int per = cfg.score_every > 0 ? cfg.score_every : std::max(n1, 1);
+    // gradient-only blocks are the search block: replayed from its CUDA graph
+    const bool graph = (P.flags & BINDER_FLAG_GRAPH) && !cfg.phase1_mc && !ctx->timing;
     int s0 = 0;
     do {
         const int ns = std::min(per, n1 - s0);
-        if (ns > 0 && (s = enqueue_diffuse(ctx, ns, (uint32_t)s0, 0, cfg.phase1_mc, &t1[s0]))) return s;
-        if ((s = enqueue_score_state(ctx, 0))) return s;
-        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k1,
-                             ctx->topk.p);
-        LAUNCHED("topk");
+        if (graph) {
+            if (!ctx->block_graph || ctx->block_graph_sig != block_sig(ctx, ns, k1)) {
+                if ((s = capture_block(ctx, ns, k1))) return s;
+            }
+            CK(cudaGraphLaunch(ctx->block_graph, ctx->stream), "graph launch");
+            ctx->launches += ctx->block_graph_launches;
+            S.order_valid = ctx->block_graph_order;
+        } else {
+            if (ns > 0 && (s = enqueue_diffuse(ctx, ns, (uint32_t)s0, 0, cfg.phase1_mc, &t1[s0]))) return s;
+            if ((s = enqueue_score_state(ctx, 0))) return s;
+            launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k1,
+                                 ctx->topk.p);
+            LAUNCHED("topk");
+        }
         s0 += std::max(ns, 1);
     } while (s0 < n1);
     if ((s = check_err(ctx))) return s;

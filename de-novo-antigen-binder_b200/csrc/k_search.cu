@@ -952,7 +952,7 @@ __global__ void k_gather_state(int total, const int* __restrict__ map, const uin
             o_aa[r] = aa[src];
             o_chi[r] = chi[src];
         }
-        if (k < 2) o_trig[2 * r + k] = trig[2 * src + k];
+        if (k < 2 && trig) o_trig[2 * r + k] = trig[2 * src + k];
     }
     if (t < 4ll * n_cand) o_stats[t] = stats[4 * cidx[t / 4] + t % 4];
 }

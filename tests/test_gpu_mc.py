@@ -19,8 +19,10 @@ HOT = [0, 1, 2, 3, 4, 5]
 COLD = [560, 561, 562, 563, 564, 565]
 
 
-def _params(pkg, oracle, shell, acc, **kw):
+def _params(pkg, oracle, shell, acc, flags=None, **kw):
     g = pkg.Params.defaults(shell_radius=shell, seed=1234, accumulate=acc, **kw)
+    if flags is not None:
+        g.flags = flags
     o = oracle.OrcParams.defaults(shell_radius=shell, seed=1234, accumulate=acc, **kw)
     return g, o
 
@@ -332,12 +334,15 @@ def test_state_select(ctx, oracle, pkg):
     assert np.array_equal(e_sel, e_all[sel])
 
 
-def test_run_allatom_small(ctx, oracle, pkg):
-    """run_allatom on config0 sizes with a short schedule vs the oracle pipeline."""
+@pytest.mark.parametrize("flags", [1, 0])
+def test_run_allatom_small(ctx, oracle, pkg, flags):
+    """run_allatom on config0 sizes with a short schedule vs the oracle pipeline;
+    phase 1 replayed from the search block's CUDA graph (flags 1) or issued
+    launch by launch (0)."""
     cfg = pkg.workloads.config0()
     ag_aa, ag_pos = _antigen(oracle, cfg)
     ctx.clear_antigens()
-    gp, op = _params(pkg, oracle, cfg["shell"][0], 0)
+    gp, op = _params(pkg, oracle, cfg["shell"][0], 0, flags=flags)
     ctx.set_params(gp)
     ctx.add_antigen(ag_aa, ag_pos)
     A = oracle.Antigen(ag_aa, ag_pos)
