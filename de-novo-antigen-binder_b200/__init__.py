@@ -184,6 +184,20 @@ _SIGS = {
     "binder_selftest_wait": (C.c_int, [C.c_void_p, C.c_uint32]),
     "binder_debug_fail_alloc": (C.c_int, [C.c_int64]),
     "binder_minimize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "binder_validate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_parse_pdb_text": (C.c_int, [C.c_char_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.POINTER(C.c_size_t)]),
+    "binder_parse_pdb_file": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_parse_peptide": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_write_pdb_ca": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_char, C.c_void_p, C.c_size_t,
+                                      C.POINTER(C.c_size_t)]),
+    "binder_write_pdb_allatom": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_char, C.c_void_p, C.c_size_t,
+                                           C.POINTER(C.c_size_t)]),
+    "binder_write_pdb_multi": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_void_p,
+                                         C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_write_fasta": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_write_json": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "binder_write_csv": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "binder_affinity_maturation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
@@ -607,6 +621,14 @@ class GpuContext:
         self._check(lib().binder_affinity_maturation(self._h, _ptr(out), _ptr(kept)))
         return out, kept
 
+    def validate(self):
+        """ValidationReport::assess (validate.rs:24-132) of every resident candidate:
+        (clashes, rama_outliers) int32 arrays."""
+        cl = np.zeros(self._state_cand, np.int32)
+        ra = np.zeros(self._state_cand, np.int32)
+        self._check(lib().binder_validate(self._h, _ptr(cl), _ptr(ra)))
+        return cl, ra
+
     def launch_cfg(self):
         c = LaunchCfg()
         self._check(lib().binder_get_launch_cfg(self._h, C.byref(c)))
@@ -778,6 +800,101 @@ class GpuContext:
         out = np.zeros(max(0, n_steps), np.float64)
         self._check(lib().binder_mlp_train(self._h, n_steps, batch, lr, huber_delta, seed, _ptr(out)))
         return out
+
+
+# ---- input and output formats (pdb.rs, report.rs): host code of the library ------------
+class CandidateReport(C.Structure):
+    """binder_candidate_report = CandidateReport (report.rs:8-20); light_sequence None
+    for single-chain candidates, clashes / rama_outliers None when not assessed."""
+    _fields_ = [("rank", C.c_int32), ("_sequence", C.c_char_p), ("_light", C.c_char_p), ("energy", C.c_float),
+                ("entropy_penalty", C.c_float), ("dg_corrected", C.c_float), ("net_charge", C.c_int32),
+                ("aggregation_risk", C.c_int32), ("n_interface", C.c_int32), ("_clashes", C.c_int32),
+                ("_rama", C.c_int32)]
+
+    @classmethod
+    def make(cls, rank, sequence, energy, entropy_penalty=0.0, dg_corrected=0.0, net_charge=0,
+             aggregation_risk=False, n_interface=0, clashes=None, rama_outliers=None, light_sequence=None):
+        return cls(rank, sequence.encode(), None if light_sequence is None else light_sequence.encode(), energy,
+                   entropy_penalty, dg_corrected, net_charge, int(aggregation_risk), n_interface,
+                   -1 if clashes is None else clashes, -1 if rama_outliers is None else rama_outliers)
+
+
+def _text(fn, *args):
+    n = C.c_size_t(0)
+    st = fn(*args, None, 0, C.byref(n))
+    if st not in (0, 9):
+        raise BinderError(st)
+    buf = C.create_string_buffer(n.value + 1)
+    st = fn(*args, buf, n.value + 1, C.byref(n))
+    if st:
+        raise BinderError(st)
+    return buf.raw[: n.value].decode()
+
+
+def _points(fn, *args):
+    n = C.c_size_t(0)
+    st = fn(*args, None, None, 0, C.byref(n))
+    if st not in (0, 9):
+        raise BinderError(st)
+    xyz = np.zeros((n.value, 3), np.float32)
+    aa = np.zeros(n.value, np.uint8)
+    if n.value:
+        st = fn(*args, _ptr(xyz), _ptr(aa), n.value, C.byref(n))
+        if st:
+            raise BinderError(st)
+    return xyz, aa
+
+
+def parse_pdb(text=None, path=None):
+    """parse_pdb (pdb.rs:19-57): the CA records as (xyz float32[n, 3], amino acids)."""
+    if path is not None:
+        return _points(lib().binder_parse_pdb_file, str(path).encode())
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    return _points(lib().binder_parse_pdb_text, b, len(b))
+
+
+def parse_peptide(seq):
+    """parse_peptide (pdb.rs:64-83): (xyz, amino acids) of an extended trace."""
+    return _points(lib().binder_parse_peptide, seq.encode())
+
+
+def write_pdb_ca(xyz, aa, chain="A"):
+    xyz, aa = _f32(xyz), _u8(aa)
+    return _text(lib().binder_write_pdb_ca, len(aa), _ptr(xyz), _ptr(aa), chain.encode())
+
+
+def write_pdb_allatom(aa, pos, chain="A"):
+    aa, pos = _u8(aa), _f32(pos)
+    return _text(lib().binder_write_pdb_allatom, len(aa), _ptr(aa), _ptr(pos), chain.encode())
+
+
+def write_pdb_multi(chains):
+    """chains: [(aa, pos, chain_id), ...] -> one PDB text with TER records."""
+    n_res = np.array([len(a) for a, _, _ in chains], np.uint64)
+    aa = _u8(np.concatenate([a for a, _, _ in chains])) if chains else _u8([])
+    pos = _f32(np.concatenate([p for _, p, _ in chains])) if chains else _f32([])
+    ids = "".join(c for _, _, c in chains).encode()
+    return _text(lib().binder_write_pdb_multi, len(chains), _ptr(n_res), _ptr(aa), _ptr(pos), ids)
+
+
+def _reports(reports):
+    arr = (CandidateReport * max(1, len(reports)))(*reports)
+    return C.cast(arr, C.c_void_p), len(reports), arr
+
+
+def write_fasta(reports):
+    p, n, keep = _reports(reports)
+    return _text(lib().binder_write_fasta, p, n)
+
+
+def write_json(reports):
+    p, n, keep = _reports(reports)
+    return _text(lib().binder_write_json, p, n)
+
+
+def write_csv(reports):
+    p, n, keep = _reports(reports)
+    return _text(lib().binder_write_csv, p, n)
 
 
 def temperature(iteration, total, t_hot=3.0, t_cold=0.02):

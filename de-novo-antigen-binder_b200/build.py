@@ -2,8 +2,8 @@
 
     python de-novo-antigen-binder_b200/build.py [--force] [--verbose]
 
-Each csrc/*.cu is compiled by nvcc for sm_100a into _build/*.o (in parallel,
-skipped when up to date) and linked with a static CUDA runtime into
+Each csrc/*.cu (and the host-only csrc/*.cpp) is compiled by nvcc for sm_100a
+into _build/*.o (in parallel, skipped when up to date) and linked with a static CUDA runtime into
 de-novo-antigen-binder_b200/libbinder_b200.so.
 """
 import argparse
@@ -44,7 +44,7 @@ def _stale(target, sources):
 
 def build(force=False, verbose=False, extra_flags=()):
     BUILD.mkdir(exist_ok=True)
-    sources = sorted(CSRC.glob("*.cu"))
+    sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
     deps = _deps()
     jobs = []
     for src in sources:

@@ -601,6 +601,7 @@ const char* binder_status_string(int s) {
         case BINDER_ERR_STATE: return "call out of order";
         case BINDER_ERR_NODEVICE: return "no usable sm_100 device";
         case BINDER_ERR_CAPACITY: return "output buffer too small";
+        case BINDER_ERR_IO: return "file could not be read";
         default: return "unknown status";
     }
 }
@@ -1948,6 +1949,27 @@ int binder_affinity_maturation(binder_ctx* ctx, double* out_energy, int32_t* out
     if (out_mutated)
         CK(cudaMemcpyAsync(out_mutated, kept.p, S.n_cand * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return BINDER_OK;
+}
+
+int binder_validate(binder_ctx* ctx, int32_t* out_clashes, int32_t* out_rama) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
+    if ((s = clear_err(ctx))) return s;
+    DBuf<int> counts;
+    CK(counts.ensure(2 * (size_t)S.n_cand), "alloc");
+    if (S.max_res > 640) return fail(ctx, BINDER_ERR_ARG, "validation holds at most 640 residues per candidate");
+    CK(launch_validate(ctx->stream, S.view(), counts.p, counts.p + S.n_cand), "validate");
+    LAUNCHED("validate");
+    std::vector<int> h(2 * (size_t)S.n_cand);
+    CK(cudaMemcpyAsync(h.data(), counts.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if ((s = check_err(ctx))) return s;  // synchronises
+    for (int c = 0; c < S.n_cand; ++c) {
+        if (out_clashes) out_clashes[c] = h[c];
+        if (out_rama) out_rama[c] = h[S.n_cand + c];
+    }
     return BINDER_OK;
 }
 

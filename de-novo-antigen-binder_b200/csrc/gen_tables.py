@@ -12,6 +12,8 @@ Layout (all indexed by AminoAcid order of atom.rs:4-25):
   BT_SC_N[20], BT_SC_REF[20][9][4] (a,b,c,chi_idx), BT_SC_GEOM[20][9][3] (bond,angle,dih)
                            side-chain build programs (rotamer.rs:288-430)
   BT_RES[20][4]            residue-level charge, epsilon, sigma, hydrophobic (atom.rs:55-104)
+  BT_SLOT_NAME[20][14][5]  PDB atom name of every slot (amber.rs:126-351)
+  BT_AA3[20][4]            three-letter residue names (atom.rs:114-120)
 
 Usage: python de-novo-antigen-binder_b200/csrc/gen_tables.py
 """
@@ -74,6 +76,11 @@ def main():
     L.append("static const float BT_RES[20][4] = {%s};" % ", ".join(
         "{%s, %s, %s, %s}" % (f(q), f(e), f(s), f(h)) for q, e, s, h in zip(
             rl["charge"], rl["lj_epsilon"], rl["lj_sigma"], rl["hydrophobic"])))
+    L.append("static const char BT_SLOT_NAME[20][14][5] = {")
+    L += ["  {%s}," % ", ".join('"%s"' % a["name"] for a in r["atoms"]) for r in res]
+    L.append("};")
+    # AminoAcid::three_letter (atom.rs:114-120): the enum names in upper case
+    L.append("static const char BT_AA3[20][4] = {%s};" % ", ".join('"%s"' % n.upper() for n in t["amino_acids"]))
     OUT.write_text("\n".join(L) + "\n")
     print("wrote", OUT)
 

@@ -22,6 +22,9 @@
 // Residue geometry keeps the reference's f32 operation order (bit-identical to
 // the CPU restatement); energies are f32 pair terms with compensated sums and
 // FP64 totals, so every keep / reject decision is the f64 energy's.
+#include <algorithm>
+#include <vector>
+
 #include "geom.cuh"
 #include "score.cuh"
 
@@ -271,6 +274,123 @@ __global__ void __launch_bounds__(MAT_WARPS * 32) k_mature(StateView st, const A
 void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, double* res_e, double* out_best,
                    int* out_kept, uint32_t* err) {
     if (st.n_cand > 0) k_mature<<<st.n_cand, MAT_WARPS * 32, 0, s>>>(st, ags, res_e, out_best, out_kept, err);
+}
+
+// ---- structure validation (validate.rs) ------------------------------------------------
+// Clash test of one atom pair (validate.rs:52-59): d^2 < (0.7 (rmh_i + rmh_j))^2, f32.
+__device__ __forceinline__ bool clash(float4 a, float4 b) {
+    const float d_sq = xdist2(xsub(a.x, b.x), xsub(a.y, b.y), xsub(a.z, b.z));
+    const float thresh = xmul(0.7f, xadd(a.w, b.w));
+    return d_sq < xmul(thresh, thresh);
+}
+
+// dihedral (validate.rs:72-86) in degrees (f32::to_degrees); atan2 evaluated in
+// double and rounded once to f32, as the CPU restatement does
+__device__ float dihedral_deg(F3 p0, F3 p1, F3 p2, F3 p3) {
+    const F3 b1 = sub3(p1, p0), b2 = sub3(p2, p1), b3 = sub3(p3, p2);
+    const F3 n1 = norm3(cross3(b1, b2));
+    const F3 n2 = norm3(cross3(b2, b3));
+    const F3 m1 = cross3(n1, norm3(b2));
+    const float x = xadd(xadd(xmul(n1.x, n2.x), xmul(n1.y, n2.y)), xmul(n1.z, n2.z));
+    const float y = xadd(xadd(xmul(m1.x, n2.x), xmul(m1.y, n2.y)), xmul(m1.z, n2.z));
+    return xmul((float)atan2((double)y, (double)x), 57.2957795130823208767981548141051703f);
+}
+
+// in_allowed_basin (validate.rs:101-108), inclusive ranges
+__device__ __forceinline__ bool allowed_basin(float phi, float psi) {
+    const bool alpha_r = phi >= -100.0f && phi <= -30.0f && psi >= -80.0f && psi <= -5.0f;
+    const bool beta = (phi >= -170.0f && phi <= -60.0f && psi >= 90.0f && psi <= 180.0f) ||
+                      (phi >= -170.0f && phi <= -60.0f && psi >= -180.0f && psi <= -150.0f);
+    const bool alpha_l = phi >= 30.0f && phi <= 100.0f && psi >= -10.0f && psi <= 80.0f;
+    return alpha_r || beta || alpha_l;
+}
+
+// One CTA per candidate: its atoms (x, y, z, r_min_half) and residue index in shared
+// memory, the atom pairs split over the threads, then the backbone torsions.
+constexpr int VAL_THREADS = 256;
+constexpr int VAL_MAX_RES = 640;  // a candidate's atoms fit the shared memory of one CTA
+__global__ void __launch_bounds__(VAL_THREADS) k_validate(StateView st, int* __restrict__ clashes,
+                                                           int* __restrict__ rama) {
+    const int c = blockIdx.x;
+    const int r0 = st.cand_res_off[c], n = st.cand_res_off[c + 1] - r0;
+    extern __shared__ __align__(16) unsigned char v_dyn[];
+    float4* at = reinterpret_cast<float4*>(v_dyn);
+    int* res = reinterpret_cast<int*>(at + (size_t)n * SLOTS);
+    __shared__ int s_n, s_count[VAL_THREADS / 32];
+    if (threadIdx.x == 0) {
+        int m = 0;
+        for (int i = 0; i < n; ++i) m += s_topo_n[st.res_aa[r0 + i]];
+        s_n = m;
+    }
+    __syncthreads();
+    // the flattened atoms, residue after residue in topology order
+    if (threadIdx.x < 32) {
+        int base = 0;
+        for (int i = 0; i < n; ++i) {
+            const int aa = st.res_aa[r0 + i], na = s_topo_n[aa];
+            if ((int)threadIdx.x < na) {
+                const float4 p = st.res_pos[(size_t)(r0 + i) * SLOT_STRIDE + threadIdx.x];
+                at[base + threadIdx.x] = make_float4(p.x, p.y, p.z, c_slot_prm[aa][threadIdx.x].y);
+                res[base + threadIdx.x] = i;
+            }
+            base += na;
+        }
+    }
+    __syncthreads();
+    const int m = s_n;
+    const long long pairs = (long long)m * (m - 1) / 2;
+    int cnt = 0;
+    for (long long t = threadIdx.x; t < pairs; t += blockDim.x) {
+        // pair t -> (i, j), i < j: row i holds m - 1 - i pairs
+        int i = (int)((2.0 * m - 1.0 - sqrt((2.0 * m - 1.0) * (2.0 * m - 1.0) - 8.0 * (double)t)) * 0.5);
+        i = max(0, min(i, m - 2));
+        while (i > 0 && (long long)i * (2 * m - i - 1) / 2 > t) --i;
+        while ((long long)(i + 1) * (2 * m - i - 2) / 2 <= t) ++i;
+        const int j = (int)(t - (long long)i * (2 * m - i - 1) / 2) + i + 1;
+        if (abs(res[i] - res[j]) <= 1) continue;
+        cnt += clash(at[i], at[j]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) s_count[threadIdx.x >> 5] = cnt;
+    // ramachandran_outliers: residues 1..n-2 (both torsions defined)
+    int out = 0;
+    for (int r = (int)threadIdx.x + 1; r + 1 < n; r += blockDim.x) {
+        const float4* p = st.res_pos + (size_t)(r0 + r) * SLOT_STRIDE;
+        const float4 cp = st.res_pos[(size_t)(r0 + r - 1) * SLOT_STRIDE + 2];
+        const float4 nn = st.res_pos[(size_t)(r0 + r + 1) * SLOT_STRIDE + 0];
+        const float phi = dihedral_deg(f3(cp), f3(p[0]), f3(p[1]), f3(p[2]));
+        const float psi = dihedral_deg(f3(p[0]), f3(p[1]), f3(p[2]), f3(nn));
+        out += !allowed_basin(phi, psi);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) out += __shfl_xor_sync(0xffffffffu, out, o);
+    __shared__ int s_rama[VAL_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) s_rama[threadIdx.x >> 5] = out;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int a = 0, b = 0;
+        for (int w = 0; w < VAL_THREADS / 32; ++w) {
+            a += s_count[w];
+            b += s_rama[w];
+        }
+        clashes[c] = a;
+        rama[c] = b;
+    }
+}
+
+cudaError_t launch_validate(cudaStream_t s, const StateView& st, int* clashes, int* rama) {
+    if (st.n_cand <= 0) return cudaSuccess;
+    int max_res = 0;  // the launch reserves the largest candidate's atoms
+    std::vector<int> off(st.n_cand + 1);
+    cudaMemcpyAsync(off.data(), st.cand_res_off, off.size() * sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    for (int c = 0; c < st.n_cand; ++c) max_res = std::max(max_res, off[c + 1] - off[c]);
+    const size_t smem = (size_t)max_res * SLOTS * (sizeof(float4) + sizeof(int));
+    if (max_res > VAL_MAX_RES) return cudaErrorInvalidValue;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_validate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_validate<<<st.n_cand, VAL_THREADS, smem, s>>>(st, clashes, rama);
+    return cudaGetLastError();
 }
 
 }  // namespace binder

@@ -151,6 +151,10 @@ void launch_min_accept(cudaStream_t s, const StateView& st, const float4* trial,
 void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, double* res_e, double* out_best,
                    int* out_kept, uint32_t* err);
 
+// ValidationReport::assess of every candidate: clash_score and ramachandran_outliers
+// (at most 640 residues per candidate, else cudaErrorInvalidValue and no launch)
+cudaError_t launch_validate(cudaStream_t s, const StateView& st, int* clashes, int* rama);
+
 // ---- k_micro.cu: FP32 peak microbenchmark; returns the flops of the launch ----
 double launch_ffma(cudaStream_t s, float* scratch, int ctas, int iters, bool packed);
 void launch_unpack_slots(cudaStream_t s, int n_res, const float4* in, float* out);

@@ -48,7 +48,8 @@ enum binder_status {
     BINDER_ERR_GRID = 6,      /* spatial grid box too large for the cell size */
     BINDER_ERR_STATE = 7,     /* call out of order (e.g. no antigen / no candidates) */
     BINDER_ERR_NODEVICE = 8,  /* no usable sm_100 device */
-    BINDER_ERR_CAPACITY = 9   /* output buffer too small; required size reported */
+    BINDER_ERR_CAPACITY = 9,  /* output buffer too small; required size reported */
+    BINDER_ERR_IO = 10        /* a file could not be read */
 };
 
 typedef struct binder_ctx binder_ctx;
@@ -363,6 +364,59 @@ int binder_minimize(binder_ctx* ctx, int steps, double* out_energy);
    residues per candidate); out_energy (may be NULL) = the final score as the
    reference returns it, out_mutated int32[n_cand] (may be NULL) = mutations kept. */
 int binder_affinity_maturation(binder_ctx* ctx, double* out_energy, int32_t* out_mutated);
+
+/* ---- structure validation (validate.rs:40-132) ---------------------------------------
+   ValidationReport::assess of every resident candidate: clash_score (validate.rs:40-63:
+   atom pairs of residues more than one apart in sequence closer than 0.7 x the sum of
+   their r_min_half) and ramachandran_outliers (validate.rs:112-132: residues with both
+   phi and psi whose pair lies outside the alpha-R / beta / alpha-L basins).
+   At most 640 residues per candidate.  out_clashes, out_rama int32[n_cand] (either
+   may be NULL). */
+int binder_validate(binder_ctx* ctx, int32_t* out_clashes, int32_t* out_rama);
+
+/* ---- input and output formats (pdb.rs, report.rs); host code, no context ---------------
+   Text results go into out[cap] NUL-terminated; BINDER_ERR_CAPACITY with *out_len =
+   the length needed (without the NUL) when cap is too small.
+   parse_pdb (pdb.rs:19-57): the CA records of a PDB text (or file) as xyz float[n][3]
+   and amino acids (AminoAcid::from_three_letter, atom.rs:127-151); BINDER_ERR_ARG when
+   there is none (EmptyInput), BINDER_ERR_CAPACITY with *out_n when cap is too small,
+   BINDER_ERR_IO when the file cannot be read. */
+int binder_parse_pdb_text(const char* text, size_t len, float* xyz, uint8_t* aa, size_t cap, size_t* out_n);
+int binder_parse_pdb_file(const char* path, float* xyz, uint8_t* aa, size_t cap, size_t* out_n);
+/* parse_peptide (pdb.rs:64-83): a one-letter sequence on an extended trace along x,
+   centred (3.8 A steps); BINDER_ERR_ARG for an empty string or an unknown letter. */
+int binder_parse_peptide(const char* seq, float* xyz, uint8_t* aa, size_t cap, size_t* out_n);
+/* write_pdb (pdb.rs:90-114): CA-only ATOM records of n residues. */
+int binder_write_pdb_ca(size_t n, const float* xyz, const uint8_t* aa, char chain, char* out, size_t cap,
+                        size_t* out_len);
+/* write_pdb_allatom (pdb.rs:121-152): every heavy atom of a slot-layout protein
+   (pos float[n_res][14][3]) with its topology atom name. */
+int binder_write_pdb_allatom(size_t n_res, const uint8_t* aa, const float* pos, char chain, char* out, size_t cap,
+                             size_t* out_len);
+/* write_pdb_multi (pdb.rs:157-191): chains c = 0..n_chains-1 of n_res[c] residues,
+   concatenated in aa / pos, chain ids chain_ids[c], one serial numbering, TER after
+   each chain. */
+int binder_write_pdb_multi(size_t n_chains, const size_t* n_res, const uint8_t* aa, const float* pos,
+                           const char* chain_ids, char* out, size_t cap, size_t* out_len);
+/* CandidateReport (report.rs:8-20); light_sequence NULL = a single-chain candidate,
+   clashes / rama_outliers < 0 = not assessed. */
+typedef struct binder_candidate_report {
+    int32_t rank;
+    const char* sequence;
+    const char* light_sequence;
+    float energy;
+    float entropy_penalty;
+    float dg_corrected;
+    int32_t net_charge;
+    int32_t aggregation_risk;
+    int32_t n_interface;
+    int32_t clashes;
+    int32_t rama_outliers;
+} binder_candidate_report;
+/* write_fasta / write_json / write_csv (report.rs:41-113). */
+int binder_write_fasta(const binder_candidate_report* reports, size_t n, char* out, size_t cap, size_t* out_len);
+int binder_write_json(const binder_candidate_report* reports, size_t n, char* out, size_t cap, size_t* out_len);
+int binder_write_csv(const binder_candidate_report* reports, size_t n, char* out, size_t cap, size_t* out_len);
 
 /* ---- learned mutation / rotamer proposal (no reference counterpart) ------------------
    A BF16 MLP, 180 -> 256 (SiLU) -> 256 (SiLU) -> 25, FP32 accumulation, trained on

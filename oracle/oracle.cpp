@@ -1155,6 +1155,61 @@ void orc_affinity_maturation(const orc_antigen* A, int n_cand, int n_res, uint8_
     });
 }
 
+// ValidationReport::assess (validate.rs:24-32) of one slot-layout protein.
+// clash_score (validate.rs:40-63): pairs i < j of the flattened atoms whose residues
+// differ by more than one, d^2 < (0.7 (rmh_i + rmh_j))^2.  ramachandran_outliers
+// (validate.rs:112-132): phi (validate.rs:89-98) and psi (:101-110) of residues with
+// both, dihedral (:72-86) in degrees (f32 to_degrees: x * 57.29578); atan2 is
+// evaluated in double and rounded once to f32 (Rust's f32::atan2 is libm's atan2f).
+static float dihedral_deg(const V3& p0, const V3& p1, const V3& p2, const V3& p3) {
+    V3 b1 = sub3(p1, p0), b2 = sub3(p2, p1), b3 = sub3(p3, p2);
+    V3 n1 = norm3(cross3(b1, b2));
+    V3 n2 = norm3(cross3(b2, b3));
+    V3 m1 = cross3(n1, norm3(b2));
+    float x = n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2];
+    float y = m1[0] * n2[0] + m1[1] * n2[1] + m1[2] * n2[2];
+    return (float)std::atan2((double)y, (double)x) * 57.2957795130823208767981548141051703f;
+}
+
+static bool in_allowed_basin(float phi, float psi) {  // validate.rs:101-108
+    bool alpha_r = (phi >= -100.0f && phi <= -30.0f) && (psi >= -80.0f && psi <= -5.0f);
+    bool beta = ((phi >= -170.0f && phi <= -60.0f) && (psi >= 90.0f && psi <= 180.0f)) ||
+                ((phi >= -170.0f && phi <= -60.0f) && (psi >= -180.0f && psi <= -150.0f));
+    bool alpha_l = (phi >= 30.0f && phi <= 100.0f) && (psi >= -10.0f && psi <= 80.0f);
+    return alpha_r || beta || alpha_l;
+}
+
+void orc_validate(int n_res, const uint8_t* aa, const float* pos, int32_t* clashes, int32_t* rama) {
+    std::vector<float> x, y, z, rmh;
+    std::vector<int> ri;
+    for (int r = 0; r < n_res; ++r)
+        for (int k = 0; k < T_TOPO_N[aa[r]]; ++k) {
+            const float* p = pos + ((size_t)r * SLOTS + k) * 3;
+            x.push_back(p[0]); y.push_back(p[1]); z.push_back(p[2]);
+            rmh.push_back(T_NB[T_TOPO_TYPE[aa[r]][k]][0]);
+            ri.push_back(r);
+        }
+    int32_t c = 0;
+    const size_t m = x.size();
+    for (size_t i = 0; i < m; ++i)
+        for (size_t j = i + 1; j < m; ++j) {
+            if (std::abs(ri[i] - ri[j]) <= 1) continue;
+            float dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+            float d_sq = dx * dx + dy * dy + dz * dz;
+            float thresh = 0.7f * (rmh[i] + rmh[j]);
+            if (d_sq < thresh * thresh) ++c;
+        }
+    *clashes = c;
+    Prot P{n_res, const_cast<uint8_t*>(aa), nullptr, const_cast<float*>(pos)};
+    int32_t out = 0;
+    for (int r = 1; r + 1 < n_res; ++r) {
+        float phi = dihedral_deg(P.at(r - 1, 2), P.at(r, 0), P.at(r, 1), P.at(r, 2));
+        float psi = dihedral_deg(P.at(r, 0), P.at(r, 1), P.at(r, 2), P.at(r + 1, 0));
+        if (!in_allowed_basin(phi, psi)) ++out;
+    }
+    *rama = out;
+}
+
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx) {
     std::vector<int32_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0);

@@ -171,6 +171,10 @@ void orc_affinity_maturation(const orc_antigen*, int n_cand, int n_res, uint8_t*
                              int acc64, double* out_energy, int32_t* out_mutated, double* out_margin,
                              int n_threads);
 
+/* ValidationReport::assess (validate.rs:24-132): clash_score and ramachandran_outliers
+   of one slot-layout protein */
+void orc_validate(int n_res, const uint8_t* aa, const float* pos, int32_t* clashes, int32_t* rama);
+
 /* stable ascending sort of energies, NaN last; first k indices (diffusion.rs:1045-1047) */
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx);
 

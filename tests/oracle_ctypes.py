@@ -354,6 +354,14 @@ class Antigen:
         return (out, ab) if with_abs else out
 
 
+def validate(aa, pos):
+    """ValidationReport::assess (validate.rs:24-132): (clashes, rama_outliers)"""
+    aa, pos = u8(aa), f32(pos)
+    cl, ra = C.c_int32(), C.c_int32()
+    lib().orc_validate(len(aa), P(aa), P(pos), C.byref(cl), C.byref(ra))
+    return cl.value, ra.value
+
+
 def disulfide(aa, pos):
     aa, pos = u8(aa), f32(pos)
     return lib().orc_disulfide(len(aa), P(aa), P(pos))

@@ -111,3 +111,21 @@ def test_minimize_and_maturation_reference_geometry(ctx, oracle, pkg):
     ga, gc, gp = ctx.state_download()
     assert e[0] <= before + 1e-3 and kept[0] == ko[0] >= 1
     assert np.array_equal(ga, aa) and np.array_equal(gp, pos) and rel_err(e, eo)[0] < 1e-5
+
+
+def test_validate_matches_oracle(ctx, oracle, pkg):
+    """clash_score and ramachandran_outliers (validate.rs:40-132) of every resident
+    candidate: integer counts, equal to the oracle's."""
+    A, aa, chi, pos = _phase1_state(ctx, oracle, pkg, 96)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=20)
+    cl, ra = ctx.validate()
+    exp = np.array([oracle.validate(aa[c * 20:(c + 1) * 20], pos[c * 20:(c + 1) * 20]) for c in range(96)])
+    assert np.array_equal(cl, exp[:, 0]) and np.array_equal(ra, exp[:, 1])
+    assert cl.sum() > 0 and ra.sum() > 0
+    # a run_allatom-style backbone (Metropolis phi / psi moves) and a clash of overlapping residues
+    ctx.state_upload(aa[:12 * 8], chi[:12 * 8], pos[:12 * 8], uniform_n_res=12)
+    ctx.diffuse(40, step0=0, with_noise=True, with_mc=True)
+    g_aa, _, g_pos = ctx.state_download()
+    cl, ra = ctx.validate()
+    exp = np.array([oracle.validate(g_aa[c * 12:(c + 1) * 12], g_pos[c * 12:(c + 1) * 12]) for c in range(8)])
+    assert np.array_equal(cl, exp[:, 0]) and np.array_equal(ra, exp[:, 1])

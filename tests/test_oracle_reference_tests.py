@@ -173,3 +173,16 @@ def test_affinity_maturation_never_worsens_the_score(oracle):
     assert after[0] <= before + 1e-3
     assert abs(after[0] - Ag.score_slots64(aa, pos, 6, full=True)[0]) < 1e-3
     assert kept[0] >= 1 and not np.all(aa == A["A"])
+
+
+def test_validation_restates_reference_tests(oracle):
+    # validate.rs:149-175
+    aa, chi, pos = _straight_chain(oracle, [0.0, 0.0, 0.0], 6)
+    assert oracle.validate(aa, pos)[0] == 0  # no clashes in a well-spaced extended chain
+    ca = np.float32([[0.0, 0.0, 0.0], [3.8, 0.0, 0.0], [0.05, 0.05, 0.05]])
+    seq = np.zeros(3, np.uint8)
+    p, _ = oracle.build_residues(ca, seq)
+    assert oracle.validate(seq, p)[0] > 0  # residues 0 and 2 on top of each other
+    aa, chi, pos = _straight_chain(oracle, [0.0, 0.0, 0.0], 5)
+    cl, ra = oracle.validate(aa, pos)
+    assert 0 <= ra <= 3  # at most the n - 2 residues with both torsions
