@@ -205,14 +205,14 @@ PROPOSAL_UNIFORM, PROPOSAL_LEARNED = 0, 1
 # learned proposal network (include/binder_gpu.h): sizes and the logged-tuple record
 MLP_IN, MLP_OUT = 180, 25
 MLP_NO_AA = 255  # amino-acid input of a mutation query (no one-hot)
-MLP_K1, MLP_H, MLP_OUT_PAD = 192, 128, 32
+MLP_K1, MLP_H, MLP_OUT_PAD = 192, 256, 32
 MLP_OFF = {"w1": 0}
 MLP_OFF["b1"] = MLP_OFF["w1"] + MLP_H * MLP_K1
 MLP_OFF["w2"] = MLP_OFF["b1"] + MLP_H
 MLP_OFF["b2"] = MLP_OFF["w2"] + MLP_H * MLP_H
 MLP_OFF["w3"] = MLP_OFF["b2"] + MLP_H
 MLP_OFF["b3"] = MLP_OFF["w3"] + MLP_OUT_PAD * MLP_H
-MLP_N_PARAMS = MLP_OFF["b3"] + MLP_OUT_PAD  # 45344
+MLP_N_PARAMS = MLP_OFF["b3"] + MLP_OUT_PAD  # 123424
 MC_TUPLE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("delta_e", "<f4"), ("cand", "<i4"),
                      ("log_ratio", "<f4"), ("residue", "<i2"), ("aa", "u1"), ("action", "u1"), ("antigen", "u1"),
                      ("accepted", "u1"), ("_pad", "u1", (2,))])

@@ -11,15 +11,15 @@ namespace binder {
 
 constexpr int MLP_IN = 180;       // 20 one-hot + 8 shells x 20 amino acids
 constexpr int MLP_K1 = 192;       // first-layer K padded to the MMA K step
-constexpr int MLP_H = 128;        // hidden width
+constexpr int MLP_H = 256;        // hidden width
 constexpr int MLP_OUT = 25;       // 20 mutation targets + 5 rotamers
 constexpr int MLP_OUT_PAD = 32;   // output rows of W3 (rows >= 25 stay zero)
 constexpr int MLP_SHELLS = 8;     // radial shells of 1.25 A out to 10 A
 constexpr int MLP_COUNT_CAP = 255;
 constexpr int MLP_NO_AA = 255;    // amino-acid input of a mutation query: none (no one-hot)
 
-// flat FP32 parameter vector: W1 [128][192], b1 [128], W2 [128][128], b2 [128],
-// W3 [32][128], b3 [32]
+// flat FP32 parameter vector: W1 [256][192], b1 [256], W2 [256][256], b2 [256],
+// W3 [32][256], b3 [32]
 constexpr int MLP_OFF_W1 = 0;
 constexpr int MLP_OFF_B1 = MLP_OFF_W1 + MLP_H * MLP_K1;
 constexpr int MLP_OFF_W2 = MLP_OFF_B1 + MLP_H;

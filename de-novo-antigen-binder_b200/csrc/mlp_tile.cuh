@@ -2,7 +2,7 @@
 // tile of at most 16 residues (the residues of one candidate that drew a move in
 // a step: a handful of rows, below the 64/128-row tiles of tcgen05.mma, so the
 // CTA's eight warps use the warp-level BF16 MMA, m16n8k16 with FP32 accumulators).
-// Weights are read from global memory (L2-resident, 88 KB, not cached in L1) in
+// Weights are read from global memory (L2-resident, 240 KB, not cached in L1) in
 // fragment order with 16-byte loads, in a few large register batches per layer; activations stay in
 // shared memory as BF16, the output as FP32.  Same arithmetic as the batched
 // tensor-core path up to the order of the FP32 sums.
@@ -142,11 +142,14 @@ __device__ __forceinline__ void mlp_tile_layer(uint4 (&w)[MT_WREGS], const __nv_
 }
 
 // Shapes: layers 1 and 2 over MT_NT n-tiles of 8 columns per warp (the 8 warps
-// cover the hidden width), each in one batch of all its k-step pairs (layer 1:
-// 6 pairs x 2 n-tiles, layer 2: 4 x 2 -- one L2 round trip per layer); layer 3
-// (32 outputs) on warps 0-3, one n-tile and 4 pairs each.
+// cover the hidden width), their k-step pairs in batches that fill the weight
+// registers (hidden width 256: layer 1's 6 pairs x 4 n-tiles in two batches of 3,
+// layer 2's 8 pairs x 4 n-tiles in four batches of 2); layer 3 (32 outputs) on
+// warps 0-3, one n-tile and all its pairs in one batch.
 constexpr int MT_NT = MLP_H / 64;
-constexpr int MT_PB1 = MLP_K1 / 32, MT_PB2 = MLP_H / 32, MT_PB3 = MLP_H / 32;
+constexpr int MT_PB1 = MT_WREGS / MT_NT < MLP_K1 / 32 ? MT_WREGS / MT_NT : MLP_K1 / 32;
+constexpr int MT_PB2 = MLP_H / 32 <= MT_WREGS / MT_NT ? MLP_H / 32 : 2;
+constexpr int MT_PB3 = MLP_H / 32;
 static_assert(MT_NT * MT_PB1 <= MT_WREGS && MT_NT * MT_PB2 <= MT_WREGS && MT_PB3 <= MT_WREGS,
               "weight batches must fit the registers");
 

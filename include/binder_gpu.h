@@ -430,12 +430,12 @@ int binder_write_csv(const binder_candidate_report* reports, size_t n, char* out
    (index 20 + 20 s + a), as BF16.
    Outputs (25): predicted energy change of a mutation to amino acid 0..19, then of
    a move to rotamer 0..4.
-   Parameters: one FP32 vector of BINDER_MLP_N_PARAMS values, W1 [128][192] (input
-   columns 180..191 zero), b1 [128], W2 [128][128], b2 [128], W3 [32][128] (rows
+   Parameters: one FP32 vector of BINDER_MLP_N_PARAMS values, W1 [256][192] (input
+   columns 180..191 zero), b1 [256], W2 [256][256], b2 [256], W3 [32][256] (rows
    25..31 zero), b3 [32] (entries 25..31 zero); W is [out][in]. */
 #define BINDER_MLP_IN 180
 #define BINDER_MLP_OUT 25
-#define BINDER_MLP_N_PARAMS 45344
+#define BINDER_MLP_N_PARAMS 123424
 
 /* One logged Metropolis proposal (32 bytes). */
 typedef struct binder_mc_tuple {

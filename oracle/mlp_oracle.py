@@ -9,7 +9,7 @@ the GPU kernels in de-novo-antigen-binder_b200/csrc/k_mlp.cu:
     log1p table rounded once to f32, BF16 round-to-nearest-even); a mutation
     query (amino acid NO_AA) carries no one-hot;
   * loss_grad(ref=...): mutation rows predict y[new] - y[old];
-  * forward() / loss_grad(): the MLP 180 -> 128 -> 128 -> 25 with SiLU in float64.
+  * forward() / loss_grad(): the MLP 180 -> 256 -> 256 -> 25 with SiLU in float64.
     With bf16=True the BF16 roundings of the GPU path are applied (weights, input
     rows, hidden activations, output and hidden gradients) and only the sums are
     exact, so the GPU's FP32 sums are compared against exact sums of the same
@@ -23,7 +23,7 @@ from __future__ import annotations
 
 import numpy as np
 
-MLP_IN, MLP_K1, MLP_H, MLP_OUT, MLP_OUT_PAD = 180, 192, 128, 25, 32
+MLP_IN, MLP_K1, MLP_H, MLP_OUT, MLP_OUT_PAD = 180, 192, 256, 25, 32
 N_AA, SHELLS = 20, 8
 OFF = {"w1": 0, "b1": MLP_H * MLP_K1}
 OFF["w2"] = OFF["b1"] + MLP_H
