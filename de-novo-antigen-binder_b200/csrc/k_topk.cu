@@ -2,7 +2,8 @@
 // stable ascending order (diffusion.rs:1042-1057 sorts with a stable sort and
 // truncates to the population).
 //
-// One CTA per segment.  Energies are mapped to order-preserving 64-bit keys
+// One CTA per segment.  k <= 64: warps keep sorted best-64 lists in registers and a
+// merge tree joins them (k_topk64).  Larger k: energies are mapped to order-preserving 64-bit keys
 // (-0.0 folded onto +0.0, NaN after every number) and paired with their index,
 // so a plain lexicographic (key, index) order is exactly the stable sort.  The
 // CTA keeps a running best-k list in shared memory and merges the segment in
@@ -112,10 +113,114 @@ __global__ void __launch_bounds__(TOPK_THREADS) k_topk(const double* __restrict_
         out_idx[(long long)seg * k + t] = (t < kept && idx[t] != INT32_MAX) ? idx[t] : -1;
 }
 
+// ---- k <= 64: warp sorts and a merge tree ---------------------------------------------
+// Each warp keeps the 64 smallest (key, index) pairs it has seen as a sorted list, two
+// per lane (positions lane and lane + 32).  A chunk of 32 new elements is sorted in
+// registers and merged in: the 64 smallest of the list and the chunk are
+// min(list[i], chunk[63 - i]) (the chunk padded with +inf), a bitonic sequence that six
+// compare-exchange stages sort.  The warps' lists are then merged pairwise in shared
+// memory, five levels for 32 warps.  (key, index) order is the stable sort's, so the
+// first k of the final list are the stable top-k.
+struct KI {
+    unsigned long long k;
+    int i;
+};
+__device__ __forceinline__ bool ki_less(const KI& a, const KI& b) { return a.k < b.k || (a.k == b.k && a.i < b.i); }
+__device__ __forceinline__ KI ki_shfl_xor(const KI& v, int m) {
+    return KI{__shfl_xor_sync(0xffffffffu, v.k, m), __shfl_xor_sync(0xffffffffu, v.i, m)};
+}
+__device__ __forceinline__ KI ki_shfl(const KI& v, int src) {
+    return KI{__shfl_sync(0xffffffffu, v.k, src), __shfl_sync(0xffffffffu, v.i, src)};
+}
+__device__ __forceinline__ KI ki_min(const KI& a, const KI& b) { return ki_less(b, a) ? b : a; }
+__device__ __forceinline__ KI ki_max(const KI& a, const KI& b) { return ki_less(b, a) ? a : b; }
+
+// ascending bitonic sort of one element per lane
+__device__ __forceinline__ KI warp_sort32(KI v, int lane) {
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const KI o = ki_shfl_xor(v, stride);
+            const bool lower = (lane & stride) == 0, up = (lane & size) == 0 || size == 32;
+            const bool take = lower == up ? ki_less(o, v) : ki_less(v, o);
+            if (take) v = o;
+        }
+    return v;
+}
+
+// (a, b) = positions lane and lane + 32 of a bitonic 64-sequence -> sorted ascending
+__device__ __forceinline__ void warp_bitonic64(KI& a, KI& b, int lane) {
+    const KI lo = ki_min(a, b), hi = ki_max(a, b);
+    a = lo;
+    b = hi;
+#pragma unroll
+    for (int stride = 16; stride > 0; stride >>= 1) {
+        const bool lower = (lane & stride) == 0;
+        const KI oa = ki_shfl_xor(a, stride), ob = ki_shfl_xor(b, stride);
+        a = lower ? ki_min(a, oa) : ki_max(a, oa);
+        b = lower ? ki_min(b, ob) : ki_max(b, ob);
+    }
+}
+
+// the 64 smallest of the sorted list (a, b) and the sorted 64-list (c, d), sorted
+__device__ __forceinline__ void warp_merge64(KI& a, KI& b, KI c, KI d, int lane) {
+    // reversed second list: position i holds element 63 - i
+    const KI rc = ki_shfl(d, 31 - lane), rd = ki_shfl(c, 31 - lane);
+    a = ki_min(a, rc);
+    b = ki_min(b, rd);
+    warp_bitonic64(a, b, lane);
+}
+
+constexpr int TOPK64_WARPS = 32;
+__global__ void __launch_bounds__(TOPK64_WARPS * 32) k_topk64(const double* __restrict__ e,
+                                                               const int* __restrict__ idx_list,
+                                                               const long long* __restrict__ seg_off, int k,
+                                                               int* __restrict__ out_idx) {
+    __shared__ unsigned long long s_k[TOPK64_WARPS][64];
+    __shared__ int s_i[TOPK64_WARPS][64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = blockIdx.x;
+    const long long b0 = seg_off[seg], n = seg_off[seg + 1] - b0;
+    const KI inf = {0xFFFFFFFFFFFFFFFFull, INT32_MAX};
+    KI a = inf, b = inf;  // this warp's best 64, sorted
+    for (long long base = (long long)warp * 32; base < n; base += TOPK64_WARPS * 32) {
+        KI v = inf;
+        if (base + lane < n) {
+            const int g = idx_list ? idx_list[b0 + base + lane] : (int)(b0 + base + lane);
+            v = KI{order_key(e[g]), g};
+        }
+        v = warp_sort32(v, lane);
+        warp_merge64(a, b, v, inf, lane);
+    }
+    // merge tree over the warps' lists
+    for (int level = 1; level < TOPK64_WARPS; level <<= 1) {
+        if ((warp & (2 * level - 1)) == level) {
+            s_k[warp][lane] = a.k; s_i[warp][lane] = a.i;
+            s_k[warp][lane + 32] = b.k; s_i[warp][lane + 32] = b.i;
+        }
+        __syncthreads();
+        if ((warp & (2 * level - 1)) == 0) {
+            const int o = warp + level;
+            const KI c = {s_k[o][lane], s_i[o][lane]}, d = {s_k[o][lane + 32], s_i[o][lane + 32]};
+            warp_merge64(a, b, c, d, lane);
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        if (lane < k) out_idx[(long long)seg * k + lane] = a.i != INT32_MAX ? a.i : -1;
+        if (lane + 32 < k) out_idx[(long long)seg * k + lane + 32] = b.i != INT32_MAX ? b.i : -1;
+    }
+}
+
 int launch_topk_segments(cudaStream_t s, const double* energies, const int* idx_list, const long long* seg_off,
                          int n_seg, int k, int* out_idx) {
     if (n_seg <= 0 || k <= 0) return 0;
     if (k > TOPK_MAX_K) return -1;
+    if (k <= 64) {
+        k_topk64<<<n_seg, TOPK64_WARPS * 32, 0, s>>>(energies, idx_list, seg_off, k, out_idx);
+        return 1;
+    }
     const size_t smem = (size_t)TOPK_SORT * (sizeof(unsigned long long) + sizeof(int));
     cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_topk<<<n_seg, TOPK_THREADS, smem, s>>>(energies, idx_list, seg_off, k, out_idx);

@@ -209,6 +209,21 @@ def test_topk_matches_stable_sort(ctx, oracle):
     assert np.array_equal(ctx.topk(big, 700), oracle.topk(big, 700))
 
 
+@pytest.mark.parametrize("n", [1, 31, 1024, 5000])
+def test_topk_small_k_matches_stable_sort(ctx, oracle, n):
+    """k <= 64 (warp sorts + merge tree): ties across warps and chunks, NaNs, -0/+0,
+    fewer elements than k."""
+    rng = np.random.default_rng(n)
+    e = rng.integers(-20, 20, size=n).astype(np.float64)  # many ties
+    e[rng.random(n) < 0.05] = np.nan
+    if n > 9:
+        e[3], e[9] = -0.0, 0.0
+    for k in (1, 17, 33, 64):
+        exp = oracle.topk(e, min(k, n))
+        got = ctx.topk(e, min(k, n))
+        assert np.array_equal(got, exp), (n, k)
+
+
 def test_topk_segmented(ctx, oracle):
     rng = np.random.default_rng(4)
     e = rng.normal(size=3000)
