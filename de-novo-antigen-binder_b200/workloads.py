@@ -223,3 +223,87 @@ def config3_slots(ag_cloud_xyz, tables, n_cand=1024, n_res=20, charged_frac=0.3)
     pos[res_of_atom, slot, 1] = g["y"]
     pos[res_of_atom, slot, 2] = g["z"]
     return aa, pos
+
+
+# ---- Fv two-chain workload (diffusion.rs:477-827, germline.rs) -------------------------
+# Germline framework scaffolds (germline.rs:42-61): FR1, CDR1 length, FR2, CDR2 length,
+# FR3, CDR3 length, FR4; VH3-23-like heavy chain and IGKV1-39-like kappa light chain.
+VH_FRAMEWORK = ("EVQLLESGGGLVQPGGSLRLSCAAS", 8, "WVRQAPGKGLEWVS", 8, "RFTISRDNSKNTLYLQMNSLRAEDTAVYYCAK", 12,
+                "WGQGTLVTVSS")
+VL_FRAMEWORK = ("DIQMTQSPSSLSASVGDRVTITC", 11, "WYQQKPGKAPKLLIY", 7, "GVPSRFSGSGSGTDFTLTISSLQPEDFATYYC", 9,
+                "FGQGTKVEIK")
+FV_LOCAL_RADIUS_SCALE = np.float32(1.3)   # diffusion.rs:54
+FV_CHAIN_MARGIN = np.float32(6.0)         # diffusion.rs:58
+INIT_RADIUS = np.float32(20.0)            # diffusion.rs:81
+
+
+def fv_layout(fw, cdr3_len=None):
+    fr1, c1, fr2, c2, fr3, c3, fr4 = fw
+    return fr1, c1, fr2, c2, fr3, c3 if cdr3_len is None else max(1, cdr3_len), fr4
+
+
+def assemble_chain(fw, cdr1, cdr2, cdr3):
+    """assemble_chain (germline.rs:91-123): sequence (AminoAcid indices) and a CDR flag
+    per residue (0 framework, 1/2/3 the CDR loop)."""
+    fr1, _, fr2, _, fr3, _, fr4 = fw
+    seq, region = [], []
+    for part, reg in ((fr1, 0), (cdr1, 1), (fr2, 0), (cdr2, 2), (fr3, 0), (cdr3, 3), (fr4, 0)):
+        codes = [AA_INDEX[c] for c in part] if isinstance(part, str) else list(part)
+        seq += codes
+        region += [reg] * len(codes)
+    return np.array(seq, np.uint8), np.array(region, np.uint8)
+
+
+def fib_sphere_offset(i, n, radius):
+    """fib_sphere_offset (diffusion.rs:501-507), f32."""
+    f = np.float32
+    n_f = f(max(n, 1))
+    y = f(1.0) - f(2.0) * (f(i) + f(0.5)) / n_f
+    r_y = np.sqrt(np.maximum(f(1.0) - y * y, f(0.0)))
+    theta = f(2.399963) * f(i)
+    return np.array([np.cos(theta) * r_y * f(radius), y * f(radius), np.sin(theta) * r_y * f(radius)], np.float32)
+
+
+def config_fv(antigen_ca, n_cand=8, h3_len=12, l3_len=9, seed=0xB200 + 5):
+    """The initial population of run_fv (diffusion.rs:704-776): per candidate a random
+    approach direction toward the antigen's Calpha centre, the heavy and light chains
+    as two clusters beside it (CDRs uniform random, Calphas on Fibonacci spheres of
+    1.3 sqrt(n) A plus uniform +-1.5 A noise).  The reference draws these from its
+    per-candidate SmallRng; here from a seeded numpy generator (the chains are
+    uploaded as they are).  Returns dict(heavy=(aa, ca, region) stacked over
+    candidates, light=..., target_radius, center)."""
+    rng = np.random.default_rng(seed)
+    vh, vl = fv_layout(VH_FRAMEWORK, h3_len), fv_layout(VL_FRAMEWORK, l3_len)
+    n_h = sum(len(p) if isinstance(p, str) else p for p in vh)
+    n_l = sum(len(p) if isinstance(p, str) else p for p in vl)
+    center = ca_center(antigen_ca)
+    f = np.float32
+    radius_h = FV_LOCAL_RADIUS_SCALE * np.sqrt(f(n_h))
+    radius_l = FV_LOCAL_RADIUS_SCALE * np.sqrt(f(n_l))
+    half_sep = (radius_h + radius_l + FV_CHAIN_MARGIN) * f(0.5)
+    approach_radius = INIT_RADIUS + max(radius_h, radius_l) + f(5.0)
+    target_radius = np.sqrt(approach_radius * approach_radius + half_sep * half_sep)
+    chains = {"heavy": ([], [], []), "light": ([], [], [])}
+    for _ in range(n_cand):
+        theta = f(rng.uniform(0.0, 2 * np.pi))
+        cos_phi = f(rng.uniform(-1.0, 1.0))
+        sin_phi = np.sqrt(max(f(1.0) - cos_phi * cos_phi, f(0.0)))
+        d = np.array([sin_phi * np.cos(theta), cos_phi, sin_phi * np.sin(theta)], np.float32)
+        approach = center + d * approach_radius
+        up = np.float32([0, 1, 0]) if abs(d[1]) < 0.9 else np.float32([1, 0, 0])
+        perp = np.cross(d, up).astype(np.float32)
+        perp = perp / max(np.float32(np.linalg.norm(perp)), np.float32(1e-8))
+        for name, fw, sign in (("heavy", vh, 1.0), ("light", vl, -1.0)):
+            cdr = [rng.integers(0, N_AA, size=fw[k]) for k in (1, 3, 5)]
+            seq, region = assemble_chain(fw, *cdr)
+            n = len(seq)
+            local = FV_LOCAL_RADIUS_SCALE * np.sqrt(f(n))
+            cc = approach + f(sign) * perp * half_sep
+            ca = np.stack([cc + fib_sphere_offset(i, n, local) + rng.uniform(-1.5, 1.5, 3).astype(np.float32)
+                           for i in range(n)]).astype(np.float32)
+            chains[name][0].append(seq)
+            chains[name][1].append(ca)
+            chains[name][2].append(region)
+    out = {k: tuple(np.concatenate(v) for v in chains[k]) for k in chains}
+    out.update(n_heavy=n_h, n_light=n_l, target_radius=float(target_radius), center=center, n_cand=n_cand)
+    return out

@@ -964,6 +964,180 @@ void step_one(const orc_antigen* A, const orc_params* prm, Prot& P, uint32_t can
         }
     }
 }
+// ---- Fv two-chain engine (diffusion.rs:477-827) --------------------------------------
+// residue_contribution_allatom (diffusion.rs:425-463) of residue r of P against the
+// Calphas of another chain Q (the Fv partner), the same arithmetic as against the antigen.
+template <class Acc>
+Acc contribution_vs_chain(const Prot& P, int r, const Prot& Q) {
+    int baa = P.aa[r];
+    int bca = T_TOPO_CA[baa];
+    V3 p = P.at(r, bca);
+    int bt = T_TOPO_TYPE[baa][bca];
+    float brm = T_NB[bt][0], be = T_NB[bt][1], bq = T_TOPO_Q[baa][bca];
+    uint8_t bh = T_TOPO_HYD[baa][bca];
+    Acc e = 0;
+    for (int i = 0; i < Q.n; ++i) {
+        int aaa = Q.aa[i];
+        int aca = T_TOPO_CA[aaa];
+        V3 pa = Q.at(i, aca);
+        float dx = p[0] - pa[0], dy = p[1] - pa[1], dz = p[2] - pa[2];
+        float r_sq = dx * dx + dy * dy + dz * dz;
+        if (r_sq > CUTOFF_SQ || r_sq < 0.25f) continue;
+        int at = T_TOPO_TYPE[aaa][aca];
+        float arm = T_NB[at][0], ae = T_NB[at][1], aq = T_TOPO_Q[aaa][aca];
+        uint8_t ah = T_TOPO_HYD[aaa][aca];
+        float r_ij = brm + arm;
+        float eps = std::sqrt(be * ae);
+        float r2 = (r_ij * r_ij) / r_sq;
+        float r6 = r2 * r2 * r2;
+        e += (Acc)(eps * (r6 * r6 - 2.0f * r6));
+        if (bq != 0.0f && aq != 0.0f) e += (Acc)(332.0f * bq * aq / std::sqrt(r_sq));
+        if (bh == 1 && ah == 1 && r_sq < 36.0f) e -= (Acc)0.5f;
+        if (hb_pair(bt, at)) e += (Acc)hbond_energy_mc(r_sq);
+    }
+    return e;
+}
+
+// fv_chain_step (diffusion.rs:560-698) of chain `chain` (0 heavy, 1 light) against the
+// antigen and the partner chain snapshot Q.  Draws: Philox streams STREAM_* + 4 * chain,
+// per residue (d.x the CDR mutation gate, d.y the rotamer-or-mutation choice or the
+// relaxation gate, d.z the rotamer / amino-acid index, d.w the acceptance draw).
+template <class Acc>
+void fv_chain_step(const orc_antigen* A, const orc_params* prm, Prot& P, const uint8_t* cdr, const Prot& Q,
+                   int chain, uint32_t cand, uint32_t step, float temp, float target_radius) {
+    const int n = P.n;
+    std::vector<float> fx(n), fy(n), fz(n);
+    for (int r = 0; r < n; ++r) {
+        V3 ca = P.at(r, T_TOPO_CA[P.aa[r]]);
+        CgAtom b = cg_atom(ca[0], ca[1], ca[2], P.aa[r]);
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        A->grid.query(b.x, b.y, b.z, [&](uint32_t i) { cg_pair(b, A->cg[i], sx, sy, sz); });
+        // VH-VL packing force: compute_forces (energy.rs:154-234) over the partner's Calphas
+        float px = 0.f, py = 0.f, pz = 0.f;
+        for (int i = 0; i < Q.n; ++i) {
+            V3 q = Q.at(i, T_TOPO_CA[Q.aa[i]]);
+            cg_pair(b, cg_atom(q[0], q[1], q[2], Q.aa[i]), px, py, pz);
+        }
+        fx[r] = sx + px; fy[r] = sy + py; fz[r] = sz + pz;
+    }
+    const float sigma = prm->noise_base * std::sqrt(temp);
+    const float* c = A->center;
+    const uint32_t sh = 4u * (uint32_t)chain;
+    for (int r = 0; r < n; ++r) {
+        V3 ca = P.at(r, T_TOPO_CA[P.aa[r]]);
+        float dx_c = ca[0] - c[0], dy_c = ca[1] - c[1], dz_c = ca[2] - c[2];
+        float d = std::fmax(std::sqrt(dx_c * dx_c + dy_c * dy_c + dz_c * dz_c), 0.001f);
+        float excess = d - target_radius;
+        float f_r = -prm->restraint_k * excess / d;
+        fx[r] += f_r * dx_c;
+        fy[r] += f_r * dy_c;
+        fz[r] += f_r * dz_c;
+        uint32_t d4[4];
+        draw(prm->seed, cand, step, STREAM_NOISE + sh, r, d4);
+        float nx = frange(d4[0], -sigma, sigma), ny = frange(d4[1], -sigma, sigma), nz = frange(d4[2], -sigma, sigma);
+        auto clampf = [&](float v) { return v > prm->max_disp ? prm->max_disp : (v < -prm->max_disp ? -prm->max_disp : v); };
+        V3 new_ca = {ca[0] + clampf(prm->step * fx[r]) + nx, ca[1] + clampf(prm->step * fy[r]) + ny,
+                     ca[2] + clampf(prm->step * fz[r]) + nz};
+        set_ca_pos(P, r, new_ca);
+    }
+    auto contrib = [&](int r) { return residue_contribution_t<Acc>(A, P, r) + contribution_vs_chain<Acc>(P, r, Q); };
+    auto ds = [&]() { return disulfide_t<Acc>(P); };
+    auto rot_move = [&](int r, uint32_t dz, uint32_t dw) {
+        int aa = P.aa[r];
+        if (T_ROT_N[aa] == 0) return;
+        float old_chi[4];
+        for (int k = 0; k < 4; ++k) old_chi[k] = P.chi[r * 4 + k];
+        int rot_idx = (int)urange(dz, (uint32_t)T_ROT_N[aa]);
+        Acc old_e = contrib(r) + ds();
+        for (int k = 0; k < 4; ++k) P.chi[r * 4 + k] = T_ROT[aa][rot_idx][k];
+        rebuild_side_chain(P, r);
+        Acc new_e = contrib(r) + ds();
+        if (!metropolis(new_e - old_e, temp, u01(dw))) {
+            for (int k = 0; k < 4; ++k) P.chi[r * 4 + k] = old_chi[k];
+            rebuild_side_chain(P, r);
+        }
+    };
+    const float mut_p = prm->mutation_p * 3.0f, rot_p = prm->rotamer_move_p * 2.0f,
+                relax_p = prm->rotamer_move_p * 0.3f;
+    for (int r = 0; r < n; ++r) {
+        uint32_t d4[4];
+        draw(prm->seed, cand, step, STREAM_MC + sh, r, d4);
+        if (cdr[r] && u01(d4[0]) < mut_p) {
+            if (u01(d4[1]) < rot_p) {
+                rot_move(r, d4[2], d4[3]);
+            } else {
+                int old_aa = P.aa[r];
+                int new_aa = (int)urange(d4[2], 20u);
+                float old_chi[4];
+                for (int k = 0; k < 4; ++k) old_chi[k] = P.chi[r * 4 + k];
+                Acc old_e = contrib(r) + ds();
+                float new_chi[4] = {0.f, 0.f, 0.f, 0.f};
+                if (T_ROT_N[new_aa] > 0)
+                    for (int k = 0; k < 4; ++k) new_chi[k] = T_ROT[new_aa][0][k];
+                mutate_residue(P, r, new_aa, new_chi);
+                Acc new_e = contrib(r) + ds();
+                if (!metropolis(new_e - old_e, temp, u01(d4[3]))) mutate_residue(P, r, old_aa, old_chi);
+            }
+        } else if (u01(d4[1]) < relax_p) {  // framework (or CDR without a draw): rotamer relaxation
+            rot_move(r, d4[2], d4[3]);
+        }
+    }
+    for (int r = 0; r < n; ++r) {  // backbone phi / psi moves, the downstream residues re-scored
+        uint32_t d4[4];
+        draw(prm->seed, cand, step, STREAM_BACKBONE + sh, r, d4);
+        if (!(u01(d4[0]) < prm->backbone_move_p)) continue;
+        float delta = frange(d4[1], -prm->max_torsion_deg, prm->max_torsion_deg) * RADS_PER_DEG;
+        bool do_phi = (d4[2] >> 31) & 1u;
+        Acc old_e = 0;
+        for (int i = r; i < n; ++i) old_e += contrib(i);
+        old_e += ds();
+        if (do_phi) perturb_phi(P, r, delta); else perturb_psi(P, r, delta);
+        Acc new_e = 0;
+        for (int i = r; i < n; ++i) new_e += contrib(i);
+        new_e += ds();
+        if (!metropolis(new_e - old_e, temp, u01(d4[3]))) {
+            if (do_phi) perturb_phi(P, r, -delta); else perturb_psi(P, r, -delta);
+        }
+    }
+}
+
+// interaction_energy_atoms (energy.rs:256-314) of two slot-layout proteins, the five
+// terms added as AtomEnergyBreakdown::total does (acc64: their f64 re-evaluation)
+double pair_energy(const Prot& G, const Prot& B, int acc64) {
+    auto flat = [](const Prot& P, std::vector<float>* v, std::vector<uint8_t>* u) {
+        int m = 0;
+        for (int r = 0; r < P.n; ++r) m += T_TOPO_N[P.aa[r]];
+        for (int k = 0; k < 6; ++k) v[k].resize(m);
+        u[0].resize(m); u[1].resize(m);
+        orc_flatten(P.n, P.aa, P.pos, v[0].data(), v[1].data(), v[2].data(), v[3].data(), v[4].data(), v[5].data(),
+                    u[0].data(), u[1].data(), nullptr);
+        return orc_cloud{v[0].data(), v[1].data(), v[2].data(), v[3].data(), v[4].data(), v[5].data(), u[0].data(),
+                         u[1].data(), m};
+    };
+    std::vector<float> gv[6], bv[6];
+    std::vector<uint8_t> gu[2], bu[2];
+    orc_cloud g = flat(G, gv, gu), b = flat(B, bv, bu);
+    if (acc64) {
+        double e[5];
+        orc_energy_atoms64(&g, &b, e, nullptr);
+        return (((e[0] + e[1]) + e[2]) + e[3]) + e[4];
+    }
+    float e[5];
+    orc_energy_atoms32(&g, &b, e);
+    return (double)((((e[0] + e[1]) + e[2]) + e[3]) + e[4]);
+}
+
+// fv_energy (diffusion.rs:541-547): antigen-VH + antigen-VL + VH-VL + both disulfide terms
+double fv_energy(const orc_antigen* A, const Prot& H, const Prot& L, int acc64) {
+    std::vector<float> chi((size_t)A->n_res * 4, 0.f);
+    Prot G{A->n_res, const_cast<uint8_t*>(A->aa.data()), chi.data(), const_cast<float*>(A->pos.data())};
+    if (acc64)
+        return pair_energy(G, H, 1) + pair_energy(G, L, 1) + pair_energy(H, L, 1) + (double)disulfide(H) +
+               (double)disulfide(L);
+    return (double)((((float)pair_energy(G, H, 0) + (float)pair_energy(G, L, 0)) + (float)pair_energy(H, L, 0) +
+                     disulfide(H)) + disulfide(L));
+}
+
 }  // namespace
 
 extern "C" {
@@ -1208,6 +1382,74 @@ void orc_validate(int n_res, const uint8_t* aa, const float* pos, int32_t* clash
         if (!in_allowed_basin(phi, psi)) ++out;
     }
     *rama = out;
+}
+
+// The iteration loop of run_fv (diffusion.rs:791-812) for every candidate: per
+// iteration the heavy chain steps against the light chain as it was, the light
+// chain against the stepped heavy chain, and the pair is kept when fv_energy drops
+// below the best, put back to the best pair when it rises (elitist).  Chains in
+// place (the best pair at the end); out_energy = best fv_energy; the step draws use
+// cand_id[c] (NULL: c); out_margin (may be NULL): the smallest |e - best| / max(|best|, 1)
+// of the keep / restore decisions.
+void orc_fv_run(const orc_antigen* A, const orc_params* prm, int n_cand, int n_h, int n_l, uint8_t* aa_h,
+                float* chi_h, float* pos_h, const uint8_t* cdr_h, uint8_t* aa_l, float* chi_l, float* pos_l,
+                const uint8_t* cdr_l, const uint32_t* cand_id, int iterations, float target_radius, int acc64,
+                double* out_energy, double* out_margin, int n_threads) {
+    parallel_for(n_cand, n_threads, [&](int64_t c) {
+        Prot H{n_h, aa_h + (size_t)c * n_h, chi_h + (size_t)c * n_h * 4, pos_h + (size_t)c * n_h * SLOTS * 3};
+        Prot L{n_l, aa_l + (size_t)c * n_l, chi_l + (size_t)c * n_l * 4, pos_l + (size_t)c * n_l * SLOTS * 3};
+        const uint32_t id = cand_id ? cand_id[c] : (uint32_t)c;
+        auto copy_of = [](const Prot& P, std::vector<uint8_t>& a, std::vector<float>& ch, std::vector<float>& p) {
+            a.assign(P.aa, P.aa + P.n);
+            ch.assign(P.chi, P.chi + (size_t)P.n * 4);
+            p.assign(P.pos, P.pos + (size_t)P.n * SLOTS * 3);
+            return Prot{P.n, a.data(), ch.data(), p.data()};
+        };
+        auto put = [](Prot& P, const Prot& S) {
+            std::copy(S.aa, S.aa + P.n, P.aa);
+            std::copy(S.chi, S.chi + (size_t)P.n * 4, P.chi);
+            std::copy(S.pos, S.pos + (size_t)P.n * SLOTS * 3, P.pos);
+        };
+        std::vector<uint8_t> bha, bla, sa;
+        std::vector<float> bhc, bhp, blc, blp, sc, sp;
+        Prot BH = copy_of(H, bha, bhc, bhp), BL = copy_of(L, bla, blc, blp);
+        double best = fv_energy(A, H, L, acc64), margin = INFINITY;
+        for (int it = 0; it < iterations; ++it) {
+            const float temp = orc_temperature(it, iterations);
+            {
+                Prot snap = copy_of(L, sa, sc, sp);
+                if (prm->accumulate == 1) fv_chain_step<float>(A, prm, H, cdr_h, snap, 0, id, (uint32_t)it, temp, target_radius);
+                else fv_chain_step<double>(A, prm, H, cdr_h, snap, 0, id, (uint32_t)it, temp, target_radius);
+            }
+            {
+                Prot snap = copy_of(H, sa, sc, sp);
+                if (prm->accumulate == 1) fv_chain_step<float>(A, prm, L, cdr_l, snap, 1, id, (uint32_t)it, temp, target_radius);
+                else fv_chain_step<double>(A, prm, L, cdr_l, snap, 1, id, (uint32_t)it, temp, target_radius);
+            }
+            const double e = fv_energy(A, H, L, acc64);
+            margin = std::min(margin, std::fabs(e - best) / std::max(std::fabs(best), 1.0));
+            if (e < best) {
+                best = e;
+                put(BH, H);
+                put(BL, L);
+            } else if (e > best) {
+                put(H, BH);
+                put(L, BL);
+            }
+        }
+        put(H, BH);
+        put(L, BL);
+        out_energy[c] = best;
+        if (out_margin) out_margin[c] = margin;
+    });
+}
+
+double orc_fv_energy(const orc_antigen* A, int n_h, const uint8_t* aa_h, const float* pos_h, int n_l,
+                     const uint8_t* aa_l, const float* pos_l, int acc64) {
+    std::vector<float> ch((size_t)n_h * 4), cl((size_t)n_l * 4);
+    Prot H{n_h, const_cast<uint8_t*>(aa_h), ch.data(), const_cast<float*>(pos_h)};
+    Prot L{n_l, const_cast<uint8_t*>(aa_l), cl.data(), const_cast<float*>(pos_l)};
+    return fv_energy(A, H, L, acc64);
 }
 
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx) {

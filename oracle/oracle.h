@@ -175,6 +175,20 @@ void orc_affinity_maturation(const orc_antigen*, int n_cand, int n_res, uint8_t*
    of one slot-layout protein */
 void orc_validate(int n_res, const uint8_t* aa, const float* pos, int32_t* clashes, int32_t* rama);
 
+/* ---- Fv two-chain engine (diffusion.rs:477-827) ----
+   The run_fv iteration loop (diffusion.rs:791-812) of every candidate: heavy chain
+   (n_h residues, cdr_h[r] != 0 for CDR positions) and light chain stepped in turn by
+   fv_chain_step against the antigen and the other chain, elitist on fv_energy
+   (acc64: its f64 re-evaluation); the Metropolis sums follow prm->accumulate.
+   Chains in place (the best pair); out_energy = the best fv_energy. */
+void orc_fv_run(const orc_antigen*, const orc_params* prm, int n_cand, int n_h, int n_l, uint8_t* aa_h,
+                float* chi_h, float* pos_h, const uint8_t* cdr_h, uint8_t* aa_l, float* chi_l, float* pos_l,
+                const uint8_t* cdr_l, const uint32_t* cand_id, int iterations, float target_radius, int acc64,
+                double* out_energy, double* out_margin, int n_threads);
+/* fv_energy (diffusion.rs:541-547) of one heavy / light pair */
+double orc_fv_energy(const orc_antigen*, int n_h, const uint8_t* aa_h, const float* pos_h, int n_l,
+                     const uint8_t* aa_l, const float* pos_l, int acc64);
+
 /* stable ascending sort of energies, NaN last; first k indices (diffusion.rs:1045-1047) */
 void orc_topk(const double* e, int64_t n, int64_t k, int32_t* out_idx);
 

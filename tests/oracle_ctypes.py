@@ -39,6 +39,7 @@ def lib():
         _L.orc_antigen_new.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float]
         _L.orc_antigen_free.argtypes = [C.c_void_p]
         _L.orc_topology_size.restype = C.c_int
+        _L.orc_fv_energy.restype = C.c_double
         for fn in ("orc_residue_contribution", "orc_residue_contribution64"):
             getattr(_L, fn).argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         _L.orc_disulfide.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
@@ -342,6 +343,27 @@ class Antigen:
         lib().orc_affinity_maturation(C.c_void_p(self.h), n_cand, n_res, P(aa), P(chi), P(pos), int(acc64), P(out),
                                       P(kept), P(margin), threads)
         return (out, kept, margin) if with_margin else (out, kept)
+
+    def fv_run(self, params, heavy, light, iterations, target_radius, cand_id=None, acc64=True, threads=8):
+        """The run_fv iteration loop (diffusion.rs:791-812); heavy / light = (aa, chi,
+        pos, cdr) stacked over candidates, updated in place to the best pairs.
+        Returns (best fv_energy, smallest relative keep / restore margin) per candidate."""
+        (ha, hc, hp, hr), (la, lc, lp, lr) = heavy, light
+        n_cand = len(cand_id)
+        n_h, n_l = len(hr) // n_cand, len(lr) // n_cand
+        out = np.zeros(n_cand, np.float64)
+        margin = np.zeros(n_cand, np.float64)
+        cid = np.ascontiguousarray(cand_id, np.uint32)
+        lib().orc_fv_run(C.c_void_p(self.h), C.byref(params), n_cand, n_h, n_l, P(ha), P(hc), P(hp), P(u8(hr)),
+                         P(la), P(lc), P(lp), P(u8(lr)), P(cid), iterations, C.c_float(target_radius), int(acc64),
+                         P(out), P(margin), threads)
+        return out, margin
+
+    def fv_energy(self, h_aa, h_pos, l_aa, l_pos, acc64=True):
+        """fv_energy (diffusion.rs:541-547) of one heavy / light pair"""
+        h_aa, h_pos, l_aa, l_pos = u8(h_aa), f32(h_pos), u8(l_aa), f32(l_pos)
+        return lib().orc_fv_energy(C.c_void_p(self.h), len(h_aa), P(h_aa), P(h_pos), len(l_aa), P(l_aa), P(l_pos),
+                                   int(acc64))
 
     def score_slots64(self, aa, pos, n_res, full=False, threads=8, with_abs=False):
         """f64 energy per candidate; with_abs also the sum of |pair term| (the
