@@ -86,6 +86,10 @@ struct AnSmem {
     int* cglist;                    // LR x CG_LIST_MAX: Verlet lists of the Langevin force
     float4* cgcentre;               // LR: list centre, skin
     int* cgnl;                      // LR: list length (-1: none yet)
+    // Fv two-chain steps: the partner chain's Calphas, as Calpha atoms (ptq, ptp: the
+    // agq / agp layout) and as residue-level bodies of the CG force (pcq, pcp: the
+    // AgView::ca_pq / ca_prm layout); R each
+    float4 *ptq, *ptp, *pcq, *pcp;
 };
 // Entries of each staged x / y / z array: room for the pad, a multiple of 4 (the
 // arrays after them keep their 16-byte alignment).
@@ -98,7 +102,7 @@ __host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
     const size_t t = (size_t)L * CG_SLOTS * 16;
     return learned && t < (size_t)MT_BYTES ? (size_t)MT_BYTES : t;
 }
-__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned) {
+__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned, int fv = 0) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
     return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + anneal_terms_bytes(R, learned) +
            (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + (size_t)anneal_xyz_len(G) * 12 +
@@ -106,9 +110,10 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
            (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1 + MLP_BIASES) * 4 : 0) +
-           15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4);  // 15: alignment of cgcentre
+           15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4) +  // 15: alignment of cgcentre
+           (fv ? 15 + (size_t)R * 64 : 0);
 }
-__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned) {
+__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned, int fv = 0) {
     AnSmem s;
     const int L = min(R, CG_RES_PER_PASS) * CG_LANES;
     auto take = [&](size_t bytes) { unsigned char* p = b; b += bytes; return p; };
@@ -159,6 +164,14 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.cgcentre = (float4*)take((size_t)LR * 16);
     s.cglist = (int*)take((size_t)LR * CG_LIST_MAX * 4);
     s.cgnl = (int*)take((size_t)LR * 4);
+    s.ptq = s.ptp = s.pcq = s.pcp = nullptr;
+    if (fv) {
+        b = (unsigned char*)(((uintptr_t)b + 15) & ~(uintptr_t)15);
+        s.ptq = (float4*)take((size_t)R * 16);
+        s.ptp = (float4*)take((size_t)R * 16);
+        s.pcq = (float4*)take((size_t)R * 16);
+        s.pcp = (float4*)take((size_t)R * 16);
+    }
     return s;
 }
 
@@ -677,16 +690,24 @@ __device__ __noinline__ void an_learned_choices(unsigned char* smem, int R, int 
 
 // EXT: the learned proposal and the proposal log are compiled in (a separate
 // instance, so the plain kernel carries none of their registers).
-template <class ACC, bool EXT>
+// FV: one chain of each Fv candidate (fv_chain_step, diffusion.rs:560-698): the
+// resident state interleaves heavy (2i) and light (2i + 1) chains, this launch steps
+// chains 2 * blockIdx.x + fv_chain against the antigen and the other chain of the pair
+// as it is in the state; Calpha energies gain the partner chain's contribution, the
+// force its compute_forces term, and the mutation / rotamer moves follow the CDR
+// flags fv_cdr (per residue) instead of the interface mask.  Draw streams + 4 * chain.
+template <class ACC, bool EXT, bool FV>
 __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                        int n_steps, uint32_t step0, int with_noise,
                                                        const float* __restrict__ temps, int R, int G, int C,
                                                        uint32_t* __restrict__ err, long long* __restrict__ stats,
                                                        MlpDev mlp, int learned, MlpTuple* __restrict__ tlog,
-                                                       unsigned long long* __restrict__ log_n, long long log_cap) {
+                                                       unsigned long long* __restrict__ log_n, long long log_cap,
+                                                       int fv_chain, const uint8_t* __restrict__ fv_cdr) {
     extern __shared__ __align__(16) unsigned char an_smem[];
-    const AnSmem S = carve(an_smem, R, G, C, learned);
-    const int c = blockIdx.x;
+    const AnSmem S = carve(an_smem, R, G, C, learned, FV ? 1 : 0);
+    const int c = FV ? 2 * (int)blockIdx.x + fv_chain : (int)blockIdx.x;
+    const uint32_t sh = FV ? 4u * (uint32_t)fv_chain : 0u;  // draw stream offset of the chain
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = st.cand_res_off[c];
     const int n = st.cand_res_off[c + 1] - r0;
@@ -726,11 +747,31 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     const float4* agq = staged ? S.agq : A.ca_atom;
     const float4* agp = staged ? S.agp : A.ca_atom_prm;
     float4* stage = S.stage + warp * STAGE_CAP;
+    // Fv: the partner chain's Calphas (it does not move during this launch)
+    int np = 0;
+    if (FV) {
+        const int pc = c ^ 1, p0 = st.cand_res_off[pc];
+        np = min(st.cand_res_off[pc + 1] - p0, R);
+        for (int i = tid; i < np; i += AN_THREADS) {
+            const float4 v = st.res_pos[(size_t)(p0 + i) * SLOT_STRIDE + 1];
+            const int a = st.res_aa[p0 + i];
+            const float4 q = s_ca_atom[a], rl = s_res[a];
+            S.ptq[i] = make_float4(v.x, v.y, v.z, q.x);
+            S.ptp[i] = make_float4(q.y, q.z, q.w, (float)s_ca_type[a]);
+            S.pcq[i] = make_float4(v.x, v.y, v.z, rl.x);
+            S.pcp[i] = make_float4(rl.y, rl.z, rl.w, 0.f);
+        }
+        __syncthreads();
+    }
     // residue_contribution_allatom of a Calpha at q with amino acid a, by the warp (the
-    // scans are noinline: one copy each instead of one per call site, less code to fetch)
+    // scans are noinline: one copy each instead of one per call site, less code to fetch);
+    // Fv: plus the contribution against the partner chain (fv_residue_contribution,
+    // diffusion.rs:551-553)
     auto ca_energy = [&](F3 q, int a) -> ACC {
-        return staged ? warp_contribution_pairs<ACC>(S.agx, S.agy, S.agz, agq, agp, nag, q, a, stage)
-                      : warp_contribution<ACC>(agq, agp, nag, q, a, stage);
+        ACC e = staged ? warp_contribution_pairs<ACC>(S.agx, S.agy, S.agz, agq, agp, nag, q, a, stage)
+                       : warp_contribution<ACC>(agq, agp, nag, q, a, stage);
+        if (FV) e = e + warp_contribution<ACC>(S.ptq, S.ptp, np, q, a, stage);
+        return e;
     };
 
     for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
@@ -782,6 +823,13 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
                                    S.tcount + g0, S.terms + (size_t)g0 * CG_SLOTS, fx, fy, fz);
                 }
                 if (gl == 0) {
+                    if (FV) {  // VH-VL packing force: compute_forces over the partner's Calphas
+                        float px = 0.0f, py = 0.0f, pz = 0.0f;
+                        for (int i = 0; i < np; ++i) cg_term(body, S.pcq[i], S.pcp[i], px, py, pz);
+                        fx = xadd(fx, px);
+                        fy = xadd(fy, py);
+                        fz = xadd(fz, pz);
+                    }
                     const float dx_c = xsub(ca.x, A.cx), dy_c = xsub(ca.y, A.cy), dz_c = xsub(ca.z, A.cz);
                     const float d = fmaxf(xsqrt(xdist2(dx_c, dy_c, dz_c)), 0.001f);
                     const float f_r = xdiv(xmul(-p.restraint_k, xsub(d, p.shell_radius)), d);
@@ -791,7 +839,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
                     float nx = 0.f, ny = 0.f, nz = 0.f;
                     if (with_noise) {
                         const float sigma = xmul(p.noise_base, xsqrt(temp));
-                        const U4 u = rng_draw(p.seed, cid, step, STREAM_NOISE, (uint32_t)r);
+                        const U4 u = rng_draw(p.seed, cid, step, STREAM_NOISE + sh, (uint32_t)r);
                         nx = frange(u.x, -sigma, sigma);
                         ny = frange(u.y, -sigma, sigma);
                         nz = frange(u.z, -sigma, sigma);
@@ -824,8 +872,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         }
         __syncthreads();
 
-        // ---- 2. interface mask (diffusion.rs:343-351) + move draws ----
-        for (int r = warp; r < n; r += AN_WARPS) {
+        // ---- 2. interface mask (diffusion.rs:343-351; Fv: CDR flags instead) + move draws ----
+        for (int r = warp; !FV && r < n; r += AN_WARPS) {
             const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
             bool hit = false;
             for (int base = 0; base < nag && !hit; base += 64) {
@@ -843,7 +891,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             if (lane == 0) S.iface[r] = hit;
         }
         for (int r = tid; r < n; r += AN_THREADS) {
-            const U4 d = rng_draw(p.seed, cid, step, STREAM_BACKBONE, (uint32_t)r);
+            const U4 d = rng_draw(p.seed, cid, step, STREAM_BACKBONE + sh, (uint32_t)r);
             const bool att = u01(d.x) < p.backbone_move_p;
             S.bb_att[r] = att;
             if (att) {
@@ -858,13 +906,33 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
 
         // ---- 3. mutation / rotamer proposals (diffusion.rs:354-399) ----
         for (int r = tid; r < n; r += AN_THREADS) {
-            const bool itf = S.iface[r] != 0;
-            const float eff_mut_p = itf ? xmul(p.mutation_p, 3.0f) : xmul(p.mutation_p, 0.4f);
-            const float eff_rot_p = itf ? xmul(p.rotamer_move_p, 2.0f) : p.rotamer_move_p;
-            const U4 d = rng_draw(p.seed, cid, step, STREAM_MC, (uint32_t)r);
+            const U4 d = rng_draw(p.seed, cid, step, STREAM_MC + sh, (uint32_t)r);
             const int aa = S.aa[r];
             int kind = MV_NONE;
-            if (u01(d.x) < eff_mut_p) {
+            if (FV) {
+                // CDR positions: mutation / rotamer moves (MUTATION_P * 3, ROTAMER_MOVE_P * 2);
+                // every residue without one: rotamer relaxation (ROTAMER_MOVE_P * 0.3)
+                if (fv_cdr[r0 + r] && u01(d.x) < xmul(p.mutation_p, 3.0f)) {
+                    if (u01(d.y) < xmul(p.rotamer_move_p, 2.0f)) {
+                        if (s_rot_n[aa] > 0) kind = MV_ROT;
+                    } else {
+                        kind = MV_MUT;
+                    }
+                } else if (u01(d.y) < xmul(p.rotamer_move_p, 0.3f) && s_rot_n[aa] > 0) {
+                    kind = MV_ROT;
+                }
+                if (kind == MV_ROT) {
+                    S.new_rot[r] = (int)urange(d.z, (uint32_t)s_rot_n[aa]);
+                    S.new_aa[r] = aa;
+                } else if (kind == MV_MUT) {
+                    S.new_aa[r] = (int)urange(d.z, (uint32_t)N_AA);
+                    S.new_rot[r] = 0;
+                }
+            }
+            const bool itf = !FV && S.iface[r] != 0;
+            const float eff_mut_p = itf ? xmul(p.mutation_p, 3.0f) : xmul(p.mutation_p, 0.4f);
+            const float eff_rot_p = itf ? xmul(p.rotamer_move_p, 2.0f) : p.rotamer_move_p;
+            if (!FV && u01(d.x) < eff_mut_p) {
                 if (u01(d.y) < eff_rot_p) {
                     if (s_rot_n[aa] > 0) {
                         kind = MV_ROT;
@@ -1129,23 +1197,28 @@ size_t anneal_smem(int max_res, int max_ag_res, int max_cells, int learned) {
 
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x) {
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x,
+                          int fv_chain, const uint8_t* fv_cdr) {
     if (st.n_cand <= 0 || n_steps <= 0 || max_res <= 0) return cudaSuccess;
     const int G = max_ag_res <= AG_STAGE_MAX ? max_ag_res : 0;
     const int C = G && max_cells <= CELL_STAGE_MAX ? max_cells : 0;
-    const int learned = x.learned ? 1 : 0;
-    const size_t smem = anneal_smem_bytes(max_res, G, C, learned);
-    const bool ext = x.learned || x.log;
+    const bool fv = fv_chain >= 0;
+    const int learned = x.learned && !fv ? 1 : 0;
+    const size_t smem = anneal_smem_bytes(max_res, G, C, learned, fv ? 1 : 0);
+    const bool ext = !fv && (x.learned || x.log);
+    const int grid = fv ? st.n_cand / 2 : st.n_cand;
+    if (grid <= 0) return cudaSuccess;
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e) return e;
-        kern<<<st.n_cand, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G, C, err,
-                                                 stats, x.mlp, learned, x.log, x.log_n, x.log_cap);
+        kern<<<grid, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G, C, err, stats,
+                                            x.mlp, learned, x.log, x.log_n, x.log_cap, fv ? fv_chain : 0, fv_cdr);
         return cudaSuccess;
     };
     cudaError_t e;
-    if (accumulate == 1) e = ext ? run(k_anneal<float, true>) : run(k_anneal<float, false>);
-    else e = ext ? run(k_anneal<double, true>) : run(k_anneal<double, false>);
+    if (fv) e = accumulate == 1 ? run(k_anneal<float, false, true>) : run(k_anneal<double, false, true>);
+    else if (accumulate == 1) e = ext ? run(k_anneal<float, true, false>) : run(k_anneal<float, false, false>);
+    else e = ext ? run(k_anneal<double, true, false>) : run(k_anneal<double, false, false>);
     if (e) return e;
     return cudaGetLastError();
 }

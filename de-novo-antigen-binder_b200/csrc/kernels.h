@@ -115,9 +115,11 @@ struct AnnealExtras {
 // accumulate: 1 = the reference's f32 sums, else f32 terms summed in double.
 // stats (may be null): 4 per candidate, += mutation/rotamer tried, accepted,
 // backbone tried, accepted.
+// fv_chain >= 0: the Fv two-chain step of chains 2i + fv_chain (fv_cdr: CDR flag per residue)
 cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                           uint32_t step0, int with_noise, const float* temps, int accumulate, int max_res,
-                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x);
+                          int max_ag_res, int max_cells, uint32_t* err, long long* stats, const AnnealExtras& x,
+                          int fv_chain = -1, const uint8_t* fv_cdr = nullptr);
 
 // ---- k_mlp.cu: the learned proposal network (features, tcgen05 GEMM, training) ----
 cudaError_t mlp_init_tables(const float* log1p_table);

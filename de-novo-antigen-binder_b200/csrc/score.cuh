@@ -160,6 +160,41 @@ __device__ __forceinline__ void group_prm(GroupSmem& s, int lane, int n, float q
     }
 }
 
+// Energy of one pair within the cutoff (r2: the reference's rounding of r^2):
+// candidate atom b / bp, antigen atom a / ap, each (x, y, z, q sqrt(332)) and
+// (r_min_half, sqrt(epsilon), hydrophobic, AMBER type).  LJ + Coulomb + hydrophobic
+// (energy.rs:269-301), with FULL the H-bond (energy.rs:303-307) and EEF1 solvation
+// (solvation.rs:34-50: ei the antigen atom's, ej the candidate atom's) terms; the
+// first three are returned in lj, coul, hyd as well.
+template <bool FULL>
+__device__ __forceinline__ float pair_energy(const float4& b, const float4& bp, const float4& a, const float4& ap,
+                                             float r2, float& lj, float& coul, float& hyd) {
+    const float ir = rsqrtf(r2);
+    const float ir2 = ir * ir;
+    const float R = bp.x + ap.x;
+    const float s2 = R * R * ir2;
+    const float s6 = s2 * s2 * s2;
+    lj = (bp.y * ap.y) * (s6 * (s6 - 2.0f));
+    coul = (b.w * a.w) * ir;
+    hyd = (r2 < HYDRO_CUTOFF_SQ) ? HYDRO_BONUS * (bp.z * ap.z) : 0.0f;
+    float e = lj + coul + hyd;
+    if (FULL) {
+        const int bt = (int)bp.w, at = (int)ap.w;
+        if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) && r2 <= HB_CUTOFF_SQ) {
+            const float z = (r2 * ir - HB_R0) / HB_SIGMA;
+            e += -HB_DEPTH * expf(-0.5f * z * z);
+        }
+        const float4 ej = c_eef1[bt];
+        if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
+            const float4 ei = c_eef1[at];
+            const float r = r2 * ir;
+            const float xi = r / ei.z, xj = r / ej.z;
+            e += -(ei.x * ej.y * expf(-(xi * xi)) * ei.w + ej.x * ei.y * expf(-(xj * xj)) * ej.w);
+        }
+    }
+    return e;
+}
+
 // One antigen atom (this lane's) against the n group atoms in shared memory, two
 // group atoms per step: dx = b - a and r^2 = (dx*dx + dy*dy) + dz*dz in packed
 // f32x2 arithmetic, the reference's roundings, hence its pair set; the terms of
@@ -172,32 +207,8 @@ __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const
     float part = 0.0f, pabs = 0.0f;
     int np = 0;
     auto term = [&](int j, float r2) {
-        const float4 b = s.pos[j];
-        const float4 bp = s.prm[j];
-        const float ir = rsqrtf(r2);
-        const float ir2 = ir * ir;
-        const float R = bp.x + ap.x;
-        const float s2 = R * R * ir2;
-        const float s6 = s2 * s2 * s2;
-        const float lj = (bp.y * ap.y) * (s6 * (s6 - 2.0f));
-        const float coul = (b.w * a.w) * ir;
-        const float hyd = (r2 < HYDRO_CUTOFF_SQ) ? HYDRO_BONUS * (bp.z * ap.z) : 0.0f;
-        float e = lj + coul + hyd;
-        if (FULL) {
-            const int bt = (int)bp.w, at = (int)ap.w;
-            if ((((c_hb[bt] & 1) && (c_hb[at] & 2)) || ((c_hb[bt] & 2) && (c_hb[at] & 1))) &&
-                r2 <= HB_CUTOFF_SQ) {
-                const float z = (r2 * ir - HB_R0) / HB_SIGMA;
-                e += -HB_DEPTH * expf(-0.5f * z * z);
-            }
-            const float4 ej = c_eef1[bt];
-            if (r2 < SOLV_CUTOFF_SQ && !(ej.y == 0.0f && ej.x == 0.0f)) {
-                const float4 ei = c_eef1[at];
-                const float r = r2 * ir;
-                const float xi = r / ei.z, xj = r / ej.z;
-                e += -(ei.x * ej.y * expf(-(xi * xi)) * ei.w + ej.x * ei.y * expf(-(xj * xj)) * ej.w);
-            }
-        }
+        float lj, coul, hyd;
+        const float e = pair_energy<FULL>(s.pos[j], s.prm[j], a, ap, r2, lj, coul, hyd);
         part += e;
         if (ABS) pabs += fabsf(lj) + fabsf(coul) + fabsf(hyd);
         if (COUNT) ++np;
