@@ -185,6 +185,9 @@ _SIGS = {
     "binder_debug_fail_alloc": (C.c_int, [C.c_int64]),
     "binder_minimize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "binder_validate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "binder_fv_upload": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int32, C.c_int32] + [C.c_void_p] * 8 +
+                         [C.c_int32, C.c_void_p]),
+    "binder_fv_run": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "binder_parse_pdb_text": (C.c_int, [C.c_char_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
                                         C.POINTER(C.c_size_t)]),
     "binder_parse_pdb_file": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -620,6 +623,41 @@ class GpuContext:
         kept = np.zeros(self._state_cand, np.int32)
         self._check(lib().binder_affinity_maturation(self._h, _ptr(out), _ptr(kept)))
         return out, kept
+
+    def fv_upload(self, heavy, light, antigen_id=0, cand_id=None):
+        """Upload an Fv population: heavy / light = (aa, chi, pos, cdr) stacked over the
+        candidates (uniform chain lengths).  The state then interleaves heavy 2i and
+        light 2i + 1."""
+        (ha, hc, hp, hr), (la, lc, lp, lr) = heavy, light
+        ha, la, hr, lr = _u8(ha), _u8(la), _u8(hr), _u8(lr)
+        hc, hp, lc, lp = _f32(hc), _f32(hp), _f32(lc), _f32(lp)
+        n = len(cand_id) if cand_id is not None else None
+        if n is None:
+            raise ValueError("cand_id (one per candidate) is required")
+        n_h, n_l = len(ha) // n, len(la) // n
+        cid = np.ascontiguousarray(cand_id, np.uint32)
+        self._check(lib().binder_fv_upload(self._h, n, n_h, n_l, _ptr(ha), _ptr(hc), _ptr(hp), _ptr(hr), _ptr(la),
+                                           _ptr(lc), _ptr(lp), _ptr(lr), antigen_id, _ptr(cid)))
+        self._state_res = n * (n_h + n_l)
+        self._state_cand = 2 * n
+        self._fv = (n, n_h, n_l)
+
+    def fv_run(self, iterations):
+        """run_fv's iteration loop on the uploaded population; returns the best
+        fv_energy per candidate (the state holds the best pairs)."""
+        n = self._fv[0]
+        out = np.zeros(n, np.float64)
+        self._check(lib().binder_fv_run(self._h, int(iterations), _ptr(out)))
+        return out
+
+    def fv_download(self):
+        """(heavy, light) = ((aa, chi, pos), (aa, chi, pos)) of the resident Fv pairs."""
+        n, n_h, n_l = self._fv
+        aa, chi, pos = self.state_download()
+        per = n_h + n_l
+        idx_h = (np.arange(n)[:, None] * per + np.arange(n_h)).ravel()
+        idx_l = (np.arange(n)[:, None] * per + n_h + np.arange(n_l)).ravel()
+        return (aa[idx_h], chi[idx_h], pos[idx_h]), (aa[idx_l], chi[idx_l], pos[idx_l])
 
     def validate(self):
         """ValidationReport::assess (validate.rs:24-132) of every resident candidate:

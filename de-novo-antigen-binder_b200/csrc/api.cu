@@ -246,6 +246,13 @@ struct binder_ctx {
     // antigen-set epoch (device word read by the gradient-step kernel)
     DBuf<int> d_ag_epoch;
     int ag_epoch = 0;
+    // Fv two-chain population (binder_fv_upload): the state interleaves the heavy (2i)
+    // and light (2i + 1) chains of fv_pairs candidates; CDR flag per residue; the best
+    // pairs of binder_fv_run
+    int fv_pairs = 0;
+    DBuf<uint8_t> fv_cdr, fv_baa;
+    DBuf<double> fv_best, fv_pair_e;
+    DBuf<float4> fv_bpos, fv_bchi, fv_btrig;
     // binder_block_io: the state download runs on a second stream beside the score
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1171,6 +1178,7 @@ static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_re
     if (aa_max >= N_AA) return fail(ctx, BINDER_ERR_ARG, "amino acid out of range");
     // a population of the same shape (candidates, residue counts, antigens, ids)
     // against the same antigen set keeps the device metadata; only the residues move
+    ctx->fv_pairs = 0;  // a new population (binder_fv_upload sets it again for an Fv one)
     const bool same_meta = S.n_cand == (int)n_cand && S.meta_epoch == ctx->ag_epoch && S.h_res_off == off &&
                            S.h_cand_ag == ag && S.h_cand_id == ids && S.h_orig == orig;
     if (same_meta) S.order_valid = false;
@@ -1219,6 +1227,7 @@ int binder_state_select(binder_ctx* ctx, const int32_t* idx, size_t n) {
         for (int r = S.h_res_off[c]; r < S.h_res_off[c + 1]; ++r) map.push_back(r);
     }
     const int total = off[n];
+    ctx->fv_pairs = 0;
     // gather residues (and statistics) into the alternate buffers, then swap them in;
     // chi sin/cos are gathered when current, else derived later for the selection only
     const bool trig = S.trig_valid && S.res_trig.p;
@@ -1970,6 +1979,112 @@ int binder_validate(binder_ctx* ctx, int32_t* out_clashes, int32_t* out_rama) {
         if (out_clashes) out_clashes[c] = h[c];
         if (out_rama) out_rama[c] = h[S.n_cand + c];
     }
+    return BINDER_OK;
+}
+
+int binder_fv_upload(binder_ctx* ctx, size_t n_cand, int32_t n_heavy, int32_t n_light, const uint8_t* aa_h,
+                     const float* chi_h, const float* pos_h, const uint8_t* cdr_h, const uint8_t* aa_l,
+                     const float* chi_l, const float* pos_l, const uint8_t* cdr_l, int32_t antigen_id,
+                     const uint32_t* cand_id) {
+    int s = enter(ctx);
+    if (s) return s;
+    if (n_cand == 0 || n_heavy <= 0 || n_light <= 0 || n_heavy > ANNEAL_MAX_RES || n_light > ANNEAL_MAX_RES)
+        return fail(ctx, BINDER_ERR_ARG, "Fv chains hold 1..%d residues", ANNEAL_MAX_RES);
+    if (!aa_h || !chi_h || !pos_h || !cdr_h || !aa_l || !chi_l || !pos_l || !cdr_l)
+        return fail(ctx, BINDER_ERR_ARG, "NULL chain array");
+    // interleave: chain 2i = heavy i, 2i + 1 = light i; both chains draw with candidate id i
+    const size_t per = (size_t)n_heavy + n_light, total = n_cand * per;
+    std::vector<int32_t> nres(2 * n_cand), agid(2 * n_cand, antigen_id);
+    std::vector<uint32_t> ids(2 * n_cand);
+    std::vector<uint8_t> aa(total), cdr(total);
+    std::vector<float> chi(total * 4), pos(total * SLOTS * 3);
+    for (size_t i = 0; i < n_cand; ++i) {
+        nres[2 * i] = n_heavy;
+        nres[2 * i + 1] = n_light;
+        ids[2 * i] = ids[2 * i + 1] = cand_id ? cand_id[i] : (uint32_t)i;
+        const size_t o = i * per;
+        std::memcpy(&aa[o], aa_h + i * n_heavy, n_heavy);
+        std::memcpy(&aa[o + n_heavy], aa_l + i * n_light, n_light);
+        std::memcpy(&cdr[o], cdr_h + i * n_heavy, n_heavy);
+        std::memcpy(&cdr[o + n_heavy], cdr_l + i * n_light, n_light);
+        std::memcpy(&chi[o * 4], chi_h + i * n_heavy * 4, n_heavy * 16);
+        std::memcpy(&chi[(o + n_heavy) * 4], chi_l + i * n_light * 4, n_light * 16);
+        std::memcpy(&pos[o * SLOTS * 3], pos_h + i * n_heavy * SLOTS * 3, (size_t)n_heavy * SLOTS * 12);
+        std::memcpy(&pos[(o + n_heavy) * SLOTS * 3], pos_l + i * n_light * SLOTS * 3, (size_t)n_light * SLOTS * 12);
+    }
+    if ((s = state_upload_impl(ctx, 2 * n_cand, nres.data(), 0, agid.data(), ids.data(), aa.data(), chi.data(),
+                                pos.data(), true)))
+        return s;
+    if ((s = upload(ctx, ctx->fv_cdr, cdr.data(), total, "cdr"))) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    ctx->fv_pairs = (int)n_cand;
+    return BINDER_OK;
+}
+
+int binder_fv_run(binder_ctx* ctx, int iterations, double* out_energy) {
+    int s = enter(ctx);
+    if (s) return s;
+    State& S = ctx->st;
+    if (ctx->fv_pairs <= 0 || S.n_cand != 2 * ctx->fv_pairs)
+        return fail(ctx, BINDER_ERR_STATE, "no Fv population uploaded");
+    if (iterations < 0) return fail(ctx, BINDER_ERR_ARG, "negative iteration count");
+    const int np = ctx->fv_pairs;
+    if ((s = ensure_trig(ctx))) return s;
+    if ((s = clear_err(ctx))) return s;
+    // temperature (diffusion.rs:102-104) of every iteration (diffusion.rs:792)
+    const binder_params& P = ctx->params;
+    std::vector<float> t(std::max(iterations, 1));
+    for (int it = 0; it < iterations; ++it)
+        t[it] = P.t_hot * std::pow(P.t_cold / P.t_hot, (float)it / (float)iterations);
+    if ((s = upload(ctx, ctx->temps, t.data(), t.size(), "temps"))) return s;
+    CK(ctx->energy.ensure(S.n_cand), "alloc");
+    CK(ctx->fv_best.ensure(np), "alloc");
+    CK(ctx->fv_pair_e.ensure(np), "alloc");
+    CK(ctx->fv_bpos.ensure((size_t)S.total_res * SLOT_STRIDE), "alloc");
+    CK(ctx->fv_baa.ensure(S.total_res), "alloc");
+    CK(ctx->fv_bchi.ensure(S.total_res), "alloc");
+    CK(ctx->fv_btrig.ensure(2 * (size_t)S.total_res), "alloc");
+    int max_ag = 0, max_cells = 0;
+    for (const auto& a : ctx->ags) {
+        const GridView& g = a->view.ca_grid;
+        max_ag = std::max(max_ag, a->n_res);
+        max_cells = std::max(max_cells, g.nx * g.ny * g.nz + 1);
+    }
+    const StepParams sp = step_params(P);
+    AnnealExtras none;
+    // fv_energy of the pairs as they are (the first best)
+    auto energies_and_keep = [&](int restore) -> int {
+        int st_ = enqueue_score_state(ctx, 1);  // each chain vs the antigen + its disulfide term
+        if (st_) return st_;
+        launch_fv_pair(ctx->stream, S.view(), ctx->fv_pair_e.p);
+        LAUNCHED("fv_pair");
+        launch_fv_keep(ctx->stream, S.view(), ctx->energy.p, ctx->fv_pair_e.p, ctx->fv_best.p, ctx->fv_bpos.p,
+                       ctx->fv_baa.p, ctx->fv_bchi.p, ctx->fv_btrig.p, restore);
+        LAUNCHED("fv_keep");
+        return BINDER_OK;
+    };
+    if ((s = energies_and_keep(2))) return s;
+    for (int it = 0; it < iterations; ++it) {
+        // heavy chains against the light chains as they are, then light against heavy
+        for (int chain = 0; chain < 2; ++chain) {
+            CK(launch_anneal(ctx->stream, S.view(), ctx->d_views.p, sp, 1, (uint32_t)it, 1, ctx->temps.p + it,
+                             P.accumulate, S.max_res, max_ag, max_cells, ctx->errf.p, S.mc_stats.p, none, chain,
+                             ctx->fv_cdr.p),
+               "fv step");
+            LAUNCHED("fv_step");
+        }
+        if ((s = energies_and_keep(0))) return s;
+    }
+    // the result is the best pair of every candidate
+    launch_fv_keep(ctx->stream, S.view(), ctx->energy.p, ctx->fv_pair_e.p, ctx->fv_best.p, ctx->fv_bpos.p,
+                   ctx->fv_baa.p, ctx->fv_bchi.p, ctx->fv_btrig.p, 1);
+    LAUNCHED("fv_keep");
+    S.order_valid = false;
+    if ((s = check_err(ctx))) return s;
+    if (out_energy)
+        CK(cudaMemcpyAsync(out_energy, ctx->fv_best.p, np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+           "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
     return BINDER_OK;
 }
 

@@ -276,6 +276,134 @@ void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, doubl
     if (st.n_cand > 0) k_mature<<<st.n_cand, MAT_WARPS * 32, 0, s>>>(st, ags, res_e, out_best, out_kept, err);
 }
 
+// ---- Fv two-chain engine (diffusion.rs:477-827) -----------------------------------------
+// The resident state interleaves the heavy (2i) and light (2i + 1) chain of each Fv
+// candidate i.
+constexpr int FVP_THREADS = 256;
+constexpr int FVP_MAX_RES = 160;  // residues of a chain the pair kernel stages
+
+// interaction_energy_atoms (energy.rs:256-314, solvation.rs:52-84) between the two chains
+// of candidate i (heavy as energy.rs's "antigen", light as its "antibody"), all five
+// terms, FP64 total; residue pairs whose bounding spheres are further apart than the
+// cutoff are skipped (they hold no pair within 10 A).
+__global__ void __launch_bounds__(FVP_THREADS) k_fv_pair(StateView st, double* __restrict__ out) {
+    const int i = blockIdx.x;
+    const int h0 = st.cand_res_off[2 * i], nh = st.cand_res_off[2 * i + 1] - h0;
+    const int l0 = st.cand_res_off[2 * i + 1], nl = st.cand_res_off[2 * i + 2] - l0;
+    __shared__ float4 s_c[2][FVP_MAX_RES];  // residue centroid, radius
+    __shared__ double s_sum[FVP_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (nh > FVP_MAX_RES || nl > FVP_MAX_RES) {
+        if (threadIdx.x == 0) out[i] = nan("");
+        return;
+    }
+    for (int t = threadIdx.x; t < nh + nl; t += blockDim.x) {
+        const int r = t < nh ? h0 + t : l0 + (t - nh);
+        const int na = c_topo_n[st.res_aa[r]];
+        const float4* p = st.res_pos + (size_t)r * SLOT_STRIDE;
+        float cx = 0.f, cy = 0.f, cz = 0.f;
+        for (int k = 0; k < na; ++k) {
+            cx += p[k].x; cy += p[k].y; cz += p[k].z;
+        }
+        cx /= na; cy /= na; cz /= na;
+        float rad = 0.f;
+        for (int k = 0; k < na; ++k) {
+            const float dx = p[k].x - cx, dy = p[k].y - cy, dz = p[k].z - cz;
+            rad = fmaxf(rad, sqrtf(dx * dx + dy * dy + dz * dz));
+        }
+        s_c[t < nh ? 0 : 1][t < nh ? t : t - nh] = make_float4(cx, cy, cz, rad * 1.0001f + 1e-3f);
+    }
+    __syncthreads();
+    float s = 0.f, comp = 0.f;  // compensated sum of this thread's pair terms
+    for (int t = threadIdx.x; t < nh * nl; t += blockDim.x) {
+        const int a = t / nl, b = t - a * nl;
+        const float4 ca = s_c[0][a], cb = s_c[1][b];
+        const float dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
+        const float reach = 10.01f + ca.w + cb.w;
+        if (dx * dx + dy * dy + dz * dz > reach * reach) continue;
+        const int aa_a = st.res_aa[h0 + a], aa_b = st.res_aa[l0 + b];
+        const int na = c_topo_n[aa_a], nb = c_topo_n[aa_b];
+        const float4* pa = st.res_pos + (size_t)(h0 + a) * SLOT_STRIDE;
+        const float4* pb = st.res_pos + (size_t)(l0 + b) * SLOT_STRIDE;
+        for (int kb = 0; kb < nb; ++kb) {
+            const float4 m = c_slot_prm[aa_b][kb];
+            const float4 B = make_float4(pb[kb].x, pb[kb].y, pb[kb].z, m.x);
+            const float4 Bp = make_float4(m.y, m.z, m.w, (float)c_slot_type[aa_b][kb]);
+            for (int ka = 0; ka < na; ++ka) {
+                const float4 n = c_slot_prm[aa_a][ka];
+                const float4 A = make_float4(pa[ka].x, pa[ka].y, pa[ka].z, n.x);
+                const float r2 = xdist2(B.x - A.x, B.y - A.y, B.z - A.z);
+                if (r2 > CUTOFF_SQ || r2 < MIN_R_SQ) continue;
+                const float4 Ap = make_float4(n.y, n.z, n.w, (float)c_slot_type[aa_a][ka]);
+                float lj, coul, hyd;
+                const float e = pair_energy<true>(B, Bp, A, Ap, r2, lj, coul, hyd);
+                const float y = e - comp, tt = s + y;
+                comp = (tt - s) - y;
+                s = tt;
+            }
+        }
+    }
+    const double v = warp_sum_d((double)s - (double)comp);
+    if (lane == 0) s_sum[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double e = 0.0;
+        for (int w = 0; w < FVP_THREADS / 32; ++w) e += s_sum[w];
+        out[i] = e;
+    }
+}
+
+// fv_energy = both chains' energies against the antigen (each with its disulfide
+// term) + the pair energy; elitist keep (diffusion.rs:800-810): a lower energy
+// becomes the best pair, a higher one is replaced by the best pair.  mode 1: put the
+// best pair back whatever the energy (the result of run_fv is the best); mode 2: the
+// pair as it is becomes the best (the start of the run, diffusion.rs:788-790).
+__global__ void k_fv_keep(StateView st, const double* __restrict__ e_chain, const double* __restrict__ e_pair,
+                          double* __restrict__ best, float4* __restrict__ b_pos, uint8_t* __restrict__ b_aa,
+                          float4* __restrict__ b_chi, float4* __restrict__ b_trig, int restore) {
+    const int i = blockIdx.x;
+    __shared__ int s_dec;
+    if (threadIdx.x == 0) {
+        const double e = e_chain[2 * i] + e_chain[2 * i + 1] + e_pair[i];
+        int dec = 0;
+        if (restore == 1) dec = -1;
+        else if (restore == 2 || e < best[i]) dec = 1;
+        else if (e > best[i]) dec = -1;
+        if (dec == 1) best[i] = e;
+        s_dec = dec;
+    }
+    __syncthreads();
+    const int dec = s_dec;
+    if (dec == 0) return;
+    const int r0 = st.cand_res_off[2 * i], r1 = st.cand_res_off[2 * i + 2];
+    for (int t = r0 * SLOT_STRIDE + (int)threadIdx.x; t < r1 * SLOT_STRIDE; t += blockDim.x) {
+        if (dec > 0) b_pos[t] = st.res_pos[t];
+        else st.res_pos[t] = b_pos[t];
+    }
+    for (int r = r0 + (int)threadIdx.x; r < r1; r += blockDim.x) {
+        if (dec > 0) {
+            b_aa[r] = st.res_aa[r];
+            b_chi[r] = st.res_chi[r];
+            b_trig[2 * r] = st.res_trig[2 * r];
+            b_trig[2 * r + 1] = st.res_trig[2 * r + 1];
+        } else {
+            st.res_aa[r] = b_aa[r];
+            st.res_chi[r] = b_chi[r];
+            st.res_trig[2 * r] = b_trig[2 * r];
+            st.res_trig[2 * r + 1] = b_trig[2 * r + 1];
+        }
+    }
+}
+
+void launch_fv_pair(cudaStream_t s, const StateView& st, double* out) {
+    if (st.n_cand >= 2) k_fv_pair<<<st.n_cand / 2, FVP_THREADS, 0, s>>>(st, out);
+}
+void launch_fv_keep(cudaStream_t s, const StateView& st, const double* e_chain, const double* e_pair, double* best,
+                    float4* b_pos, uint8_t* b_aa, float4* b_chi, float4* b_trig, int restore) {
+    if (st.n_cand >= 2)
+        k_fv_keep<<<st.n_cand / 2, 256, 0, s>>>(st, e_chain, e_pair, best, b_pos, b_aa, b_chi, b_trig, restore);
+}
+
 // ---- structure validation (validate.rs) ------------------------------------------------
 // Clash test of one atom pair (validate.rs:52-59): d^2 < (0.7 (rmh_i + rmh_j))^2, f32.
 __device__ __forceinline__ bool clash(float4 a, float4 b) {

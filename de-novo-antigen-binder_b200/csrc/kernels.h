@@ -153,6 +153,11 @@ void launch_min_accept(cudaStream_t s, const StateView& st, const float4* trial,
 void launch_mature(cudaStream_t s, const StateView& st, const AgView* ags, double* res_e, double* out_best,
                    int* out_kept, uint32_t* err);
 
+// Fv pairs (chains 2i, 2i + 1 of the state): the all-atom energy between the chains (at
+// most 160 residues per chain, else NaN), and the elitist keep / restore of each pair
+void launch_fv_pair(cudaStream_t s, const StateView& st, double* out);
+void launch_fv_keep(cudaStream_t s, const StateView& st, const double* e_chain, const double* e_pair, double* best,
+                    float4* b_pos, uint8_t* b_aa, float4* b_chi, float4* b_trig, int restore);
 // ValidationReport::assess of every candidate: clash_score and ramachandran_outliers
 // (at most 640 residues per candidate, else cudaErrorInvalidValue and no launch)
 cudaError_t launch_validate(cudaStream_t s, const StateView& st, int* clashes, int* rama);

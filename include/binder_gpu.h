@@ -365,6 +365,29 @@ int binder_minimize(binder_ctx* ctx, int steps, double* out_energy);
    reference returns it, out_mutated int32[n_cand] (may be NULL) = mutations kept. */
 int binder_affinity_maturation(binder_ctx* ctx, double* out_energy, int32_t* out_mutated);
 
+/* ---- Fv two-chain engine (diffusion.rs:477-827) ---------------------------------------
+   Upload n_cand Fv candidates: heavy chains of n_heavy residues and light chains of
+   n_light (each at most 128), slot layout concatenated per chain, cdr_* = nonzero at
+   CDR positions (germline.rs:66-88), all against resident antigen antigen_id;
+   cand_id[i] (NULL = i) is the Philox counter word of candidate i.  The resident state
+   then holds 2 n_cand chains, heavy i at 2i and light i at 2i + 1 (binder_state_download
+   returns them so). */
+int binder_fv_upload(binder_ctx* ctx, size_t n_cand, int32_t n_heavy, int32_t n_light, const uint8_t* aa_h,
+                     const float* chi_h, const float* pos_h, const uint8_t* cdr_h, const uint8_t* aa_l,
+                     const float* chi_l, const float* pos_l, const uint8_t* cdr_l, int32_t antigen_id,
+                     const uint32_t* cand_id);
+/* The iteration loop of run_fv (diffusion.rs:791-812) on the uploaded Fv population:
+   per iteration (temperature(it, iterations)) every heavy chain takes one
+   fv_chain_step (diffusion.rs:560-698: Langevin with the grid force of the antigen and
+   the compute_forces term of the light chain, restraint to params.shell_radius, CDR
+   mutation / rotamer and rotamer-relaxation Metropolis moves, backbone moves, energies
+   against the antigen and the partner), then every light chain against the stepped
+   heavy chain; the pair is kept when fv_energy (diffusion.rs:541-547) drops below its
+   best and put back to the best when it rises.  Draws: Philox with the streams of
+   binder_diffuse offset by 4 for the light chain.  Afterwards the state holds the best
+   pairs; out_energy double[n_cand] (may be NULL) = their fv_energy. */
+int binder_fv_run(binder_ctx* ctx, int iterations, double* out_energy);
+
 /* ---- structure validation (validate.rs:40-132) ---------------------------------------
    ValidationReport::assess of every resident candidate: clash_score (validate.rs:40-63:
    atom pairs of residues more than one apart in sequence closer than 0.7 x the sum of
