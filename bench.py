@@ -703,7 +703,7 @@ def run_learned_anneal_only(args):
 
 def run_block_only(args):
     """Small profiling case for the search block: 3 eagerly issued blocks of the
-    bench workload at launch shape (cg_warps, cg_lanes[, cg_order])."""
+    bench workload at launch shape (cg_warps, cg_lanes[, cg_order[, cg_queue[, cg_flat]]])."""
     import torch
     from __graft_entry__ import load_package
     pkg = load_package()
@@ -711,14 +711,14 @@ def run_block_only(args):
     ctx.set_params(pkg.Params.defaults(flags=0))
     cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, 0)
     shape = [int(x) for x in args.block_only.split(",")]
-    w, lanes, order = (shape + [1])[:3]
-    ctx.set_launch_cfg(8, 4, w, lanes, order)
+    w, lanes, order, queue, flat = (shape + [1, 1, 0][len(shape) - 2:])[:5]  # defaults: order 1, queue 1, flat 0
+    ctx.set_launch_cfg(8, 4, w, lanes, order, 0, queue, flat)
     ctx.state_upload(pop.aa, chi, pos, uniform_n_res=int(pop.n_res[0]))
     for k in range(3):
         ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K)
     torch.cuda.synchronize()
-    print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "cg_order": order, "blocks": 3}}),
-          flush=True)
+    print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "cg_order": order, "cg_queue": queue,
+                                     "cg_flat": flat, "blocks": 3}}), flush=True)
     ctx.close()
     return 0
 
@@ -818,7 +818,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal time-to-target runs")
     ap.add_argument("--phase2-only", type=int, default=0, metavar="STEPS",
                     help="profiling case: one launch of STEPS Langevin + Metropolis steps on 64 candidates")
-    ap.add_argument("--block-only", default="", metavar="WARPS,LANES[,ORDER]",
+    ap.add_argument("--block-only", default="", metavar="WARPS,LANES[,ORDER[,QUEUE[,FLAT]]]",
                     help="profiling case: 3 search blocks at this gradient-step launch shape")
     ap.add_argument("--mlp-only", type=int, default=0, metavar="ROWS",
                     help="profiling case: 3 loss + gradient passes of the proposal network on ROWS rows")
