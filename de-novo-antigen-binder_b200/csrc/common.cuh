@@ -60,6 +60,10 @@ __device__ __forceinline__ float xdist2(float dx, float dy, float dz) {
 
 // Packed pairs of f32 (element 0 in the low word) and the sm_100 two-wide FP32
 // instructions; each element is rounded exactly as the scalar instruction rounds it.
+// A packed multiply feeding a packed add may still be fused by the code generator
+// (measured on sm_100a: a pair at r^2 = 100.000008 in the reference's rounding came
+// out as 100.0), so wherever a result must keep the reference's two roundings the
+// products and sums go through the scalar x* helpers above (f2_dist2 below).
 __device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
     return (uint64_t)__float_as_uint(lo) | ((uint64_t)__float_as_uint(hi) << 32);
 }
@@ -80,6 +84,11 @@ __device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
 }
 __device__ __forceinline__ float f2_lo(uint64_t v) { return __uint_as_float((uint32_t)v); }
 __device__ __forceinline__ float f2_hi(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+// the reference's r^2 of both elements of packed differences (scalar, never fused)
+__device__ __forceinline__ void f2_dist2(uint64_t dx, uint64_t dy, uint64_t dz, float& lo, float& hi) {
+    lo = xdist2(f2_lo(dx), f2_lo(dy), f2_lo(dz));
+    hi = xdist2(f2_hi(dx), f2_hi(dy), f2_hi(dz));
+}
 
 // Transcendentals of the Metropolis path (acceptance exp, H-bond and disulfide
 // Gaussians, rotation by a random torsion): evaluated in double and rounded once

@@ -300,9 +300,7 @@ __device__ __noinline__ ACC warp_contribution_pairs(const float* __restrict__ ax
             const uint64_t dx = f2_sub(cx, *(const uint64_t*)&ax[i]);
             const uint64_t dy = f2_sub(cy, *(const uint64_t*)&ay[i]);
             const uint64_t dz = f2_sub(cz, *(const uint64_t*)&az[i]);
-            const uint64_t r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
-            r0 = f2_lo(r2);
-            r1 = f2_hi(r2);
+            f2_dist2(dx, dy, dz, r0, r1);
             in0 = !(r0 > CUTOFF_SQ || r0 < MIN_R_SQ);
             in1 = i + 1 < nag && !(r1 > CUTOFF_SQ || r1 < MIN_R_SQ);
         }

@@ -196,9 +196,9 @@ __device__ __forceinline__ float pair_energy(const float4& b, const float4& bp, 
 }
 
 // One antigen atom (this lane's) against the n group atoms in shared memory, two
-// group atoms per step: dx = b - a and r^2 = (dx*dx + dy*dy) + dz*dz in packed
-// f32x2 arithmetic, the reference's roundings, hence its pair set; the terms of
-// the pairs within the cutoff are added in group-atom order.
+// group atoms per step: dx = b - a in packed f32x2 arithmetic, r^2 = (dx*dx + dy*dy)
+// + dz*dz with the reference's roundings (scalar, never fused), hence its pair set;
+// the terms of the pairs within the cutoff (packed) are added in group-atom order.
 template <bool KAHAN, bool FULL, bool ABS, bool COUNT>
 __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const float4* __restrict__ prm,
                                             const GroupSmem& s, int n, int idx, Acc& acc) {
@@ -221,8 +221,8 @@ __device__ __forceinline__ void group_pairs(const float4* __restrict__ pq, const
         const uint64_t dx = f2_sub(*(const uint64_t*)&s.sx[j], ax);
         const uint64_t dy = f2_sub(*(const uint64_t*)&s.sy[j], ay);
         const uint64_t dz = f2_sub(*(const uint64_t*)&s.sz[j], az);
-        const uint64_t r2 = f2_add(f2_add(f2_mul(dx, dx), f2_mul(dy, dy)), f2_mul(dz, dz));
-        const float r2a = f2_lo(r2), r2b = f2_hi(r2);
+        float r2a, r2b;
+        f2_dist2(dx, dy, dz, r2a, r2b);
         const bool ina = r2a <= CUTOFF_SQ && r2a >= MIN_R_SQ;
         const bool inb = r2b <= CUTOFF_SQ && r2b >= MIN_R_SQ;  // j + 1 = n: a pad, +inf
         if (FULL) {
