@@ -122,15 +122,18 @@ struct State {
     // Metropolis statistics, 4 per candidate (tried / accepted: mutation+rotamer, backbone)
     DBuf<long long> mc_stats;
     int n_segments = 0;
+    long long max_segment = 0;  // candidates of the largest segment
     // residue order by Calpha cell (an autotuned order of the gradient-step and
     // scoring kernels)
     DBuf<int> key_base, keys, key_counts, key_cursor, order;
+    DBuf<int> bal_order;  // gradient-step order with work-balanced tasks (cg_order 3)
     int n_keys = 0;
     bool order_valid = false;
     // the gradient-step kernel's Verlet lists (csrc/k_search.cu), valid per residue
     DBuf<int> cg_list;
     DBuf<float4> cg_centre;
     DBuf<int4> cg_meta;
+    DBuf<uint8_t> cg_work;  // per residue: the flat gradient-step kernel's work estimate
     const int* ag_epoch = nullptr;  // the context's device epoch word
     // scoring work queue and per-residue energies
     DBuf<int> queue;
@@ -156,6 +159,7 @@ struct State {
         v.cg_list = cg_list.p;
         v.cg_centre = cg_centre.p;
         v.cg_meta = cg_meta.p;
+        v.cg_work = cg_work.p;
         v.ag_epoch = ag_epoch;
         return v;
     }
@@ -241,6 +245,16 @@ struct binder_ctx {
     std::vector<uint64_t> block_graph_sig;  // what the captured launches baked in
     int block_graph_launches = 0;
     bool block_graph_order = false;  // the residue order is valid after a replay
+    // enqueued (binder_block without outputs) blocks run as a pipeline: each block's
+    // graph sums and selects the previous block's residue energies on the side stream
+    // beside its own gradient steps; sel_pending: the last block's selection (top-sel_k)
+    // is still to run (flushed by the next call that is not such a block)
+    cudaGraphExec_t pipe_graph = nullptr;
+    std::vector<uint64_t> pipe_graph_sig;
+    int pipe_graph_launches = 0;
+    bool pipe_graph_order = false;
+    bool sel_pending = false;
+    int sel_k = 0;
     std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
     MlpState mlp;
     // antigen-set epoch (device word read by the gradient-step kernel)
@@ -256,9 +270,17 @@ struct binder_ctx {
     // binder_block_io: the state download runs on a second stream beside the score
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    void drop_graph() {
+    void drop_block_graph() {
         if (block_graph) cudaGraphExecDestroy(block_graph);
         block_graph = nullptr;
+    }
+    void drop_pipe_graph() {
+        if (pipe_graph) cudaGraphExecDestroy(pipe_graph);
+        pipe_graph = nullptr;
+    }
+    void drop_graph() {
+        drop_block_graph();
+        drop_pipe_graph();
     }
     ~binder_ctx() {
         drop_graph();
@@ -314,12 +336,21 @@ cudaError_t init_mlp_tables() {
     return e ? e : anneal_init_mlp_table(t);
 }
 
-int enter(binder_ctx* ctx) {
+int flush_select(binder_ctx* ctx);
+
+// Every entry point starts here; the pending selection of an enqueued block runs
+// first, so that nothing sees or replaces the residue energies before it.
+int enter_keep(binder_ctx* ctx) {
     if (!ctx) return BINDER_ERR_ARG;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     ctx->err.clear();
     return BINDER_OK;
+}
+int enter(binder_ctx* ctx) {
+    int s = enter_keep(ctx);
+    if (s) return s;
+    return ctx->sel_pending ? flush_select(ctx) : BINDER_OK;
 }
 
 // Reset the device error word before a group of launches.
@@ -1118,6 +1149,8 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     S.h_cand_id = ids;
     S.h_orig = orig;
     S.n_segments = n_ag;
+    S.max_segment = 0;
+    for (int a = 0; a < n_ag; ++a) S.max_segment = std::max(S.max_segment, g_off[a + 1] - g_off[a]);
     int s;
     if ((s = upload(ctx, S.cand_res_off, off.data(), off.size(), "state")) ||
         (s = upload(ctx, S.cand_ag, ag.data(), ag.size(), "state")) ||
@@ -1138,6 +1171,7 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     if ((s = upload(ctx, S.key_base, kb.data(), kb.size(), "state"))) return s;
     CK(S.keys.ensure(std::max(total, 1)), "alloc");
     CK(S.order.ensure(std::max(total, 1)), "alloc");
+    CK(S.bal_order.ensure(std::max(total, 1)), "alloc");
     CK(S.key_counts.ensure(nk + 1), "alloc");
     CK(S.key_cursor.ensure(nk + 1), "alloc");
     CK(S.queue.ensure(2), "alloc");  // scoring and gradient-step work queues
@@ -1193,7 +1227,9 @@ static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_re
         CK(S.cg_list.ensure((size_t)total * CG_LIST_CAP), "alloc");
         CK(S.cg_centre.ensure(total), "alloc");
         CK(S.cg_meta.ensure(total), "alloc");
+        CK(S.cg_work.ensure(total), "alloc");
         CK(cudaMemsetAsync(S.cg_meta.p, 0xFF, S.cg_meta.n * sizeof(int4), ctx->stream), "memset");
+        CK(cudaMemsetAsync(S.cg_work.p, 0, S.cg_work.n, ctx->stream), "memset");
     }
     launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
     if (total) LAUNCHED("pack_slots");
@@ -1368,10 +1404,19 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
         return BINDER_OK;
     }
     int s;
+    const int* order = S.order.p;
     if (ctx->cfg.cg_order == 0) {
         if ((s = enqueue_order(ctx))) return s;  // sorted before the steps, kept for the score
     } else {
         S.order_valid = false;  // residues move: the cell order is stale
+    }
+    int order_mode = ctx->cfg.cg_order;
+    if (order_mode == 3 && !S.cg_work.p) order_mode = 1;
+    if (order_mode == 3) {  // tasks balanced by the work estimates of the previous launch
+        launch_balance_order(ctx->stream, S.view(), ctx->cfg.cg_flat ? ctx->cfg.cg_flat : 32 / ctx->cfg.cg_lanes,
+                             S.bal_order.p);
+        LAUNCHED("balance_order");
+        order = S.bal_order.p;
     }
     int max_ag = 0, max_cells = 0;
     for (const auto& a : ctx->ags) {
@@ -1387,8 +1432,8 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
             break;
         }
     launch_diffuse(ctx->stream, S.view(), ctx->d_views.p, step_params(ctx->params), n_steps, step0, with_noise,
-                   temps ? ctx->temps.p : nullptr, ctx->errf.p, S.order.p, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
-                   ctx->cfg.cg_order, max_ag, max_cells, stage_ag, ctx->cfg.cg_queue ? S.queue.p + 1 : nullptr,
+                   temps ? ctx->temps.p : nullptr, ctx->errf.p, order, ctx->cfg.cg_warps, ctx->cfg.cg_lanes,
+                   order_mode, max_ag, max_cells, stage_ag, ctx->cfg.cg_queue ? S.queue.p + 1 : nullptr,
                    ctx->cfg.cg_flat);
     LAUNCHED("diffuse");
     return BINDER_OK;
@@ -1418,6 +1463,48 @@ int enqueue_score_state(binder_ctx* ctx, int full) {
     ctx->launches += launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
                                         score_scratch(ctx), persistent_ctas(ctx), ctx->cfg.score_warps) - 1;
     LAUNCHED("score_state");
+    return BINDER_OK;
+}
+
+// Score the resident state and select each segment's stable top-k into ctx->topk:
+// one fused launch for the candidate sums and the selection when it fits (k <= 64,
+// segments of at most 4096 candidates), else the sums and launch_topk_segments.
+int enqueue_score_topk(binder_ctx* ctx, int full, int k, cudaEvent_t mid = nullptr, bool defer = false) {
+    State& S = ctx->st;
+    if (k <= 0 && !mid) return enqueue_score_state(ctx, full);
+    if (k > 0 && full != 2 && S.n_segments > 0 && sum_topk_fits(k, S.max_segment)) {
+        CK(ctx->energy.ensure(S.n_cand), "alloc");
+        if (!S.order_valid && ctx->cfg.score_order == 0) {
+            int s = enqueue_order(ctx);
+            if (s) return s;
+        }
+        ScoreOut o{ctx->energy.p, nullptr, nullptr, nullptr, ctx->errf.p};
+        const SumTopk tk{S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k, ctx->topk.p, mid, defer};
+        ctx->launches += launch_score_state(ctx->stream, S.view(), ctx->d_views.p, ctx->params.accumulate, full, o,
+                                            score_scratch(ctx), persistent_ctas(ctx), ctx->cfg.score_warps, &tk) - 1;
+        LAUNCHED("score_state_topk");
+        return BINDER_OK;
+    }
+    int s = enqueue_score_state(ctx, full);
+    if (s) return s;
+    if (mid) CK(cudaEventRecord(mid, ctx->stream), "event");
+    if (k > 0) {
+        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
+                             ctx->topk.p);
+        LAUNCHED("topk");
+    }
+    return BINDER_OK;
+}
+
+// The candidate sums and top-k of the residue energies the last enqueued block left
+// (binder_block without outputs, pipelined graph), on the context stream.
+int flush_select(binder_ctx* ctx) {
+    State& S = ctx->st;
+    ctx->sel_pending = false;
+    if (S.n_cand == 0 || ctx->sel_k <= 0) return BINDER_OK;
+    const SumTopk tk{S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, ctx->sel_k, ctx->topk.p, nullptr, false};
+    launch_sum_select(ctx->stream, S.view(), S.res_e.p, 0, ctx->energy.p, tk);
+    LAUNCHED("sum_select");
     return BINDER_OK;
 }
 }  // namespace
@@ -1458,13 +1545,8 @@ int enqueue_block(binder_ctx* ctx, int n_steps, int k, cudaEvent_t* ev) {
     if (ev) CK(cudaEventRecord(ev[0], ctx->stream), "event");
     if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return s;
     if (ev) CK(cudaEventRecord(ev[1], ctx->stream), "event");
-    if ((s = enqueue_score_state(ctx, 0))) return s;
-    if (ev) CK(cudaEventRecord(ev[2], ctx->stream), "event");
-    if (k > 0) {
-        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
-                             ctx->topk.p);
-        LAUNCHED("topk");
-    }
+    // timed: ev[2] between the residue scoring and the candidate sums + selection
+    if ((s = enqueue_score_topk(ctx, 0, k, ev ? ev[2] : nullptr))) return s;
     if (ev) CK(cudaEventRecord(ev[3], ctx->stream), "event");
     return BINDER_OK;
 }
@@ -1481,7 +1563,8 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
         (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
-                          S.key_counts.p, S.key_cursor.p, S.order.p, S.queue.p, S.res_e.p, S.res_abs.p,
+                          S.key_counts.p, S.key_cursor.p, S.order.p, S.bal_order.p, S.queue.p, S.res_e.p,
+                          S.res_abs.p,
                           ctx->energy.p, ctx->topk.p, ctx->errf.p, ctx->d_views.p};
     for (const void* q : ptrs) v.push_back((uint64_t)(uintptr_t)q);
     unsigned char pb[sizeof(binder_params)];
@@ -1494,10 +1577,67 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
     return v;
 }
 
+// The second stream and its fork / join events (created on first use).
+int ensure_side(binder_ctx* ctx) {
+    if (!ctx->side) {
+        CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking), "stream");
+        CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event");
+        CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "event");
+    }
+    return BINDER_OK;
+}
+
+// A block of the pipeline: the previous block's candidate sums and top-k on the side
+// stream beside this block's gradient steps, then this block's residue energies
+// (their sums and top-k follow in the next block, or in flush_select).  The sums
+// read only the residue energies, which nothing rewrites before the join.
+int enqueue_block_pipe(binder_ctx* ctx, int n_steps, int k) {
+    State& S = ctx->st;
+    int s;
+    CK(cudaEventRecord(ctx->ev_fork, ctx->stream), "event");
+    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0), "event");
+    const SumTopk tk{S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k, ctx->topk.p, nullptr, false};
+    launch_sum_select(ctx->side, S.view(), S.res_e.p, 0, ctx->energy.p, tk);
+    LAUNCHED("sum_select");
+    CK(cudaEventRecord(ctx->ev_join, ctx->side), "event");
+    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return s;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0), "event");
+    return enqueue_score_topk(ctx, 0, k, nullptr, true);
+}
+
+int capture_pipe(binder_ctx* ctx, int n_steps, int k) {
+    ctx->drop_pipe_graph();
+    int s = ensure_side(ctx);
+    if (s) return s;
+    const uint64_t l0 = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    s = enqueue_block_pipe(ctx, n_steps, k);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (s || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        ctx->launches = l0;
+        return s ? s : cuda_fail(ctx, e, "end capture");
+    }
+    e = cudaGraphInstantiate(&ctx->pipe_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->pipe_graph = nullptr;
+        ctx->launches = l0;
+        return cuda_fail(ctx, e, "graph instantiate");
+    }
+    ctx->pipe_graph_launches = (int)(ctx->launches - l0);
+    ctx->pipe_graph_order = ctx->st.order_valid;
+    ctx->launches = l0;
+    ctx->pipe_graph_sig = block_sig(ctx, n_steps, k);
+    return BINDER_OK;
+}
+
 // Capture enqueue_block into ctx->block_graph (buffers are sized beforehand, so
 // the capture allocates nothing).
 int capture_block(binder_ctx* ctx, int n_steps, int k) {
-    ctx->drop_graph();
+    ctx->drop_block_graph();
     const uint64_t l0 = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     int s = enqueue_block(ctx, n_steps, k, nullptr);
@@ -1602,9 +1742,9 @@ int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* c) {
     if ((c->score_warps != 4 && c->score_warps != 8 && c->score_warps != 16) || c->score_ctas_per_sm < 1 ||
         c->score_ctas_per_sm > 32 || (c->cg_warps != 2 && c->cg_warps != 4 && c->cg_warps != 8) ||
         (c->cg_lanes != 4 && c->cg_lanes != 8) || (c->cg_lanes == 4 && c->cg_warps == 8) || c->cg_order < 0 ||
-        c->cg_order > 2 || c->score_order < 0 || c->score_order > 1 ||
+        c->cg_order > 3 || c->score_order < 0 || c->score_order > 1 ||
         c->cg_queue < 0 || c->cg_queue > 1 ||
-        (c->cg_flat != 0 && c->cg_flat != 8 && c->cg_flat != 16 && c->cg_flat != 32) ||
+        (c->cg_flat != 0 && c->cg_flat != 4 && c->cg_flat != 8 && c->cg_flat != 16 && c->cg_flat != 32) ||
         (c->cg_flat == 32 && c->cg_warps != 4) || (c->cg_flat && c->cg_warps != 4 && c->cg_warps != 8))
         return fail(ctx, BINDER_ERR_ARG, "unsupported launch shape");
     ctx->cfg.score_warps = c->score_warps;
@@ -1642,9 +1782,9 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
     float best_ms = 1e30f;
     // lane-group shapes (flat 0: lanes x warps) and flat shapes (residues per warp x warps)
     const int shapes[][3] = {{0, 4, 2}, {0, 4, 4}, {0, 8, 2}, {0, 8, 4}, {0, 8, 8},
-                             {32, 8, 4}, {16, 8, 4}, {16, 8, 8}, {8, 8, 4}, {8, 8, 8}};
+                             {32, 8, 4}, {16, 8, 4}, {16, 8, 8}, {8, 8, 4}, {8, 8, 8}, {4, 8, 4}, {4, 8, 8}};
     for (int queue : {0, 1})
-    for (int order : {0, 1, 2})
+    for (int order : {0, 1, 2, 3})
         for (const auto& sh : shapes) {
             if (s) break;
             ctx->cfg.cg_flat = sh[0];
@@ -1699,12 +1839,12 @@ int binder_autotune(binder_ctx* ctx, int reps, binder_launch_cfg* out) {
 
 int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* out_e, int32_t* out_topk) {
     (void)step0;
-    int s = enter(ctx);
+    const bool async = out_e == nullptr && out_topk == nullptr;
+    int s = async ? enter_keep(ctx) : enter(ctx);  // an enqueued block may take over the pending selection
     if (s) return s;
     State& S = ctx->st;
     if (S.n_cand == 0) return fail(ctx, BINDER_ERR_STATE, "no candidates uploaded");
     if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
-    const bool async = out_e == nullptr && out_topk == nullptr;
     if ((ctx->params.flags & BINDER_FLAG_AUTOTUNE) && !ctx->async_pending) {
         const std::string key = tune_key(ctx);
         bool known = false;
@@ -1717,10 +1857,22 @@ int binder_block(binder_ctx* ctx, int n_steps, uint32_t step0, int k, double* ou
     CK(ctx->energy.ensure(S.n_cand), "alloc");
     if (k > 0) CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
     const bool tm = ctx->timing && ctx->ev_blocks < TIMING_RING;
+    const bool pipe = async && !tm && (ctx->params.flags & BINDER_FLAG_GRAPH) && k > 0 && S.n_segments > 0 &&
+                      sum_topk_fits(k, S.max_segment);
+    if (ctx->sel_pending && (!pipe || ctx->sel_k != k) && (s = flush_select(ctx))) return s;
     if (tm) {
         // per-phase events: the launches are issued one by one
         if ((s = enqueue_block(ctx, n_steps, k, &ctx->ev[4 * ctx->ev_blocks]))) return s;
         ctx->ev_blocks++;
+    } else if (pipe) {
+        if (!ctx->pipe_graph || ctx->pipe_graph_sig != block_sig(ctx, n_steps, k)) {
+            if ((s = capture_pipe(ctx, n_steps, k))) return s;
+        }
+        CK(cudaGraphLaunch(ctx->pipe_graph, ctx->stream), "graph launch");
+        ctx->launches += ctx->pipe_graph_launches;
+        S.order_valid = ctx->pipe_graph_order;
+        ctx->sel_pending = true;
+        ctx->sel_k = k;
     } else if (ctx->params.flags & BINDER_FLAG_GRAPH) {
         if (!ctx->block_graph || ctx->block_graph_sig != block_sig(ctx, n_steps, k)) {
             if ((s = capture_block(ctx, n_steps, k))) return s;
@@ -1758,11 +1910,7 @@ int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_
     int s = state_upload_impl(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos, false);
     if (s) return s;
     State& S = ctx->st;
-    if (!ctx->side) {
-        CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking), "stream");
-        CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event");
-        CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "event");
-    }
+    if ((s = ensure_side(ctx))) return s;
     if (ctx->params.flags & BINDER_FLAG_AUTOTUNE) {
         const std::string key = tune_key(ctx);
         bool known = false;
@@ -1787,11 +1935,8 @@ int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_
     CK(cudaMemcpyAsync(chi, S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->side), "D2H");
     CK(cudaMemcpyAsync(aa, S.res_aa.p, total, cudaMemcpyDeviceToHost, ctx->side), "D2H");
     CK(cudaEventRecord(ctx->ev_join, ctx->side), "event");
-    if ((s = enqueue_score_state(ctx, 0))) return s;
+    if ((s = enqueue_score_topk(ctx, 0, k))) return s;
     if (k > 0) {
-        launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k,
-                             ctx->topk.p);
-        LAUNCHED("topk");
         if (out_topk)
             CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * k * sizeof(int), cudaMemcpyDeviceToHost,
                                ctx->stream),
@@ -1851,10 +1996,7 @@ int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* o
             S.order_valid = ctx->block_graph_order;
         } else {
             if (ns > 0 && (s = enqueue_diffuse(ctx, ns, (uint32_t)s0, 0, cfg.phase1_mc, &t1[s0]))) return s;
-            if ((s = enqueue_score_state(ctx, 0))) return s;
-            launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k1,
-                                 ctx->topk.p);
-            LAUNCHED("topk");
+            if ((s = enqueue_score_topk(ctx, 0, k1))) return s;
         }
         s0 += std::max(ns, 1);
     } while (s0 < n1);
@@ -1871,11 +2013,8 @@ int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* o
     if ((s = clear_err(ctx))) return s;
     if (n2 > 0 && (s = enqueue_diffuse(ctx, n2, (uint32_t)n1, 1, 1, t2.data()))) return s;
     // final allatom_energy and ranking (diffusion.rs:1092-1098)
-    if ((s = enqueue_score_state(ctx, 1))) return s;
     const int k2 = cfg.top_n;
-    launch_topk_segments(ctx->stream, ctx->energy.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.n_segments, k2,
-                         ctx->topk.p);
-    LAUNCHED("topk");
+    if ((s = enqueue_score_topk(ctx, 1, k2))) return s;
     std::vector<double> e(S.n_cand);
     std::vector<int32_t> rank((size_t)S.n_segments * k2);
     if ((s = fetch_energies(ctx, S.n_cand, e.data(), nullptr, nullptr))) return s;

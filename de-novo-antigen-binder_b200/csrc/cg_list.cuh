@@ -90,6 +90,84 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
 }
 
 
+// The same list built by a whole warp in one pass, into 16-bit positions (antigens of
+// at most 65536 Calphas): the lanes find the atom ranges of 32 (dx, dy) columns at a
+// time, a warp prefix sum over the range lengths concatenates them in column order
+// (ascending positions), and the warp tests 32 consecutive atoms of the concatenation
+// per round, each lane finding its column by a binary search over the prefix; a
+// ballot orders the hits.  Writes at most CG_LIST_MAX entries to out and returns the
+// length (all lanes; above CG_LIST_MAX: unusable).
+static __device__ __noinline__ int build_cg_list_warp(const GridView& g, const float4* __restrict__ ca_pq, F3 p,
+                                                      int lane, uint16_t* out, float skin) {
+    const float R = 10.0f + skin + 0.01f, R2 = R * R;
+    const int c[3] = {cell_coord(p.x, g.inv), cell_coord(p.y, g.inv), cell_coord(p.z, g.inv)};
+    if (cell_far(c[0], c[1], c[2]) || !(R <= 8.0f * g.cell)) return CG_LIST_MAX + 1;
+    const int K = (int)ceilf(R / g.cell), W = 2 * K + 1, ncol = W * W;
+    const float pp[3] = {p.x, p.y, p.z};
+    auto slab2 = [&](int d, int o) {
+        const float lo = (float)(c[d] + o) * g.cell, hi = lo + g.cell;
+        const float dd = fmaxf(fmaxf(lo - pp[d], pp[d] - hi), 0.0f);
+        return dd * dd;
+    };
+    const unsigned lt = (1u << lane) - 1u;
+    int n = 0;
+    for (int col0 = 0; col0 < ncol; col0 += 32) {
+        // this lane's column: its z-run of cells within R, as a range of sorted positions
+        int a0 = 0, len = 0;
+        const int col = col0 + lane;
+        if (col < ncol) {
+            const int ox = col / W - K, oy = col % W - K;
+            const float dxy = slab2(0, ox) + slab2(1, oy);
+            const int X = c[0] + ox - g.ox, Y = c[1] + oy - g.oy;
+            if (dxy <= R2 && X >= 0 && Y >= 0 && X < g.nx && Y < g.ny) {
+                int zl = -K, zh = K;
+                while (zl <= K && dxy + slab2(2, zl) > R2) ++zl;
+                while (zh >= zl && dxy + slab2(2, zh) > R2) --zh;
+                const int Z0 = max(c[2] + zl - g.oz, 0), Z1 = min(c[2] + zh - g.oz, g.nz - 1);
+                if (zl <= zh && Z0 <= Z1) {
+                    const int base = (X * g.ny + Y) * g.nz;
+                    a0 = g.cell_start[base + Z0];
+                    len = g.cell_start[base + Z1 + 1] - a0;
+                }
+            }
+        }
+        int incl = len;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        for (int f0 = 0; f0 < tot; f0 += 32) {
+            const int f = f0 + lane;
+            const int fq = min(f, tot - 1);
+            // the first column whose inclusive prefix exceeds fq (every lane searches)
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                if (v <= fq) lo += step;
+            }
+            const int v_lo = __shfl_sync(0xffffffffu, incl, lo);
+            const int len_lo = __shfl_sync(0xffffffffu, len, lo);
+            const int a_lo = __shfl_sync(0xffffffffu, a0, lo);
+            const int i = a_lo + (fq - (v_lo - len_lo));
+            bool hit = false;
+            if (f < tot) {
+                const float4 a = ca_pq[i];
+                const float dx = p.x - a.x, dy = p.y - a.y, dz = p.z - a.z;
+                hit = dx * dx + dy * dy + dz * dz <= R2;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            const int w = n + __popc(m & lt);
+            if (hit && w < CG_LIST_MAX) out[w] = (uint16_t)i;
+            n += __popc(m);
+        }
+    }
+    __syncwarp();
+    return n;
+}
+
 constexpr int CG_IN_MAX = 48;      // in-cutoff list entries a residue holds per step
 constexpr float CG_NEAR_SQ = 99.0f;  // r^2 below which a pair is in adjacent 10 A cells
 

@@ -184,6 +184,7 @@ struct StateView {
     int* cg_list;             // total_res * CG list capacity: sorted antigen Calpha positions
     float4* cg_centre;        // total_res: list centre
     int4* cg_meta;            // total_res: {length, antigen, antigen-set epoch, 0}
+    uint8_t* cg_work;         // total_res: work estimate of the residue's next launch (may be null)
     const int* ag_epoch;      // device word: the antigen-set epoch (bumped when antigens change)
 };
 

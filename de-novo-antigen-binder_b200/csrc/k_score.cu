@@ -17,6 +17,7 @@
 // fixed order (deterministic).
 #include "kernels.h"
 #include "score.cuh"
+#include "topk.cuh"
 
 namespace binder {
 
@@ -379,6 +380,209 @@ __global__ void k_sum_residues(StateView st, const double* __restrict__ res_e, c
     if (out_abs) out_abs[c] = ea;
 }
 
+// Candidate sums and survivor selection in one launch (k <= 64, segments of at most
+// SS_MAX candidates): one CTA per segment.  Thread t adds the residue energies of the
+// segment's entries t, t + 1024, ... in residue order (the k_sum_residues sums, loads
+// issued ahead of the additions) and keeps their order-preserving keys.  A radix select, 8 bits
+// of the 64-bit key per pass from the top, finds the bucket that holds the k-th
+// smallest key: every key below it is a survivor, and of the keys in it (all equal
+// after the last pass) the ones earliest in the segment, which is candidate-index
+// order.  One warp sorts the k survivors by (key, index): the stable top-k of the
+// segment, as k_topk64 computes it.  A pass costs three barriers; it ends early
+// once the bucket holds exactly the survivors still missing (typically after the
+// third pass, when the bucket holds a single key).
+constexpr int SS_THREADS = 1024;
+constexpr int SS_PER = 4;
+constexpr int SS_MAX = SS_THREADS * SS_PER;
+
+__global__ void __launch_bounds__(SS_THREADS) k_sum_select(StateView st, const double* __restrict__ res_e, int full,
+                                                           double* __restrict__ out, const int* __restrict__ idx_list,
+                                                           const long long* __restrict__ seg_off, int k,
+                                                           int* __restrict__ out_idx) {
+    __shared__ int s_hist[256];
+    __shared__ unsigned long long s_sel_k[64];
+    __shared__ int s_sel_i[64];
+    __shared__ unsigned long long s_prefix;
+    __shared__ int s_need, s_cnt, s_nsel;
+    __shared__ unsigned long long s_prefix_tot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = blockIdx.x;
+    const long long b0 = seg_off[seg];
+    const int n = (int)(seg_off[seg + 1] - b0);
+    const int kk = min(k, n);
+    // this thread's candidates: segment entries t + SS_THREADS * q
+    unsigned long long key[SS_PER];
+    int cid[SS_PER];
+#pragma unroll
+    for (int q = 0; q < SS_PER; ++q) {
+        const int j = (int)threadIdx.x + SS_THREADS * q;
+        key[q] = 0xFFFFFFFFFFFFFFFFull;
+        cid[q] = -1;
+        if (j < n) {
+            const int c = idx_list ? idx_list[b0 + j] : (int)(b0 + j);
+            const int r0 = st.cand_res_off[c], r1 = st.cand_res_off[c + 1];
+            double e = 0.0;
+            int r = r0;
+            for (; r + 4 <= r1; r += 4) {
+                const double v0 = res_e[r], v1 = res_e[r + 1], v2 = res_e[r + 2], v3 = res_e[r + 3];
+                e += v0;
+                e += v1;
+                e += v2;
+                e += v3;
+            }
+            for (; r < r1; ++r) e += res_e[r];
+            if (full) e += (double)disulfide_energy(st, c);
+            out[c] = e;
+            key[q] = order_key(e);
+            cid[q] = c;
+        }
+    }
+    if (threadIdx.x == 0) {
+        s_prefix = 0ull;
+        s_need = kk;
+        s_cnt = 0;
+        s_nsel = 0;
+    }
+    // ---- radix select of the kk-th smallest key ----
+    unsigned long long mask = 0ull;
+    bool all_in = false;  // the final bucket holds exactly the survivors still missing
+    for (int shift = 56; shift >= 0 && kk > 0; shift -= 8) {
+        for (int t = threadIdx.x; t < 256; t += SS_THREADS) s_hist[t] = 0;
+        __syncthreads();
+        const unsigned long long prefix = s_prefix;
+#pragma unroll
+        for (int q = 0; q < SS_PER; ++q) {
+            if (q * SS_THREADS >= n) break;  // no thread holds entry q
+            // one shared atomic per distinct digit of the warp: the lowest lane still
+            // pending takes every lane with its digit
+            const bool in = cid[q] >= 0 && (key[q] & mask) == prefix;
+            const int dg = in ? (int)((key[q] >> shift) & 255ull) : -1;
+            unsigned pend = __ballot_sync(0xffffffffu, in);
+            while (pend) {
+                const int leader = __ffs(pend) - 1;
+                const int d = __shfl_sync(0xffffffffu, dg, leader);
+                const unsigned same = __ballot_sync(0xffffffffu, in && dg == d);
+                if (lane == leader) atomicAdd(&s_hist[d], __popc(same));
+                pend &= ~same;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {  // the digit whose bucket holds the s_need-th key
+            const int need = s_need;
+            int h[8], loc = 0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                h[i] = s_hist[lane * 8 + i];
+                loc += h[i];
+            }
+            int inc = loc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += v;
+            }
+            const int exc = inc - loc;
+            if (exc < need && need <= inc) {
+                int cum = exc;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (cum + h[i] >= need) {
+                        s_prefix = prefix | ((unsigned long long)(lane * 8 + i) << shift);
+                        s_need = need - cum;
+                        s_cnt = h[i];
+                        break;
+                    }
+                    cum += h[i];
+                }
+            }
+        }
+        __syncthreads();
+        mask |= 0xFFull << shift;
+        if (s_cnt == s_need) {
+            all_in = true;
+            break;
+        }
+    }
+    __syncthreads();
+    // ---- the survivors: keys below the bucket, and the bucket's first s_need ----
+    const unsigned long long prefix = s_prefix;
+    const int need = s_need;
+    // rank of each bucket member in segment order (entry t + 1024 q: q major), from a
+    // block scan of the per-q membership flags packed 16 bits per q (only needed when
+    // the bucket holds more keys than survivors missing)
+    int rank[SS_PER] = {0, 0, 0, 0};
+    if (!all_in && kk > 0) {
+        unsigned long long mine = 0ull;
+#pragma unroll
+        for (int q = 0; q < SS_PER; ++q)
+            if (cid[q] >= 0 && (key[q] & mask) == prefix) mine |= 1ull << (16 * q);
+        unsigned long long inc = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        __shared__ unsigned long long s_wsum[32];
+        if (lane == 31) s_wsum[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            const unsigned long long w = s_wsum[lane];
+            unsigned long long wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long v = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += v;
+            }
+            s_wsum[lane] = wi - w;
+            if (lane == 31) s_prefix_tot = wi;  // per-q totals of the bucket
+        }
+        __syncthreads();
+        const unsigned long long before = s_wsum[warp] + inc - mine;  // earlier threads, per q
+        const unsigned long long tot = s_prefix_tot;
+        int base = 0;
+#pragma unroll
+        for (int q = 0; q < SS_PER; ++q) {
+            rank[q] = base + (int)((before >> (16 * q)) & 0xFFFFull);
+            base += (int)((tot >> (16 * q)) & 0xFFFFull);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < SS_PER; ++q) {
+        if (cid[q] < 0 || kk == 0) continue;
+        const bool below = key[q] < prefix;  // prefix has zeros under the mask
+        bool take = below;
+        if (!below && (key[q] & mask) == prefix) take = all_in || rank[q] < need;
+        if (take) {
+            const int p = atomicAdd(&s_nsel, 1);
+            if (p < 64) {
+                s_sel_k[p] = key[q];
+                s_sel_i[p] = cid[q];
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {  // sort the kk survivors by (key, index)
+        const KI inf = {0xFFFFFFFFFFFFFFFFull, INT32_MAX};
+        KI a = lane < kk ? KI{s_sel_k[lane], s_sel_i[lane]} : inf;
+        KI b = lane + 32 < kk ? KI{s_sel_k[lane + 32], s_sel_i[lane + 32]} : inf;
+        a = warp_sort32(a, lane);
+        b = warp_sort32(b, lane);
+        KI hi = inf;
+        warp_merge64(a, hi, b, inf, lane);
+        int* oi = out_idx + (long long)seg * k;
+        if (lane < k) oi[lane] = a.i != INT32_MAX ? a.i : -1;
+        if (lane + 32 < k) oi[lane + 32] = hi.i != INT32_MAX ? hi.i : -1;
+    }
+}
+
+bool sum_topk_fits(int k, long long max_segment) { return k > 0 && k <= 64 && max_segment <= SS_MAX; }
+
+void launch_sum_select(cudaStream_t s, const StateView& st, const double* res_e, int full, double* energy,
+                       const SumTopk& tk) {
+    if (st.n_cand <= 0 || tk.n_seg <= 0) return;
+    k_sum_select<<<tk.n_seg, SS_THREADS, 0, s>>>(st, res_e, full, energy, tk.idx_list, tk.seg_off, tk.k, tk.out_idx);
+}
+
 template <int NW>
 static void score_residues_nw(cudaStream_t s, int g, const StateView& st, const AgView* ags, bool kahan, bool full,
                               bool abs_, bool count, const ScoreOut& o, const StateScoreScratch& scr) {
@@ -394,7 +598,8 @@ static void score_residues_nw(cudaStream_t s, int g, const StateView& st, const 
 }
 
 int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& o, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta) {
+                       const ScoreOut& o, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta,
+                       const SumTopk* tk) {
     if (st.n_cand <= 0) return 0;
     const bool kahan = accumulate == 0, abs_ = o.abs_sum != nullptr, count = o.pairs != nullptr;
     const int g = grid_ctas > 0 ? grid_ctas : 148 * 4;
@@ -404,9 +609,14 @@ int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, i
         case 16: score_residues_nw<16>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
         default: score_residues_nw<8>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
     }
-    if (!count)
+    if (!count && tk && !abs_) {
+        if (tk->defer) return 2;  // the sums and the selection come later (launch_sum_select)
+        if (tk->mid) cudaEventRecord(tk->mid, s);
+        launch_sum_select(s, st, scr.res_e, full, o.energy, *tk);
+    } else if (!count) {
         k_sum_residues<<<(st.n_cand + 127) / 128, 128, 0, s>>>(st, scr.res_e, abs_ ? scr.res_abs : nullptr, full,
                                                                o.energy, o.abs_sum);
+    }
     return count ? 2 : 3;  // launches issued (memset counted)
 }
 

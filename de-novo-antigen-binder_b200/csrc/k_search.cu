@@ -96,10 +96,11 @@ __device__ __noinline__ void cg_force_walk(const AgView* __restrict__ ag, float 
 
 
 // Residue of a lane group's slot: the cell-sorted permutation (order_mode 0), the
-// state's own order (1: candidate after candidate), or a stride through it (2:
+// state's own order (1: candidate after candidate), a stride through it (2:
 // slot * CG_STRIDE mod total, a bijection when total is coprime to the prime
 // CG_STRIDE) that spreads each warp's residues over unrelated candidates, so the
-// costly residues in contact are shared out evenly.  Results never depend on it.
+// costly residues in contact are shared out evenly, or the work-balanced permutation
+// of k_balance_order (3).  Results never depend on it.
 constexpr long long CG_STRIDE = 1000003;
 __device__ __forceinline__ int res_of_slot(const int* __restrict__ order, int mode, int slot, int total) {
     if (mode == 2) return (int)(((long long)slot * CG_STRIDE) % total);
@@ -457,13 +458,13 @@ struct FlatWarp {
     const float4* pq[R];        // the residue's antigen Calphas (shared memory when staged)
     const float4* aprm[R];
     const int4* acell[R];
-    const int* list[R];         // the residue's Verlet list in the state's list storage
     int pref[R + 1];            // exclusive prefix of the list lengths scanned this step
     int rid[R];                 // residue index (-1: no residue)
     int nat[R];                 // atoms of the residue
     int hit[FLAT_HCAP];         // residue slot << 26 | antigen Calpha position
     float3 term[FLAT_HCAP];
     float3 dl[FLAT_DSTEPS][R];  // recorded translations
+    uint16_t sl[R][CG_LIST_MAX];  // the residues' Verlet lists for the launch (positions)
 };
 
 // Apply the recorded translations 0..nd-1 to every atom of the warp's residues.
@@ -488,16 +489,18 @@ __device__ __forceinline__ void flat_flush(const StateView& st, FlatWarp<R>& fw,
 }
 
 template <int W, int R>
-__global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, const AgView* __restrict__ ags, StepParams p,
+__global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_flat(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                            int n_steps, uint32_t step0, int with_noise,
                                                            const float* __restrict__ temps, uint32_t* __restrict__ err,
                                                            const int* __restrict__ order, int order_mode,
                                                            int stage_cap, int stage_ag, int* __restrict__ queue) {
-    static_assert(R == 8 || R == 16 || R == 32, "residues per warp");
+    static_assert(R == 4 || R == 8 || R == 16 || R == 32, "residues per warp");
     constexpr int RPC = W * R;  // residues per CTA
-    __shared__ FlatWarp<R> s_fw[W];
     __shared__ int s_stage_ag;
-    extern __shared__ __align__(16) unsigned char cg_dyn[];
+    // dynamic shared memory: the warps' FlatWarp records, then the antigen staging
+    extern __shared__ __align__(16) unsigned char cg_dyn_all[];
+    FlatWarp<R>* s_fw = reinterpret_cast<FlatWarp<R>*>(cg_dyn_all);
+    unsigned char* cg_dyn = cg_dyn_all + W * sizeof(FlatWarp<R>);
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     FlatWarp<R>& fw = s_fw[threadIdx.x >> 5];
@@ -542,8 +545,9 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
     }
     const int epoch = st.ag_epoch ? *st.ag_epoch : -2;
 
-    // Build residue q's list with the whole warp (all lanes call; q's antigen, centre
-    // and skin are taken from lane q).  Returns the length on every lane.
+    // Build residue q's list into shared memory with the whole warp (all lanes call;
+    // q's antigen, centre and skin are taken from lane q).  Returns the length on
+    // every lane.
     auto warp_build = [&](int q, int a, F3 centre, float skin) -> int {
         a = __shfl_sync(0xffffffffu, a, q);
         centre.x = __shfl_sync(0xffffffffu, centre.x, q);
@@ -556,8 +560,7 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
             g.cell_start = sstart;
             pq = spq;
         }
-        int* list = st.cg_list + (size_t)fw.rid[q] * CG_LIST_MAX;
-        return build_cg_list<32>(g, pq, centre, lane, 0xffffffffu, list, skin);
+        return build_cg_list_warp(g, pq, centre, lane, fw.sl[q], skin);
     };
 
     int task = blockIdx.x * W + (int)(threadIdx.x >> 5);
@@ -595,12 +598,12 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
             fw.pq[lane] = staged ? spq : Ap->ca_pq;
             fw.aprm[lane] = staged ? sprm : Ap->ca_prm;
             fw.acell[lane] = staged ? scell : Ap->ca_cell;
-            fw.list[lane] = st.cg_list + (size_t)(valid ? r : 0) * CG_LIST_MAX;
         }
         // the list of the previous launch when it was built for this antigen set and
         // antigen and still covers the Calpha, else a new one
         F3 centre = ca;
         int nl = 0;
+        int nreb = 0;  // lists this residue builds in the launch
         bool dirty = false;
         float skin = CG_SKIN;
         bool need = false;
@@ -621,6 +624,25 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
             }
             need = !reuse;
         }
+        {  // the carried lists into shared memory: all residues' entries, 32 per round
+            const int nc = (valid && !need) ? nl : 0;
+            int inc = nc;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc += v;
+            }
+            const int tot = __shfl_sync(0xffffffffu, inc, 31);
+            if (lane < R) fw.pref[lane + 1] = inc;
+            if (lane == 0) fw.pref[0] = 0;
+            __syncwarp();
+            int q = 0;
+            for (int f = lane; f < tot; f += 32) {
+                while (fw.pref[q + 1] <= f) ++q;
+                const int k = f - fw.pref[q];
+                fw.sl[q][k] = (uint16_t)__ldg(st.cg_list + (size_t)fw.rid[q] * CG_LIST_MAX + k);
+            }
+        }
         __syncwarp();
         for (unsigned m = __ballot_sync(0xffffffffu, need); m; m &= m - 1) {
             const int q = __ffs(m) - 1;
@@ -628,6 +650,7 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
             if (lane == q) {
                 nl = n;
                 dirty = true;
+                ++nreb;
             }
         }
         int nd = 0;  // recorded translations
@@ -663,7 +686,7 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
                     int code = 0;
                     if (f < total) {
                         while (fw.pref[rq + 1] <= f) ++rq;
-                        const int i = fw.list[rq][f - fw.pref[rq]];
+                        const int i = fw.sl[rq][f - fw.pref[rq]];
                         const float4 b = fw.body[rq];
                         const float4 ap = fw.pq[rq][i];
                         const float r_sq = xdist2(xsub(b.x, ap.x), xsub(b.y, ap.y), xsub(b.z, ap.z));
@@ -762,12 +785,36 @@ __global__ void __launch_bounds__(W * 32, 24 / W) k_langevin_flat(StateView st, 
                 if (lane == q) {
                     nl = n;
                     dirty = true;
+                    ++nreb;
                 }
             }
         }
         if (valid && dirty) {  // keep the list for the next launch
             st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
             st.cg_meta[r] = make_int4(nl, a, epoch, 0);
+        }
+        if (valid && st.cg_work)  // the next launch's work estimate (k_balance_order)
+            st.cg_work[r] = (uint8_t)min(255, (nl <= CG_LIST_MAX ? nl : 200) + 32 * nreb);
+        {  // rebuilt lists back to the state's list storage, all residues' entries at once
+            const int nc = (valid && dirty && nl <= CG_LIST_MAX) ? nl : 0;
+            int inc = nc;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, inc, d);
+                if (lane >= d) inc += v;
+            }
+            const int tot = __shfl_sync(0xffffffffu, inc, 31);
+            __syncwarp();
+            if (lane < R) fw.pref[lane + 1] = inc;
+            if (lane == 0) fw.pref[0] = 0;
+            __syncwarp();
+            int q = 0;
+            for (int f = lane; f < tot; f += 32) {
+                while (fw.pref[q + 1] <= f) ++q;
+                const int k = f - fw.pref[q];
+                st.cg_list[(size_t)fw.rid[q] * CG_LIST_MAX + k] = fw.sl[q][k];
+            }
+            __syncwarp();
         }
         if (!queue) break;
     }
@@ -825,6 +872,114 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
     k_res_scatter<<<(st.total_res + 255) / 256, 256, 0, s>>>(st.total_res, keys, cursor, order);
 }
 
+// ---- residue order balancing the gradient-step tasks --------------------------------
+// The flat gradient-step kernel leaves, per residue, a work estimate for the next
+// launch (cg_work: its Verlet-list length plus a charge per list rebuild this launch;
+// 0 before the first launch).  Residues sorted by it, heaviest first (32 bins), are
+// dealt to the tasks of R residues in snake order (ranks 0..T-1 to tasks 0..T-1,
+// ranks T..2T-1 to tasks T-1..0, ...), so every task takes one residue of each work
+// band and no task of long lists holds up the launch.  Which warp computes a residue
+// never changes its arithmetic, so any order gives the same trajectories.  One CTA,
+// no atomics: a warp counts its residues per bin with five ballots (one per bin bit;
+// lane L owns bin L), a block scan over (bin, warp) gives every warp its offset per
+// bin, and a second pass ranks each residue by its bin's offset, the count of its
+// bin in the warp's earlier rounds and the lower lanes of its round.
+constexpr int BAL_THREADS = 1024;
+constexpr int BAL_BINS = 32;         // one per lane
+constexpr int BAL_SMEM = 40960;      // work bytes staged in shared memory up to this many residues
+
+__device__ __forceinline__ int bal_bin(uint8_t w) { return (255 - (int)w) >> 3; }
+
+// lanes of this round whose bin is `b` (valid lanes only), from the five bin-bit ballots
+__device__ __forceinline__ unsigned bal_match(const unsigned (&bits)[5], unsigned valid, int b) {
+    unsigned m = valid;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) m &= ((b >> k) & 1) ? bits[k] : ~bits[k];
+    return m;
+}
+
+__global__ void __launch_bounds__(BAL_THREADS) k_balance_order(int n, const uint8_t* __restrict__ work, int R,
+                                                               int* __restrict__ order) {
+    __shared__ int s_h[BAL_BINS * 32];  // [bin][warp]: counts, then offsets
+    __shared__ int s_wsum[32];
+    __shared__ __align__(16) uint8_t s_w[BAL_SMEM];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int rounds = (n + BAL_THREADS - 1) / BAL_THREADS;
+    // the work bytes into shared memory (16 bytes per load, all loads independent)
+    const bool staged = n <= BAL_SMEM;
+    if (staged) {
+        const int n16 = n / 16;
+        const uint4* w16 = reinterpret_cast<const uint4*>(work);
+        for (int t = threadIdx.x; t < n16; t += BAL_THREADS) reinterpret_cast<uint4*>(s_w)[t] = __ldg(&w16[t]);
+        for (int t = n16 * 16 + (int)threadIdx.x; t < n; t += BAL_THREADS) s_w[t] = work[t];
+        __syncthreads();
+    }
+    const uint8_t* wk = staged ? s_w : work;
+    int cnt = 0;  // residues of bin `lane` in this warp
+    for (int i = 0; i < rounds; ++i) {
+        const int r = (int)threadIdx.x + i * BAL_THREADS;
+        const bool v = r < n;
+        const int b = v ? bal_bin(wk[r]) : 0;
+        unsigned bits[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) bits[k] = __ballot_sync(0xffffffffu, v && ((b >> k) & 1));
+        cnt += __popc(bal_match(bits, __ballot_sync(0xffffffffu, v), lane));
+    }
+    s_h[lane * 32 + warp] = cnt;
+    __syncthreads();
+    // exclusive scan of the 1024 (bin, warp) counts, bin-major: one per thread
+    const int c = s_h[threadIdx.x];
+    int inc = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += x;
+    }
+    if (lane == 31) s_wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = s_wsum[lane];
+        int wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int x = __shfl_up_sync(0xffffffffu, wi, d);
+            if (lane >= d) wi += x;
+        }
+        s_wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    s_h[threadIdx.x] = s_wsum[warp] + inc - c;
+    __syncthreads();
+    int run = s_h[lane * 32 + warp];  // lane L: next rank of bin L in this warp
+    const int T = n / R, full = T * R;
+    for (int i = 0; i < rounds; ++i) {
+        const int r = (int)threadIdx.x + i * BAL_THREADS;
+        const bool v = r < n;
+        const int b = v ? bal_bin(wk[r]) : 0;
+        unsigned bits[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) bits[k] = __ballot_sync(0xffffffffu, v && ((b >> k) & 1));
+        const unsigned valid = __ballot_sync(0xffffffffu, v);
+        const int base = __shfl_sync(0xffffffffu, run, b);
+        const int rank = base + __popc(bal_match(bits, valid, b) & lt);
+        run += __popc(bal_match(bits, valid, lane));
+        if (v) {
+            int slot = rank;
+            if (rank < full) {
+                const int round = rank / T, pos = rank - round * T;
+                slot = ((round & 1) ? T - 1 - pos : pos) * R + round;
+            }
+            order[slot] = r;
+        }
+    }
+}
+
+void launch_balance_order(cudaStream_t s, const StateView& st, int residues_per_task, int* order) {
+    if (st.total_res <= 0 || !st.cg_work) return;
+    k_balance_order<<<1, BAL_THREADS, 0, s>>>(st.total_res, st.cg_work, std::max(residues_per_task, 1), order);
+}
+
 template <int W, int G>
 static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
                       uint32_t step0, int with_noise, const float* temps, uint32_t* err, const int* order,
@@ -854,17 +1009,18 @@ static void diffuse_flat(cudaStream_t s, const StateView& st, const AgView* ags,
     const long long tasks = ((long long)st.total_res + R - 1) / R;
     long long ctas = (tasks + W - 1) / W;
     auto kern = k_langevin_flat<W, R>;
-    if (stage_bytes > 0) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes);
+    const int dyn = (int)(W * sizeof(FlatWarp<R>)) + stage_bytes;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (queue) {  // persistent: the CTAs that are resident at once
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, stage_bytes);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn);
         ctas = std::min(ctas, (long long)std::max(1, sms * std::max(per_sm, 1)));
         cudaMemsetAsync(queue, 0, sizeof(int), s);
     }
-    kern<<<(int)ctas, threads, stage_bytes, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode,
-                                                 stage_bytes, stage_ag, queue);
+    kern<<<(int)ctas, threads, dyn, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode,
+                                         stage_bytes, stage_ag, queue);
 }
 
 void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, const StepParams& p, int n_steps,
@@ -876,7 +1032,8 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
     // antigen staging: up to 96 KB of dynamic shared memory per CTA
     const size_t sb = cg_stage_bytes(max_ag_res, max_ag_cells);
     const int stage = sb <= 96 * 1024 ? (int)sb : 0;
-    if (flat_res && st.cg_list && st.cg_meta && st.cg_centre) {
+    // the flat form keeps 16-bit list positions: antigens of at most 65536 Calphas
+    if (flat_res && st.cg_list && st.cg_meta && st.cg_centre && max_ag_res <= 65536) {
 #define BINDER_FLAT(W, R)                                                                                    \
     diffuse_flat<W, R>(s, st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode, stage,          \
                        stage ? stage_ag : -1, queue)
@@ -884,6 +1041,9 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
         else if (flat_res == 16) {
             if (warps_per_cta <= 4) BINDER_FLAT(4, 16);
             else BINDER_FLAT(8, 16);
+        } else if (flat_res == 4) {
+            if (warps_per_cta <= 4) BINDER_FLAT(4, 4);
+            else BINDER_FLAT(8, 4);
         } else {
             if (warps_per_cta <= 4) BINDER_FLAT(4, 8);
             else BINDER_FLAT(8, 8);

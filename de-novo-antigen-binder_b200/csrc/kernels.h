@@ -59,8 +59,27 @@ struct StateScoreScratch {
     double* res_e;     // total_res
     double* res_abs;   // total_res (abs sums)
 };
+// Survivor selection fused into the candidate sums of launch_score_state (k <= 64,
+// every segment at most 4096 candidates, listed in ascending candidate index;
+// sum_topk_fits): the stable top-k of each segment into out_idx, as
+// launch_topk_segments computes it.
+struct SumTopk {
+    const int* idx_list;
+    const long long* seg_off;
+    int n_seg;
+    int k;
+    int* out_idx;
+    cudaEvent_t mid;  // recorded between the residue scoring and this launch (may be null)
+    bool defer;       // score the residues only; launch_sum_select follows later
+};
+bool sum_topk_fits(int k, long long max_segment);
+// the candidate sums of res_e (residue energies of launch_score_state) and the
+// selection, as launch_score_state runs them after the residues
+void launch_sum_select(cudaStream_t s, const StateView& st, const double* res_e, int full, double* energy,
+                       const SumTopk& tk);
 int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, int accumulate, int full,
-                       const ScoreOut& out, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta);
+                       const ScoreOut& out, const StateScoreScratch& scr, int grid_ctas, int warps_per_cta,
+                       const SumTopk* tk = nullptr);
 
 void launch_uniform_offsets(cudaStream_t s, long long* off, int n_cand, long long n_ab);
 
@@ -80,6 +99,9 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
                     int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
                     int stage_ag, int* queue, int flat_res);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
+// Residue order of the gradient-step launch with tasks of residues_per_task residues
+// balanced by the Verlet-list lengths carried in the state (one CTA).
+void launch_balance_order(cudaStream_t s, const StateView& st, int residues_per_task, int* order);
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);
 void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);

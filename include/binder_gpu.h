@@ -306,15 +306,18 @@ typedef struct binder_launch_cfg {
     int32_t cg_lanes;           /* lanes per residue of the gradient-step kernel: 4 (with 2 or 4
                                    warps per CTA) or 8 */
     int32_t cg_order;           /* residue order of the gradient-step kernel: 0 by Calpha cell,
-                                   1 candidate after candidate, 2 strided (work spread out) */
+                                   1 candidate after candidate, 2 strided (work spread out),
+                                   3 tasks balanced by the work estimates (Verlet-list lengths,
+                                   rebuilds) of the previous launch (one ordering launch before
+                                   the steps) */
     int32_t score_order;        /* work-queue order of the scoring kernel: 0 by Calpha cell (three
                                    sorting launches after every move), 1 residue index */
     int32_t cg_queue;           /* gradient-step kernel: 0 one CTA per residue batch, 1 persistent
                                    CTAs whose warps take residue batches from a work queue */
     int32_t cg_flat;            /* gradient-step kernel: 0 the lane-group form (cg_lanes lanes per
-                                   residue); 8, 16 or 32 the flat form with that many residues per
-                                   warp (the warp scans their concatenated lists together; 32 with
-                                   4 warps per CTA, 8 and 16 with 4 or 8) */
+                                   residue); 4, 8, 16 or 32 the flat form with that many residues
+                                   per warp (the warp scans their concatenated lists together; 32
+                                   with 4 warps per CTA, 4, 8 and 16 with 4 or 8) */
 } binder_launch_cfg;
 int binder_get_launch_cfg(binder_ctx* ctx, binder_launch_cfg* out);
 int binder_set_launch_cfg(binder_ctx* ctx, const binder_launch_cfg* cfg);
@@ -540,8 +543,11 @@ int binder_mlp_train(binder_ctx* ctx, int n_steps, int batch, float lr, float hu
 void* binder_stream(binder_ctx* ctx);
 /* With timing on, binder_block records CUDA events on the context stream around
    each of its phases (up to 4096 blocks).  binder_timing_summary synchronises,
-   returns the summed [gradient steps, scoring, top-k] milliseconds and the
-   number of blocks recorded since binder_set_timing, and restarts the record. */
+   returns the summed [gradient steps, scoring, selection] milliseconds and the
+   number of blocks recorded since binder_set_timing, and restarts the record.
+   Scoring is the residue pair energies; selection is the candidate sums and the
+   top-k (one fused launch when k <= 64 and every segment holds at most 4096
+   candidates, else the sums are part of scoring). */
 int binder_set_timing(binder_ctx* ctx, int on);
 int binder_timing_summary(binder_ctx* ctx, double* out_ms_sums, int32_t* out_blocks);
 /* In-cutoff pair counts of the resident state: Calpha pairs of n_steps gradient

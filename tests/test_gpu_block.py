@@ -52,7 +52,10 @@ def test_graph_block_matches_eager(ctx, oracle, pkg):
 @pytest.mark.parametrize("shape", [(4, 1, 2, 4, 0, 1, 0), (16, 8, 4, 8, 1, 0, 1), (8, 2, 4, 4, 2, 1, 1),
                                    (8, 4, 2, 8, 0, 0, 0), (8, 4, 8, 8, 2, 1, 0), (8, 4, 8, 8, 1, 1, 1),
                                    (8, 4, 2, 4, 0, 0, 1), (8, 4, 4, 8, 1, 0, 1, 32), (8, 4, 8, 8, 0, 1, 1, 16),
-                                   (8, 4, 8, 8, 2, 0, 0, 8), (8, 4, 4, 8, 1, 1, 0, 16)])
+                                   (8, 4, 8, 8, 3, 1, 0, 8), (8, 4, 8, 8, 3, 1, 1, 8), (8, 4, 4, 8, 3, 0, 1, 16),
+                                   (8, 4, 8, 8, 3, 1, 0), (8, 4, 2, 4, 3, 0, 1),
+                                   (8, 4, 8, 8, 2, 0, 0, 8), (8, 4, 4, 8, 1, 1, 0, 16), (8, 4, 8, 8, 1, 1, 1, 4),
+                                   (8, 4, 4, 8, 2, 0, 1, 4)])
 def test_launch_shapes_bit_identical(ctx, oracle, pkg, shape):
     aa, chi, pos, n_res = _setup(ctx, oracle, pkg)
     ctx.set_launch_cfg(8, 4, 8, 8, 0, 0, 0)
@@ -69,8 +72,8 @@ def test_autotune_restores_state_and_caches(ctx, oracle, pkg, tmp_path, monkeypa
     ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
     cfg = ctx.autotune(reps=2)
     assert cfg.score_warps in (4, 8, 16) and cfg.cg_warps in (2, 4, 8) and 1 <= cfg.score_ctas_per_sm <= 8
-    assert cfg.cg_lanes in (4, 8) and cfg.cg_order in (0, 1, 2) and cfg.score_order in (0, 1) and cfg.cg_queue in (0, 1)
-    assert cfg.cg_flat in (0, 8, 16, 32)
+    assert cfg.cg_lanes in (4, 8) and cfg.cg_order in (0, 1, 2, 3) and cfg.score_order in (0, 1) and cfg.cg_queue in (0, 1)
+    assert cfg.cg_flat in (0, 4, 8, 16, 32)
     _, _, p_after = ctx.state_download()
     assert np.array_equal(p_after, pos)  # the timing runs worked on a copy
     got = [ctx.block(10, 10 * b, k=64) for b in range(3)], ctx.state_download()
@@ -180,3 +183,95 @@ def test_block_io_edge_cases(ctx, oracle, pkg):
     with pytest.raises(pkg.BinderError) as err:
         ctx.block_io(bad, chi.copy(), pos.copy(), 5, k=8, uniform_n_res=n_res)
     assert err.value.name == "BINDER_ERR_ARG"
+
+
+def _seg_topk(e, ag_id, n_seg, k):
+    """Per antigen, the stable top-k of its candidates' energies (NaN last), -1 padded."""
+    out = np.full((n_seg, k), -1, np.int64)
+    for a in range(n_seg):
+        idx = np.nonzero(ag_id == a)[0]
+        key = np.where(np.isnan(e[idx]), np.inf, e[idx])
+        o = idx[np.lexsort((idx, np.isnan(e[idx]), key))][:k]
+        out[a, :len(o)] = o
+    return out
+
+
+@pytest.mark.parametrize("n_cand,k,dup", [(3000, 64, True), (3000, 1, False), (1000, 17, True), (5000, 64, False)])
+def test_fused_selection_one_segment(ctx, oracle, pkg, n_cand, k, dup):
+    """Scoring + selection of the block (candidate sums and top-k in one launch when
+    k <= 64 and the segment holds at most 4096 candidates, 128 per CTA, the
+    segment's last CTA merging; 5000 candidates take the two-launch path): the
+    stable top-k of the returned energies, ties (duplicated candidates) by index,
+    on repeated calls and through the graph."""
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, n_cand=n_cand)
+    if dup:  # candidates 2j and 2j + 1 identical: equal energies
+        for c in range(0, n_cand - 1, 2):
+            sl, sl2 = slice(c * n_res, (c + 1) * n_res), slice((c + 1) * n_res, (c + 2) * n_res)
+            aa[sl2], chi[sl2], pos[sl2] = aa[sl], chi[sl], pos[sl]
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    for flags in (0, pkg.FLAG_GRAPH):
+        ctx.set_params(pkg.Params.defaults(shell_radius=ctx.params.shell_radius, seed=5, flags=flags))
+        for b in range(2):
+            e, top = ctx.block(5 * b, 5 * b, k=k)
+            assert np.array_equal(top, _seg_topk(e, np.zeros(n_cand, int), 1, k))
+            assert np.array_equal(top[0], ctx.topk(e, k))
+            assert np.array_equal(e, ctx.score_state())
+    if dup:
+        assert len(np.unique(e)) <= (n_cand + 1) // 2
+
+
+def test_fused_selection_segments(ctx, pkg):
+    """Eight antigens, ragged candidates: each segment's stable top-k; a segment with
+    fewer candidates than k is padded with -1."""
+    cfg = pkg.workloads.config2(n_cand=1200)
+    ctx.clear_antigens()
+    ctx.set_params(pkg.Params.defaults(shell_radius=26.0, seed=6))
+    for ag_aa, ag_ca in cfg["antigens"]:
+        p_a, _ = ctx.build_residues(ag_ca, ag_aa)
+        ctx.add_antigen(ag_aa, p_a)
+    pop = cfg["pop"]
+    ag_id = pop.antigen_id.copy()
+    ag_id[ag_id == 7] = 6  # antigen 7 without candidates, antigen 6 with twice as many
+    keep = np.ones(len(ag_id), bool)
+    keep[np.nonzero(ag_id == 0)[0][40:]] = False  # antigen 0: 40 candidates < k
+    off = np.concatenate([[0], np.cumsum(pop.n_res)])
+    rs = np.concatenate([np.arange(off[c], off[c + 1]) for c in np.nonzero(keep)[0]])
+    pos, chi = ctx.build_residues(pop.ca[rs], pop.aa[rs])
+    n_res, ag_k = pop.n_res[keep], ag_id[keep]
+    ctx.state_upload(pop.aa[rs], chi, pos, n_res=n_res, antigen_id=ag_k)
+    for k in (64, 50):
+        e, top = ctx.block(10, 0, k=k, n_segments=8)
+        assert np.array_equal(top, _seg_topk(e, ag_k, 8, k))
+        assert np.all(top[7] == -1) and np.sum(top[0] >= 0) == 40
+
+
+def test_enqueued_blocks_pipeline(ctx, oracle, pkg):
+    """Enqueued blocks (binder_block without outputs, graph on) sum and select each
+    block's energies beside the next block's gradient steps; binder_block_fetch, or any
+    other call, runs the last block's selection first.  Results equal the synchronous
+    blocks', whatever comes between."""
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, n_cand=512, flags=pkg.FLAG_GRAPH)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    sync = [ctx.block(10, 10 * b, k=64) for b in range(5)]
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    for b in range(5):
+        ctx.block_async(10, 10 * b, 64)
+    e, top = ctx.block_fetch(64)
+    assert np.array_equal(e, sync[4][0]) and np.array_equal(top, sync[4][1])
+    # a call between the enqueued blocks and the fetch (the selection runs before it)
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    for b in range(3):
+        ctx.block_async(10, 10 * b, 64)
+    assert np.array_equal(ctx.score_state(), sync[2][0])
+    e, top = ctx.block_fetch(64)
+    assert np.array_equal(e, sync[2][0]) and np.array_equal(top, sync[2][1])
+    # k changes between enqueued blocks; a synchronous block after enqueued ones
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    ctx.block_async(10, 0, 64)
+    ctx.block_async(10, 10, 16)
+    e, top = ctx.block_fetch(16)
+    assert np.array_equal(e, sync[1][0]) and np.array_equal(top[0], sync[1][1][0][:16])
+    ctx.state_upload(aa, chi, pos, uniform_n_res=n_res)
+    ctx.block_async(10, 0, 64)
+    e, top = ctx.block(10, 10, k=64)
+    assert np.array_equal(e, sync[1][0]) and np.array_equal(top, sync[1][1])
