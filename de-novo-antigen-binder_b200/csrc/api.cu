@@ -357,6 +357,8 @@ int enter(binder_ctx* ctx) {
 int clear_err(binder_ctx* ctx) {
     CK(ctx->errf.ensure(1), "alloc err");
     CK(cudaMemsetAsync(ctx->errf.p, 0, sizeof(uint32_t), ctx->stream), "memset err");
+    // the persistent kernels' work queues, left zero by every launch that completes
+    if (ctx->st.queue.p) CK(cudaMemsetAsync(ctx->st.queue.p, 0, 4 * sizeof(int), ctx->stream), "memset queues");
     return BINDER_OK;
 }
 
@@ -1174,7 +1176,9 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     CK(S.bal_order.ensure(std::max(total, 1)), "alloc");
     CK(S.key_counts.ensure(nk + 1), "alloc");
     CK(S.key_cursor.ensure(nk + 1), "alloc");
-    CK(S.queue.ensure(2), "alloc");  // scoring and gradient-step work queues
+    // scoring and gradient-step work queues ([0], [1]) and their done counts ([2], [3])
+    CK(S.queue.ensure(4), "alloc");
+    CK(cudaMemsetAsync(S.queue.p, 0, 4 * sizeof(int), ctx->stream), "memset");
     CK(S.res_e.ensure(std::max(total, 1)), "alloc");
     CK(S.res_abs.ensure(std::max(total, 1)), "alloc");
     S.order_valid = false;

@@ -188,6 +188,22 @@ struct StateView {
     const int* ag_epoch;      // device word: the antigen-set epoch (bumped when antigens change)
 };
 
+// Work queues of persistent kernels: queue[0] hands out tasks, queue[2] counts the
+// CTAs that are done.  Every CTA calls queue_retire once at its end; the last one
+// leaves both counters zero for the next launch, so that no reset is launched
+// between kernels.  (The host zeroes them when it allocates them and before each
+// call's first launch.)
+__device__ __forceinline__ void queue_retire(int* queue) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 2, 1) == (int)gridDim.x - 1) {
+            atomicExch(queue, 0);
+            atomicExch(queue + 2, 0);
+        }
+    }
+}
+
 // spatial.rs:61-67: (x * inv).floor() as i32 — one f32 multiply, floor, saturating cast
 __device__ __forceinline__ int cell_coord(float v, float inv) { return sat_i32(floorf(xmul(v, inv))); }
 

@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(NW * 32) k_score_residues(StateView st, const 
         for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
         if (lane == 0 && p) atomicAdd((unsigned long long*)pair_count, (unsigned long long)p);
     }
+    queue_retire(queue);
 }
 
 template <class Src, int NW, bool KAHAN, bool FULL, bool ABS, bool COUNT>
@@ -603,21 +604,20 @@ int launch_score_state(cudaStream_t s, const StateView& st, const AgView* ags, i
     if (st.n_cand <= 0) return 0;
     const bool kahan = accumulate == 0, abs_ = o.abs_sum != nullptr, count = o.pairs != nullptr;
     const int g = grid_ctas > 0 ? grid_ctas : 148 * 4;
-    cudaMemsetAsync(scr.queue, 0, sizeof(int), s);
     switch (warps_per_cta) {
         case 4: score_residues_nw<4>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
         case 16: score_residues_nw<16>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
         default: score_residues_nw<8>(s, g, st, ags, kahan, full, abs_, count, o, scr); break;
     }
     if (!count && tk && !abs_) {
-        if (tk->defer) return 2;  // the sums and the selection come later (launch_sum_select)
+        if (tk->defer) return 1;  // the sums and the selection come later (launch_sum_select)
         if (tk->mid) cudaEventRecord(tk->mid, s);
         launch_sum_select(s, st, scr.res_e, full, o.energy, *tk);
     } else if (!count) {
         k_sum_residues<<<(st.n_cand + 127) / 128, 128, 0, s>>>(st, scr.res_e, abs_ ? scr.res_abs : nullptr, full,
                                                                o.energy, o.abs_sum);
     }
-    return count ? 2 : 3;  // launches issued (memset counted)
+    return count ? 1 : 2;  // launches issued
 }
 
 void launch_score_state_count(cudaStream_t s, const StateView& st, const AgView* ags, long long* pairs,

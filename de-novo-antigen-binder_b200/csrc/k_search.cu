@@ -429,6 +429,7 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
         residue_task(slot_id);
         if (!queue) break;
     }
+    if (queue) queue_retire(queue);
 }
 
 // ---- gradient steps, flat form -------------------------------------------------------
@@ -445,8 +446,9 @@ __global__ void __launch_bounds__(CG_WARPS * 32, 24 / CG_WARPS) k_langevin(State
 // (set_ca_pos, allatom.rs:289-293) is recorded and the atoms take the recorded
 // translations one after another, in step order, when the record is full and at
 // the end -- the same additions in the same order as translating them every step.
-// Lists live in the state's list storage (global memory); a residue that leaves
-// its skin gets a new list built by the whole warp.  A list that overflows, or a
+// A task's lists live in shared memory (16-bit positions) for the launch and the
+// state's list storage carries them between launches; a residue that leaves its
+// skin gets a new list built by the whole warp in one pass.  A list that overflows, or a
 // cell index near the i32 limits, sends the residue to the one-lane 27-cell walk.
 constexpr int FLAT_HCAP = 128;   // hits a warp holds per round
 constexpr int FLAT_DSTEPS = 10;  // step translations recorded before the atoms take them
@@ -818,6 +820,7 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
         }
         if (!queue) break;
     }
+    if (queue) queue_retire(queue);
 }
 
 // ---- launchers ----------------------------------------------------------------------
@@ -875,109 +878,115 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
 // ---- residue order balancing the gradient-step tasks --------------------------------
 // The flat gradient-step kernel leaves, per residue, a work estimate for the next
 // launch (cg_work: its Verlet-list length plus a charge per list rebuild this launch;
-// 0 before the first launch).  Residues sorted by it, heaviest first (32 bins), are
+// 0 before the first launch).  Residues sorted by it, heaviest first (16 bins), are
 // dealt to the tasks of R residues in snake order (ranks 0..T-1 to tasks 0..T-1,
 // ranks T..2T-1 to tasks T-1..0, ...), so every task takes one residue of each work
 // band and no task of long lists holds up the launch.  Which warp computes a residue
-// never changes its arithmetic, so any order gives the same trajectories.  One CTA,
-// no atomics: a warp counts its residues per bin with five ballots (one per bin bit;
-// lane L owns bin L), a block scan over (bin, warp) gives every warp its offset per
-// bin, and a second pass ranks each residue by its bin's offset, the count of its
-// bin in the warp's earlier rounds and the lower lanes of its round.
+// never changes its arithmetic, so any order gives the same trajectories.
+// One CTA, a counting sort without atomics: thread t takes a contiguous chunk of the
+// residues and counts its bins in its own column of a shared-memory table; one
+// block scan per bin (two bins per 32-bit word) turns the table into offsets in
+// (bin, thread) order; each thread then ranks its chunk in order.
 constexpr int BAL_THREADS = 1024;
-constexpr int BAL_BINS = 32;         // one per lane
-constexpr int BAL_SMEM = 40960;      // work bytes staged in shared memory up to this many residues
+constexpr int BAL_BINS = 16;
+constexpr int BAL_SMEM = 131072;  // work bytes staged in (dynamic) shared memory up to this many residues
 
-__device__ __forceinline__ int bal_bin(uint8_t w) { return (255 - (int)w) >> 3; }
-
-// lanes of this round whose bin is `b` (valid lanes only), from the five bin-bit ballots
-__device__ __forceinline__ unsigned bal_match(const unsigned (&bits)[5], unsigned valid, int b) {
-    unsigned m = valid;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) m &= ((b >> k) & 1) ? bits[k] : ~bits[k];
-    return m;
-}
+__device__ __forceinline__ int bal_bin(uint8_t w) { return (255 - (int)w) >> 4; }
 
 __global__ void __launch_bounds__(BAL_THREADS) k_balance_order(int n, const uint8_t* __restrict__ work, int R,
                                                                int* __restrict__ order) {
-    __shared__ int s_h[BAL_BINS * 32];  // [bin][warp]: counts, then offsets
-    __shared__ int s_wsum[32];
-    __shared__ __align__(16) uint8_t s_w[BAL_SMEM];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    const int rounds = (n + BAL_THREADS - 1) / BAL_THREADS;
-    // the work bytes into shared memory (16 bytes per load, all loads independent)
+    __shared__ uint32_t s_c[BAL_BINS / 2][BAL_THREADS];  // bins 2i (low half), 2i + 1 (high half) per thread
+    __shared__ uint32_t s_wsum[BAL_BINS / 2][32];
+    __shared__ uint32_t s_base[BAL_BINS];
+    extern __shared__ __align__(16) uint8_t s_w[];  // n bytes when staged
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const bool staged = n <= BAL_SMEM;
-    if (staged) {
+    if (staged) {  // the work bytes, 16 per load, all loads independent
         const int n16 = n / 16;
         const uint4* w16 = reinterpret_cast<const uint4*>(work);
-        for (int t = threadIdx.x; t < n16; t += BAL_THREADS) reinterpret_cast<uint4*>(s_w)[t] = __ldg(&w16[t]);
-        for (int t = n16 * 16 + (int)threadIdx.x; t < n; t += BAL_THREADS) s_w[t] = work[t];
-        __syncthreads();
+        for (int i = t; i < n16; i += BAL_THREADS) reinterpret_cast<uint4*>(s_w)[i] = __ldg(&w16[i]);
+        for (int i = n16 * 16 + t; i < n; i += BAL_THREADS) s_w[i] = work[i];
     }
     const uint8_t* wk = staged ? s_w : work;
-    int cnt = 0;  // residues of bin `lane` in this warp
-    for (int i = 0; i < rounds; ++i) {
-        const int r = (int)threadIdx.x + i * BAL_THREADS;
-        const bool v = r < n;
-        const int b = v ? bal_bin(wk[r]) : 0;
-        unsigned bits[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) bits[k] = __ballot_sync(0xffffffffu, v && ((b >> k) & 1));
-        cnt += __popc(bal_match(bits, __ballot_sync(0xffffffffu, v), lane));
-    }
-    s_h[lane * 32 + warp] = cnt;
+    for (int i = 0; i < BAL_BINS / 2; ++i) s_c[i][t] = 0u;
     __syncthreads();
-    // exclusive scan of the 1024 (bin, warp) counts, bin-major: one per thread
-    const int c = s_h[threadIdx.x];
-    int inc = c;
+    const int per = (n + BAL_THREADS - 1) / BAL_THREADS;
+    const int r0 = min(n, t * per), r1 = min(n, r0 + per);
+    for (int r = r0; r < r1; ++r) {
+        const int b = bal_bin(wk[r]);
+        s_c[b >> 1][t] += (b & 1) ? 0x10000u : 1u;
+    }
+    // exclusive scan over threads of every bin pair (counts < 65536 per bin)
+    uint32_t v[BAL_BINS / 2], inc[BAL_BINS / 2];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int x = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc += x;
+    for (int i = 0; i < BAL_BINS / 2; ++i) {
+        v[i] = s_c[i][t];
+        inc[i] = v[i];
     }
-    if (lane == 31) s_wsum[warp] = inc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+#pragma unroll
+        for (int i = 0; i < BAL_BINS / 2; ++i) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc[i], d);
+            if (lane >= d) inc[i] += x;
+        }
+    if (lane == 31)
+#pragma unroll
+        for (int i = 0; i < BAL_BINS / 2; ++i) s_wsum[i][warp] = inc[i];
     __syncthreads();
-    if (warp == 0) {
-        const int w = s_wsum[lane];
-        int wi = w;
+    if (warp < BAL_BINS / 2) {  // warp i scans the warp totals of bin pair i
+        const uint32_t w = s_wsum[warp][lane];
+        uint32_t wi = w;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            const int x = __shfl_up_sync(0xffffffffu, wi, d);
+            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, d);
             if (lane >= d) wi += x;
         }
-        s_wsum[lane] = wi - w;
+        s_wsum[warp][lane] = wi - w;
+        if (lane == 31) {  // bin totals
+            s_base[2 * warp] = wi & 0xFFFFu;
+            s_base[2 * warp + 1] = wi >> 16;
+        }
     }
     __syncthreads();
-    s_h[threadIdx.x] = s_wsum[warp] + inc - c;
-    __syncthreads();
-    int run = s_h[lane * 32 + warp];  // lane L: next rank of bin L in this warp
-    const int T = n / R, full = T * R;
-    for (int i = 0; i < rounds; ++i) {
-        const int r = (int)threadIdx.x + i * BAL_THREADS;
-        const bool v = r < n;
-        const int b = v ? bal_bin(wk[r]) : 0;
-        unsigned bits[5];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) bits[k] = __ballot_sync(0xffffffffu, v && ((b >> k) & 1));
-        const unsigned valid = __ballot_sync(0xffffffffu, v);
-        const int base = __shfl_sync(0xffffffffu, run, b);
-        const int rank = base + __popc(bal_match(bits, valid, b) & lt);
-        run += __popc(bal_match(bits, valid, lane));
-        if (v) {
-            int slot = rank;
-            if (rank < full) {
-                const int round = rank / T, pos = rank - round * T;
-                slot = ((round & 1) ? T - 1 - pos : pos) * R + round;
-            }
-            order[slot] = r;
+    if (t == 0) {  // bin bases, heaviest bin first
+        uint32_t run = 0;
+        for (int b = 0; b < BAL_BINS; ++b) {
+            const uint32_t c = s_base[b];
+            s_base[b] = run;
+            run += c;
         }
+    }
+    __syncthreads();
+    uint32_t off[BAL_BINS];  // this thread's next rank per bin
+#pragma unroll
+    for (int i = 0; i < BAL_BINS / 2; ++i) {
+        const uint32_t before = s_wsum[i][warp] + inc[i] - v[i];
+        off[2 * i] = s_base[2 * i] + (before & 0xFFFFu);
+        off[2 * i + 1] = s_base[2 * i + 1] + (before >> 16);
+    }
+    const int T = n / R, full = T * R;
+    for (int r = r0; r < r1; ++r) {
+        const int b = bal_bin(wk[r]);
+        int rank = 0;
+#pragma unroll
+        for (int i = 0; i < BAL_BINS; ++i)
+            if (i == b) rank = (int)off[i]++;
+        int slot = rank;
+        if (rank < full) {
+            const int round = rank / T, pos = rank - round * T;
+            slot = ((round & 1) ? T - 1 - pos : pos) * R + round;
+        }
+        order[slot] = r;
     }
 }
 
 void launch_balance_order(cudaStream_t s, const StateView& st, int residues_per_task, int* order) {
     if (st.total_res <= 0 || !st.cg_work) return;
-    k_balance_order<<<1, BAL_THREADS, 0, s>>>(st.total_res, st.cg_work, std::max(residues_per_task, 1), order);
+    const int dyn = st.total_res <= BAL_SMEM ? (st.total_res + 15) / 16 * 16 : 0;
+    cudaFuncSetAttribute(k_balance_order, cudaFuncAttributeMaxDynamicSharedMemorySize, BAL_SMEM);
+    k_balance_order<<<1, BAL_THREADS, dyn, s>>>(st.total_res, st.cg_work, std::max(residues_per_task, 1), order);
 }
 
 template <int W, int G>
@@ -995,7 +1004,6 @@ static void diffuse_w(cudaStream_t s, const StateView& st, const AgView* ags, co
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, stage_bytes);
         ctas = std::min(ctas, (long long)std::max(1, sms * std::max(per_sm, 1)));
-        cudaMemsetAsync(queue, 0, sizeof(int), s);
     }
     kern<<<(int)ctas, threads, stage_bytes, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, nullptr, order,
                                                  order_mode, stage_bytes, stage_ag, queue);
@@ -1017,7 +1025,6 @@ static void diffuse_flat(cudaStream_t s, const StateView& st, const AgView* ags,
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, dyn);
         ctas = std::min(ctas, (long long)std::max(1, sms * std::max(per_sm, 1)));
-        cudaMemsetAsync(queue, 0, sizeof(int), s);
     }
     kern<<<(int)ctas, threads, dyn, s>>>(st, ags, p, n_steps, step0, with_noise, temps, err, order, order_mode,
                                          stage_bytes, stage_ag, queue);

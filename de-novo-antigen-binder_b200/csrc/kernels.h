@@ -55,7 +55,7 @@ int launch_score_flat(cudaStream_t s, const float* atoms, const long long* offse
 // warps over a residue work queue; per-residue FP64 energies summed per candidate.
 struct StateScoreScratch {
     const int* order;  // residue visiting order (may be null)
-    int* queue;        // work counter (reset by the launcher)
+    int* queue;        // work counter, queue[2] the done count (left zero by queue_retire)
     double* res_e;     // total_res
     double* res_abs;   // total_res (abs sums)
 };
