@@ -569,11 +569,11 @@ def run_batched(pkg, ctx, torch, ext):
 
 
 # DRAM bytes (read + write) of one launch of each block kernel, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --block-only 8,8,1,1,8`,
+# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --block-only 8,8,1,0,8`,
 # the same per-launch work and launch shape as the timed blocks
-NCU_DRAM_BYTES = {"langevin_cg": 7_163_904 + 4_864, "score_allatom": 3_969_280}
+NCU_DRAM_BYTES = {"langevin_cg": 7_159_040 + 2_048, "score_allatom": 3_888_384}
 NCU_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of "
-                   "bench.py --block-only 8,8,1,1,8 (cold cache, serialised)")
+                   "bench.py --block-only 8,8,1,0,8 (cold cache, serialised)")
 
 SCHEDULES = (150, 200, 250, 300, 375, 450, 600)  # annealed schedule lengths of the learned-proposal study
 LEARNED_SEEDS = tuple(range(21, 33))
@@ -703,20 +703,24 @@ def run_learned_anneal_only(args):
 
 
 def run_block_only(args):
-    """Small profiling case for the search block: 3 eagerly issued blocks of the
-    bench workload at launch shape (cg_warps, cg_lanes[, cg_order[, cg_queue[, cg_flat]]])."""
+    """Small profiling case for the search block: 3 enqueued blocks (CUDA graph, the
+    selection of each block beside the next block's steps) of the bench workload at
+    launch shape (cg_warps, cg_lanes[, cg_order[, cg_queue[, cg_flat]]])."""
     import torch
     from __graft_entry__ import load_package
     pkg = load_package()
     ctx = pkg.GpuContext.create(0)
-    ctx.set_params(pkg.Params.defaults(flags=0))
+    ctx.set_params(pkg.Params.defaults(flags=pkg.FLAG_GRAPH))
     cfg, ag_aa, ag_pos, pop, pos, chi = build_workload(pkg, ctx, 0)
     shape = [int(x) for x in args.block_only.split(",")]
     w, lanes, order, queue, flat = (shape + [1, 1, 0][len(shape) - 2:])[:5]  # defaults: order 1, queue 1, flat 0
-    ctx.set_launch_cfg(8, 4, w, lanes, order, 0, queue, flat)
+    # scoring: 16 warps x 4 CTAs per SM, residue-index queue order (the shape the
+    # autotuner keeps for this workload)
+    ctx.set_launch_cfg(16, 4, w, lanes, order, 1, queue, flat)
     ctx.state_upload(pop.aa, chi, pos, uniform_n_res=int(pop.n_res[0]))
-    for k in range(3):
-        ctx.block(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K)
+    for k in range(3):  # enqueued blocks, as the bench issues them (graph replays)
+        ctx.block_async(N_STEPS_PER_BLOCK, k * N_STEPS_PER_BLOCK, TOP_K)
+    ctx.block_fetch(TOP_K)
     torch.cuda.synchronize()
     print(json.dumps({"block_only": {"cg_warps": w, "cg_lanes": lanes, "cg_order": order, "cg_queue": queue,
                                      "cg_flat": flat, "blocks": 3}}), flush=True)
