@@ -1983,6 +1983,7 @@ int binder_run_allatom(binder_ctx* ctx, const binder_run_cfg* cfg_in, int32_t* o
     for (int i = 0; i < n2; ++i) t2[i] = temp(i, n2);
     const int k1 = cfg.survivors;
     CK(ctx->topk.ensure((size_t)S.n_segments * std::max(k1, cfg.top_n)), "alloc");
+    CK(ctx->energy.ensure(S.n_cand), "alloc");  // before the block graph's capture
     if ((s = clear_err(ctx))) return s;
     // ---- phase 1: blocks of score_every steps, each scored with its survivors ----
     const int per = cfg.score_every > 0 ? cfg.score_every : std::max(n1, 1);
