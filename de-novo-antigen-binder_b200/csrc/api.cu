@@ -126,14 +126,13 @@ struct State {
     // residue order by Calpha cell (an autotuned order of the gradient-step and
     // scoring kernels)
     DBuf<int> key_base, keys, key_counts, key_cursor, order;
-    DBuf<int> bal_order;  // gradient-step order with work-balanced tasks (cg_order 3)
     int n_keys = 0;
     bool order_valid = false;
     // the gradient-step kernel's Verlet lists (csrc/k_search.cu), valid per residue
     DBuf<int> cg_list;
     DBuf<float4> cg_centre;
     DBuf<int4> cg_meta;
-    DBuf<uint8_t> cg_work;  // per residue: the flat gradient-step kernel's work estimate
+    DBuf<int> cg_bal;  // the flat gradient-step kernel's work-balanced order (cg_bal_* in common.cuh)
     const int* ag_epoch = nullptr;  // the context's device epoch word
     // scoring work queue and per-residue energies
     DBuf<int> queue;
@@ -159,7 +158,7 @@ struct State {
         v.cg_list = cg_list.p;
         v.cg_centre = cg_centre.p;
         v.cg_meta = cg_meta.p;
-        v.cg_work = cg_work.p;
+        v.cg_bal = cg_bal.p;
         v.ag_epoch = ag_epoch;
         return v;
     }
@@ -1173,7 +1172,9 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
     if ((s = upload(ctx, S.key_base, kb.data(), kb.size(), "state"))) return s;
     CK(S.keys.ensure(std::max(total, 1)), "alloc");
     CK(S.order.ensure(std::max(total, 1)), "alloc");
-    CK(S.bal_order.ensure(std::max(total, 1)), "alloc");
+    // the flat gradient-step kernel's balanced order: epoch, counts and buckets start empty
+    CK(S.cg_bal.ensure(cg_bal_ints(std::max(total, 1))), "alloc");
+    CK(cudaMemsetAsync(S.cg_bal.p, 0, CG_BAL_HEADER * sizeof(int), ctx->stream), "memset");
     CK(S.key_counts.ensure(nk + 1), "alloc");
     CK(S.key_cursor.ensure(nk + 1), "alloc");
     // scoring and gradient-step work queues ([0], [1]) and their done counts ([2], [3])
@@ -1231,9 +1232,7 @@ static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_re
         CK(S.cg_list.ensure((size_t)total * CG_LIST_CAP), "alloc");
         CK(S.cg_centre.ensure(total), "alloc");
         CK(S.cg_meta.ensure(total), "alloc");
-        CK(S.cg_work.ensure(total), "alloc");
         CK(cudaMemsetAsync(S.cg_meta.p, 0xFF, S.cg_meta.n * sizeof(int4), ctx->stream), "memset");
-        CK(cudaMemsetAsync(S.cg_work.p, 0, S.cg_work.n, ctx->stream), "memset");
     }
     launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
     if (total) LAUNCHED("pack_slots");
@@ -1414,14 +1413,9 @@ int enqueue_diffuse(binder_ctx* ctx, int n_steps, uint32_t step0, int with_noise
     } else {
         S.order_valid = false;  // residues move: the cell order is stale
     }
+    // order 3 (work-balanced tasks) is built by the flat kernel for its next launch
     int order_mode = ctx->cfg.cg_order;
-    if (order_mode == 3 && !S.cg_work.p) order_mode = 1;
-    if (order_mode == 3) {  // tasks balanced by the work estimates of the previous launch
-        launch_balance_order(ctx->stream, S.view(), ctx->cfg.cg_flat ? ctx->cfg.cg_flat : 32 / ctx->cfg.cg_lanes,
-                             S.bal_order.p);
-        LAUNCHED("balance_order");
-        order = S.bal_order.p;
-    }
+    if (order_mode == 3 && (!ctx->cfg.cg_flat || !S.cg_bal.p)) order_mode = 1;
     int max_ag = 0, max_cells = 0;
     for (const auto& a : ctx->ags) {
         const GridView& gv = a->view.ca_grid;
@@ -1567,7 +1561,7 @@ std::vector<uint64_t> block_sig(binder_ctx* ctx, int n_steps, int k) {
         (uint64_t)ctx->ags.size()};
     const void* ptrs[] = {S.cand_res_off.p, S.cand_ag.p, S.cand_id.p, S.res_aa.p, S.res_chi.p, S.res_pos.p,
                           S.res_trig.p, S.res_cand.p, S.ag_cand_idx.p, S.ag_cand_off.p, S.key_base.p, S.keys.p,
-                          S.key_counts.p, S.key_cursor.p, S.order.p, S.bal_order.p, S.queue.p, S.res_e.p,
+                          S.key_counts.p, S.key_cursor.p, S.order.p, S.cg_bal.p, S.queue.p, S.res_e.p,
                           S.res_abs.p,
                           ctx->energy.p, ctx->topk.p, ctx->errf.p, ctx->d_views.p};
     for (const void* q : ptrs) v.push_back((uint64_t)(uintptr_t)q);

@@ -184,9 +184,27 @@ struct StateView {
     int* cg_list;             // total_res * CG list capacity: sorted antigen Calpha positions
     float4* cg_centre;        // total_res: list centre
     int4* cg_meta;            // total_res: {length, antigen, antigen-set epoch, 0}
-    uint8_t* cg_work;         // total_res: work estimate of the residue's next launch (may be null)
+    int* cg_bal;              // work-balanced residue order of the flat gradient-step kernel (cg_bal_*)
     const int* ag_epoch;      // device word: the antigen-set epoch (bumped when antigens change)
 };
+
+// Work-balanced residue order of the flat gradient-step kernel, built by the kernel
+// itself for its next launch: every residue, at the end of its task, appends its
+// index to the bucket of its work band (Verlet-list length plus a charge per rebuild,
+// CG_BAL_BINS bands, heaviest first) of the buffer of parity epoch ^ 1; the next
+// launch reads the buckets of its own parity as the ranks 0..n-1 (band by band) and
+// deals them to its tasks in snake order.  Layout of cg_bal: [0] epoch, [1] CTAs
+// done, [2 + 16 * parity + band] bucket counts, then the buckets, total_res entries
+// each.  The last CTA of a launch zeroes the counts it read and advances the epoch.
+constexpr int CG_BAL_BINS = 16;
+constexpr int CG_BAL_HEADER = 2 + 2 * CG_BAL_BINS;
+__host__ __device__ inline size_t cg_bal_ints(int total_res) {
+    return (size_t)CG_BAL_HEADER + (size_t)2 * CG_BAL_BINS * (size_t)total_res;
+}
+__device__ __forceinline__ int* cg_bal_count(int* bal, int parity) { return bal + 2 + CG_BAL_BINS * parity; }
+__device__ __forceinline__ int* cg_bal_bucket(int* bal, int total_res, int parity, int band) {
+    return bal + CG_BAL_HEADER + ((size_t)(parity * CG_BAL_BINS + band)) * (size_t)total_res;
+}
 
 // Work queues of persistent kernels: queue[0] hands out tasks, queue[2] counts the
 // CTAs that are done.  Every CTA calls queue_retire once at its end; the last one

@@ -99,8 +99,8 @@ __device__ __noinline__ void cg_force_walk(const AgView* __restrict__ ag, float 
 // state's own order (1: candidate after candidate), a stride through it (2:
 // slot * CG_STRIDE mod total, a bijection when total is coprime to the prime
 // CG_STRIDE) that spreads each warp's residues over unrelated candidates, so the
-// costly residues in contact are shared out evenly, or the work-balanced permutation
-// of k_balance_order (3).  Results never depend on it.
+// costly residues in contact are shared out evenly; the flat kernel's order 3
+// (work-balanced tasks) is its own (slot_res).  Results never depend on it.
 constexpr long long CG_STRIDE = 1000003;
 __device__ __forceinline__ int res_of_slot(const int* __restrict__ order, int mode, int slot, int total) {
     if (mode == 2) return (int)(((long long)slot * CG_STRIDE) % total);
@@ -506,17 +506,49 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     FlatWarp<R>& fw = s_fw[threadIdx.x >> 5];
+    // order 3: the ranks of this launch are the buckets the previous launch filled
+    // (cg_bal_* in common.cuh); identity while they do not hold every residue
+    __shared__ int s_bpre[CG_BAL_BINS + 1];
+    __shared__ int s_bpar, s_bvalid;
+    const bool bal = order_mode == 3 && st.cg_bal;
+    if (bal) {
+        if (threadIdx.x == 0) {
+            const int par = st.cg_bal[0] & 1;
+            const int* cnt = cg_bal_count(st.cg_bal, par);
+            int run = 0;
+            for (int b = 0; b < CG_BAL_BINS; ++b) {
+                s_bpre[b] = run;
+                run += cnt[b];
+            }
+            s_bpre[CG_BAL_BINS] = run;
+            s_bpar = par;
+            s_bvalid = run == st.total_res;
+        }
+        __syncthreads();
+    }
+    const int bal_T = st.total_res / R, bal_full = bal_T * R;
+    auto slot_res = [&](int slot) -> int {
+        if (!bal) return res_of_slot(order, order_mode, slot, st.total_res);
+        if (!s_bvalid) return slot;
+        int rank = slot;
+        if (slot < bal_full) {  // snake deal: task t takes ranks j*T + t (j even), j*T + T-1-t (j odd)
+            const int t = slot / R, j = slot - t * R;
+            rank = j * bal_T + ((j & 1) ? bal_T - 1 - t : t);
+        }
+        int b = 0;
+        while (b + 1 < CG_BAL_BINS && s_bpre[b + 1] <= rank) ++b;
+        return cg_bal_bucket(st.cg_bal, st.total_res, s_bpar, b)[rank - s_bpre[b]];
+    };
     // antigen staging, as k_langevin does it
     if (threadIdx.x == 0) {
         int a0 = stage_ag, a1 = stage_ag;
         if (a0 < 0 && !queue) {
             const int first = blockIdx.x * RPC;
             const int last = min(first + RPC, st.total_res) - 1;
-            a0 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, first, st.total_res)]];
-            a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, last, st.total_res)]];
-            if (order_mode == 2)
-                for (int q = first; q <= last && a1 == a0; ++q)
-                    a1 = st.cand_ag[st.res_cand[res_of_slot(order, order_mode, q, st.total_res)]];
+            a0 = st.cand_ag[st.res_cand[slot_res(first)]];
+            a1 = st.cand_ag[st.res_cand[slot_res(last)]];
+            if (order_mode >= 2)
+                for (int q = first; q <= last && a1 == a0; ++q) a1 = st.cand_ag[st.res_cand[slot_res(q)]];
         }
         bool fits = a0 >= 0 && a0 == a1;
         if (fits) {
@@ -577,7 +609,7 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
         // ---- this lane's residue (lanes >= R own none) ----
         const int slot_id = task * R + lane;
         const bool valid = lane < R && slot_id < st.total_res;
-        const int r = valid ? res_of_slot(order, order_mode, slot_id, st.total_res) : 0;
+        const int r = valid ? slot_res(slot_id) : 0;
         const int c = valid ? st.res_cand[r] : 0;
         const int r_local = valid ? r - st.cand_res_off[c] : 0;
         const uint32_t cid = valid ? st.cand_id[c] : 0u;
@@ -795,8 +827,12 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
             st.cg_centre[r] = make_float4(centre.x, centre.y, centre.z, skin);
             st.cg_meta[r] = make_int4(nl, a, epoch, 0);
         }
-        if (valid && st.cg_work)  // the next launch's work estimate (k_balance_order)
-            st.cg_work[r] = (uint8_t)min(255, (nl <= CG_LIST_MAX ? nl : 200) + 32 * nreb);
+        if (bal && valid) {  // the next launch's ranks: this residue into its work band
+            const int w = min(255, (nl <= CG_LIST_MAX ? nl : 200) + 32 * nreb);
+            const int band = (255 - w) >> 4;
+            const int k = atomicAdd(cg_bal_count(st.cg_bal, s_bpar ^ 1) + band, 1);
+            if (k < st.total_res) cg_bal_bucket(st.cg_bal, st.total_res, s_bpar ^ 1, band)[k] = r;
+        }
         {  // rebuilt lists back to the state's list storage, all residues' entries at once
             const int nc = (valid && dirty && nl <= CG_LIST_MAX) ? nl : 0;
             int inc = nc;
@@ -821,6 +857,19 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
         if (!queue) break;
     }
     if (queue) queue_retire(queue);
+    if (bal) {  // the last CTA empties the buckets it read and hands the new ones over
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(st.cg_bal + 1, 1) == (int)gridDim.x - 1) {
+                int* cnt = cg_bal_count(st.cg_bal, s_bpar);
+                for (int b = 0; b < CG_BAL_BINS; ++b) cnt[b] = 0;
+                st.cg_bal[1] = 0;
+                __threadfence();
+                atomicAdd(st.cg_bal, 1);
+            }
+        }
+    }
 }
 
 // ---- launchers ----------------------------------------------------------------------
@@ -873,120 +922,6 @@ void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags
     k_res_key_hist<<<(st.total_res + 255) / 256, 256, 0, s>>>(st, ags, key_base, keys, counts);
     launch_exclusive_scan(s, counts, n_keys, cursor);
     k_res_scatter<<<(st.total_res + 255) / 256, 256, 0, s>>>(st.total_res, keys, cursor, order);
-}
-
-// ---- residue order balancing the gradient-step tasks --------------------------------
-// The flat gradient-step kernel leaves, per residue, a work estimate for the next
-// launch (cg_work: its Verlet-list length plus a charge per list rebuild this launch;
-// 0 before the first launch).  Residues sorted by it, heaviest first (16 bins), are
-// dealt to the tasks of R residues in snake order (ranks 0..T-1 to tasks 0..T-1,
-// ranks T..2T-1 to tasks T-1..0, ...), so every task takes one residue of each work
-// band and no task of long lists holds up the launch.  Which warp computes a residue
-// never changes its arithmetic, so any order gives the same trajectories.
-// One CTA, a counting sort without atomics: thread t takes a contiguous chunk of the
-// residues and counts its bins in its own column of a shared-memory table; one
-// block scan per bin (two bins per 32-bit word) turns the table into offsets in
-// (bin, thread) order; each thread then ranks its chunk in order.
-constexpr int BAL_THREADS = 1024;
-constexpr int BAL_BINS = 16;
-constexpr int BAL_SMEM = 131072;  // work bytes staged in (dynamic) shared memory up to this many residues
-
-__device__ __forceinline__ int bal_bin(uint8_t w) { return (255 - (int)w) >> 4; }
-
-__global__ void __launch_bounds__(BAL_THREADS) k_balance_order(int n, const uint8_t* __restrict__ work, int R,
-                                                               int* __restrict__ order) {
-    __shared__ uint32_t s_c[BAL_BINS / 2][BAL_THREADS];  // bins 2i (low half), 2i + 1 (high half) per thread
-    __shared__ uint32_t s_wsum[BAL_BINS / 2][32];
-    __shared__ uint32_t s_base[BAL_BINS];
-    extern __shared__ __align__(16) uint8_t s_w[];  // n bytes when staged
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const bool staged = n <= BAL_SMEM;
-    if (staged) {  // the work bytes, 16 per load, all loads independent
-        const int n16 = n / 16;
-        const uint4* w16 = reinterpret_cast<const uint4*>(work);
-        for (int i = t; i < n16; i += BAL_THREADS) reinterpret_cast<uint4*>(s_w)[i] = __ldg(&w16[i]);
-        for (int i = n16 * 16 + t; i < n; i += BAL_THREADS) s_w[i] = work[i];
-    }
-    const uint8_t* wk = staged ? s_w : work;
-#pragma unroll
-    for (int i = 0; i < BAL_BINS / 2; ++i) s_c[i][t] = 0u;
-    __syncthreads();
-    const int per = (n + BAL_THREADS - 1) / BAL_THREADS;
-    const int r0 = min(n, t * per), r1 = min(n, r0 + per);
-    for (int r = r0; r < r1; ++r) {
-        const int b = bal_bin(wk[r]);
-        s_c[b >> 1][t] += (b & 1) ? 0x10000u : 1u;
-    }
-    // exclusive scan over threads of every bin pair (counts < 65536 per bin)
-    uint32_t v[BAL_BINS / 2], inc[BAL_BINS / 2];
-#pragma unroll
-    for (int i = 0; i < BAL_BINS / 2; ++i) {
-        v[i] = s_c[i][t];
-        inc[i] = v[i];
-    }
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1)
-#pragma unroll
-        for (int i = 0; i < BAL_BINS / 2; ++i) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, inc[i], d);
-            if (lane >= d) inc[i] += x;
-        }
-    if (lane == 31)
-#pragma unroll
-        for (int i = 0; i < BAL_BINS / 2; ++i) s_wsum[i][warp] = inc[i];
-    __syncthreads();
-    if (warp < BAL_BINS / 2) {  // warp i scans the warp totals of bin pair i
-        const uint32_t w = s_wsum[warp][lane];
-        uint32_t wi = w;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, d);
-            if (lane >= d) wi += x;
-        }
-        s_wsum[warp][lane] = wi - w;
-        if (lane == 31) {  // bin totals
-            s_base[2 * warp] = wi & 0xFFFFu;
-            s_base[2 * warp + 1] = wi >> 16;
-        }
-    }
-    __syncthreads();
-    if (t == 0) {  // bin bases, heaviest bin first
-        uint32_t run = 0;
-        for (int b = 0; b < BAL_BINS; ++b) {
-            const uint32_t c = s_base[b];
-            s_base[b] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-    uint32_t off[BAL_BINS];  // this thread's next rank per bin
-#pragma unroll
-    for (int i = 0; i < BAL_BINS / 2; ++i) {
-        const uint32_t before = s_wsum[i][warp] + inc[i] - v[i];
-        off[2 * i] = s_base[2 * i] + (before & 0xFFFFu);
-        off[2 * i + 1] = s_base[2 * i + 1] + (before >> 16);
-    }
-    const int T = n / R, full = T * R;
-    for (int r = r0; r < r1; ++r) {
-        const int b = bal_bin(wk[r]);
-        int rank = 0;
-#pragma unroll
-        for (int i = 0; i < BAL_BINS; ++i)
-            if (i == b) rank = (int)off[i]++;
-        int slot = rank;
-        if (rank < full) {
-            const int round = rank / T, pos = rank - round * T;
-            slot = ((round & 1) ? T - 1 - pos : pos) * R + round;
-        }
-        order[slot] = r;
-    }
-}
-
-void launch_balance_order(cudaStream_t s, const StateView& st, int residues_per_task, int* order) {
-    if (st.total_res <= 0 || !st.cg_work) return;
-    const int dyn = st.total_res <= BAL_SMEM ? (st.total_res + 15) / 16 * 16 : 0;
-    cudaFuncSetAttribute(k_balance_order, cudaFuncAttributeMaxDynamicSharedMemorySize, BAL_SMEM);
-    k_balance_order<<<1, BAL_THREADS, dyn, s>>>(st.total_res, st.cg_work, std::max(residues_per_task, 1), order);
 }
 
 template <int W, int G>

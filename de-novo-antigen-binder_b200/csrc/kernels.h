@@ -99,9 +99,6 @@ void launch_diffuse(cudaStream_t s, const StateView& st, const AgView* ags, cons
                     int warps_per_cta, int lanes_per_res, int order_mode, int max_ag_res, int max_ag_cells,
                     int stage_ag, int* queue, int flat_res);
 // residue permutation sorted by (antigen, Calpha cell); key_base[a] = first key of antigen a
-// Residue order of the gradient-step launch with tasks of residues_per_task residues
-// balanced by the Verlet-list lengths carried in the state (one CTA).
-void launch_balance_order(cudaStream_t s, const StateView& st, int residues_per_task, int* order);
 void launch_residue_order(cudaStream_t s, const StateView& st, const AgView* ags, const int* key_base, int n_keys,
                           int* keys, int* counts, int* cursor, int* order);
 void launch_pack_slots(cudaStream_t s, int n_res, const float* in, float4* out);

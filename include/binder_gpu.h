@@ -307,9 +307,10 @@ typedef struct binder_launch_cfg {
                                    warps per CTA) or 8 */
     int32_t cg_order;           /* residue order of the gradient-step kernel: 0 by Calpha cell,
                                    1 candidate after candidate, 2 strided (work spread out),
-                                   3 tasks balanced by the work estimates (Verlet-list lengths,
-                                   rebuilds) of the previous launch (one ordering launch before
-                                   the steps) */
+                                   3 (flat form) tasks balanced by the work of the previous
+                                   launch (Verlet-list lengths, rebuilds): each launch leaves its
+                                   residues in work bands for the next, which deals them to its
+                                   tasks heaviest first; no extra launch */
     int32_t score_order;        /* work-queue order of the scoring kernel: 0 by Calpha cell (three
                                    sorting launches after every move), 1 residue index */
     int32_t cg_queue;           /* gradient-step kernel: 0 one CTA per residue batch, 1 persistent
