@@ -90,15 +90,16 @@ __device__ __noinline__ int build_cg_list(const GridView& g, const float4* __res
 }
 
 
-// The same list built by a whole warp in one pass, into 16-bit positions (antigens of
-// at most 65536 Calphas): the lanes find the atom ranges of 32 (dx, dy) columns at a
-// time, a warp prefix sum over the range lengths concatenates them in column order
-// (ascending positions), and the warp tests 32 consecutive atoms of the concatenation
-// per round, each lane finding its column by a binary search over the prefix; a
-// ballot orders the hits.  Writes at most CG_LIST_MAX entries to out and returns the
-// length (all lanes; above CG_LIST_MAX: unusable).
-static __device__ __noinline__ int build_cg_list_warp(const GridView& g, const float4* __restrict__ ca_pq, F3 p,
-                                                      int lane, uint16_t* out, float skin) {
+// The same list built by a whole warp in one pass (positions as T: 16-bit for
+// antigens of at most 65536 Calphas, or int): the lanes find the atom ranges of 32
+// (dx, dy) columns at a time, a warp prefix sum over the range lengths concatenates
+// them in column order (ascending positions), and the warp tests 32 consecutive
+// atoms of the concatenation per round, each lane finding its column by a binary
+// search over the prefix; a ballot orders the hits.  Writes at most CG_LIST_MAX
+// entries to out and returns the length (all lanes; above CG_LIST_MAX: unusable).
+template <typename T>
+__device__ __noinline__ int build_cg_list_warp(const GridView& g, const float4* __restrict__ ca_pq, F3 p, int lane,
+                                               T* out, float skin) {
     const float R = 10.0f + skin + 0.01f, R2 = R * R;
     const int c[3] = {cell_coord(p.x, g.inv), cell_coord(p.y, g.inv), cell_coord(p.z, g.inv)};
     if (cell_far(c[0], c[1], c[2]) || !(R <= 8.0f * g.cell)) return CG_LIST_MAX + 1;
@@ -160,7 +161,7 @@ static __device__ __noinline__ int build_cg_list_warp(const GridView& g, const f
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             const int w = n + __popc(m & lt);
-            if (hit && w < CG_LIST_MAX) out[w] = (uint16_t)i;
+            if (hit && w < CG_LIST_MAX) out[w] = (T)i;
             n += __popc(m);
         }
     }

@@ -806,6 +806,36 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             const int g0 = tid - gl;  // first thread of the group
             for (int base = 0; base < n; base += CG_RES_PER_PASS) {
                 const int r = base + tid / CG_LANES;
+                if (lists) {
+                    // lists the residues' Calphas outran: rebuilt by the whole warp, one
+                    // residue after another (a one-pass build with 32 lanes instead of a
+                    // two-pass build with the group's 8 lanes)
+                    bool need = false;
+                    F3 ca = {0.f, 0.f, 0.f};
+                    float skin = CG_SKIN;
+                    if (gl == 0 && r < n) {
+                        ca = f3(S.pos[r * SLOT_STRIDE + 1]);
+                        const float4 cc = S.cgcentre[r];
+                        const int nl = S.cgnl[r];
+                        const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
+                        need = nl < 0 || !(mx * mx + my * my + mz * mz <= (cc.w - 0.01f) * (cc.w - 0.01f));
+                        skin = nl < 0 ? CG_SKIN : fminf(2.0f * cc.w, CG_SKIN_MAX);
+                    }
+                    for (unsigned m = __ballot_sync(0xffffffffu, need); m; m &= m - 1) {
+                        const int q = __ffs(m) - 1;
+                        const int rq = __shfl_sync(0xffffffffu, r, q);
+                        const F3 cq = {__shfl_sync(0xffffffffu, ca.x, q), __shfl_sync(0xffffffffu, ca.y, q),
+                                       __shfl_sync(0xffffffffu, ca.z, q)};
+                        const float sq = __shfl_sync(0xffffffffu, skin, q);
+                        const int nl = build_cg_list_warp<int>(A.ca_grid, A.ca_pq, cq, lane,
+                                                               S.cglist + (size_t)rq * CG_LIST_MAX, sq);
+                        if (lane == q) {
+                            S.cgcentre[rq] = make_float4(cq.x, cq.y, cq.z, sq);
+                            S.cgnl[rq] = nl;
+                        }
+                    }
+                    __syncwarp();
+                }
                 if (r >= n) continue;  // whole groups leave together
                 const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
                 if (gl == 0 && err && (!isfinite(ca.x) || !isfinite(ca.y) || !isfinite(ca.z))) atomicOr(err, ERRF_NAN);

@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(W * 32, (R <= 4 ? 32 : 24) / W) k_langevin_fla
             g.cell_start = sstart;
             pq = spq;
         }
-        return build_cg_list_warp(g, pq, centre, lane, fw.sl[q], skin);
+        return build_cg_list_warp<uint16_t>(g, pq, centre, lane, fw.sl[q], skin);
     };
 
     int task = blockIdx.x * W + (int)(threadIdx.x >> 5);
