@@ -102,10 +102,11 @@ __host__ __device__ inline size_t anneal_terms_bytes(int R, int learned) {
     const size_t t = (size_t)L * CG_SLOTS * 16;
     return learned && t < (size_t)MT_BYTES ? (size_t)MT_BYTES : t;
 }
-__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned, int fv = 0) {
+__host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int learned, int fv = 0,
+                                                    int warps = AN_WARPS) {
     const int L = (R < CG_RES_PER_PASS ? R : CG_RES_PER_PASS) * CG_LANES;
     return (size_t)R * SLOT_STRIDE * 16 * 3 + (size_t)R * 16 * 5 + anneal_terms_bytes(R, learned) +
-           (size_t)AN_WARPS * STAGE_CAP * 16 + (size_t)G * 64 + (size_t)anneal_xyz_len(G) * 12 +
+           (size_t)warps * STAGE_CAP * 16 + (size_t)G * 64 + (size_t)anneal_xyz_len(G) * 12 +
            ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
            (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
@@ -113,7 +114,7 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4) +  // 15: alignment of cgcentre
            (fv ? 15 + (size_t)R * 64 : 0);
 }
-__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned, int fv = 0) {
+__device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learned, int fv = 0, int warps = AN_WARPS) {
     AnSmem s;
     const int L = min(R, CG_RES_PER_PASS) * CG_LANES;
     auto take = [&](size_t bytes) { unsigned char* p = b; b += bytes; return p; };
@@ -125,7 +126,7 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.ldelta = (float4*)take((size_t)R * 16);
     s.bb_trig = (float4*)take((size_t)R * 16);
     s.terms = (float4*)take(anneal_terms_bytes(R, learned));
-    s.stage = (float4*)take((size_t)AN_WARPS * STAGE_CAP * 16);
+    s.stage = (float4*)take((size_t)warps * STAGE_CAP * 16);
     s.agq = (float4*)take((size_t)G * 16);
     s.agp = (float4*)take((size_t)G * 16);
     s.cgq = (float4*)take((size_t)G * 16);
@@ -475,7 +476,7 @@ __device__ void rotate_downstream(const AnSmem& S, int n, int r, bool phi, float
     const F3 axis = norm3(sub3(a1, a0));
     const F3 origin = a1;
     const int n_at_r = s_topo_n[S.aa[r]];
-    for (int idx = threadIdx.x; idx < (n - r) * SLOT_STRIDE; idx += AN_THREADS) {
+    for (int idx = threadIdx.x; idx < (n - r) * SLOT_STRIDE; idx += blockDim.x) {
         const int q = r + idx / SLOT_STRIDE, k = idx % SLOT_STRIDE;
         const bool mv = q == r ? (phi ? (k >= 2 && k < n_at_r) : k == 3) : k < s_topo_n[S.aa[q]];
         if (mv) {
@@ -694,16 +695,18 @@ __device__ __noinline__ void an_learned_choices(unsigned char* smem, int R, int 
 // as it is in the state; Calpha energies gain the partner chain's contribution, the
 // force its compute_forces term, and the mutation / rotamer moves follow the CDR
 // flags fv_cdr (per residue) instead of the interface mask.  Draw streams + 4 * chain.
-template <class ACC, bool EXT, bool FV>
-__global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
+template <class ACC, bool EXT, bool FV, int W>
+__global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st, const AgView* __restrict__ ags, StepParams p,
                                                        int n_steps, uint32_t step0, int with_noise,
                                                        const float* __restrict__ temps, int R, int G, int C,
                                                        uint32_t* __restrict__ err, long long* __restrict__ stats,
                                                        MlpDev mlp, int learned, MlpTuple* __restrict__ tlog,
                                                        unsigned long long* __restrict__ log_n, long long log_cap,
                                                        int fv_chain, const uint8_t* __restrict__ fv_cdr) {
+    static_assert(W == AN_WARPS || (W == 2 * AN_WARPS && !EXT), "8 warps, or 16 without the network");
+    constexpr int NT = W * 32;  // threads of the CTA
     extern __shared__ __align__(16) unsigned char an_smem[];
-    const AnSmem S = carve(an_smem, R, G, C, learned, FV ? 1 : 0);
+    const AnSmem S = carve(an_smem, R, G, C, learned, FV ? 1 : 0, W);
     const int c = FV ? 2 * (int)blockIdx.x + fv_chain : (int)blockIdx.x;
     const uint32_t sh = FV ? 4u * (uint32_t)fv_chain : 0u;  // draw stream offset of the chain
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -718,7 +721,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     const bool staged = nag <= G;
     const int ncell = A.ca_grid.nx * A.ca_grid.ny * A.ca_grid.nz + 1;
     const bool cells_staged = staged && ncell <= C;
-    for (int i = tid; staged && i < nag; i += AN_THREADS) {
+    for (int i = tid; staged && i < nag; i += NT) {
         const float4 q = A.ca_atom[i];
         S.agq[i] = q;
         S.agp[i] = A.ca_atom_prm[i];
@@ -729,11 +732,11 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         S.agz[i] = q.z;
     }
     if (tid == 0 && staged && (nag & 1)) S.agx[nag] = S.agy[nag] = S.agz[nag] = 1e30f;
-    for (int i = tid; cells_staged && i < ncell; i += AN_THREADS) S.cgcell[i] = A.ca_grid.cell_start[i];
+    for (int i = tid; cells_staged && i < ncell; i += NT) S.cgcell[i] = A.ca_grid.cell_start[i];
     if (EXT && learned) {  // the network's features and epilogues read these every step
-        for (int i = tid; staged && i < nag; i += AN_THREADS) S.agaa[i] = A.res_aa[i];
-        for (int i = tid; i <= MLP_COUNT_CAP; i += AN_THREADS) S.lg1p[i] = g_an_log1p[i];
-        for (int i = tid; i < MLP_BIASES; i += AN_THREADS)
+        for (int i = tid; staged && i < nag; i += NT) S.agaa[i] = A.res_aa[i];
+        for (int i = tid; i <= MLP_COUNT_CAP; i += NT) S.lg1p[i] = g_an_log1p[i];
+        for (int i = tid; i < MLP_BIASES; i += NT)
             S.mbias[i] = i < MLP_H ? mlp.b1[i] : i < 2 * MLP_H ? mlp.b2[i - MLP_H] : mlp.b3[i - 2 * MLP_H];
     }
     __syncthreads();
@@ -750,7 +753,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
     if (FV) {
         const int pc = c ^ 1, p0 = st.cand_res_off[pc];
         np = min(st.cand_res_off[pc + 1] - p0, R);
-        for (int i = tid; i < np; i += AN_THREADS) {
+        for (int i = tid; i < np; i += NT) {
             const float4 v = st.res_pos[(size_t)(p0 + i) * SLOT_STRIDE + 1];
             const int a = st.res_aa[p0 + i];
             const float4 q = s_ca_atom[a], rl = s_res[a];
@@ -772,8 +775,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         return e;
     };
 
-    for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
-    for (int r = tid; r < n; r += AN_THREADS) {
+    for (int i = tid; i < n * SLOT_STRIDE; i += NT) S.pos[i] = st.res_pos[(size_t)r0 * SLOT_STRIDE + i];
+    for (int r = tid; r < n; r += NT) {
         const int a = st.res_aa[r0 + r];
         const float4 chi = st.res_chi[r0 + r];
         S.aa[r] = a;
@@ -792,7 +795,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         }
     }
     const bool lists = anneal_list_res(R) > 0;  // Verlet lists of the Langevin force
-    for (int r = tid; lists && r < n; r += AN_THREADS) S.cgnl[r] = -1;
+    for (int r = tid; lists && r < n; r += NT) S.cgnl[r] = -1;
     long long n_mc = 0, n_mc_acc = 0, n_bb = 0, n_bb_acc = 0;
     __syncthreads();
 
@@ -804,7 +807,9 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             const int gl = tid % CG_LANES;
             const unsigned gmask = ((1u << CG_LANES) - 1u) << (lane & ~(CG_LANES - 1));
             const int g0 = tid - gl;  // first thread of the group
-            for (int base = 0; base < n; base += CG_RES_PER_PASS) {
+            // the first CG_RES_PER_PASS * CG_LANES threads (whole warps; with 16 warps the
+            // others wait at the barrier below)
+            for (int base = 0; tid < CG_RES_PER_PASS * CG_LANES && base < n; base += CG_RES_PER_PASS) {
                 const int r = base + tid / CG_LANES;
                 if (lists) {
                     // lists the residues' Calphas outran: rebuilt by the whole warp, one
@@ -889,7 +894,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             S.iscal[IS_LASTCYS] = -1;
         }
         __syncthreads();
-        for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) {
+        for (int i = tid; i < n * SLOT_STRIDE; i += NT) {
             const int r = i / SLOT_STRIDE, k = i % SLOT_STRIDE;
             if (k < s_topo_n[S.aa[r]]) {
                 const float4 d = S.ldelta[r];
@@ -901,7 +906,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         __syncthreads();
 
         // ---- 2. interface mask (diffusion.rs:343-351; Fv: CDR flags instead) + move draws ----
-        for (int r = warp; !FV && r < n; r += AN_WARPS) {
+        for (int r = warp; !FV && r < n; r += W) {
             const F3 ca = f3(S.pos[r * SLOT_STRIDE + 1]);
             bool hit = false;
             for (int base = 0; base < nag && !hit; base += 64) {
@@ -918,7 +923,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             }
             if (lane == 0) S.iface[r] = hit;
         }
-        for (int r = tid; r < n; r += AN_THREADS) {
+        for (int r = tid; r < n; r += NT) {
             const U4 d = rng_draw(p.seed, cid, step, STREAM_BACKBONE + sh, (uint32_t)r);
             const bool att = u01(d.x) < p.backbone_move_p;
             S.bb_att[r] = att;
@@ -933,7 +938,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         __syncthreads();
 
         // ---- 3. mutation / rotamer proposals (diffusion.rs:354-399) ----
-        for (int r = tid; r < n; r += AN_THREADS) {
+        for (int r = tid; r < n; r += NT) {
             const U4 d = rng_draw(p.seed, cid, step, STREAM_MC + sh, (uint32_t)r);
             const int aa = S.aa[r];
             int kind = MV_NONE;
@@ -988,13 +993,13 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             an_learned_choices(an_smem, R, G, C, n, agq, staged ? S.agaa : A.res_aa, nag, mlp, temp);
         // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
         // the Calpha energies before / after each move on warps 0..3 (one warp each)
-        if (warp >= AN_WARPS / 2) {
-            for (int t = tid - AN_THREADS / 2; t < 2 * n; t += AN_THREADS / 2) {
+        if (warp >= W / 2) {
+            for (int t = tid - NT / 2; t < 2 * n; t += NT / 2) {
                 const int r = t >> 1;
                 if (S.kind[r] != MV_NONE) build_move(S, r, (t & 1) ? SEL_REJ : SEL_PROP);
             }
         } else {
-            for (int t = warp; t < 2 * n; t += AN_WARPS / 2) {
+            for (int t = warp; t < 2 * n; t += W / 2) {
                 const int r = t >> 1, which = t & 1;
                 const int kind = S.kind[r];
                 if (kind == MV_NONE) continue;
@@ -1084,7 +1089,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             }
         }
         __syncthreads();
-        for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) {
+        for (int i = tid; i < n * SLOT_STRIDE; i += NT) {
             const int r = i / SLOT_STRIDE;
             const int sl = S.sel[r];
             if (sl == SEL_PROP) S.pos[i] = S.prop[i];
@@ -1105,7 +1110,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
                 S.dscal[0] = (double)disulfide_of<ACC, false>(S, n, -1, nullptr, 0);
                 S.iscal[IS_DVALID] = 1;
             }
-            for (int i = r + warp; i < n; i += AN_WARPS) {
+            for (int i = r + warp; i < n; i += W) {
                 if (S.valid[i]) continue;
                 const ACC e = ca_energy(f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i]);
                 if (lane == 0) {
@@ -1122,7 +1127,7 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
             const float4 bt = S.bb_trig[r];
             rotate_downstream(S, n, r, phi, bt.x, bt.y);
             __syncthreads();
-            for (int i = r + 1 + warp; i < n; i += AN_WARPS) {
+            for (int i = r + 1 + warp; i < n; i += W) {
                 const ACC e = ca_energy(f3(S.pos[i * SLOT_STRIDE + 1]), S.aa[i]);
                 if (lane == 0) S.c_new[i] = (double)e;
             }
@@ -1153,8 +1158,8 @@ __global__ void __launch_bounds__(AN_THREADS, 2) k_anneal(StateView st, const Ag
         }
     }
 
-    for (int i = tid; i < n * SLOT_STRIDE; i += AN_THREADS) st.res_pos[(size_t)r0 * SLOT_STRIDE + i] = S.pos[i];
-    for (int r = tid; r < n; r += AN_THREADS) {
+    for (int i = tid; i < n * SLOT_STRIDE; i += NT) st.res_pos[(size_t)r0 * SLOT_STRIDE + i] = S.pos[i];
+    for (int r = tid; r < n; r += NT) {
         st.res_aa[r0 + r] = (uint8_t)S.aa[r];
         st.res_chi[r0 + r] = S.chi[r];
         st.res_trig[2 * (r0 + r)] = S.trig[2 * r];
@@ -1236,17 +1241,37 @@ cudaError_t launch_anneal(cudaStream_t s, const StateView& st, const AgView* ags
     const bool ext = !fv && (x.learned || x.log);
     const int grid = fv ? st.n_cand / 2 : st.n_cand;
     if (grid <= 0) return cudaSuccess;
-    auto run = [&](auto kern) -> cudaError_t {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // a grid that leaves SMs idle (the 64 survivors of phase 2) takes 16 warps per
+    // candidate: the per-residue passes (Calpha energies, builds, backbone moves) need
+    // fewer rounds; the network path keeps 8
+    int sms = 148;
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const bool wide = !ext && grid <= sms;
+    const size_t smem16 = anneal_smem_bytes(max_res, G, C, learned, fv ? 1 : 0, 2 * AN_WARPS);
+    auto run = [&](auto kern, int warps) -> cudaError_t {
+        const size_t sm = warps == AN_WARPS ? smem : smem16;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e) return e;
-        kern<<<grid, AN_THREADS, smem, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G, C, err, stats,
-                                            x.mlp, learned, x.log, x.log_n, x.log_cap, fv ? fv_chain : 0, fv_cdr);
+        kern<<<grid, warps * 32, sm, s>>>(st, ags, p, n_steps, step0, with_noise, temps, max_res, G, C, err, stats,
+                                          x.mlp, learned, x.log, x.log_n, x.log_cap, fv ? fv_chain : 0, fv_cdr);
         return cudaSuccess;
     };
+    constexpr int W8 = AN_WARPS, W16 = 2 * AN_WARPS;
     cudaError_t e;
-    if (fv) e = accumulate == 1 ? run(k_anneal<float, false, true>) : run(k_anneal<double, false, true>);
-    else if (accumulate == 1) e = ext ? run(k_anneal<float, true, false>) : run(k_anneal<float, false, false>);
-    else e = ext ? run(k_anneal<double, true, false>) : run(k_anneal<double, false, false>);
+    if (fv) {
+        if (accumulate == 1) e = wide ? run(k_anneal<float, false, true, W16>, W16) : run(k_anneal<float, false, true, W8>, W8);
+        else e = wide ? run(k_anneal<double, false, true, W16>, W16) : run(k_anneal<double, false, true, W8>, W8);
+    } else if (ext) {
+        e = accumulate == 1 ? run(k_anneal<float, true, false, W8>, W8) : run(k_anneal<double, true, false, W8>, W8);
+    } else if (accumulate == 1) {
+        e = wide ? run(k_anneal<float, false, false, W16>, W16) : run(k_anneal<float, false, false, W8>, W8);
+    } else {
+        e = wide ? run(k_anneal<double, false, false, W16>, W16) : run(k_anneal<double, false, false, W8>, W8);
+    }
     if (e) return e;
     return cudaGetLastError();
 }
