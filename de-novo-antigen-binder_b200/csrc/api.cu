@@ -254,6 +254,11 @@ struct binder_ctx {
     bool pipe_graph_order = false;
     bool sel_pending = false;
     int sel_k = 0;
+    // binder_block_io as one graph (copies in, block, copies out) for pinned host arrays
+    cudaGraphExec_t io_graph = nullptr;
+    std::vector<uint64_t> io_graph_sig;
+    int io_graph_launches = 0;
+    bool io_graph_order = false;
     std::vector<std::pair<std::string, LaunchCfg>> tune_cache;
     MlpState mlp;
     // antigen-set epoch (device word read by the gradient-step kernel)
@@ -277,9 +282,14 @@ struct binder_ctx {
         if (pipe_graph) cudaGraphExecDestroy(pipe_graph);
         pipe_graph = nullptr;
     }
+    void drop_io_graph() {
+        if (io_graph) cudaGraphExecDestroy(io_graph);
+        io_graph = nullptr;
+    }
     void drop_graph() {
         drop_block_graph();
         drop_pipe_graph();
+        drop_io_graph();
     }
     ~binder_ctx() {
         drop_graph();
@@ -1191,9 +1201,11 @@ int set_state_meta(binder_ctx* ctx, const std::vector<int>& off, const std::vect
 extern "C" {
 
 // The upload; sync = wait for the copies (the caller may reuse its arrays at once).
+// copy_data false: validate, set the metadata and size the buffers, but leave the
+// residue arrays and their packing to the caller (binder_block_io's graph)
 static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_t uniform_n_res,
                              const int32_t* antigen_id, const uint32_t* cand_id, const uint8_t* aa,
-                             const float* chi, const float* pos, bool sync) {
+                             const float* chi, const float* pos, bool sync, bool copy_data = true) {
     int s = enter(ctx);
     if (s) return s;
     if (ctx->ags.empty()) return fail(ctx, BINDER_ERR_STATE, "no antigen added");
@@ -1222,20 +1234,27 @@ static int state_upload_impl(binder_ctx* ctx, size_t n_cand, const int32_t* n_re
                            S.h_cand_ag == ag && S.h_cand_id == ids && S.h_orig == orig;
     if (same_meta) S.order_valid = false;
     else if ((s = set_state_meta(ctx, off, ag, ids, orig))) return s;
-    if ((s = upload(ctx, S.res_aa, aa, (size_t)total, "state"))) return s;
     S.trig_valid = false;
+    CK(S.res_aa.ensure(total), "alloc");
     CK(S.res_chi.ensure(total), "alloc");
-    if (total) CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
-    if ((s = upload(ctx, S.stage, pos, (size_t)total * SLOTS * 3, "state"))) return s;
+    CK(S.stage.ensure((size_t)total * SLOTS * 3), "alloc");
     CK(S.res_pos.ensure((size_t)total * SLOT_STRIDE), "alloc");
+    if (copy_data && total) {
+        CK(cudaMemcpyAsync(S.res_aa.p, aa, (size_t)total, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+        CK(cudaMemcpyAsync(S.stage.p, pos, (size_t)total * SLOTS * 3 * 4, cudaMemcpyHostToDevice, ctx->stream),
+           "H2D");
+    }
     if (S.cg_meta.n < (size_t)total || !S.cg_meta.p) {  // fresh list storage: every list invalid
         CK(S.cg_list.ensure((size_t)total * CG_LIST_CAP), "alloc");
         CK(S.cg_centre.ensure(total), "alloc");
         CK(S.cg_meta.ensure(total), "alloc");
         CK(cudaMemsetAsync(S.cg_meta.p, 0xFF, S.cg_meta.n * sizeof(int4), ctx->stream), "memset");
     }
-    launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
-    if (total) LAUNCHED("pack_slots");
+    if (copy_data) {
+        launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
+        if (total) LAUNCHED("pack_slots");
+    }
     CK(S.mc_stats.ensure(4 * n_cand), "alloc");
     CK(cudaMemsetAsync(S.mc_stats.p, 0, 4 * n_cand * sizeof(long long), ctx->stream), "memset");
     if (sync) CK(cudaStreamSynchronize(ctx->stream), "synchronize");
@@ -1903,45 +1922,124 @@ int binder_block_io(binder_ctx* ctx, size_t n_cand, const int32_t* n_res, int32_
                     const int32_t* antigen_id, const uint32_t* cand_id, uint8_t* aa, float* chi, float* pos,
                     int n_steps, int k, double* out_e, int32_t* out_topk) {
     if (n_steps < 0 || k < 0 || k > 1024) return fail(ctx, BINDER_ERR_ARG, "bad n_steps or k");
-    // no wait after the upload: the write-back into the same arrays comes later on
-    // the streams, after the kernels that follow the copies
-    int s = state_upload_impl(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos, false);
+    // the metadata and buffers first; the residue arrays travel with the block
+    int s = state_upload_impl(ctx, n_cand, n_res, uniform_n_res, antigen_id, cand_id, aa, chi, pos, false, false);
     if (s) return s;
     State& S = ctx->st;
     if ((s = ensure_side(ctx))) return s;
+    bool tuned = true;
     if (ctx->params.flags & BINDER_FLAG_AUTOTUNE) {
         const std::string key = tune_key(ctx);
         bool known = false;
         for (const auto& e : ctx->tune_cache) known |= e.first == key;
-        if (!known && (s = binder_autotune(ctx, 5, nullptr))) return s;
+        tuned = known;
     }
     ctx->async_pending = false;  // any enqueued blocks ran on the replaced state
     if ((s = clear_err(ctx))) return s;
     CK(ctx->energy.ensure(S.n_cand), "alloc");
     if (k > 0) CK(ctx->topk.ensure((size_t)S.n_segments * k), "alloc");
+    CK(ctx->h_energy.ensure(2 * (size_t)S.n_cand), "alloc host");
     ctx->last_k = k;
     const int total = S.total_res;
-    CK(S.stage.ensure((size_t)total * SLOTS * 3), "alloc");
-    if (n_steps > 0 && (s = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return s;
-    // the moved residues go back to the host on the second stream while this one
-    // scores them (both only read the positions)
-    CK(cudaEventRecord(ctx->ev_fork, ctx->stream), "event");
-    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0), "event");
-    launch_unpack_slots(ctx->side, total, S.res_pos.p, S.stage.p);
-    LAUNCHED("unpack_slots");
-    CK(cudaMemcpyAsync(pos, S.stage.p, (size_t)total * SLOTS * 3 * 4, cudaMemcpyDeviceToHost, ctx->side), "D2H");
-    CK(cudaMemcpyAsync(chi, S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->side), "D2H");
-    CK(cudaMemcpyAsync(aa, S.res_aa.p, total, cudaMemcpyDeviceToHost, ctx->side), "D2H");
-    CK(cudaEventRecord(ctx->ev_join, ctx->side), "event");
-    if ((s = enqueue_score_topk(ctx, 0, k))) return s;
-    if (k > 0) {
-        if (out_topk)
+    if (!tuned) {  // the autotuner times launch shapes on the uploaded state
+        if (total) {
+            CK(cudaMemcpyAsync(S.res_aa.p, aa, (size_t)total, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+            CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+            CK(cudaMemcpyAsync(S.stage.p, pos, (size_t)total * SLOTS * 3 * 4, cudaMemcpyHostToDevice, ctx->stream),
+               "H2D");
+            launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
+            LAUNCHED("pack_slots");
+        }
+        if ((s = binder_autotune(ctx, 5, nullptr))) return s;
+        if ((s = clear_err(ctx))) return s;
+    }
+    // the copies in, the block, the moved residues out on the second stream while
+    // the first one scores them (both only read the positions), the energies and
+    // survivors out: one graph when every host array is pinned (it bakes their
+    // addresses in), else the same launches one by one
+    auto enqueue = [&]() -> int {
+        int e = 0;
+        if (total) {
+            CK(cudaMemcpyAsync(S.res_aa.p, aa, (size_t)total, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+            CK(cudaMemcpyAsync(S.res_chi.p, chi, (size_t)total * 16, cudaMemcpyHostToDevice, ctx->stream), "H2D");
+            CK(cudaMemcpyAsync(S.stage.p, pos, (size_t)total * SLOTS * 3 * 4, cudaMemcpyHostToDevice, ctx->stream),
+               "H2D");
+            launch_pack_slots(ctx->stream, total, S.stage.p, S.res_pos.p);
+            LAUNCHED("pack_slots");
+        }
+        if (n_steps > 0 && (e = enqueue_diffuse(ctx, n_steps, 0, 0, 0, nullptr))) return e;
+        CK(cudaEventRecord(ctx->ev_fork, ctx->stream), "event");
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0), "event");
+        if (total) {
+            launch_unpack_slots(ctx->side, total, S.res_pos.p, S.stage.p);
+            LAUNCHED("unpack_slots");
+            CK(cudaMemcpyAsync(pos, S.stage.p, (size_t)total * SLOTS * 3 * 4, cudaMemcpyDeviceToHost, ctx->side),
+               "D2H");
+            CK(cudaMemcpyAsync(chi, S.res_chi.p, (size_t)total * 16, cudaMemcpyDeviceToHost, ctx->side), "D2H");
+            CK(cudaMemcpyAsync(aa, S.res_aa.p, total, cudaMemcpyDeviceToHost, ctx->side), "D2H");
+        }
+        CK(cudaEventRecord(ctx->ev_join, ctx->side), "event");
+        if ((e = enqueue_score_topk(ctx, 0, k))) return e;
+        if (k > 0 && out_topk)
             CK(cudaMemcpyAsync(out_topk, ctx->topk.p, (size_t)S.n_segments * k * sizeof(int), cudaMemcpyDeviceToHost,
                                ctx->stream),
                "D2H");
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0), "event");
+        CK(cudaMemcpyAsync(ctx->h_energy.p, ctx->energy.p, S.n_cand * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "energy D2H");
+        return BINDER_OK;
+    };
+    auto pinned = [](const void* p) {
+        if (!p) return true;
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    };
+    const bool graph = (ctx->params.flags & BINDER_FLAG_GRAPH) && !ctx->timing && total > 0 && pinned(aa) &&
+                       pinned(chi) && pinned(pos) && (k == 0 || !out_topk || pinned(out_topk));
+    if (graph) {
+        std::vector<uint64_t> sig = block_sig(ctx, n_steps, k);
+        for (const void* q : {(const void*)aa, (const void*)chi, (const void*)pos, (const void*)out_topk,
+                              (const void*)ctx->h_energy.p, (const void*)S.stage.p, (const void*)ctx->side})
+            sig.push_back((uint64_t)(uintptr_t)q);
+        if (!ctx->io_graph || ctx->io_graph_sig != sig) {
+            ctx->drop_io_graph();
+            const uint64_t l0 = ctx->launches;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            s = enqueue();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (s || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                ctx->launches = l0;
+                return s ? s : cuda_fail(ctx, e, "end capture");
+            }
+            e = cudaGraphInstantiate(&ctx->io_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                ctx->io_graph = nullptr;
+                ctx->launches = l0;
+                return cuda_fail(ctx, e, "graph instantiate");
+            }
+            ctx->io_graph_launches = (int)(ctx->launches - l0);
+            ctx->io_graph_order = S.order_valid;
+            ctx->launches = l0;
+            ctx->io_graph_sig = sig;
+        }
+        CK(cudaGraphLaunch(ctx->io_graph, ctx->stream), "graph launch");
+        ctx->launches += ctx->io_graph_launches;
+        S.order_valid = ctx->io_graph_order;
+    } else if ((s = enqueue())) {
+        return s;
     }
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0), "event");
-    return fetch_energies(ctx, S.n_cand, out_e, nullptr, nullptr);  // synchronises both streams
+    if ((s = check_err(ctx))) return s;  // synchronises; the side stream joined before the energies
+    if (out_e) std::memcpy(out_e, ctx->h_energy.p, S.n_cand * sizeof(double));
+    return BINDER_OK;
 }
 
 void binder_default_run_cfg(binder_run_cfg* c) {

@@ -275,3 +275,29 @@ def test_enqueued_blocks_pipeline(ctx, oracle, pkg):
     ctx.block_async(10, 0, 64)
     e, top = ctx.block(10, 10, k=64)
     assert np.array_equal(e, sync[1][0]) and np.array_equal(top, sync[1][1])
+
+
+def test_block_io_graph_with_pinned_arrays(ctx, oracle, pkg):
+    """binder_block_io with pinned host arrays runs as one CUDA graph (copies in, block,
+    copies out): the same energies, survivors and written-back residues as with
+    pageable arrays (launches one by one), on repeated calls and a new population."""
+    import torch
+    aa, chi, pos, n_res = _setup(ctx, oracle, pkg, n_cand=256, flags=pkg.FLAG_GRAPH)
+    chi, pos = np.array(chi, np.float32), np.array(pos, np.float32)
+    pa = torch.empty(aa.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    pc = torch.empty(chi.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pp = torch.empty(pos.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pt = torch.empty(64, dtype=torch.int32, pin_memory=True).numpy()
+    a, c, p = aa.copy(), chi.copy(), pos.copy()
+    pa[:], pc[:], pp[:] = aa, chi, pos
+    for step in range(3):
+        e0, t0 = ctx.block_io(a, c, p, 10, k=64, uniform_n_res=n_res)
+        e1, t1 = ctx.block_io(pa, pc, pp, 10, k=64, uniform_n_res=n_res, out_top=pt)
+        assert np.array_equal(e0, e1) and np.array_equal(t0, t1) and np.array_equal(t0[0], pt)
+        assert np.array_equal(a, pa) and np.array_equal(c, pc) and np.array_equal(p, pp)
+    rng = np.random.default_rng(4)
+    pp[:] = pos + rng.normal(scale=0.05, size=pos.shape).astype(np.float32)
+    p = pp.copy()
+    e0, t0 = ctx.block_io(a, c, p, 5, k=64, uniform_n_res=n_res)
+    e1, t1 = ctx.block_io(pa, pc, pp, 5, k=64, uniform_n_res=n_res, out_top=pt)
+    assert np.array_equal(e0, e1) and np.array_equal(t0, t1) and np.array_equal(p, pp)
