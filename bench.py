@@ -569,11 +569,11 @@ def run_batched(pkg, ctx, torch, ext):
 
 
 # DRAM bytes (read + write) of one launch of each block kernel, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --block-only 8,8,1,0,8`,
+# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --block-only 8,8,3,0,8`,
 # the same per-launch work and launch shape as the timed blocks
-NCU_DRAM_BYTES = {"langevin_cg": 7_159_040 + 2_048, "score_allatom": 3_888_384}
+NCU_DRAM_BYTES = {"langevin_cg": 7_249_152, "score_allatom": 3_888_384}
 NCU_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of "
-                   "bench.py --block-only 8,8,1,0,8 (cold cache, serialised)")
+                   "bench.py --block-only 8,8,3,0,8 (cold cache, serialised)")
 
 SCHEDULES = (150, 200, 250, 300, 375, 450, 600)  # annealed schedule lengths of the learned-proposal study
 LEARNED_SEEDS = tuple(range(21, 33))
