@@ -14,9 +14,10 @@
 //     Calpha and amino acid; residues interact only through the disulfide term.
 //     So every residue's proposal, its rejection rebuild and both Calpha energies
 //     are computed in parallel (builds on one half of the warps, energies on the
-//     other), and one thread then takes the decisions in residue order, updating
-//     the disulfide energy wherever a Cys is involved — the reference's
-//     sequential sweep, exactly.
+//     other); one thread takes the decisions that involve a Cys in residue order,
+//     updating the disulfide energy, and records the disulfide energy current at
+//     every other move's turn; those moves, which leave it unchanged, are then
+//     decided in parallel — the reference's sequential sweep, exactly.
 //  4. Backbone phi/psi sweep (:403-418): sequential over the attempted moves;
 //     per move the Calpha energies of residues r..n are evaluated by warps, the
 //     downstream atoms rotated by all threads (Rodrigues, allatom.rs:397-479), and
@@ -74,7 +75,8 @@ struct AnSmem {
     AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
     double* dscal;                  // [0] disulfide energy of the current state
-    double* lhr;                    // R: log Hastings ratio of the move
+    double* lhr;                    // R: log Hastings ratio of the move (network path); otherwise
+                                    // the disulfide energy current at the move's turn
     float *u_acc, *bb_u;            // R
     int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
     int *rot, *mvl;                 // R: rotamer index of the state (-1 unknown), residues with a move
@@ -1033,6 +1035,10 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
                 const int oa = S.aa[r];
                 const int na = kind == MV_MUT ? S.new_aa[r] : oa;
                 const bool cys = oa == CYS || na == CYS;
+                if (!EXT && !cys) {  // decided in parallel below, with the disulfide energy of its turn
+                    S.lhr[r] = (double)D;
+                    continue;
+                }
                 const int ncys_new = ncys + (na == CYS) - (oa == CYS);
                 ACC Dn = D;
                 if (cys)
@@ -1089,6 +1095,39 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
             }
         }
         __syncthreads();
+        if (!EXT) {
+            // the moves that involve no Cys leave the disulfide energy as it is, so each
+            // is decided on its own with the disulfide energy current at its turn (the
+            // loop above recorded it): the same decisions as the sequential sweep
+            for (int r = tid; r < n; r += NT) {
+                const int kind = S.kind[r];
+                if (kind == MV_NONE || S.valid[r]) continue;  // valid: decided above (Cys)
+                const int oa = S.aa[r];
+                const int na = kind == MV_MUT ? S.new_aa[r] : oa;
+                const ACC D = (ACC)S.lhr[r];
+                const ACC old_e = (ACC)S.c_old[r] + D;
+                const ACC new_e = (ACC)S.c_new[r] + D;
+                const bool acc = metropolis(new_e - old_e, temp, S.u_acc[r]);
+                ++n_mc;
+                n_mc_acc += acc;
+                if (acc) {
+                    S.sel[r] = SEL_PROP;
+                    S.aa[r] = na;
+                    const int rot = S.new_rot[r];
+                    const bool has = s_rot_n[na] > 0;
+                    S.chi[r] = has ? s_rot_chi[na][rot] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const ChiTrig t = has ? rot_trig(na, rot) : zero_trig();
+                    S.trig[2 * r] = make_float4(t.t[0].x, t.t[0].y, t.t[1].x, t.t[1].y);
+                    S.trig[2 * r + 1] = make_float4(t.t[2].x, t.t[2].y, t.t[3].x, t.t[3].y);
+                    S.c_cur[r] = S.c_new[r];
+                } else {
+                    S.sel[r] = SEL_REJ;
+                    S.c_cur[r] = S.c_old[r];
+                }
+                S.valid[r] = 1;
+            }
+            __syncthreads();
+        }
         for (int i = tid; i < n * SLOT_STRIDE; i += NT) {
             const int r = i / SLOT_STRIDE;
             const int sl = S.sel[r];
@@ -1165,11 +1204,11 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
         st.res_trig[2 * (r0 + r)] = S.trig[2 * r];
         st.res_trig[2 * (r0 + r) + 1] = S.trig[2 * r + 1];
     }
-    if (tid == 0 && stats) {
-        stats[4 * c] += n_mc;
-        stats[4 * c + 1] += n_mc_acc;
-        stats[4 * c + 2] += n_bb;
-        stats[4 * c + 3] += n_bb_acc;
+    if (stats && (n_mc || n_bb)) {  // the decisions are spread over the threads
+        atomicAdd((unsigned long long*)&stats[4 * c], (unsigned long long)n_mc);
+        atomicAdd((unsigned long long*)&stats[4 * c + 1], (unsigned long long)n_mc_acc);
+        atomicAdd((unsigned long long*)&stats[4 * c + 2], (unsigned long long)n_bb);
+        atomicAdd((unsigned long long*)&stats[4 * c + 3], (unsigned long long)n_bb_acc);
     }
 }
 
