@@ -75,8 +75,9 @@ struct AnSmem {
     AgView* ag;
     double *c_cur, *c_old, *c_new;  // R: Calpha energies (exact f32 values when ACC = float)
     double* dscal;                  // [0] disulfide energy of the current state
-    double* lhr;                    // R: log Hastings ratio of the move (network path); otherwise
-                                    // the disulfide energy current at the move's turn
+    double* lhr;                    // R: log Hastings ratio of the move (network path)
+    double* d_turn;                 // R: the disulfide energy current at the move's turn (moves
+                                    // without a Cys, decided after the sequential pass)
     float *u_acc, *bb_u;            // R
     int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
     int *rot, *mvl;                 // R: rotamer index of the state (-1 unknown), residues with a move
@@ -111,7 +112,7 @@ __host__ __device__ inline size_t anneal_smem_bytes(int R, int G, int C, int lea
            (size_t)warps * STAGE_CAP * 16 + (size_t)G * 64 + (size_t)anneal_xyz_len(G) * 12 +
            ((size_t)C * 4 + 15) / 16 * 16 +
            ((sizeof(AgView) + 15) / 16) * 16 +
-           (size_t)R * 8 * 3 + 16 + (size_t)R * 8 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
+           (size_t)R * 8 * 3 + 16 + (size_t)R * 8 * 2 + (size_t)R * 4 * 2 + (size_t)R * 4 * 9 + (size_t)L * 4 +
            (size_t)R * 4 * 3 + 32 + (learned ? ((size_t)G + 15) / 16 * 16 + (MLP_COUNT_CAP + 1 + MLP_BIASES) * 4 : 0) +
            15 + (size_t)anneal_list_res(R) * (CG_LIST_MAX * 4 + 16 + 4) +  // 15: alignment of cgcentre
            (fv ? 15 + (size_t)R * 64 : 0);
@@ -143,6 +144,7 @@ __device__ inline AnSmem carve(unsigned char* b, int R, int G, int C, int learne
     s.c_new = (double*)take((size_t)R * 8);
     s.dscal = (double*)take(16);
     s.lhr = (double*)take((size_t)R * 8);
+    s.d_turn = (double*)take((size_t)R * 8);
     s.u_acc = (float*)take((size_t)R * 4);
     s.bb_u = (float*)take((size_t)R * 4);
     s.aa = (int*)take((size_t)R * 4);
@@ -1020,7 +1022,10 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
             }
         }
         __syncthreads();
-        // the sweep's decisions, in residue order
+        // the sweep's decisions, in residue order; moves without a Cys are deferred to
+        // the parallel pass below, except while the proposal log is written (its
+        // records keep residue order within a candidate)
+        const bool defer = !EXT || !tlog;
         if (tid == 0) {
             int ncys = S.iscal[IS_NCYS];
             bool have_d = false;
@@ -1035,8 +1040,8 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
                 const int oa = S.aa[r];
                 const int na = kind == MV_MUT ? S.new_aa[r] : oa;
                 const bool cys = oa == CYS || na == CYS;
-                if (!EXT && !cys) {  // decided in parallel below, with the disulfide energy of its turn
-                    S.lhr[r] = (double)D;
+                if (defer && !cys) {  // decided in parallel below, with the disulfide energy of its turn
+                    S.d_turn[r] = (double)D;
                     continue;
                 }
                 const int ncys_new = ncys + (na == CYS) - (oa == CYS);
@@ -1095,7 +1100,7 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
             }
         }
         __syncthreads();
-        if (!EXT) {
+        if (defer) {
             // the moves that involve no Cys leave the disulfide energy as it is, so each
             // is decided on its own with the disulfide energy current at its turn (the
             // loop above recorded it): the same decisions as the sequential sweep
@@ -1104,13 +1109,15 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
                 if (kind == MV_NONE || S.valid[r]) continue;  // valid: decided above (Cys)
                 const int oa = S.aa[r];
                 const int na = kind == MV_MUT ? S.new_aa[r] : oa;
-                const ACC D = (ACC)S.lhr[r];
+                const ACC D = (ACC)S.d_turn[r];
                 const ACC old_e = (ACC)S.c_old[r] + D;
                 const ACC new_e = (ACC)S.c_new[r] + D;
-                const bool acc = metropolis(new_e - old_e, temp, S.u_acc[r]);
+                const bool acc = EXT ? mh_accept(new_e - old_e, temp, S.u_acc[r], S.lhr[r])
+                                     : metropolis(new_e - old_e, temp, S.u_acc[r]);
                 ++n_mc;
                 n_mc_acc += acc;
                 if (acc) {
+                    if (EXT) S.rot[r] = kind == MV_ROT ? S.new_rot[r] : (s_rot_n[na] > 0 ? 0 : -1);
                     S.sel[r] = SEL_PROP;
                     S.aa[r] = na;
                     const int rot = S.new_rot[r];
