@@ -2581,9 +2581,9 @@ int binder_mlp_set_params(binder_ctx* ctx, const float* params) {
     CK(M.w2t.ensure(MLP_H * MLP_H), "mlp alloc");
     CK(M.w3.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
     CK(M.w3t.ensure(MLP_OUT_PAD * MLP_H), "mlp alloc");
-    CK(M.f1.ensure((MLP_H / 8) * (MLP_K1 / 32) * 32), "mlp alloc");
-    CK(M.f2.ensure((MLP_H / 8) * (MLP_H / 32) * 32), "mlp alloc");
-    CK(M.f3.ensure((MLP_OUT_PAD / 8) * (MLP_H / 32) * 32), "mlp alloc");
+    CK(M.f1.ensure((MLP_H / 16) * (MLP_K1 / 16) * 32), "mlp alloc");
+    CK(M.f2.ensure((MLP_H / 16) * (MLP_H / 16) * 32), "mlp alloc");
+    CK(M.f3.ensure((MLP_OUT_PAD / 16) * (MLP_H / 16) * 32), "mlp alloc");
     CK(M.loss.ensure(1), "mlp alloc");
     CK(cudaMemcpyAsync(M.w.p, params, MLP_N_PARAMS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream), "mlp H2D");
     CK(cudaMemsetAsync(M.g.p, 0, MLP_N_PARAMS * sizeof(float), ctx->stream), "mlp memset");

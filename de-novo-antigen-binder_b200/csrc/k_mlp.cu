@@ -179,8 +179,9 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// logistic sigmoid with the fast exponential (the results are rounded to BF16)
-__device__ __forceinline__ float sigmoid_fast(float z) { return __frcp_rn(1.0f + __expf(-z)); }
+// logistic sigmoid with the fast exponential and the approximate reciprocal (the
+// results are rounded to BF16); the network tile of the Metropolis kernel uses the same
+__device__ __forceinline__ float sigmoid_fast(float z) { return rcp_approx(1.0f + __expf(-z)); }
 
 // ---- C[M x N] = A[M x K] * B[N x K]^T on the tensor cores ----------------------------
 // One CTA of 256 threads per 128-row tile of A (blockIdx.x) and K slice (blockIdx.y,
@@ -426,20 +427,16 @@ __global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g
     w[i] -= lr * (a / bc1) / (sqrtf(b / bc2) + eps);
 }
 
-// 16-byte fragment-order element (t, sp, lane) of W [N][K] at w (FP32 master copy)
-__device__ __forceinline__ uint4 pack_frag(const float* __restrict__ w, int K, int t, int sp, int lane) {
-    const int n = t * 8 + lane / 4, g = 2 * (lane % 4);
-    uint32_t v[4];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int k0 = (2 * sp + h) * 16;
-        const __nv_bfloat162 lo = __floats2bfloat162_rn(w[(size_t)n * K + k0 + g], w[(size_t)n * K + k0 + g + 1]);
-        const __nv_bfloat162 hi =
-            __floats2bfloat162_rn(w[(size_t)n * K + k0 + 8 + g], w[(size_t)n * K + k0 + 8 + g + 1]);
-        v[2 * h] = *(const uint32_t*)&lo;
-        v[2 * h + 1] = *(const uint32_t*)&hi;
-    }
-    return make_uint4(v[0], v[1], v[2], v[3]);
+// 16-byte fragment-order element (mt, s, lane) of W [N][K] at w (FP32 master copy)
+__device__ __forceinline__ uint4 pack_frag(const float* __restrict__ w, int K, int mt, int s, int lane) {
+    const int g = lane / 4, c = 2 * (lane % 4), k0 = 16 * s;
+    const float* r0 = w + (size_t)(16 * mt + g) * K + k0;
+    const float* r1 = w + (size_t)(16 * mt + g + 8) * K + k0;
+    const __nv_bfloat162 a0 = __floats2bfloat162_rn(r0[c], r0[c + 1]);
+    const __nv_bfloat162 a1 = __floats2bfloat162_rn(r1[c], r1[c + 1]);
+    const __nv_bfloat162 a2 = __floats2bfloat162_rn(r0[8 + c], r0[9 + c]);
+    const __nv_bfloat162 a3 = __floats2bfloat162_rn(r1[8 + c], r1[9 + c]);
+    return make_uint4(*(const uint32_t*)&a0, *(const uint32_t*)&a1, *(const uint32_t*)&a2, *(const uint32_t*)&a3);
 }
 
 // BF16 copies of the weights: W1 [H][192], W2 [H][H] and W2^T, W3 [32][H] and W3^T,
@@ -447,17 +444,17 @@ __device__ __forceinline__ uint4 pack_frag(const float* __restrict__ w, int K, i
 // largest of them)
 __global__ void k_pack_weights(const float* __restrict__ p, MlpBf16 o) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < (MLP_H / 8) * (MLP_K1 / 32) * 32) {
-        const int lane = t % 32, sp = (t / 32) % (MLP_K1 / 32), nt = t / (32 * (MLP_K1 / 32));
-        o.f1[t] = pack_frag(p + MLP_OFF_W1, MLP_K1, nt, sp, lane);
+    if (t < (MLP_H / 16) * (MLP_K1 / 16) * 32) {
+        const int lane = t % 32, ks = (t / 32) % (MLP_K1 / 16), mt = t / (32 * (MLP_K1 / 16));
+        o.f1[t] = pack_frag(p + MLP_OFF_W1, MLP_K1, mt, ks, lane);
     }
-    if (t < (MLP_H / 8) * (MLP_H / 32) * 32) {
-        const int lane = t % 32, sp = (t / 32) % (MLP_H / 32), nt = t / (32 * (MLP_H / 32));
-        o.f2[t] = pack_frag(p + MLP_OFF_W2, MLP_H, nt, sp, lane);
+    if (t < (MLP_H / 16) * (MLP_H / 16) * 32) {
+        const int lane = t % 32, ks = (t / 32) % (MLP_H / 16), mt = t / (32 * (MLP_H / 16));
+        o.f2[t] = pack_frag(p + MLP_OFF_W2, MLP_H, mt, ks, lane);
     }
-    if (t < (MLP_OUT_PAD / 8) * (MLP_H / 32) * 32) {
-        const int lane = t % 32, sp = (t / 32) % (MLP_H / 32), nt = t / (32 * (MLP_H / 32));
-        o.f3[t] = pack_frag(p + MLP_OFF_W3, MLP_H, nt, sp, lane);
+    if (t < (MLP_OUT_PAD / 16) * (MLP_H / 16) * 32) {
+        const int lane = t % 32, ks = (t / 32) % (MLP_H / 16), mt = t / (32 * (MLP_H / 16));
+        o.f3[t] = pack_frag(p + MLP_OFF_W3, MLP_H, mt, ks, lane);
     }
     if (t < MLP_H * MLP_K1) o.w1[t] = __float2bfloat16_rn(p[MLP_OFF_W1 + t]);
     if (t < MLP_H * MLP_H) {

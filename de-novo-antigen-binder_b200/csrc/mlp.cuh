@@ -36,6 +36,14 @@ __host__ __device__ __forceinline__ int mlp_shell(float r2) {
            (r2 >= 56.25f) + (r2 >= 76.5625f);
 }
 
+// Approximate reciprocal (PTX rcp.approx.ftz.f32: within 1 ulp; 1 / inf = 0), for
+// the sigmoid of the network's SiLU, whose results are rounded to BF16.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Counts of antigen Calphas by (shell, amino acid) around (x, y, z), by one warp:
 // cnt[shell * 20 + aa] += 1 for every antigen Calpha with r^2 < 100 (the
 // reference's f32 rounding of r^2).  cnt is zeroed by the caller.  Each lane reads
@@ -98,14 +106,14 @@ struct GemmArgs {
     GemmEpi e;
 };
 
-// Fragment order of a BF16 weight matrix W [N][K] for the warp-level MMA
-// (m16n8k16, B operand "col"): element (t, sp, l) (t = n-tile of 8 outputs, sp =
-// pair of 16-wide k-steps, l = lane) is 16 bytes holding, for the k-steps s = 2 sp
-// and 2 sp + 1 (k0 = 16 s), n = 8 t + l / 4, g = 2 (l % 4):
-// {W[n][k0+g], W[n][k0+g+1], W[n][k0+8+g], W[n][k0+8+g+1]} of s = 2 sp, then of
-// s = 2 sp + 1 -- the lane's b0, b1 registers of both k-steps in one 16-byte load,
-// a warp's loads 512 contiguous bytes.
-__host__ __device__ constexpr int frag_index(int t, int sp, int lane, int K) { return (t * (K / 32) + sp) * 32 + lane; }
+// Fragment order of a BF16 weight matrix W [N][K] for the warp-level MMA with the
+// weights as the A operand (m16n8k16, A row-major: 16 outputs x 16 k; the rows of
+// the network's input are the N = 8 columns): element (mt, s, l) (mt = tile of 16
+// outputs, s = 16-wide k-step, l = lane; g = l / 4, c = 2 (l % 4), k0 = 16 s) is 16
+// bytes holding {W[16mt+g][k0+c], W[16mt+g][k0+c+1]}, {W[16mt+g+8][k0+c], ..+1},
+// {W[16mt+g][k0+8+c], ..+1}, {W[16mt+g+8][k0+8+c], ..+1} -- the lane's a0..a3
+// registers of one MMA in one 16-byte load; a warp's loads are 512 contiguous bytes.
+__host__ __device__ constexpr int frag_index(int mt, int s, int lane, int K) { return (mt * (K / 16) + s) * 32 + lane; }
 
 // BF16 weight copies used by the GEMMs and the Metropolis kernel's network tile
 struct MlpBf16 {
@@ -114,9 +122,9 @@ struct MlpBf16 {
     __nv_bfloat16* w2t;  // [H][H] transposed
     __nv_bfloat16* w3;   // [32][H]
     __nv_bfloat16* w3t;  // [H][32] transposed
-    uint4* f1;           // W1 in fragment order (H/8 n-tiles x 6 k-step pairs x 32 lanes)
-    uint4* f2;           // W2 in fragment order (H/8 x H/32 x 32)
-    uint4* f3;           // W3 in fragment order (4 x H/32 x 32)
+    uint4* f1;           // W1 in fragment order (H/16 output tiles x 12 k-steps x 32 lanes)
+    uint4* f2;           // W2 in fragment order (H/16 x H/16 x 32)
+    uint4* f3;           // W3 in fragment order (2 x H/16 x 32)
 };
 
 // One logged Metropolis proposal (binder_mc_tuple of the C ABI, 32 bytes).
