@@ -4,10 +4,13 @@
 //
 // Per step, in the reference's order:
 //  1. Langevin: coarse-grained force, restraint, noise, 2 A clamp, rigid
-//     translation (diffusion.rs:306-339).  Eight lanes per residue split the 27
-//     probe cells (reference order) into consecutive runs; each lane evaluates
-//     the in-cutoff pair terms of its run and lane 0 adds them lane by lane, which
-//     is the reference's sequential sum.
+//     translation (diffusion.rs:306-339).  A residue's force comes from its Verlet
+//     list (8 lanes per residue, 16 in the 16-warp instance), whose in-cutoff
+//     entries in list order are the reference's pairs in its order; its lane 0
+//     adds their terms in that order, which is the reference's sequential sum.
+//     Candidates too long for lists: eight lanes per residue split the 27 probe
+//     cells (reference order) into consecutive runs and lane 0 adds the runs'
+//     terms lane by lane.
 //  2. Interface mask: any antigen Calpha within sqrt(iface_cutoff_sq) (:343-351).
 //  3. Mutation / rotamer sweep (:354-399).  A move at residue r changes only
 //     residue r's atoms, and the Calpha-level energy of r depends only on r's
@@ -552,7 +555,7 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
     fx = sx; fy = sy; fz = sz;
 }
 
-// compute_forces_with_grid for the residue of a group of CG_LANES lanes from its
+// compute_forces_with_grid for the residue of a group of GL lanes from its
 // Verlet list (cg_list.cuh), kept in shared memory across the steps of the launch
 // and rebuilt, with twice the skin up to CG_SKIN_MAX, when the Calpha leaves the
 // skin of the list centre (a backbone move or the steps' drift).  The list entries
@@ -561,9 +564,11 @@ __device__ void group_cg_force(const AgView& A, const CgB& body, int gl, unsigne
 // terms and lane 0 sums them in that order -- the sum of the 27-cell walk.  A list
 // that overflows, or cells near the i32 limits, fall back to the one-lane walk.
 // in / terms: the group's per-step scratch.  The force is in lane 0.
+template <int GL>
 __device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, unsigned gmask, int* list,
                                     float4* centre, int* nlp, int* in, float4* terms, float& fx, float& fy,
                                     float& fz) {
+    static_assert(CG_IN_MAX % GL == 0, "a round compacts whole group steps");
     const GridView& g = A.ca_grid;
     const F3 ca = {body.x, body.y, body.z};
     float4 cc = *centre;
@@ -571,7 +576,7 @@ __device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, un
     const float mx = ca.x - cc.x, my = ca.y - cc.y, mz = ca.z - cc.z;
     if (nl < 0 || !(mx * mx + my * my + mz * mz <= (cc.w - 0.01f) * (cc.w - 0.01f))) {
         const float skin = nl < 0 ? CG_SKIN : fminf(2.0f * cc.w, CG_SKIN_MAX);
-        nl = build_cg_list<CG_LANES>(g, A.ca_pq, ca, gl, gmask, list, skin);
+        nl = build_cg_list<GL>(g, A.ca_pq, ca, gl, gmask, list, skin);
         cc = make_float4(ca.x, ca.y, ca.z, skin);
         __syncwarp(gmask);
         if (gl == 0) {
@@ -586,12 +591,12 @@ __device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, un
     } else {
         const bool near_adjacent = g.cell >= 10.0f && fabsf(ca.x) < 1e4f && fabsf(ca.y) < 1e4f &&
                                    fabsf(ca.z) < 1e4f;  // see k_langevin
-        const int gshift = (int)(threadIdx.x & 31) & ~(CG_LANES - 1);
+        const int gshift = (int)(threadIdx.x & 31) & ~(GL - 1);
         const unsigned below = (1u << gl) - 1u;
         int from = 0;
         while (from < nl) {  // group-uniform
             int n_in = 0;
-            while (from < nl && n_in + CG_LANES <= CG_IN_MAX) {
+            while (from < nl && n_in + GL <= CG_IN_MAX) {
                 const int j = from + gl;
                 bool ok = false;
                 int i = 0;
@@ -606,13 +611,13 @@ __device__ void group_cg_force_list(const AgView& A, const CgB& body, int gl, un
                              abs((long long)ce.z - cz) <= 1;
                     }
                 }
-                const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & ((1u << CG_LANES) - 1u);
+                const unsigned m = (__ballot_sync(gmask, ok) >> gshift) & (GL == 32 ? ~0u : ((1u << GL) - 1u));
                 if (ok) in[n_in + __popc(m & below)] = i;
                 n_in += __popc(m);
-                from += CG_LANES;
+                from += GL;
             }
             __syncwarp(gmask);
-            for (int k = gl; k < n_in; k += CG_LANES) {
+            for (int k = gl; k < n_in; k += GL) {
                 const int i = in[k];
                 float tx, ty, tz;
                 cg_term_parts(body, A.ca_pq[i], A.ca_prm[i], tx, ty, tz);
@@ -806,15 +811,19 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
     for (int s = 0; s < n_steps; ++s) {
         const uint32_t step = step0 + (uint32_t)s;
         const float temp = temps ? temps[s] : p.t_hot;
-        // ---- 1. Langevin (diffusion.rs:306-339): CG_LANES lanes per residue ----
+        // ---- 1. Langevin (diffusion.rs:306-339): CG_LANES lanes per residue, LW with
+        // Verlet lists (16 in the 16-warp instance: the list scans and terms take half
+        // the rounds; the sum in list order by the group's lane 0 is the same) ----
         {
-            const int gl = tid % CG_LANES;
-            const unsigned gmask = ((1u << CG_LANES) - 1u) << (lane & ~(CG_LANES - 1));
+            constexpr int LW = W == 2 * AN_WARPS ? 2 * CG_LANES : CG_LANES;
+            const int glanes = lists ? LW : CG_LANES;
+            const int gl = tid % glanes;
+            const unsigned gmask = ((1u << glanes) - 1u) << (lane & ~(glanes - 1));
             const int g0 = tid - gl;  // first thread of the group
-            // the first CG_RES_PER_PASS * CG_LANES threads (whole warps; with 16 warps the
-            // others wait at the barrier below)
-            for (int base = 0; tid < CG_RES_PER_PASS * CG_LANES && base < n; base += CG_RES_PER_PASS) {
-                const int r = base + tid / CG_LANES;
+            // the first CG_RES_PER_PASS groups (whole warps; with 16 warps and 8-lane
+            // groups the others wait at the barrier below)
+            for (int base = 0; tid < CG_RES_PER_PASS * glanes && base < n; base += CG_RES_PER_PASS) {
+                const int r = base + tid / glanes;
                 if (lists) {
                     // lists the residues' Calphas outran: rebuilt by the whole warp, one
                     // residue after another (a one-pass build with 32 lanes instead of a
@@ -851,10 +860,12 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
                 const CgB body = cg_body(ca.x, ca.y, ca.z, S.aa[r]);
                 float fx, fy, fz;
                 if (lists) {
-                    // the group's scratch: the CG_SLOTS term slots of its lanes
-                    unsigned char* scratch = (unsigned char*)(S.terms + (size_t)g0 * CG_SLOTS);
-                    group_cg_force_list(A, body, gl, gmask, S.cglist + (size_t)r * CG_LIST_MAX, S.cgcentre + r,
-                                        S.cgnl + r, (int*)(scratch + CG_IN_MAX * 16), (float4*)scratch, fx, fy, fz);
+                    // the group's scratch: the term slots of CG_LANES lanes
+                    unsigned char* scratch =
+                        (unsigned char*)(S.terms + (size_t)(tid / glanes) * CG_LANES * CG_SLOTS);
+                    group_cg_force_list<LW>(A, body, gl, gmask, S.cglist + (size_t)r * CG_LIST_MAX,
+                                            S.cgcentre + r, S.cgnl + r, (int*)(scratch + CG_IN_MAX * 16),
+                                            (float4*)scratch, fx, fy, fz);
                 } else {
                     group_cg_force(A, body, gl, gmask, S.terms + (size_t)tid * CG_SLOTS, S.tcount + tid,
                                    S.tcount + g0, S.terms + (size_t)g0 * CG_SLOTS, fx, fy, fz);

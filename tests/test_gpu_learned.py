@@ -125,6 +125,35 @@ def test_learned_hastings_ratios_match_oracle_network(ctx, pkg):
     assert pred.mean() < yf[:, :20].mean()
 
 
+def test_learned_hastings_ratios_with_two_tiles_per_step(ctx, pkg):
+    """More than 8 moves in a candidate-step: the network runs on a second 8-row
+    tile in the same step; every logged ratio still matches the oracle network."""
+    ag_aa, ag_pos, aa, chi, pos, n_res = _setup(ctx, pkg, n_cand=32, seed=81)
+    p = pkg.mlp_init_params(6)
+    p[pkg.MLP_OFF["b3"]:pkg.MLP_OFF["b3"] + 20] = np.linspace(-1, 1, 20)
+    ctx.mlp_set_params(p)
+    prm = ctx.params
+    prm.mutation_p = 0.45  # x3 at the interface, x0.4 elsewhere: about 8-12 moves per step
+    ctx.set_params(prm)
+    ctx.set_proposal(True, t_prop_min=3.0)
+    ctx.mc_log(100000)
+    (a1, c1, p1), st = _run(ctx, aa, chi, pos, n_res, steps=8)
+    tup = ctx.mc_log_fetch()
+    ctx.mc_log(0)
+    ctx.set_proposal(False)
+    assert len(tup) == st[:, 0].sum()
+    # some candidate averaged more than 8 moves per step: it had steps of two tiles
+    assert st[:, 0].max() > 8 * 8 and st[:, 0].sum() > 32 * 8 * 4
+    mut = tup[tup["action"] < 20]
+    ca = np.stack([mut["x"], mut["y"], mut["z"]], 1)
+    yf, _ = mo.forward(p, mo.features(ag_pos[:, 1, :], ag_aa, ca, np.full(len(mut), mo.NO_AA)), bf16_path=True)
+    lg = -yf[:, :20] / 3.0
+    ref = lg[np.arange(len(mut)), mut["aa"].astype(int)] - lg[np.arange(len(mut)), mut["action"].astype(int)]
+    assert np.abs(mut["log_ratio"] - ref).max() < 0.05
+    rot = tup[(tup["action"] >= 20) & (tup["log_ratio"] != 0.0)]
+    assert len(rot) > 20  # rotamer moves from library rotamers are learned too
+
+
 def test_logged_tuples_train_the_network(ctx, pkg):
     ag_aa, ag_pos, aa, chi, pos, n_res = _setup(ctx, pkg, n_cand=128, seed=80)
     ctx.set_proposal(False)
