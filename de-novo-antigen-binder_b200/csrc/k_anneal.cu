@@ -58,7 +58,7 @@ constexpr int AG_STAGE_MAX = 1024;                   // antigen Calphas staged i
 constexpr int CELL_STAGE_MAX = 4096;                 // Calpha-grid cells staged in shared memory
 enum : int { MV_NONE = 0, MV_ROT = 1, MV_MUT = 2 };
 enum : int { SEL_KEEP = 0, SEL_PROP = 1, SEL_REJ = 2 };
-enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3, IS_NMV = 4 };
+enum : int { IS_DVALID = 0, IS_DECISION = 1, IS_NCYS = 2, IS_LASTCYS = 3, IS_NMV = 4, IS_NTASK = 5 };
 
 // Shared-memory carve of one CTA for candidates of up to R residues and antigens
 // of up to G staged Calphas.
@@ -82,7 +82,9 @@ struct AnSmem {
     double* d_turn;                 // R: the disulfide energy current at the move's turn (moves
                                     // without a Cys, decided after the sequential pass)
     float *u_acc, *bb_u;            // R
-    int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface, *tcount;
+    int *aa, *kind, *new_aa, *new_rot, *sel, *valid, *bb_att, *bb_phi, *iface;
+    int* tcount;                    // L (>= 2R): Langevin term counts of the lanes; after the Langevin step
+                                    // the Calpha-energy tasks of the step's moves, 2 r + (0 before, 1 after)
     int *rot, *mvl;                 // R: rotamer index of the state (-1 unknown), residues with a move
     uint32_t* dz;                   // R: the move's choice draw
     int* iscal;
@@ -100,6 +102,7 @@ struct AnSmem {
 // Entries of each staged x / y / z array: room for the pad, a multiple of 4 (the
 // arrays after them keep their 16-byte alignment).
 __host__ __device__ inline int anneal_xyz_len(int G) { return G > 0 ? (G + 4) & ~3 : 0; }
+static_assert(32 * CG_LANES >= 2 * ANNEAL_MAX_RES, "the term counts hold two energy tasks per residue");
 // Residues with Verlet lists in shared memory: candidates of up to one Langevin
 // pass (CG_RES_PER_PASS residues); longer ones walk the 27 cells every step.
 __host__ __device__ inline int anneal_list_res(int R) { return R <= CG_RES_PER_PASS ? R : 0; }
@@ -907,6 +910,7 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
             S.iscal[IS_DVALID] = 0;  // disulfide energy stale
             S.iscal[IS_NCYS] = 0;
             S.iscal[IS_LASTCYS] = -1;
+            S.iscal[IS_NTASK] = 0;
         }
         __syncthreads();
         for (int i = tid; i < n * SLOT_STRIDE; i += NT) {
@@ -1000,24 +1004,31 @@ __global__ void __launch_bounds__(W * 32, W == 8 ? 2 : 1) k_anneal(StateView st,
                 S.lhr[r] = 0.0;
             }
             if (aa == CYS) atomicAdd(&S.iscal[IS_NCYS], 1);
+            if (kind != MV_NONE) {  // its two energy tasks (in any order: each writes its own results)
+                const int k = atomicAdd(&S.iscal[IS_NTASK], 2);
+                S.tcount[k] = 2 * r;  // the Langevin step's term counts are free until the next step
+                S.tcount[k + 1] = 2 * r + 1;
+            }
         }
         __syncthreads();
         // learned proposal: the choice of each drawn move comes from the network
         // (same draw d.z, inverse CDF) and the move carries its Hastings ratio
         if (EXT && learned && temp <= mlp.t_max)
             an_learned_choices(an_smem, R, G, C, n, agq, staged ? S.agaa : A.res_aa, nag, mlp, temp);
-        // proposals and rejection rebuilds on warps 4..7 (two threads per residue),
-        // the Calpha energies before / after each move on warps 0..3 (one warp each)
+        // proposals and rejection rebuilds on the upper half of the warps (two threads per
+        // residue), the Calpha energies before / after each move on the lower half, the
+        // listed tasks dealt one per warp in turn
         if (warp >= W / 2) {
             for (int t = tid - NT / 2; t < 2 * n; t += NT / 2) {
                 const int r = t >> 1;
                 if (S.kind[r] != MV_NONE) build_move(S, r, (t & 1) ? SEL_REJ : SEL_PROP);
             }
         } else {
-            for (int t = warp; t < 2 * n; t += W / 2) {
+            const int ntask = S.iscal[IS_NTASK];
+            for (int k = warp; k < ntask; k += W / 2) {
+                const int t = S.tcount[k];
                 const int r = t >> 1, which = t & 1;
                 const int kind = S.kind[r];
-                if (kind == MV_NONE) continue;
                 const bool same = kind == MV_ROT || S.new_aa[r] == S.aa[r];
                 if (which == 1 && same) continue;  // same Calpha, same amino acid: same energy
                 const int a = which ? S.new_aa[r] : S.aa[r];
