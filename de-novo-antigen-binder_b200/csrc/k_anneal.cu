@@ -433,7 +433,10 @@ __device__ int warp_sample(const float* y, int n, double inv_tp, uint32_t dz) {
 
 // The residue a move leaves: which = SEL_PROP builds the proposal, SEL_REJ the state
 // after a rejection (rebuild_side_chain with the old chi, or mutate_residue back to
-// the old amino acid around the same Calpha; allatom.rs:244-384).
+// the old amino acid around the same Calpha; allatom.rs:244-384).  The two kinds
+// differ only in the backbone the side chain is built on (the current one, or the
+// ideal one around the Calpha), so lanes of a warp building different kinds share
+// the side-chain loop.
 __device__ void build_move(const AnSmem& S, int r, int which) {
     const int oa = S.aa[r];
     const int kind = S.kind[r];
@@ -441,27 +444,31 @@ __device__ void build_move(const AnSmem& S, int r, int which) {
     const float4* cur = S.pos + (size_t)r * SLOT_STRIDE;
     float4* out = (which == SEL_PROP ? S.prop : S.rej) + (size_t)r * SLOT_STRIDE;
     const ChiTrig old_t = unpack_trig(S.trig[2 * r], S.trig[2 * r + 1]);
+    const bool side_only = kind == MV_ROT || na == oa;  // side chain rebuilt on the current backbone
     F3 atoms[SLOTS];
-    if (kind == MV_ROT || na == oa) {
-        // side chain rebuilt on the current backbone (N, CA, C, O[, CB])
-        ChiTrig t = old_t;
+    int a, n_bb;
+    ChiTrig t = old_t;
+    if (side_only) {
+        a = oa;
         if (which == SEL_PROP) {
             if (kind == MV_ROT) t = rot_trig(oa, S.new_rot[r]);
             else t = s_rot_n[oa] > 0 ? rot_trig(oa, 0) : zero_trig();
         }
-        const int n_bb = 4 + (oa != GLY ? 1 : 0);
+        n_bb = 4 + (oa != GLY ? 1 : 0);  // N, CA, C, O[, CB]
         for (int k = 0; k < n_bb; ++k) atoms[k] = f3(cur[k]);
-        build_side_chain(oa, atoms, n_bb, t);
-        const int n_at = s_topo_n[oa];
+    } else {
+        // ideal backbone around the Calpha with the new (or, rejected, the old) residue
+        a = which == SEL_PROP ? na : oa;
+        if (which == SEL_PROP) t = s_rot_n[na] > 0 ? rot_trig(na, 0) : zero_trig();
+        n_bb = ideal_backbone(f3(cur[1]), a, atoms);
+    }
+    build_side_chain(a, atoms, n_bb, t);
+    const int n_at = s_topo_n[a];
+    if (side_only) {
         for (int k = 0; k < SLOT_STRIDE; ++k)
             out[k] = (k >= n_bb && k < n_at) ? make_float4(atoms[k].x, atoms[k].y, atoms[k].z, 0.f) : cur[k];
     } else {
-        // ideal backbone around the Calpha with the new (or, rejected, the old) residue
-        const int a = which == SEL_PROP ? na : oa;
-        const ChiTrig t = which == SEL_PROP ? (s_rot_n[na] > 0 ? rot_trig(na, 0) : zero_trig()) : old_t;
-        const int n_bb = ideal_backbone(f3(cur[1]), a, atoms);
-        build_side_chain(a, atoms, n_bb, t);
-        store_residue(out, atoms, s_topo_n[a]);
+        store_residue(out, atoms, n_at);
     }
 }
 
