@@ -379,7 +379,7 @@ __device__ __forceinline__ bool mh_accept(ACC de, float temp, float u, double lh
 // Features of the tile rows: row i = residue mvl[base + i]; the one-hot of its amino
 // acid for a rotamer query, none for a mutation query (the network's mutation
 // outputs then depend on the environment alone, the same before and after the
-// move); one warp per row (rows i and i + 8).  ag_aa and the log1p table are the
+// move); one warp per row (8 rows, 8 warps).  ag_aa and the log1p table are the
 // shared-memory copies when staged.
 __device__ void an_tile_features(const AnSmem& S, const MlpTile& T, const int* rows_of, int base, int rows,
                                  const float4* agq, const uint8_t* ag_aa, int nag, const float* lg1p) {
